@@ -1,0 +1,98 @@
+/*
+ * slopegpu.h -- C ABI of the B200 Newton-step hot path for SSR/LL continuation on P2
+ * finite elements (drop-in for the native layer of Beremi/slope_stability_octave).
+ *
+ * Conventions
+ *   - Every function returns SG_OK (0) or a negative SG_ERR_* code; sg_last_error()
+ *     gives the message of the calling thread's last failure.  Nothing aborts.
+ *   - Host-buffer entry points ("drop-in") take and return plain host arrays with the
+ *     reference MEX layouts (Octave column-major == per-point AoS), copy to the device,
+ *     compute, copy back and return when done.  Callers own every buffer.
+ *   - *_dev entry points take device pointers and a cudaStream_t (as void*), enqueue
+ *     work and return without synchronising.
+ *   - Indices in the reference-facing arrays (scatter maps, pattern I/J) are 1-based
+ *     like Octave's; everything internal to the device is 0-based.
+ *   - Branch ids: 0 elastic, 1 smooth face, 2 left edge, 3 right edge, 4 apex.
+ */
+#ifndef SLOPEGPU_H
+#define SLOPEGPU_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum {
+    SG_OK = 0,
+    SG_ERR_ARG = -1,      /* invalid argument (null pointer, bad size, bad option) */
+    SG_ERR_CUDA = -2,     /* CUDA runtime error (message has the CUDA error string) */
+    SG_ERR_NOMEM = -3,    /* device or host allocation failed */
+    SG_ERR_STATE = -4,    /* object used before the required set-up step */
+    SG_ERR_NUMERIC = -5,  /* numerical breakdown (NaN/Inf, singular coarse matrix) */
+    SG_ERR_NODEVICE = -6  /* no CUDA device visible */
+};
+
+int sg_abi_version(void);
+const char *sg_last_error(void);
+int sg_device_count(void);
+
+/* ------------------------------------------------------------------------------
+ * (a1, a2) Mohr-Coulomb return mapping + consistent tangent, 3D.
+ * Replaces constitutive_problem_3D_SDS_mex / constitutive_problem_3D_S_mex
+ * (+CONSTITUTIVE_PROBLEM/mex/constitutive_problem_3D_SDS_mex.c:29-64,
+ *  constitutive_problem_3D_S_mex.c:29-59; per-point kernel constitutive_3D_kernel.h:101-410).
+ *   E       6 x n_int  engineering strain (e11,e22,e33,g12,g23,g13), column-major
+ *   c_bar, sin_phi, shear, bulk, lame   1 x n_int  (bulk is accepted and unused, as in the MEX)
+ *   S       6 x n_int  out
+ *   DS      36 x n_int out, column-major 6x6 per point (k = i + 6 j); NULL = stress only
+ *   branch  n_int      out, optional (NULL)
+ * ---------------------------------------------------------------------------- */
+int sg_constitutive3d(const double *E, const double *c_bar, const double *sin_phi,
+                      const double *shear, const double *bulk, const double *lame,
+                      int64_t n_int, double *S, double *DS, uint8_t *branch);
+int sg_constitutive3d_dev(const double *E, const double *c_bar, const double *sin_phi,
+                          const double *shear, const double *bulk, const double *lame,
+                          int64_t n_int, double *S, double *DS, uint8_t *branch, void *stream);
+
+/* (a3) 2D plane-strain twin.  Replaces constitutive_problem_2D_{SDS,S}_mex
+ * (+CONSTITUTIVE_PROBLEM/mex/constitutive_problem_2D_SDS_mex.c, kernel
+ *  constitutive_2D_kernel.h:36-369).  E 3 x n_int, S 4 x n_int (s11,s22,s12,s33),
+ *  DS 9 x n_int (3x3 column-major) or NULL. */
+int sg_constitutive2d(const double *E, const double *c_bar, const double *sin_phi,
+                      const double *shear, const double *bulk, const double *lame,
+                      int64_t n_int, double *S, double *DS, uint8_t *branch);
+int sg_constitutive2d_dev(const double *E, const double *c_bar, const double *sin_phi,
+                          const double *shear, const double *bulk, const double *lame,
+                          int64_t n_int, double *S, double *DS, uint8_t *branch, void *stream);
+
+/* (a4) Davis strength reduction, +CONSTITUTIVE_PROBLEM/reduction.m:25-58 (types 'A','B','C';
+ * type 'C' is applied point-wise).  Device pointers. */
+int sg_reduction_dev(const double *c0, const double *phi, const double *psi, double lambda,
+                     char davis_type, int64_t n, double *c_bar, double *sin_phi, void *stream);
+
+/* ------------------------------------------------------------------------------
+ * (b3, b5) Element-level tangent assembly.  Replaces assemble_K_tangent_vals /
+ * assemble_K_tangent_vals_2D (+ASSEMBLY/mex/assemble_K_tangent_vals.c:38-172,
+ * assemble_K_tangent_vals_2D.c:31-165): V_tang[map-1] += (sum_q B_q'(w_q D_q)B_q)_loc.
+ *   DPhi1..3  n_p x n_int (DPhi3 unused/NULL in 2D), DS (ns^2) x n_int, WEIGHT 1 x n_int
+ *   scatter_map (dim*n_p)^2 x n_e int64, 1-based, 0 = skip (Dirichlet)
+ *   V_tang nnz_out (zeroed and written by the call)
+ * ---------------------------------------------------------------------------- */
+int sg_assemble_ktangent3d(const double *DPhi1, const double *DPhi2, const double *DPhi3,
+                           const double *DS, const double *WEIGHT, const int64_t *scatter_map,
+                           int32_t n_p, int64_t n_int, int64_t n_e, int32_t n_q,
+                           int64_t nnz_out, double *V_tang);
+int sg_assemble_ktangent2d(const double *DPhi1, const double *DPhi2, const double *DS,
+                           const double *WEIGHT, const int64_t *scatter_map, int32_t n_p,
+                           int64_t n_int, int64_t n_e, int32_t n_q, int64_t nnz_out,
+                           double *V_tang);
+int sg_assemble_ktangent_dev(int dim, const double *DPhi1, const double *DPhi2, const double *DPhi3,
+                             const double *DS, const double *WEIGHT, const int64_t *scatter_map,
+                             int32_t n_p, int64_t n_e, int32_t n_q, int64_t nnz_out,
+                             double *V_tang, void *stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* SLOPEGPU_H */

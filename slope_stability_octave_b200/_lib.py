@@ -1,0 +1,67 @@
+"""ctypes binding of libslopegpu.so, the C ABI declared in include/slopegpu.h.
+
+The library is loaded from this package directory (built in-tree by
+``python -m slope_stability_octave_b200.build``).  There is no fallback: if the shared
+library is missing or a call fails, a ``SlopeGPUError`` is raised.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libslopegpu.so")
+
+vp = C.c_void_p
+i32, i64, f64, ch = C.c_int32, C.c_int64, C.c_double, C.c_char
+cint = C.c_int
+
+# name -> argtypes (restype int unless listed in _RESTYPES)
+SIGNATURES = {
+    "sg_abi_version": [],
+    "sg_last_error": [],
+    "sg_device_count": [],
+    "sg_constitutive3d": [vp] * 6 + [i64, vp, vp, vp],
+    "sg_constitutive3d_dev": [vp] * 6 + [i64, vp, vp, vp, vp],
+    "sg_constitutive2d": [vp] * 6 + [i64, vp, vp, vp],
+    "sg_constitutive2d_dev": [vp] * 6 + [i64, vp, vp, vp, vp],
+    "sg_reduction_dev": [vp, vp, vp, f64, ch, i64, vp, vp, vp],
+    "sg_assemble_ktangent3d": [vp] * 6 + [i32, i64, i64, i32, i64, vp],
+    "sg_assemble_ktangent2d": [vp] * 5 + [i32, i64, i64, i32, i64, vp],
+    "sg_assemble_ktangent_dev": [cint] + [vp] * 6 + [i32, i64, i32, i64, vp, vp],
+}
+_RESTYPES = {"sg_last_error": C.c_char_p}
+
+
+class SlopeGPUError(RuntimeError):
+    pass
+
+
+_lib = None
+
+
+def lib() -> C.CDLL:
+    """Load (once) and return the native library; raise if it is missing."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise SlopeGPUError(
+                f"{LIB_PATH} not found: build it with `python -m slope_stability_octave_b200.build`")
+        L = C.CDLL(LIB_PATH)
+        for name, args in SIGNATURES.items():
+            fn = getattr(L, name)
+            fn.argtypes = args
+            fn.restype = _RESTYPES.get(name, cint)
+        _lib = L
+    return _lib
+
+
+def check(rc: int, what: str = "") -> None:
+    if rc != 0:
+        msg = lib().sg_last_error().decode(errors="replace")
+        raise SlopeGPUError(f"{what or 'slopegpu'} failed ({rc}): {msg}")
+
+
+def call(name: str, *args) -> None:
+    """Call a status-returning C-ABI function and raise on failure."""
+    check(getattr(lib(), name)(*args), name)

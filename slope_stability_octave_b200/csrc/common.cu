@@ -1,0 +1,79 @@
+// Library-wide helpers: error capture, device queries, scratch buffers.
+#include <cuda_runtime.h>
+
+#include <cstdio>
+#include <string>
+
+#include "sg_common.cuh"
+
+namespace sg {
+
+static thread_local std::string g_last_error;
+
+int set_error(int code, const std::string &msg) {
+    g_last_error = msg;
+    return code;
+}
+
+int cuda_error(cudaError_t e, const char *what) {
+    char buf[512];
+    snprintf(buf, sizeof buf, "%s: %s (%s)", what, cudaGetErrorString(e), cudaGetErrorName(e));
+    if (e == cudaErrorMemoryAllocation) return set_error(SG_ERR_NOMEM, buf);
+    if (e == cudaErrorNoDevice || e == cudaErrorInsufficientDriver) return set_error(SG_ERR_NODEVICE, buf);
+    return set_error(SG_ERR_CUDA, buf);
+}
+
+int sm_count() {
+    static thread_local int dev_cached = -1, sms = 148;
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) return sms;
+    if (dev != dev_cached) {
+        int v = 0;
+        if (cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, dev) == cudaSuccess && v > 0) sms = v;
+        dev_cached = dev;
+    }
+    return sms;
+}
+
+int Scratch::reserve(size_t want) {
+    int dev = 0;
+    SG_CUDA(cudaGetDevice(&dev));
+    if (ptr && bytes >= want && dev == device) return SG_OK;
+    if (ptr) {
+        int cur = dev;
+        cudaSetDevice(device);
+        cudaFree(ptr);
+        cudaSetDevice(cur);
+        ptr = nullptr;
+        bytes = 0;
+    }
+    cudaError_t e = cudaMalloc(&ptr, want);
+    if (e != cudaSuccess) {
+        ptr = nullptr;
+        return cuda_error(e, "scratch allocation");
+    }
+    bytes = want;
+    device = dev;
+    return SG_OK;
+}
+
+Scratch::~Scratch() {
+    // Process teardown: the context may already be gone; ignore errors.
+    if (ptr) cudaFree(ptr);
+}
+
+}  // namespace sg
+
+extern "C" int sg_abi_version(void) { return 1; }
+
+extern "C" const char *sg_last_error(void) { return sg::g_last_error.c_str(); }
+
+extern "C" int sg_device_count(void) {
+    int n = 0;
+    cudaError_t e = cudaGetDeviceCount(&n);
+    if (e != cudaSuccess) {
+        sg::cuda_error(e, "cudaGetDeviceCount");
+        return 0;
+    }
+    return n;
+}

@@ -1,0 +1,49 @@
+// Shared helpers for the slopegpu library: status codes, error capture, launch shapes.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <string>
+
+#include "../../include/slopegpu.h"
+
+namespace sg {
+
+// Records a message for sg_last_error() (thread-local) and returns the code.
+int set_error(int code, const std::string &msg);
+int cuda_error(cudaError_t e, const char *what);
+
+#define SG_CUDA(call)                                          \
+    do {                                                       \
+        cudaError_t _e = (call);                               \
+        if (_e != cudaSuccess) return sg::cuda_error(_e, #call); \
+    } while (0)
+
+#define SG_CHECK_ARG(cond, msg)                                \
+    do {                                                       \
+        if (!(cond)) return sg::set_error(SG_ERR_ARG, msg);    \
+    } while (0)
+
+// Launch shape: grid sized in multiples of the SM count (148 on B200) for
+// grid-stride kernels, capped by the work.
+int sm_count();
+inline unsigned grid_for(int64_t work, int block, int per_sm = 8) {
+    int64_t need = (work + block - 1) / block;
+    int64_t cap = (int64_t)sm_count() * per_sm;
+    if (need < 1) need = 1;
+    return (unsigned)(need < cap ? need : cap);
+}
+
+// Growable device scratch owned by the library (host-buffer entry points only).
+struct Scratch {
+    void *ptr = nullptr;
+    size_t bytes = 0;
+    int device = -1;
+    int reserve(size_t want);
+    ~Scratch();
+};
+
+inline cudaStream_t as_stream(void *s) { return reinterpret_cast<cudaStream_t>(s); }
+
+}  // namespace sg

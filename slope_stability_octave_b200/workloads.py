@@ -1,0 +1,149 @@
+"""Seeded synthetic workloads with the shapes and value ranges of the benchmark configs.
+
+The reference publishes no input data for these sizes; the inputs here are generated:
+
+* ``constitutive_points``: per-point materials c ~ U[5,15] kPa, phi ~ U[25,45] deg, psi = 0,
+  E = 40 MPa, nu = 0.3 (Davis-B reduced at lambda = 1) and engineering strains whose
+  return mapping lands in a chosen branch (elastic, smooth face, left edge, right edge,
+  apex; 20 % each by default).  Strains are drawn in principal space (mean strain and a
+  deviator with a uniform Lode angle, scaled by the point's yield strain), rotated by a
+  random rotation, and kept only if the branch decision has a relative margin of at least
+  ``margin`` on every criterion, and the principal strains are separated, so that 1-ulp
+  differences between CPU and GPU libm cannot change the branch.
+* ``box_mesh_config1``: the 80 x 40 x 40 m box split into 6 P2 tets per unit cell.
+"""
+from __future__ import annotations
+
+import numpy as np
+
+from . import fem
+
+BRANCH_NAMES = ("elastic", "smooth", "left_edge", "right_edge", "apex")
+
+
+def _principal(E):
+    """Ordered principal strains of Voigt engineering strains (n, 6) via the Lode-angle
+    formula used by the return mapping."""
+    t = E.copy()
+    t[:, 3:] *= 0.5
+    I1 = t[:, 0] + t[:, 1] + t[:, 2]
+    I2 = (t[:, 0] * t[:, 1] + t[:, 0] * t[:, 2] + t[:, 1] * t[:, 2] - t[:, 3] ** 2 - t[:, 4] ** 2 - t[:, 5] ** 2)
+    I3 = (t[:, 0] * t[:, 1] * t[:, 2] - t[:, 2] * t[:, 3] ** 2 - t[:, 1] * t[:, 5] ** 2 - t[:, 0] * t[:, 4] ** 2
+          + 2 * t[:, 3] * t[:, 4] * t[:, 5])
+    Q = np.maximum((I1 * I1 - 3 * I2) / 9, 0.0)
+    R = (-2 * I1 ** 3 + 9 * I1 * I2 - 27 * I3) / 54
+    sq = np.sqrt(Q)
+    with np.errstate(divide="ignore", invalid="ignore"):
+        c = np.clip(np.where(Q < 1e-30, 1.0, R / (sq * Q)), -1, 1)
+    th = np.where(Q < 1e-30, 0.0, np.arccos(c) / 3)
+    e1 = -2 * sq * np.cos(th + 2 * np.pi / 3) + I1 / 3
+    e2 = -2 * sq * np.cos(th - 2 * np.pi / 3) + I1 / 3
+    e3 = -2 * sq * np.cos(th) + I1 / 3
+    return e1, e2, e3, I1
+
+
+def classify3d(E, c_bar, sin_phi, shear, lame):
+    """Branch of each point and the smallest relative margin over all branch criteria."""
+    e1, e2, e3, I1 = _principal(E)
+    s = sin_phi
+    f = 2 * shear * ((1 + s) * e1 - (1 - s) * e3) + 2 * lame * s * I1 - c_bar
+    gsl = (e1 - e2) / (1 + s)
+    gsr = (e2 - e3) / (1 - s)
+    den_s = 4 * lame * s * s + 4 * shear * (1 + s * s)
+    ls = f / den_s
+    den_l = 4 * lame * s * s + shear * (1 + s) ** 2 + 2 * shear * (1 - s) ** 2
+    ll = (shear * ((1 + s) * (e1 + e2) - 2 * (1 - s) * e3) + 2 * lame * s * I1 - c_bar) / den_l
+    gla = (e1 + e2 - 2 * e3) / (3 - s)
+    den_r = 4 * lame * s * s + 2 * shear * (1 + s) ** 2 + shear * (1 - s) ** 2
+    lr = (shear * (2 * (1 + s) * e1 - (1 - s) * (e2 + e3)) + 2 * lame * s * I1 - c_bar) / den_r
+    gra = (2 * e1 - e2 - e3) / (3 + s)
+    br = np.full(E.shape[0], 4, np.uint8)
+    el = f <= 0
+    sm = ~el & (ls <= gsl) & (ls <= gsr)
+    lf = ~el & ~sm & (gsl < gsr) & (ll >= gsl) & (ll <= gla)
+    rt = ~el & ~sm & ~lf & (gsl > gsr) & (lr >= gsr) & (lr <= gra)
+    br[el], br[sm], br[lf], br[rt] = 0, 1, 2, 3
+
+    def rel(a, b):
+        return np.abs(a - b) / np.maximum(np.maximum(np.abs(a), np.abs(b)), 1e-300)
+    scale_f = np.abs(c_bar) + np.abs(2 * shear * ((1 + s) * e1 - (1 - s) * e3)) + np.abs(2 * lame * s * I1)
+    margin = np.abs(f) / scale_f
+    for a, b in ((ls, gsl), (ls, gsr), (gsl, gsr), (ll, gsl), (ll, gla), (lr, gsr), (lr, gra)):
+        margin = np.minimum(margin, rel(a, b))
+    spread = np.abs(e1) + np.abs(e3) + 1e-300
+    margin = np.minimum(margin, np.minimum(e1 - e2, e2 - e3) / spread)
+    return br, margin
+
+
+def _random_rotations(rng, n):
+    q = rng.normal(size=(n, 4))
+    q /= np.linalg.norm(q, axis=1, keepdims=True)
+    w, x, y, z = q.T
+    return np.stack([
+        np.stack([1 - 2 * (y * y + z * z), 2 * (x * y - z * w), 2 * (x * z + y * w)], -1),
+        np.stack([2 * (x * y + z * w), 1 - 2 * (x * x + z * z), 2 * (y * z - x * w)], -1),
+        np.stack([2 * (x * z - y * w), 2 * (y * z + x * w), 1 - 2 * (x * x + y * y)], -1)], 1)
+
+
+# proposal (mean lo, mean hi, deviator lo, deviator hi) in units of the yield strain
+_PROPOSALS = {0: (-1.0, 0.3, 0.0, 1.0), 1: (-2.0, 2.0, 0.0, 4.0), 2: (-2.0, 2.0, 0.0, 4.0),
+              3: (-2.0, 2.0, 0.0, 4.0), 4: (0.0, 3.0, 0.0, 3.0)}
+
+
+def constitutive_points(n, seed=20261203, fractions=(0.2, 0.2, 0.2, 0.2, 0.2), margin=1e-8,
+                        young=40000.0, poisson=0.3, sort_by_branch=False):
+    """Seeded per-point inputs for the constitutive kernels (config 1 draws)."""
+    rng = np.random.default_rng(seed)
+    c0 = rng.uniform(5.0, 15.0, n)
+    phi_deg = rng.uniform(25.0, 45.0, n)
+    mat = fem.elastic_fields_from_point_draws(c0, phi_deg, young, poisson)
+    c_bar, sin_phi = fem.davis_reduction(mat["c0"], mat["phi"], mat["psi"], 1.0, "B")
+    counts = np.floor(np.asarray(fractions) * n).astype(np.int64)
+    counts[0] += n - counts.sum()
+    target = np.repeat(np.arange(5, dtype=np.uint8), counts)
+    rng.shuffle(target)
+    if sort_by_branch:
+        target = np.sort(target)
+    ey = c_bar / (2 * mat["shear"])
+    prin = np.zeros((n, 3))
+    todo = np.arange(n)
+    for _ in range(400):
+        if todo.size == 0:
+            break
+        t = target[todo]
+        lo_m = np.array([_PROPOSALS[int(b)][0] for b in range(5)])[t]
+        hi_m = np.array([_PROPOSALS[int(b)][1] for b in range(5)])[t]
+        lo_r = np.array([_PROPOSALS[int(b)][2] for b in range(5)])[t]
+        hi_r = np.array([_PROPOSALS[int(b)][3] for b in range(5)])[t]
+        k = todo.size
+        m = ey[todo] * rng.uniform(lo_m, hi_m, k)
+        r = ey[todo] * rng.uniform(lo_r, hi_r, k)
+        th = rng.uniform(0.0, np.pi / 3, k)
+        e = np.stack([m + r * np.cos(th + 2 * np.pi / 3 * j) for j in range(3)], 1)
+        Ed = np.zeros((k, 6))
+        Ed[:, :3] = e
+        br, mg = classify3d(Ed, c_bar[todo], sin_phi[todo], mat["shear"][todo], mat["lame"][todo])
+        ok = (br == t) & (mg >= margin)
+        prin[todo[ok]] = e[ok]
+        todo = todo[~ok]
+    if todo.size:
+        raise RuntimeError(f"could not place {todo.size} points in their target branch")
+    R = _random_rotations(rng, n)
+    eps = np.einsum("nij,nj,nkj->nik", R, prin, R)
+    E = np.stack([eps[:, 0, 0], eps[:, 1, 1], eps[:, 2, 2], 2 * eps[:, 0, 1], 2 * eps[:, 1, 2], 2 * eps[:, 0, 2]], 1)
+    # the rotation perturbs the principal values by rounding: re-check and re-draw the few
+    # points whose margin fell below the threshold (keeps the guarantee exact)
+    br, mg = classify3d(E, c_bar, sin_phi, mat["shear"], mat["lame"])
+    bad = np.nonzero((br != target) | (mg < margin))[0]
+    if bad.size:
+        E[bad] = 0.0
+        E[bad, :3] = prin[bad]
+        br_b, mg_b = classify3d(E[bad], c_bar[bad], sin_phi[bad], mat["shear"][bad], mat["lame"][bad])
+        if np.any((br_b != target[bad]) | (mg_b < margin)):
+            raise RuntimeError("margin check failed after rotation")
+    return dict(E=np.ascontiguousarray(E), c_bar=c_bar, sin_phi=sin_phi, target=target, **mat)
+
+
+def box_mesh_config1(nx=80, ny=40, nz=40):
+    """Config-1 mesh: 80 x 40 x 40 unit cells -> 768,000 P2 tets, 1,056,321 nodes."""
+    return fem.mesh_p2_box(nx, ny, nz, 1.0)

@@ -1,0 +1,47 @@
+"""The C-ABI library loads and exports every entry point declared in include/slopegpu.h.
+No compute call is made here (CPU-only machine)."""
+import ctypes
+import os
+import re
+
+from slope_stability_octave_b200 import _lib
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def declared_symbols():
+    names = set()
+    inc = os.path.join(ROOT, "include")
+    for fn in os.listdir(inc):
+        if fn.endswith(".h"):
+            text = open(os.path.join(inc, fn)).read()
+            text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+            names |= set(re.findall(r"\b(sg_[a-z0-9_]+)\s*\(", text))
+    return names
+
+
+def test_library_exports_all_declared_symbols():
+    L = _lib.lib()
+    names = declared_symbols()
+    assert len(names) >= 10
+    missing = [n for n in sorted(names) if not hasattr(L, n)]
+    assert not missing, f"not exported: {missing}"
+
+
+def test_binding_covers_every_declared_symbol():
+    assert declared_symbols() <= set(_lib.SIGNATURES)
+
+
+def test_abi_version_and_error_string():
+    L = _lib.lib()
+    assert L.sg_abi_version() >= 1
+    assert isinstance(L.sg_last_error(), bytes)
+
+
+def test_argument_errors_need_no_device():
+    """Invalid arguments are rejected before any device work."""
+    L = _lib.lib()
+    rc = L.sg_reduction_dev(None, None, None, 1.0, b"Z", 10, None, None, None)
+    assert rc == -1 and b"Davis" in L.sg_last_error()
+    rc = L.sg_constitutive3d(None, None, None, None, None, None, ctypes.c_int64(-1), None, None, None)
+    assert rc == -1
