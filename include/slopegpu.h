@@ -92,6 +92,65 @@ int sg_assemble_ktangent_dev(int dim, const double *DPhi1, const double *DPhi2, 
                              int32_t n_p, int64_t n_e, int32_t n_q, int64_t nnz_out,
                              double *V_tang, void *stream);
 
+/* ------------------------------------------------------------------------------
+ * Device-resident mesh (set-up once per mesh).  Replaces the one-time part of the
+ * CONSTITUTIVE object: set_element_data + init_K_r_pattern + build_scatter_map
+ * (+CONSTITUTIVE_PROBLEM/CONSTITUTIVE.m:393-464, 538-635).
+ *   elem   n_p x n_e (column-major, 0-based node ids)
+ *   DPhi*  n_p x n_int physical basis gradients, weight 1 x n_int (ASSEMBLY outputs)
+ *   Q      dim x n_n free-DOF mask (column-major, 1 = free)
+ * The stiffness lives in a node-adjacency block pattern (dim x dim blocks, all nodes);
+ * Dirichlet DOFs carry identity rows/columns there.  The reference's scalar K(Q,Q)
+ * pattern (Octave find() order) and its scatter map are produced on request.
+ * ---------------------------------------------------------------------------- */
+typedef struct sg_mesh sg_mesh;
+typedef struct sg_bsr sg_bsr;
+
+int sg_mesh_create(int dim, int32_t n_p, int32_t n_q, int64_t n_n, int64_t n_e, const int32_t *elem,
+                   const double *DPhi1, const double *DPhi2, const double *DPhi3, const double *weight,
+                   const uint8_t *Q, sg_mesh **out);
+int sg_mesh_destroy(sg_mesh *mesh);
+/* sizes[0..4] = n_dof (dim*n_n), n_Q, nnz of K(Q,Q), BSR blocks, n_int */
+int sg_mesh_sizes(const sg_mesh *mesh, int64_t *sizes);
+/* borrowed pointer to the mesh's block pattern (valid until sg_mesh_destroy) */
+int sg_mesh_bsr(const sg_mesh *mesh, const sg_bsr **bsr);
+/* (b1) ref_I, ref_J: 1-based pattern of K(Q,Q) in find() order; transpose_perm: 1-based
+ * position of (J,I) for every (I,J) (CONSTITUTIVE.m:445-454).  Any pointer may be NULL. */
+int sg_mesh_pattern(const sg_mesh *mesh, int64_t *ref_I, int64_t *ref_J, int64_t *transpose_perm);
+/* (b2) the reference's element scatter map, (dim*n_p)^2 x n_e int64 (CONSTITUTIVE.m:582-635) */
+int sg_mesh_scatter_map(const sg_mesh *mesh, int64_t *scatter_map);
+/* 0-based DOF index of every free DOF, in order (Octave find(Q(:)) - 1) */
+int sg_mesh_free_dofs(const sg_mesh *mesh, int64_t *q_flat);
+
+/* (a5) E = B U: U dim x n_n (column-major), E n_strain x n_int (CONSTITUTIVE.m:218) */
+int sg_strain_dev(const sg_mesh *mesh, const double *U, double *E, void *stream);
+/* (a6) F = B' (w .* S(1:n_strain,:)): S has s_rows rows per point; F dim x n_n (CONSTITUTIVE.m:281) */
+int sg_force_dev(const sg_mesh *mesh, const double *S, int32_t s_rows, double *F, void *stream);
+/* (b3) K_t = sum_e B'(w DS)B into the block pattern (values zeroed first) */
+int sg_assemble_bsr_dev(const sg_mesh *mesh, const double *DS, double *K, void *stream);
+/* DS_elast of CONSTITUTIVE.m:413-422 per point (n_strain^2 x n_int) */
+int sg_elastic_ds_dev(const sg_mesh *mesh, const double *shear, const double *bulk, double *DS, void *stream);
+/* Ks = (K + K')/2 on the block pattern */
+int sg_symmetrize_bsr_dev(const sg_mesh *mesh, const double *K, double *Ks, void *stream);
+/* (b4) K_r = sym(r K_el + (1-r) K_t) with Dirichlet identity (CONSTITUTIVE.m:515-532) */
+int sg_kr_blend_dev(const sg_mesh *mesh, double r, const double *K_el, const double *K_t, double *K_r, void *stream);
+/* block-pattern values -> V in the reference's find() order (nnz of K(Q,Q)) */
+int sg_bsr_to_ref_dev(sg_mesh *mesh, const double *K, double *V_ref, void *stream);
+
+/* ------------------------------------------------------------------------------
+ * (c2) Block sparse matrix-vector product and reductions (device pointers).
+ * ---------------------------------------------------------------------------- */
+/* info[0..2] = block size, block rows, blocks */
+int sg_bsr_info(const sg_bsr *A, int64_t *info);
+int sg_bsr_spmv_dev(const sg_bsr *A, const double *vals, const double *x, double *y, void *stream);
+/* *result = x'y (synchronises the stream) */
+int sg_dot_dev(int64_t n, const double *x, const double *y, double *result, void *stream);
+/* *result = sum mask .* (a - b).^2  (b, mask may be NULL; synchronises the stream) */
+int sg_masked_diff_norm2_dev(int64_t n, const double *a, const double *b, const double *mask, double *result,
+                             void *stream);
+/* y = a x + b y */
+int sg_axpby_dev(int64_t n, double a, const double *x, double b, double *y, void *stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -29,6 +29,27 @@ SIGNATURES = {
     "sg_assemble_ktangent3d": [vp] * 6 + [i32, i64, i64, i32, i64, vp],
     "sg_assemble_ktangent2d": [vp] * 5 + [i32, i64, i64, i32, i64, vp],
     "sg_assemble_ktangent_dev": [cint] + [vp] * 6 + [i32, i64, i32, i64, vp, vp],
+    # mesh and element operators
+    "sg_mesh_create": [cint, i32, i32, i64, i64, vp, vp, vp, vp, vp, vp, vp],
+    "sg_mesh_destroy": [vp],
+    "sg_mesh_sizes": [vp, vp],
+    "sg_mesh_bsr": [vp, vp],
+    "sg_mesh_pattern": [vp, vp, vp, vp],
+    "sg_mesh_scatter_map": [vp, vp],
+    "sg_mesh_free_dofs": [vp, vp],
+    "sg_strain_dev": [vp, vp, vp, vp],
+    "sg_force_dev": [vp, vp, i32, vp, vp],
+    "sg_assemble_bsr_dev": [vp, vp, vp, vp],
+    "sg_elastic_ds_dev": [vp, vp, vp, vp, vp],
+    "sg_symmetrize_bsr_dev": [vp, vp, vp, vp],
+    "sg_kr_blend_dev": [vp, f64, vp, vp, vp, vp],
+    "sg_bsr_to_ref_dev": [vp, vp, vp, vp],
+    # sparse and vector operations
+    "sg_bsr_info": [vp, vp],
+    "sg_bsr_spmv_dev": [vp, vp, vp, vp, vp],
+    "sg_dot_dev": [i64, vp, vp, vp, vp],
+    "sg_masked_diff_norm2_dev": [i64, vp, vp, vp, vp, vp],
+    "sg_axpby_dev": [i64, f64, vp, f64, vp, vp],
 }
 _RESTYPES = {"sg_last_error": C.c_char_p}
 

@@ -24,7 +24,7 @@ BUILD = os.path.join(CSRC, "_build")
 NVCC_FLAGS = [
     "-O3", "-std=c++17", "-lineinfo",
     "-gencode", "arch=compute_100a,code=sm_100a",
-    "-Xcompiler", "-fPIC,-O2", "--expt-relaxed-constexpr",
+    "-Xcompiler", "-fPIC,-O2,-fopenmp", "--expt-relaxed-constexpr",
     "-I" + os.path.join(ROOT, "include"),
 ]
 
@@ -82,7 +82,7 @@ def build(verbose: bool = False, force: bool = False) -> str:
     newest_obj = max(os.path.getmtime(o) for o in objs)
     if force or not os.path.exists(OUT) or os.path.getmtime(OUT) < newest_obj:
         cmd = [nvcc, "-shared", "-gencode", "arch=compute_100a,code=sm_100a", "-cudart", "static",
-               "-o", OUT] + objs + (["-ccbin", ccbin] if ccbin else []) + ["-lpthread"]
+               "-o", OUT] + objs + (["-ccbin", ccbin] if ccbin else []) + ["-lpthread", "-lgomp"]
         r = subprocess.run(cmd, capture_output=True, text=True)
         if r.returncode != 0:
             raise RuntimeError(f"link failed:\n{r.stdout}\n{r.stderr}")

@@ -1,0 +1,1028 @@
+// (d1, d2) Smoothed-aggregation AMG preconditioner: host set-up of the hierarchy's
+// structure, device numeric set-up on every value update, and the V-cycle apply.
+//
+// The reference preconditions DFGMRES with one BoomerAMG V-cycle
+// (+LINEAR_SOLVERS/mex/hypre_boomeramg_mex.cpp:751-796, max_iter = 1, tol = 0) and re-runs the
+// set-up after every value update (:1151-1213).  HYPRE is not part of this build; this is an
+// AMG of its own design for the same role:
+//
+//   structure (host, once per pattern)   aggregation of the node-block graph, tentative
+//       prolongator T from the near-null space (6 rigid-body modes in 3D, 3 in 2D) by a
+//       per-aggregate QR, and fixed-pattern product plans for A T, A P and P' (A P)
+//   numerics (device, every update)      block-Jacobi inverse, lambda_max(D^-1 A) by power
+//       iteration, P = T - omega D^-1 A T (omega = 4 / (3 lambda_max)), R = P', A P,
+//       A_c = P' (A P); coarsest level: dense Gauss-Jordan inverse
+//   apply (device)                       V(1,1) cycle with degree-2 Chebyshev smoothing on
+//       D^-1 A over [lambda_max / 30, 1.1 lambda_max], in FP64 or FP32 (mixed precision)
+//
+// Every product is a gather over a precomputed list, so the numeric set-up uses no atomics
+// and is deterministic.
+#include <cuda_runtime.h>
+#include <omp.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <array>
+#include <new>
+#include <type_traits>
+#include <vector>
+
+#include "linalg.cuh"
+#include "mesh.h"
+#include "sg_common.cuh"
+
+namespace sg {
+
+struct Pattern {  // CSR of blocks (rectangular)
+    int64_t nrows = 0, ncols = 0, nblk = 0;
+    std::vector<int32_t> rp, col;
+    int32_t *d_rp = nullptr, *d_col = nullptr;
+};
+
+struct Plan {  // for every output block: a list of (first, second) input block indices
+    std::vector<int64_t> ptr;
+    std::vector<int32_t> a, b;
+    int64_t *d_ptr = nullptr;
+    int32_t *d_a = nullptr, *d_b = nullptr;
+};
+
+struct Level {
+    int b = 3, bc = 6;             // block size, coarse block size
+    int64_t n = 0;                 // block rows
+    const sg_bsr *Aext = nullptr;  // level 0: caller's pattern
+    Pattern Aown;                  // coarse levels: own pattern
+    const int32_t *d_Arp = nullptr, *d_Acol = nullptr, *d_Adiag = nullptr;
+    int64_t Anblk = 0;
+    const double *Avals = nullptr;  // level 0: caller's values (set at update)
+    double *Aown_vals = nullptr;    // coarse levels
+    float *A32 = nullptr;
+    int32_t *d_diag_own = nullptr;
+    double *Dinv = nullptr;
+    float *Dinv32 = nullptr;
+    double *lmax = nullptr;        // device scalar
+    uint8_t *d_dead = nullptr;     // per DOF: dead coarse DOF (identity row), coarse levels only
+    // transfer to the next level
+    std::vector<int32_t> agg;
+    int32_t *d_agg = nullptr;
+    double *T = nullptr;           // n * b * bc
+    Pattern P, R, AP;
+    int32_t *d_R_from_P = nullptr;
+    Plan at_plan, ap_plan, ac_plan;  // at: (A block) per P block; ap: (A, P); ac: (P, AP)
+    double *Pv = nullptr, *Rv = nullptr, *APv = nullptr;
+    float *P32 = nullptr, *R32 = nullptr;
+    // vectors
+    double *x = nullptr, *rhs = nullptr, *r = nullptr, *d = nullptr, *t = nullptr;
+    float *x32 = nullptr, *rhs32 = nullptr, *r32 = nullptr, *d32 = nullptr;
+};
+
+struct AmgOptions {
+    int max_levels = 10;
+    int coarse_size = 1200;   // stop coarsening at this many DOFs
+    int cheb_degree = 2;
+    double cheb_ratio = 30.0;
+    int power_its = 10;
+    int mixed = 0;            // 1: FP32 V-cycle
+    double omega_scale = 4.0 / 3.0;
+};
+
+}  // namespace sg
+
+struct sg_amg {
+    sg::AmgOptions opt;
+    std::vector<sg::Level> L;
+    int64_t nc_dense = 0;      // coarsest dense size (DOFs)
+    double *Ainv = nullptr;    // dense inverse, nc_dense^2
+    float *Ainv32 = nullptr;
+    double *colk = nullptr, *rowk = nullptr;
+    double *dots = nullptr;    // reduction scratch
+    int device = 0;
+    int updated = 0;
+};
+
+namespace sg {
+
+template <typename T>
+static int dalloc(T **p, size_t n) {
+    *p = nullptr;
+    if (n == 0) n = 1;
+    SG_CUDA(cudaMalloc((void **)p, n * sizeof(T)));
+    return SG_OK;
+}
+template <typename T>
+static int dup(T **p, const std::vector<T> &v) {
+    int rc = dalloc(p, v.size());
+    if (rc) return rc;
+    if (!v.empty()) SG_CUDA(cudaMemcpy(*p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice));
+    return SG_OK;
+}
+
+// ------------------------------------------------------------------ host structure set-up
+
+// Three-phase aggregation of the block graph (rp, col), rows with active[i] == 0 excluded.
+static int64_t aggregate(int64_t n, const std::vector<int32_t> &rp, const std::vector<int32_t> &col,
+                         const std::vector<uint8_t> &active, std::vector<int32_t> &agg) {
+    agg.assign(n, -1);
+    int32_t na = 0;
+    for (int64_t i = 0; i < n; ++i) {  // phase 1: roots whose neighbourhood is untouched
+        if (!active[i] || agg[i] >= 0) continue;
+        bool free_nb = true;
+        for (int32_t p = rp[i]; p < rp[i + 1]; ++p) {
+            const int32_t j = col[p];
+            if (active[j] && agg[j] >= 0) { free_nb = false; break; }
+        }
+        if (!free_nb) continue;
+        for (int32_t p = rp[i]; p < rp[i + 1]; ++p) {
+            const int32_t j = col[p];
+            if (active[j]) agg[j] = na;
+        }
+        agg[i] = na++;
+    }
+    std::vector<int32_t> add(n, -1);
+    for (int64_t i = 0; i < n; ++i) {  // phase 2: join the neighbouring aggregate seen most
+        if (!active[i] || agg[i] >= 0) continue;
+        int32_t best = -1, bestc = 0;
+        for (int32_t p = rp[i]; p < rp[i + 1]; ++p) {
+            const int32_t a = agg[col[p]];
+            if (a < 0) continue;
+            int32_t c = 0;
+            for (int32_t q = rp[i]; q < rp[i + 1]; ++q) c += (agg[col[q]] == a);
+            if (c > bestc) { bestc = c; best = a; }
+        }
+        add[i] = best;
+    }
+    for (int64_t i = 0; i < n; ++i)
+        if (add[i] >= 0) agg[i] = add[i];
+    for (int64_t i = 0; i < n; ++i) {  // phase 3: leftovers form their own aggregates
+        if (!active[i] || agg[i] >= 0) continue;
+        for (int32_t p = rp[i]; p < rp[i + 1]; ++p) {
+            const int32_t j = col[p];
+            if (active[j] && agg[j] < 0) agg[j] = na;
+        }
+        agg[i] = na++;
+    }
+    return na;
+}
+
+// Per-aggregate thin QR (modified Gram-Schmidt, two passes) of the near-null space rows.
+// B: n*b rows x k columns (row-major).  Outputs T (n*b x k), Bc (na*k x k) and dead flags.
+static void tentative(int64_t n, int b, int k, int64_t na, const std::vector<int32_t> &agg,
+                      const std::vector<double> &B, std::vector<double> &T, std::vector<double> &Bc,
+                      std::vector<uint8_t> &dead) {
+    std::vector<std::vector<int32_t>> members(na);
+    for (int64_t i = 0; i < n; ++i)
+        if (agg[i] >= 0) members[agg[i]].push_back((int32_t)i);
+    T.assign((size_t)n * b * k, 0.0);
+    Bc.assign((size_t)na * k * k, 0.0);
+    dead.assign((size_t)na * k, 0);
+#pragma omp parallel for schedule(dynamic, 64)
+    for (int64_t a = 0; a < na; ++a) {
+        const auto &mem = members[a];
+        const int m = (int)mem.size() * b;
+        std::vector<double> Qm((size_t)m * k), Rm((size_t)k * k, 0.0);
+        for (int r = 0; r < m; ++r) {
+            const int64_t row = (int64_t)mem[r / b] * b + r % b;
+            for (int c = 0; c < k; ++c) Qm[(size_t)r * k + c] = B[(size_t)row * k + c];
+        }
+        double scale = 0.0;
+        for (double v : Qm) scale = std::max(scale, std::fabs(v));
+        for (int c = 0; c < k; ++c) {
+            double nrm0 = 0.0;
+            for (int r = 0; r < m; ++r) nrm0 += Qm[(size_t)r * k + c] * Qm[(size_t)r * k + c];
+            nrm0 = std::sqrt(nrm0);
+            for (int pass = 0; pass < 2; ++pass) {
+                for (int c2 = 0; c2 < c; ++c2) {
+                    double h = 0.0;
+                    for (int r = 0; r < m; ++r) h += Qm[(size_t)r * k + c2] * Qm[(size_t)r * k + c];
+                    for (int r = 0; r < m; ++r) Qm[(size_t)r * k + c] -= h * Qm[(size_t)r * k + c2];
+                    Rm[(size_t)c2 * k + c] += h;
+                }
+            }
+            double nrm = 0.0;
+            for (int r = 0; r < m; ++r) nrm += Qm[(size_t)r * k + c] * Qm[(size_t)r * k + c];
+            nrm = std::sqrt(nrm);
+            if (nrm <= 1e-10 * std::max(nrm0, scale * 1e-3) || nrm == 0.0) {
+                for (int r = 0; r < m; ++r) Qm[(size_t)r * k + c] = 0.0;
+                for (int c2 = 0; c2 < k; ++c2) Rm[(size_t)c * k + c2] = 0.0;
+                dead[(size_t)a * k + c] = 1;
+                continue;
+            }
+            Rm[(size_t)c * k + c] = nrm;
+            for (int r = 0; r < m; ++r) Qm[(size_t)r * k + c] /= nrm;
+        }
+        for (int r = 0; r < m; ++r) {
+            const int64_t row = (int64_t)mem[r / b] * b + r % b;
+            for (int c = 0; c < k; ++c) T[(size_t)row * k + c] = Qm[(size_t)r * k + c];
+        }
+        for (size_t t = 0; t < Rm.size(); ++t) Bc[(size_t)a * k * k + t] = Rm[t];
+    }
+}
+
+// Row-wise symbolic product helper: for each row, collect (col, a, b) triples, sort by col,
+// emit the pattern row and the plan (list of (a, b) per output block).
+template <typename F>
+static void build_product(int64_t nrows, Pattern &out, Plan &plan, F collect) {
+    std::vector<std::vector<int32_t>> cols(nrows);
+    std::vector<std::vector<int64_t>> cnt(nrows);
+    std::vector<std::vector<int32_t>> la(nrows), lb(nrows);
+#pragma omp parallel for schedule(dynamic, 256)
+    for (int64_t i = 0; i < nrows; ++i) {
+        std::vector<std::array<int32_t, 3>> tr;
+        collect(i, tr);
+        std::sort(tr.begin(), tr.end());
+        auto &c = cols[i];
+        auto &n = cnt[i];
+        auto &A = la[i];
+        auto &B = lb[i];
+        for (size_t t = 0; t < tr.size(); ++t) {
+            if (c.empty() || c.back() != tr[t][0]) {
+                c.push_back(tr[t][0]);
+                n.push_back(0);
+            }
+            n.back()++;
+            A.push_back(tr[t][1]);
+            B.push_back(tr[t][2]);
+        }
+    }
+    out.nrows = nrows;
+    out.rp.assign(nrows + 1, 0);
+    for (int64_t i = 0; i < nrows; ++i) out.rp[i + 1] = out.rp[i] + (int32_t)cols[i].size();
+    out.nblk = out.rp[nrows];
+    out.col.resize(out.nblk);
+    plan.ptr.assign(out.nblk + 1, 0);
+    for (int64_t i = 0; i < nrows; ++i)
+        for (size_t t = 0; t < cols[i].size(); ++t) plan.ptr[out.rp[i] + t + 1] = cnt[i][t];
+    for (int64_t p = 0; p < out.nblk; ++p) plan.ptr[p + 1] += plan.ptr[p];
+    plan.a.resize(plan.ptr[out.nblk]);
+    plan.b.resize(plan.ptr[out.nblk]);
+#pragma omp parallel for schedule(dynamic, 256)
+    for (int64_t i = 0; i < nrows; ++i) {
+        std::copy(cols[i].begin(), cols[i].end(), out.col.begin() + out.rp[i]);
+        const int64_t base = plan.ptr[out.rp[i]];
+        std::copy(la[i].begin(), la[i].end(), plan.a.begin() + base);
+        std::copy(lb[i].begin(), lb[i].end(), plan.b.begin() + base);
+        std::vector<int32_t>().swap(cols[i]);
+        std::vector<int32_t>().swap(la[i]);
+        std::vector<int32_t>().swap(lb[i]);
+    }
+}
+
+static int upload_pattern(Pattern &p) {
+    int rc = dup(&p.d_rp, p.rp);
+    if (!rc) rc = dup(&p.d_col, p.col);
+    return rc;
+}
+static int upload_plan(Plan &p) {
+    int rc = dup(&p.d_ptr, p.ptr);
+    if (!rc) rc = dup(&p.d_a, p.a);
+    if (!rc) rc = dup(&p.d_b, p.b);
+    return rc;
+}
+
+// ------------------------------------------------------------------ device numerics
+
+// In-register Gauss-Jordan inverse of a small SPD block (no pivoting needed for SPD).
+template <int B>
+__device__ __forceinline__ void inv_block(const double *a, double *out) {
+    double m[B][2 * B];
+#pragma unroll
+    for (int i = 0; i < B; ++i)
+#pragma unroll
+        for (int j = 0; j < B; ++j) {
+            m[i][j] = a[i * B + j];
+            m[i][B + j] = (i == j) ? 1.0 : 0.0;
+        }
+#pragma unroll
+    for (int k = 0; k < B; ++k) {
+        const double piv = m[k][k];
+        const double ip = (piv != 0.0) ? 1.0 / piv : 0.0;
+#pragma unroll
+        for (int j = 0; j < 2 * B; ++j) m[k][j] *= ip;
+#pragma unroll
+        for (int i = 0; i < B; ++i) {
+            if (i == k) continue;
+            const double f = m[i][k];
+#pragma unroll
+            for (int j = 0; j < 2 * B; ++j) m[i][j] -= f * m[k][j];
+        }
+    }
+#pragma unroll
+    for (int i = 0; i < B; ++i)
+#pragma unroll
+        for (int j = 0; j < B; ++j) out[i * B + j] = m[i][B + j];
+}
+
+template <int B>
+__global__ void k_block_diag_inv(int64_t n, const int32_t *__restrict__ diag, const double *__restrict__ A,
+                                 double *__restrict__ Dinv, float *__restrict__ Dinv32) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        double a[B * B], o[B * B];
+        const int64_t p = diag[i];
+#pragma unroll
+        for (int t = 0; t < B * B; ++t) a[t] = (p >= 0) ? A[p * B * B + t] : ((t % (B + 1)) == 0 ? 1.0 : 0.0);
+        inv_block<B>(a, o);
+#pragma unroll
+        for (int t = 0; t < B * B; ++t) {
+            Dinv[i * B * B + t] = o[t];
+            if (Dinv32) Dinv32[i * B * B + t] = (float)o[t];
+        }
+    }
+}
+
+// y = Dinv x (blockwise), optionally scaled by s (device scalar, inverted when inv != 0)
+template <int B, typename T>
+__global__ void k_dinv_apply(int64_t n, const T *__restrict__ Dinv, const T *__restrict__ x, T *__restrict__ y) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        T xv[B];
+#pragma unroll
+        for (int b = 0; b < B; ++b) xv[b] = x[i * B + b];
+#pragma unroll
+        for (int a = 0; a < B; ++a) {
+            T s = 0;
+#pragma unroll
+            for (int b = 0; b < B; ++b) s += Dinv[(i * B + a) * B + b] * xv[b];
+            y[i * B + a] = s;
+        }
+    }
+}
+
+// Chebyshev step on D^-1 A with bounds [lmax/ratio, 1.1 lmax]:
+//   first (k == 0):  d = D^-1 r / theta;               x += d
+//   next  (k >= 1):  d = c1 d + c2 D^-1 r;             x += d
+// rho_k follows rho_0 = 1/sigma, rho_{k} = 1/(2 sigma - rho_{k-1}).
+template <int B, typename T>
+__global__ void k_cheb(int64_t n, int k, double ratio, const double *__restrict__ lmax, const T *__restrict__ Dinv,
+                       const T *__restrict__ r, T *__restrict__ d, T *__restrict__ x, int x_is_zero) {
+    const double hi = 1.1 * lmax[0], lo = lmax[0] / ratio;
+    const double theta = 0.5 * (hi + lo), delta = 0.5 * (hi - lo), sigma = theta / delta;
+    double rho = 1.0 / sigma, c1 = 0.0, c2 = 1.0 / theta;
+    for (int s = 1; s <= k; ++s) {
+        const double rn = 1.0 / (2.0 * sigma - rho);
+        c1 = rn * rho;
+        c2 = 2.0 * rn / delta;
+        rho = rn;
+    }
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        T rv[B];
+#pragma unroll
+        for (int b = 0; b < B; ++b) rv[b] = r[i * B + b];
+#pragma unroll
+        for (int a = 0; a < B; ++a) {
+            T s = 0;
+#pragma unroll
+            for (int b = 0; b < B; ++b) s += Dinv[(i * B + a) * B + b] * rv[b];
+            const T dn = (k == 0) ? (T)c2 * s : (T)c1 * d[i * B + a] + (T)c2 * s;
+            d[i * B + a] = dn;
+            x[i * B + a] = (x_is_zero && k == 0) ? dn : x[i * B + a] + dn;
+        }
+    }
+}
+
+// P block (i,J) = [agg(i) == J] T_i - omega Dinv_i sum_{p in list} A_p T_{col(p)},  omega = s / lmax
+template <int B, int BC>
+__global__ void k_smooth_prolongator(int64_t n, const int32_t *__restrict__ Prp, const int32_t *__restrict__ Pcol,
+                                     const int64_t *__restrict__ lptr, const int32_t *__restrict__ la,
+                                     const int32_t *__restrict__ Acol, const double *__restrict__ A,
+                                     const double *__restrict__ T, const int32_t *__restrict__ agg,
+                                     const double *__restrict__ Dinv, const double *__restrict__ lmax, double oscale,
+                                     double *__restrict__ P) {
+    const double omega = oscale / lmax[0];
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        for (int32_t q = Prp[i]; q < Prp[i + 1]; ++q) {
+            double acc[B * BC];
+#pragma unroll
+            for (int t = 0; t < B * BC; ++t) acc[t] = 0.0;
+            for (int64_t l = lptr[q]; l < lptr[q + 1]; ++l) {
+                const int32_t p = la[l];
+                const double *a = A + (int64_t)p * B * B;
+                const double *tk = T + (int64_t)Acol[p] * B * BC;
+#pragma unroll
+                for (int r = 0; r < B; ++r)
+#pragma unroll
+                    for (int m = 0; m < B; ++m) {
+                        const double av = a[r * B + m];
+#pragma unroll
+                        for (int c = 0; c < BC; ++c) acc[r * BC + c] += av * tk[m * BC + c];
+                    }
+            }
+            const double *di = Dinv + i * B * B;
+            const bool own = agg[i] == Pcol[q];
+            const double *ti = T + i * B * BC;
+#pragma unroll
+            for (int r = 0; r < B; ++r)
+#pragma unroll
+                for (int c = 0; c < BC; ++c) {
+                    double s = 0.0;
+#pragma unroll
+                    for (int m = 0; m < B; ++m) s += di[r * B + m] * acc[m * BC + c];
+                    P[(int64_t)q * B * BC + r * BC + c] = (own ? ti[r * BC + c] : 0.0) - omega * s;
+                }
+        }
+    }
+}
+
+// R block k = transpose of P block from[k]
+template <int B, int BC>
+__global__ void k_transpose_blocks(int64_t nblk, const int32_t *__restrict__ from, const double *__restrict__ P,
+                                   double *__restrict__ R) {
+    const int64_t total = nblk * B * BC;
+    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < total; t += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t k = t / (B * BC);
+        const int e = (int)(t - k * B * BC), c = e / B, r = e - c * B;  // R(c, r) = P(r, c)
+        R[t] = P[(int64_t)from[k] * B * BC + r * BC + c];
+    }
+}
+
+// AP block = sum over plan pairs A_a (B x B) * P_b (B x BC)
+template <int B, int BC>
+__global__ void k_gather_AP(int64_t nblk, const int64_t *__restrict__ lptr, const int32_t *__restrict__ la,
+                            const int32_t *__restrict__ lb, const double *__restrict__ A, const double *__restrict__ P,
+                            double *__restrict__ AP) {
+    for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q < nblk; q += (int64_t)gridDim.x * blockDim.x) {
+        double acc[B * BC];
+#pragma unroll
+        for (int t = 0; t < B * BC; ++t) acc[t] = 0.0;
+        for (int64_t l = lptr[q]; l < lptr[q + 1]; ++l) {
+            const double *a = A + (int64_t)la[l] * B * B;
+            const double *p = P + (int64_t)lb[l] * B * BC;
+#pragma unroll
+            for (int r = 0; r < B; ++r)
+#pragma unroll
+                for (int m = 0; m < B; ++m) {
+                    const double av = a[r * B + m];
+#pragma unroll
+                    for (int c = 0; c < BC; ++c) acc[r * BC + c] += av * p[m * BC + c];
+                }
+        }
+#pragma unroll
+        for (int t = 0; t < B * BC; ++t) AP[q * B * BC + t] = acc[t];
+    }
+}
+
+// Ac block (I,J) = sum over plan pairs P_a' (BC x B) * AP_b (B x BC); dead DOFs get identity
+template <int B, int BC>
+__global__ void k_gather_Ac(int64_t nrows, const int32_t *__restrict__ rp, const int32_t *__restrict__ col,
+                            const int64_t *__restrict__ lptr, const int32_t *__restrict__ la,
+                            const int32_t *__restrict__ lb, const double *__restrict__ P,
+                            const double *__restrict__ AP, const uint8_t *__restrict__ dead,
+                            double *__restrict__ Ac) {
+    for (int64_t I = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; I < nrows; I += (int64_t)gridDim.x * blockDim.x) {
+        for (int32_t q = rp[I]; q < rp[I + 1]; ++q) {
+            const int64_t J = col[q];
+            double acc[BC * BC];
+#pragma unroll
+            for (int t = 0; t < BC * BC; ++t) acc[t] = 0.0;
+            for (int64_t l = lptr[q]; l < lptr[q + 1]; ++l) {
+                const double *p = P + (int64_t)la[l] * B * BC;
+                const double *ap = AP + (int64_t)lb[l] * B * BC;
+#pragma unroll
+                for (int m = 0; m < B; ++m)
+#pragma unroll
+                    for (int r = 0; r < BC; ++r) {
+                        const double pv = p[m * BC + r];
+#pragma unroll
+                        for (int c = 0; c < BC; ++c) acc[r * BC + c] += pv * ap[m * BC + c];
+                    }
+            }
+#pragma unroll
+            for (int r = 0; r < BC; ++r)
+#pragma unroll
+                for (int c = 0; c < BC; ++c) {
+                    double v = acc[r * BC + c];
+                    if (dead[I * BC + r] || dead[J * BC + c]) v = (I == J && r == c) ? 1.0 : 0.0;
+                    Ac[(int64_t)q * BC * BC + r * BC + c] = v;
+                }
+        }
+    }
+}
+
+__global__ void k_to_float(int64_t n, const double *__restrict__ a, float *__restrict__ b) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        b[i] = (float)a[i];
+}
+__global__ void k_to_double(int64_t n, const float *__restrict__ a, double *__restrict__ b) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        b[i] = (double)a[i];
+}
+
+// deterministic pseudo-random start vector for the power iteration
+__global__ void k_init_vec(int64_t n, double *__restrict__ v) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        uint64_t h = (uint64_t)i * 0x9E3779B97F4A7C15ull + 0x632BE59BD9B4E019ull;
+        h ^= h >> 31;
+        h *= 0xBF58476D1CE4E5B9ull;
+        h ^= h >> 29;
+        v[i] = 0.5 + (double)(h >> 11) * (1.0 / 9007199254740992.0);
+    }
+}
+
+// lmax = sqrt(dots[0]) ; v = w / lmax
+__global__ void k_power_norm(int64_t n, const double *__restrict__ w, const double *__restrict__ dots,
+                             double *__restrict__ v, double *__restrict__ lmax) {
+    const double nrm = sqrt(dots[0]);
+    const double inv = nrm > 0.0 ? 1.0 / nrm : 0.0;
+    if (blockIdx.x == 0 && threadIdx.x == 0) lmax[0] = nrm > 0.0 ? nrm : 1.0;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        v[i] = w[i] * inv;
+}
+
+// dense coarsest matrix from the block pattern
+template <int B>
+__global__ void k_bsr_to_dense(int64_t nrows, const int32_t *__restrict__ rp, const int32_t *__restrict__ col,
+                               const double *__restrict__ A, int64_t N, double *__restrict__ D) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < nrows; i += (int64_t)gridDim.x * blockDim.x)
+        for (int32_t p = rp[i]; p < rp[i + 1]; ++p) {
+            const int64_t j = col[p];
+#pragma unroll
+            for (int a = 0; a < B; ++a)
+#pragma unroll
+                for (int b = 0; b < B; ++b) D[(i * B + a) * N + j * B + b] = A[(int64_t)p * B * B + a * B + b];
+        }
+}
+
+// Gauss-Jordan inversion (SPD, no pivoting), pivot k: save column k and the scaled row k
+__global__ void k_gj_save(int64_t N, int64_t k, const double *__restrict__ D, double *__restrict__ colk,
+                          double *__restrict__ rowk) {
+    const double piv = D[k * N + k];
+    const double ip = piv != 0.0 ? 1.0 / piv : 0.0;
+    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < N; t += (int64_t)gridDim.x * blockDim.x) {
+        colk[t] = D[t * N + k];
+        rowk[t] = D[k * N + t] * ip;
+    }
+}
+__global__ void k_gj_update(int64_t N, int64_t k, double *__restrict__ D, const double *__restrict__ colk,
+                            const double *__restrict__ rowk) {
+    const double piv = colk[k];
+    const double ip = piv != 0.0 ? 1.0 / piv : 0.0;
+    const int64_t total = N * N;
+    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < total; t += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t i = t / N, j = t - i * N;
+        double v;
+        if (i == k && j == k) v = ip;
+        else if (i == k) v = rowk[j];
+        else if (j == k) v = -colk[i] * ip;
+        else v = D[t] - colk[i] * rowk[j];
+        D[t] = v;
+    }
+}
+
+template <typename T>
+__global__ void k_dense_gemv(int64_t N, const T *__restrict__ M, const T *__restrict__ x, T *__restrict__ y) {
+    // one warp per row
+    const int lane = threadIdx.x & 31;
+    const int64_t warp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+    const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    for (int64_t i = warp; i < N; i += nw) {
+        T s = 0;
+        for (int64_t j = lane; j < N; j += 32) s += M[i * N + j] * x[j];
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1) s += __shfl_xor_sync(0xffffffffu, s, off);
+        if (lane == 0) y[i] = s;
+    }
+}
+
+// ------------------------------------------------------------------ dispatch helpers
+
+#define SG_B_DISPATCH(bval, BODY)                                 \
+    switch (bval) {                                               \
+        case 2: { constexpr int BB = 2; BODY; } break;            \
+        case 3: { constexpr int BB = 3; BODY; } break;            \
+        case 6: { constexpr int BB = 6; BODY; } break;            \
+        default: return set_error(SG_ERR_ARG, "AMG block size must be 2, 3 or 6"); \
+    }
+
+#define SG_BBC_DISPATCH(bv, bcv, BODY)                                            \
+    if (bv == 3 && bcv == 6) { constexpr int BB = 3, BC = 6; BODY; }              \
+    else if (bv == 6 && bcv == 6) { constexpr int BB = 6, BC = 6; BODY; }         \
+    else if (bv == 2 && bcv == 3) { constexpr int BB = 2, BC = 3; BODY; }         \
+    else if (bv == 3 && bcv == 3) { constexpr int BB = 3, BC = 3; BODY; }         \
+    else return set_error(SG_ERR_ARG, "unsupported AMG block shape");
+
+static int free_level(Level &l) {
+    auto F = [](void *p) { if (p) cudaFree(p); };
+    F(l.Aown.d_rp); F(l.Aown.d_col); F(l.d_diag_own); F(l.Aown_vals); F(l.A32); F(l.Dinv); F(l.Dinv32);
+    F(l.lmax); F(l.d_dead); F(l.d_agg); F(l.T); F(l.P.d_rp); F(l.P.d_col); F(l.R.d_rp); F(l.R.d_col);
+    F(l.AP.d_rp); F(l.AP.d_col); F(l.d_R_from_P);
+    for (Plan *p : {&l.at_plan, &l.ap_plan, &l.ac_plan}) { F(p->d_ptr); F(p->d_a); F(p->d_b); }
+    F(l.Pv); F(l.Rv); F(l.APv); F(l.P32); F(l.R32);
+    F(l.x); F(l.rhs); F(l.r); F(l.d); F(l.t); F(l.x32); F(l.rhs32); F(l.r32); F(l.d32);
+    return SG_OK;
+}
+
+static int alloc_level_buffers(Level &L, int mixed) {
+    const size_t nb = (size_t)L.n * L.b;
+    int rc = dalloc(&L.Dinv, nb * L.b);
+    if (!rc) rc = dalloc(&L.lmax, 4);
+    if (!rc) rc = dalloc(&L.x, nb);
+    if (!rc) rc = dalloc(&L.rhs, nb);
+    if (!rc) rc = dalloc(&L.r, nb);
+    if (!rc) rc = dalloc(&L.d, nb);
+    if (!rc) rc = dalloc(&L.t, nb);
+    if (!rc && mixed) {
+        rc = dalloc(&L.Dinv32, nb * L.b);
+        if (!rc) rc = dalloc(&L.A32, (size_t)L.Anblk * L.b * L.b);
+        if (!rc) rc = dalloc(&L.x32, nb);
+        if (!rc) rc = dalloc(&L.rhs32, nb);
+        if (!rc) rc = dalloc(&L.r32, nb);
+        if (!rc) rc = dalloc(&L.d32, nb);
+    }
+    return rc;
+}
+
+// Structure of the transfer from level L (pattern rp/col, near-null space B) to the next
+// level.  Returns the coarse pattern, coarse near-null space and dead-DOF flags.
+static int setup_transfer(Level &L, const std::vector<int32_t> &rp, const std::vector<int32_t> &col,
+                          const std::vector<double> &B, int nns, int64_t na, Pattern &Ac, std::vector<double> &Bc,
+                          std::vector<uint8_t> &dead, int mixed) {
+    const int64_t n = L.n;
+    const int b = L.b, bc = nns;
+    L.bc = bc;
+    std::vector<double> T;
+    tentative(n, b, nns, na, L.agg, B, T, Bc, dead);
+    // P pattern + plan for A T: P block (i, J) <- A blocks (i, k) with agg(k) == J
+    build_product(n, L.P, L.at_plan, [&](int64_t i, std::vector<std::array<int32_t, 3>> &tr) {
+        for (int32_t p = rp[i]; p < rp[i + 1]; ++p) {
+            const int32_t a = L.agg[col[p]];
+            if (a >= 0) tr.push_back({a, p, 0});
+        }
+    });
+    L.P.ncols = na;
+    // R = P' pattern and the block map
+    Pattern &R = L.R;
+    R.nrows = na;
+    R.ncols = n;
+    R.rp.assign(na + 1, 0);
+    for (int32_t c : L.P.col) R.rp[c + 1]++;
+    for (int64_t I = 0; I < na; ++I) R.rp[I + 1] += R.rp[I];
+    R.nblk = L.P.nblk;
+    R.col.resize(R.nblk);
+    std::vector<int32_t> fill(R.rp.begin(), R.rp.end() - 1), from(R.nblk), pblk_of_r(R.nblk);
+    for (int64_t i = 0; i < n; ++i)
+        for (int32_t q = L.P.rp[i]; q < L.P.rp[i + 1]; ++q) {
+            const int32_t I = L.P.col[q];
+            R.col[fill[I]] = (int32_t)i;
+            from[fill[I]++] = q;
+        }
+    // AP pattern + plan: (i, J) <- pairs (A block (i, k), P block (k, J))
+    build_product(n, L.AP, L.ap_plan, [&](int64_t i, std::vector<std::array<int32_t, 3>> &tr) {
+        for (int32_t p = rp[i]; p < rp[i + 1]; ++p) {
+            const int32_t k = col[p];
+            for (int32_t q = L.P.rp[k]; q < L.P.rp[k + 1]; ++q) tr.push_back({L.P.col[q], p, q});
+        }
+    });
+    L.AP.ncols = na;
+    // Ac pattern + plan: (I, J) <- pairs (P block (i, I), AP block (i, J))
+    build_product(na, Ac, L.ac_plan, [&](int64_t I, std::vector<std::array<int32_t, 3>> &tr) {
+        for (int32_t k = R.rp[I]; k < R.rp[I + 1]; ++k) {
+            const int32_t i = R.col[k];
+            const int32_t pblk = from[k];
+            for (int32_t q = L.AP.rp[i]; q < L.AP.rp[i + 1]; ++q) tr.push_back({L.AP.col[q], pblk, q});
+        }
+    });
+    Ac.ncols = na;
+    int rc = dup(&L.d_R_from_P, from);
+    if (!rc) rc = dup(&L.d_agg, L.agg);
+    if (!rc) rc = dup(&L.T, T);
+    if (!rc) rc = upload_pattern(L.P);
+    if (!rc) rc = upload_pattern(L.R);
+    if (!rc) rc = upload_pattern(L.AP);
+    if (!rc) rc = upload_plan(L.at_plan);
+    if (!rc) rc = upload_plan(L.ap_plan);
+    if (!rc) rc = upload_plan(L.ac_plan);
+    if (!rc) rc = dalloc(&L.Pv, (size_t)L.P.nblk * b * bc);
+    if (!rc) rc = dalloc(&L.Rv, (size_t)L.P.nblk * b * bc);
+    if (!rc) rc = dalloc(&L.APv, (size_t)L.AP.nblk * b * bc);
+    if (!rc && mixed) rc = dalloc(&L.P32, (size_t)L.P.nblk * b * bc);
+    if (!rc && mixed) rc = dalloc(&L.R32, (size_t)L.P.nblk * b * bc);
+    for (Plan *pl : {&L.at_plan, &L.ap_plan, &L.ac_plan}) {  // host copies no longer needed
+        std::vector<int64_t>().swap(pl->ptr);
+        std::vector<int32_t>().swap(pl->a);
+        std::vector<int32_t>().swap(pl->b);
+    }
+    return rc;
+}
+
+static int build_hierarchy(sg_amg *h, const sg_bsr *A0, const double *nullspace, int nns, const uint8_t *fixed) {
+    const AmgOptions &o = h->opt;
+    h->L.reserve(o.max_levels + 1);
+    std::vector<int32_t> rp = A0->row_ptr, col = A0->col;
+    int b = A0->b;
+    int64_t n = A0->n_rows;
+    std::vector<double> B((size_t)n * b * nns);
+    std::vector<uint8_t> active(n, 0), dead;
+    for (int64_t i = 0; i < n; ++i)
+        for (int a = 0; a < b; ++a) {
+            const int64_t row = i * b + a;
+            const bool fx = fixed && fixed[row];
+            for (int c = 0; c < nns; ++c) B[(size_t)row * nns + c] = fx ? 0.0 : nullspace[(size_t)c * n * b + row];
+            if (!fx) active[i] = 1;
+        }
+    for (int lev = 0;; ++lev) {
+        h->L.emplace_back();
+        Level &L = h->L.back();
+        L.b = b;
+        L.n = n;
+        int rc = SG_OK;
+        if (lev == 0) {
+            L.Aext = A0;
+            L.d_Arp = A0->d_row_ptr;
+            L.d_Acol = A0->d_col;
+            L.d_Adiag = A0->d_diag;
+            L.Anblk = A0->n_blocks;
+        } else {
+            L.Aown.nrows = n;
+            L.Aown.ncols = n;
+            L.Aown.rp = rp;
+            L.Aown.col = col;
+            L.Aown.nblk = rp[n];
+            rc = upload_pattern(L.Aown);
+            std::vector<int32_t> diag(n, -1);
+            for (int64_t i = 0; i < n; ++i)
+                for (int32_t p = rp[i]; p < rp[i + 1]; ++p)
+                    if (col[p] == i) diag[i] = p;
+            if (!rc) rc = dup(&L.d_diag_own, diag);
+            if (!rc) rc = dalloc(&L.Aown_vals, (size_t)L.Aown.nblk * b * b);
+            if (!rc) rc = dup(&L.d_dead, dead);
+            L.d_Arp = L.Aown.d_rp;
+            L.d_Acol = L.Aown.d_col;
+            L.d_Adiag = L.d_diag_own;
+            L.Anblk = L.Aown.nblk;
+        }
+        if (!rc) rc = alloc_level_buffers(L, o.mixed);
+        if (rc) return rc;
+        const int64_t ndof = n * b;
+        int64_t na = 0;
+        const bool last = (ndof <= o.coarse_size) || (lev + 1 >= o.max_levels);
+        if (!last) na = aggregate(n, rp, col, active, L.agg);
+        if (last || na == 0 || na * nns >= ndof * 3 / 4) {
+            std::vector<int32_t>().swap(L.agg);
+            h->nc_dense = ndof;
+            rc = dalloc(&h->Ainv, (size_t)ndof * ndof);
+            if (!rc) rc = dalloc(&h->colk, ndof);
+            if (!rc) rc = dalloc(&h->rowk, ndof);
+            if (!rc && o.mixed) rc = dalloc(&h->Ainv32, (size_t)ndof * ndof);
+            return rc;
+        }
+        Pattern Ac;
+        std::vector<double> Bc;
+        std::vector<uint8_t> dead_c;
+        rc = setup_transfer(L, rp, col, B, nns, na, Ac, Bc, dead_c, o.mixed);
+        if (rc) return rc;
+        rp = std::move(Ac.rp);
+        col = std::move(Ac.col);
+        b = nns;
+        n = na;
+        B = std::move(Bc);
+        dead = std::move(dead_c);
+        active.assign(n, 0);
+        for (int64_t i = 0; i < n; ++i)
+            for (int c = 0; c < b; ++c) active[i] |= !dead[(size_t)i * b + c];
+    }
+}
+
+// ------------------------------------------------------------------ numeric set-up
+
+static int level_values(Level &L, const double **vals) {
+    *vals = L.Aext ? L.Avals : L.Aown_vals;
+    return SG_OK;
+}
+
+static int power_lmax(sg_amg *h, Level &L, const double *A, cudaStream_t st) {
+    const int64_t nd = L.n * L.b;
+    k_init_vec<<<grid_for(nd, 256), 256, 0, st>>>(nd, L.d);
+    int rc = SG_OK;
+    for (int it = 0; it < h->opt.power_its && !rc; ++it) {
+        rc = rect_spmv<double, double>(L.b, L.b, L.n, L.d_Arp, L.d_Acol, A, L.d, L.t, 1.0, 0.0, nullptr, 0, st);
+        if (rc) break;
+        SG_B_DISPATCH(L.b, (k_dinv_apply<BB, double><<<grid_for(L.n, 256), 256, 0, st>>>(L.n, L.Dinv, L.t, L.r)));
+        rc = multidot(nd, 1, L.r, nd, L.r, h->dots, h->dots + DOT_BLOCKS, st);
+        if (rc) break;
+        k_power_norm<<<grid_for(nd, 256), 256, 0, st>>>(nd, L.r, h->dots + DOT_BLOCKS, L.d, L.lmax);
+    }
+    SG_CUDA(cudaGetLastError());
+    return rc;
+}
+
+static int numeric_update(sg_amg *h, cudaStream_t st) {
+    const int nl = (int)h->L.size();
+    for (int l = 0; l < nl; ++l) {
+        Level &L = h->L[l];
+        const double *A;
+        level_values(L, &A);
+        SG_B_DISPATCH(L.b, (k_block_diag_inv<BB><<<grid_for(L.n, 128), 128, 0, st>>>(L.n, L.d_Adiag, A, L.Dinv, L.Dinv32)));
+        SG_CUDA(cudaGetLastError());
+        if (h->opt.mixed) {
+            const int64_t nv = L.Anblk * L.b * L.b;
+            k_to_float<<<grid_for(nv, 256), 256, 0, st>>>(nv, A, L.A32);
+        }
+        if (l == nl - 1) {
+            // coarsest: dense Gauss-Jordan inverse
+            const int64_t N = h->nc_dense;
+            SG_CUDA(cudaMemsetAsync(h->Ainv, 0, sizeof(double) * N * N, st));
+            SG_B_DISPATCH(L.b, (k_bsr_to_dense<BB><<<grid_for(L.n, 128), 128, 0, st>>>(L.n, L.d_Arp, L.d_Acol, A, N, h->Ainv)));
+            for (int64_t k = 0; k < N; ++k) {
+                k_gj_save<<<grid_for(N, 256), 256, 0, st>>>(N, k, h->Ainv, h->colk, h->rowk);
+                k_gj_update<<<grid_for(N * N, 256, 16), 256, 0, st>>>(N, k, h->Ainv, h->colk, h->rowk);
+            }
+            if (h->opt.mixed) k_to_float<<<grid_for(N * N, 256), 256, 0, st>>>(N * N, h->Ainv, h->Ainv32);
+            SG_CUDA(cudaGetLastError());
+            break;
+        }
+        int rc = power_lmax(h, L, A, st);
+        if (rc) return rc;
+        Level &C = h->L[l + 1];
+        SG_BBC_DISPATCH(L.b, L.bc, ({
+            k_smooth_prolongator<BB, BC><<<grid_for(L.n, 128), 128, 0, st>>>(
+                L.n, L.P.d_rp, L.P.d_col, L.at_plan.d_ptr, L.at_plan.d_a, L.d_Acol, A, L.T, L.d_agg, L.Dinv, L.lmax,
+                h->opt.omega_scale, L.Pv);
+            k_transpose_blocks<BB, BC><<<grid_for(L.P.nblk * BB * BC, 256), 256, 0, st>>>(L.P.nblk, L.d_R_from_P, L.Pv, L.Rv);
+            k_gather_AP<BB, BC><<<grid_for(L.AP.nblk, 128), 128, 0, st>>>(L.AP.nblk, L.ap_plan.d_ptr, L.ap_plan.d_a,
+                                                                          L.ap_plan.d_b, A, L.Pv, L.APv);
+            k_gather_Ac<BB, BC><<<grid_for(C.n, 64), 64, 0, st>>>(C.n, C.d_Arp, C.d_Acol, L.ac_plan.d_ptr,
+                                                                  L.ac_plan.d_a, L.ac_plan.d_b, L.Pv, L.APv, C.d_dead,
+                                                                  C.Aown_vals);
+        }));
+        SG_CUDA(cudaGetLastError());
+        if (h->opt.mixed) {
+            const int64_t np_ = L.P.nblk * L.b * L.bc;
+            k_to_float<<<grid_for(np_, 256), 256, 0, st>>>(np_, L.Pv, L.P32);
+            k_to_float<<<grid_for(np_, 256), 256, 0, st>>>(np_, L.Rv, L.R32);
+        }
+    }
+    SG_CUDA(cudaGetLastError());
+    return SG_OK;
+}
+
+// ------------------------------------------------------------------ V-cycle
+
+template <typename T>
+struct LevelView {
+    const T *A, *Dinv, *P, *R;
+    T *x, *rhs, *r, *d;
+};
+
+template <typename T>
+static LevelView<T> view(Level &L);
+template <>
+LevelView<double> view<double>(Level &L) {
+    return {L.Aext ? L.Avals : L.Aown_vals, L.Dinv, L.Pv, L.Rv, L.x, L.rhs, L.r, L.d};
+}
+template <>
+LevelView<float> view<float>(Level &L) {
+    return {L.A32, L.Dinv32, L.P32, L.R32, L.x32, L.rhs32, L.r32, L.d32};
+}
+
+template <typename T>
+static int smooth(sg_amg *h, Level &L, LevelView<T> &v, bool x_zero, cudaStream_t st) {
+    const int deg = h->opt.cheb_degree;
+    int rc = SG_OK;
+    for (int k = 0; k < deg && !rc; ++k) {
+        const T *r = v.rhs;
+        if (!(x_zero && k == 0)) {
+            rc = rect_spmv<T, T>(L.b, L.b, L.n, L.d_Arp, L.d_Acol, v.A, v.x, v.r, 1.0, 0.0, v.rhs, 1, st);
+            if (rc) return rc;
+            r = v.r;
+        }
+        const int xz = (x_zero && k == 0) ? 1 : 0;
+        SG_B_DISPATCH(L.b, (k_cheb<BB, T><<<grid_for(L.n, 256), 256, 0, st>>>(L.n, k, h->opt.cheb_ratio, L.lmax, v.Dinv, r, v.d, v.x, xz)));
+    }
+    SG_CUDA(cudaGetLastError());
+    return rc;
+}
+
+template <typename T>
+static int vcycle(sg_amg *h, int l, cudaStream_t st) {
+    Level &L = h->L[l];
+    LevelView<T> v = view<T>(L);
+    if (l == (int)h->L.size() - 1) {
+        const T *M = std::is_same<T, float>::value ? (const T *)h->Ainv32 : (const T *)h->Ainv;
+        k_dense_gemv<T><<<grid_for(h->nc_dense * 32, 256), 256, 0, st>>>(h->nc_dense, M, v.rhs, v.x);
+        SG_CUDA(cudaGetLastError());
+        return SG_OK;
+    }
+    Level &C = h->L[l + 1];
+    LevelView<T> c = view<T>(C);
+    int rc = smooth<T>(h, L, v, true, st);
+    if (!rc) rc = rect_spmv<T, T>(L.b, L.b, L.n, L.d_Arp, L.d_Acol, v.A, v.x, v.r, 1.0, 0.0, v.rhs, 1, st);
+    if (!rc) rc = rect_spmv<T, T>(L.bc, L.b, C.n, L.R.d_rp, L.R.d_col, v.R, v.r, c.rhs, 1.0, 0.0, nullptr, 0, st);
+    if (!rc) rc = vcycle<T>(h, l + 1, st);
+    if (!rc) rc = rect_spmv<T, T>(L.b, L.bc, L.n, L.P.d_rp, L.P.d_col, v.P, c.x, v.x, 1.0, 1.0, nullptr, 0, st);
+    if (!rc) rc = smooth<T>(h, L, v, false, st);
+    return rc;
+}
+
+}  // namespace sg
+
+using namespace sg;
+
+extern "C" int sg_amg_create(const sg_bsr *A, const double *nullspace, int32_t nns, const uint8_t *fixed,
+                             const double *opts, int32_t n_opts, sg_amg **out) {
+    SG_CHECK_ARG(out, "null output handle");
+    *out = nullptr;
+    SG_CHECK_ARG(A && nullspace, "null pattern or near-null space");
+    SG_CHECK_ARG(nns > 0 && nns <= 6, "near-null space dimension must be 1..6");
+    SG_CHECK_ARG((A->b == 3 && nns == 6) || (A->b == 2 && nns == 3) || (A->b == 3 && nns == 3),
+                 "supported (block, near-null) sizes: (3,6), (3,3), (2,3)");
+    sg_amg *h = new (std::nothrow) sg_amg();
+    if (!h) return set_error(SG_ERR_NOMEM, "host allocation");
+    cudaGetDevice(&h->device);
+    // opts: [max_levels, coarse_size, cheb_degree, cheb_ratio, power_its, mixed, omega_scale]
+    if (opts) {
+        if (n_opts > 0 && opts[0] > 0) h->opt.max_levels = (int)opts[0];
+        if (n_opts > 1 && opts[1] > 0) h->opt.coarse_size = (int)opts[1];
+        if (n_opts > 2 && opts[2] > 0) h->opt.cheb_degree = (int)opts[2];
+        if (n_opts > 3 && opts[3] > 1) h->opt.cheb_ratio = opts[3];
+        if (n_opts > 4 && opts[4] > 0) h->opt.power_its = (int)opts[4];
+        if (n_opts > 5) h->opt.mixed = opts[5] != 0.0;
+        if (n_opts > 6 && opts[6] > 0) h->opt.omega_scale = opts[6];
+    }
+    int rc = dalloc(&h->dots, DOT_BLOCKS + 64);
+    if (!rc) rc = build_hierarchy(h, A, nullspace, nns, fixed);
+    if (rc) {
+        for (auto &L : h->L) free_level(L);
+        cudaFree(h->Ainv); cudaFree(h->Ainv32); cudaFree(h->colk); cudaFree(h->rowk); cudaFree(h->dots);
+        delete h;
+        return rc;
+    }
+    *out = h;
+    return SG_OK;
+}
+
+extern "C" int sg_amg_destroy(sg_amg *h) {
+    if (!h) return SG_OK;
+    int cur = 0;
+    cudaGetDevice(&cur);
+    cudaSetDevice(h->device);
+    for (auto &L : h->L) free_level(L);
+    cudaFree(h->Ainv);
+    cudaFree(h->Ainv32);
+    cudaFree(h->colk);
+    cudaFree(h->rowk);
+    cudaFree(h->dots);
+    cudaSetDevice(cur);
+    delete h;
+    return SG_OK;
+}
+
+// Numeric set-up for new values of the level-0 matrix (device pointer, kept by reference
+// until the next update: the caller must not free or overwrite it while applying).
+extern "C" int sg_amg_update(sg_amg *h, const double *Avals, void *stream) {
+    SG_CHECK_ARG(h && Avals, "null argument");
+    h->L[0].Avals = Avals;
+    int rc = numeric_update(h, as_stream(stream));
+    if (!rc) h->updated = 1;
+    return rc;
+}
+
+// z = one V-cycle applied to r (device pointers, FP64 in and out).
+extern "C" int sg_amg_apply(sg_amg *h, const double *r, double *z, void *stream) {
+    SG_CHECK_ARG(h && r && z, "null argument");
+    if (!h->updated) return set_error(SG_ERR_STATE, "sg_amg_update must be called before sg_amg_apply");
+    const cudaStream_t st = as_stream(stream);
+    Level &L = h->L[0];
+    const int64_t nd = L.n * L.b;
+    int rc;
+    if (h->opt.mixed) {
+        k_to_float<<<grid_for(nd, 256), 256, 0, st>>>(nd, r, L.rhs32);
+        rc = vcycle<float>(h, 0, st);
+        if (!rc) k_to_double<<<grid_for(nd, 256), 256, 0, st>>>(nd, L.x32, z);
+    } else {
+        SG_CUDA(cudaMemcpyAsync(L.rhs, r, sizeof(double) * nd, cudaMemcpyDeviceToDevice, st));
+        rc = vcycle<double>(h, 0, st);
+        if (!rc) SG_CUDA(cudaMemcpyAsync(z, L.x, sizeof(double) * nd, cudaMemcpyDeviceToDevice, st));
+    }
+    SG_CUDA(cudaGetLastError());
+    return rc;
+}
+
+// info: [levels, dense size, then per level: block size, block rows, blocks] (capacity 3 + 3*10)
+extern "C" int sg_amg_info(const sg_amg *h, int64_t *info, int32_t cap) {
+    SG_CHECK_ARG(h && info && cap >= 2, "bad argument");
+    info[0] = (int64_t)h->L.size();
+    info[1] = h->nc_dense;
+    int k = 2;
+    for (const auto &L : h->L) {
+        if (k + 3 > cap) break;
+        info[k++] = L.b;
+        info[k++] = L.n;
+        info[k++] = L.Anblk;
+    }
+    return SG_OK;
+}
+
+// Copy level l's matrix values (and, if not the coarsest, P values) to host buffers for checks.
+extern "C" int sg_amg_export(const sg_amg *h, int32_t l, int32_t *A_rp, int32_t *A_col, double *A_vals,
+                             int32_t *P_rp, int32_t *P_col, double *P_vals) {
+    SG_CHECK_ARG(h && l >= 0 && l < (int)h->L.size(), "bad level");
+    const Level &L = h->L[l];
+    const double *A = L.Aext ? L.Avals : L.Aown_vals;
+    if (A_rp) SG_CUDA(cudaMemcpy(A_rp, L.d_Arp, sizeof(int32_t) * (L.n + 1), cudaMemcpyDeviceToHost));
+    if (A_col) SG_CUDA(cudaMemcpy(A_col, L.d_Acol, sizeof(int32_t) * L.Anblk, cudaMemcpyDeviceToHost));
+    if (A_vals && A) SG_CUDA(cudaMemcpy(A_vals, A, sizeof(double) * L.Anblk * L.b * L.b, cudaMemcpyDeviceToHost));
+    if (l + 1 < (int)h->L.size()) {
+        if (P_rp) memcpy(P_rp, L.P.rp.data(), sizeof(int32_t) * (L.n + 1));
+        if (P_col) memcpy(P_col, L.P.col.data(), sizeof(int32_t) * L.P.nblk);
+        if (P_vals) SG_CUDA(cudaMemcpy(P_vals, L.Pv, sizeof(double) * L.P.nblk * L.b * L.bc, cudaMemcpyDeviceToHost));
+    }
+    return SG_OK;
+}

@@ -1,0 +1,337 @@
+// (a5, a6, b1-b4) Element operators on the device-resident mesh.
+//
+//   strain     E = B U                        CONSTITUTIVE.m:218,251 (B of elastic_stiffness_matrix_3D.m:105-132)
+//   force      F = B' (w .* S)                CONSTITUTIVE.m:268-285
+//   assemble   K_t = sum_e sum_q B'(w D)B     assemble_K_tangent_vals.c:77-171, into the node-adjacency BSR
+//   elastic_ds DS_elast                       CONSTITUTIVE.m:413-422 (2D IOTA quirk kept, see below)
+//   kr_blend   K_r = sym(r K_el + (1-r) K_t)  CONSTITUTIVE.m:515-532, with Dirichlet rows/columns
+//                                             replaced by identity so the full-DOF system has the
+//                                             K(Q,Q) solution on the free DOFs
+//   to_ref     K values in the reference's find() order (drop-in output of build_K_r_QQ_vals)
+//
+// Strain rows: 3D (e11, e22, e33, g12, g23, g13); 2D (e11, e22, g12).
+#include <cuda_runtime.h>
+
+#include <vector>
+
+#include "mesh.h"
+#include "sg_common.cuh"
+
+namespace sg {
+
+template <int DIM>
+__global__ void k_strain(const int32_t *__restrict__ elem, const double *__restrict__ dphi, int np, int nq,
+                         int64_t n_int, const double *__restrict__ U, double *__restrict__ E) {
+    constexpr int NS = DIM == 3 ? 6 : 3;
+    for (int64_t g = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; g < n_int; g += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t e = g / nq;
+        const double *d = dphi + g * DIM * np;
+        double s[NS];
+#pragma unroll
+        for (int a = 0; a < NS; ++a) s[a] = 0.0;
+        for (int i = 0; i < np; ++i) {
+            const int64_t v = elem[e * np + i];
+            const double d1 = d[i], d2 = d[np + i];
+            if (DIM == 3) {
+                const double d3 = d[2 * np + i];
+                const double ux = U[3 * v], uy = U[3 * v + 1], uz = U[3 * v + 2];
+                s[0] += d1 * ux;
+                s[1] += d2 * uy;
+                s[2] += d3 * uz;
+                s[3] += d2 * ux + d1 * uy;
+                s[4] += d3 * uy + d2 * uz;
+                s[5] += d3 * ux + d1 * uz;
+            } else {
+                const double ux = U[2 * v], uy = U[2 * v + 1];
+                s[0] += d1 * ux;
+                s[1] += d2 * uy;
+                s[2] += d2 * ux + d1 * uy;
+            }
+        }
+#pragma unroll
+        for (int a = 0; a < NS; ++a) E[g * NS + a] = s[a];
+    }
+}
+
+// One thread per (element, local node): sums the element's quadrature points, then adds
+// its dim force components with atomics (F must be zeroed first).
+template <int DIM>
+__global__ void k_force(const int32_t *__restrict__ elem, const double *__restrict__ dphi,
+                        const double *__restrict__ w, int np, int nq, int64_t n_e, const double *__restrict__ S,
+                        int s_rows, double *__restrict__ F) {
+    const int64_t total = n_e * np;
+    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < total; t += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t e = t / np;
+        const int i = (int)(t - e * np);
+        double f[DIM];
+#pragma unroll
+        for (int c = 0; c < DIM; ++c) f[c] = 0.0;
+        for (int q = 0; q < nq; ++q) {
+            const int64_t g = e * nq + q;
+            const double *d = dphi + g * DIM * np;
+            const double *s = S + g * s_rows;
+            const double wq = w[g];
+            const double d1 = d[i], d2 = d[np + i];
+            if (DIM == 3) {
+                const double d3 = d[2 * np + i];
+                f[0] += wq * (d1 * s[0] + d2 * s[3] + d3 * s[5]);
+                f[1] += wq * (d2 * s[1] + d1 * s[3] + d3 * s[4]);
+                f[2] += wq * (d3 * s[2] + d2 * s[4] + d1 * s[5]);
+            } else {
+                f[0] += wq * (d1 * s[0] + d2 * s[2]);
+                f[1] += wq * (d2 * s[1] + d1 * s[2]);
+            }
+        }
+        const int64_t v = elem[e * np + i];
+#pragma unroll
+        for (int c = 0; c < DIM; ++c) atomicAdd(&F[v * DIM + c], f[c]);
+    }
+}
+
+// Nonzeros of column (node j, comp c) of the local B at one point.
+template <int DIM>
+__device__ __forceinline__ void bcol(const double *d, int np, int j, int c, int r[3], double v[3]) {
+    const double d1 = d[j], d2 = d[np + j];
+    if (DIM == 3) {
+        const double d3 = d[2 * np + j];
+        if (c == 0) { r[0] = 0; v[0] = d1; r[1] = 3; v[1] = d2; r[2] = 5; v[2] = d3; }
+        else if (c == 1) { r[0] = 1; v[0] = d2; r[1] = 3; v[1] = d1; r[2] = 4; v[2] = d3; }
+        else { r[0] = 2; v[0] = d3; r[1] = 4; v[1] = d2; r[2] = 5; v[2] = d1; }
+    } else {
+        if (c == 0) { r[0] = 0; v[0] = d1; r[1] = 2; v[1] = d2; }
+        else { r[0] = 1; v[0] = d2; r[1] = 2; v[1] = d1; }
+        r[2] = 0; v[2] = 0.0;
+    }
+}
+
+// One thread per (element, local column (node j, comp c)); accumulates the whole column of
+// the element matrix over the element's points in registers, then adds it into the BSR
+// blocks (node_i, node_j) with one atomic per entry.
+template <int DIM, int NP>
+__global__ void __launch_bounds__(128) k_assemble_bsr(const int32_t *__restrict__ pair_blk,
+                                                      const double *__restrict__ dphi, const double *__restrict__ w,
+                                                      int nq, int64_t n_e, const double *__restrict__ DS,
+                                                      double *__restrict__ K) {
+    constexpr int NS = DIM == 3 ? 6 : 3;
+    constexpr int NL = DIM * NP;
+    const int64_t total = n_e * NL;
+    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < total; t += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t e = t / NL;
+        const int col = (int)(t - e * NL);
+        const int j = col / DIM, c = col - j * DIM;
+        double acc[NL];
+#pragma unroll
+        for (int k = 0; k < NL; ++k) acc[k] = 0.0;
+        for (int q = 0; q < nq; ++q) {
+            const int64_t g = e * nq + q;
+            const double *d = dphi + g * DIM * NP;
+            const double *D = DS + g * NS * NS;
+            const double wq = w[g];
+            int r[3];
+            double v[3];
+            bcol<DIM>(d, NP, j, c, r, v);
+            double db[NS];
+#pragma unroll
+            for (int a = 0; a < NS; ++a) {
+                double s = D[a + NS * r[0]] * v[0] + D[a + NS * r[1]] * v[1];
+                if (DIM == 3) s += D[a + NS * r[2]] * v[2];
+                db[a] = wq * s;
+            }
+#pragma unroll
+            for (int i = 0; i < NP; ++i) {
+                const double d1 = d[i], d2 = d[NP + i];
+                if (DIM == 3) {
+                    const double d3 = d[2 * NP + i];
+                    acc[3 * i + 0] += d1 * db[0] + d2 * db[3] + d3 * db[5];
+                    acc[3 * i + 1] += d2 * db[1] + d1 * db[3] + d3 * db[4];
+                    acc[3 * i + 2] += d3 * db[2] + d2 * db[4] + d1 * db[5];
+                } else {
+                    acc[2 * i + 0] += d1 * db[0] + d2 * db[2];
+                    acc[2 * i + 1] += d2 * db[1] + d1 * db[2];
+                }
+            }
+        }
+        const int32_t *pb = pair_blk + e * NP * NP;
+#pragma unroll
+        for (int i = 0; i < NP; ++i) {
+            const int64_t blk = pb[i * NP + j];   // block (node_i, node_j)
+#pragma unroll
+            for (int cp = 0; cp < DIM; ++cp) atomicAdd(&K[blk * DIM * DIM + cp * DIM + c], acc[DIM * i + cp]);
+        }
+    }
+}
+
+// DS_elast = 2 * shear * DEV + bulk * VOL with IOTA = [1;1;1; zeros(ns-3,1)] (CONSTITUTIVE.m:413-422).
+// For ns == 3 (2D) the reference's IOTA has three ones, so VOL is the all-ones 3x3 matrix;
+// that arithmetic is reproduced as is.
+template <int NS>
+__global__ void k_elastic_ds(const double *__restrict__ shear, const double *__restrict__ bulk, int64_t n,
+                             double *__restrict__ DS) {
+    for (int64_t g = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; g < n; g += (int64_t)gridDim.x * blockDim.x) {
+        const double G = shear[g], Kb = bulk[g];
+#pragma unroll
+        for (int j = 0; j < NS; ++j)
+#pragma unroll
+            for (int i = 0; i < NS; ++i) {
+                const double vol = (i < 3 && j < 3) ? 1.0 : 0.0;
+                const double id = (i == j) ? ((NS == 6) ? (i < 3 ? 1.0 : 0.5) : (i < 2 ? 1.0 : 0.5)) : 0.0;
+                const double dev = id - vol / 3.0;
+                DS[g * NS * NS + i + NS * j] = 2.0 * dev * G + vol * Kb;
+            }
+    }
+}
+
+// K_r for every BSR entry: v1 = r Kel + (1-r) Kt at (i,j), v2 the same at (j,i), K_r = (v1+v2)/2;
+// Dirichlet rows/columns are zero with a unit diagonal.  Kel may be null (r is then ignored).
+template <int DIM>
+__global__ void k_kr_blend(int64_t n_blocks, const int32_t *__restrict__ row_of, const int32_t *__restrict__ col,
+                           const int32_t *__restrict__ tr, const double *__restrict__ mask, double r,
+                           const double *__restrict__ Kel, const double *__restrict__ Kt, double *__restrict__ Kr) {
+    constexpr int BB = DIM * DIM;
+    const int64_t total = n_blocks * BB;
+    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < total; t += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t p = t / BB;
+        const int ab = (int)(t - p * BB), a = ab / DIM, b = ab - a * DIM;
+        const int64_t I = row_of[p], J = col[p];
+        const int64_t pt = tr[p];
+        const double ra = mask[I * DIM + a], cb = mask[J * DIM + b];
+        double out;
+        if (ra != 0.0 && cb != 0.0) {
+            const double el1 = Kel ? Kel[p * BB + ab] : 0.0, el2 = Kel ? Kel[pt * BB + b * DIM + a] : 0.0;
+            const double v1 = r * el1 + (1.0 - r) * Kt[p * BB + ab];
+            const double v2 = r * el2 + (1.0 - r) * Kt[pt * BB + b * DIM + a];
+            out = (v1 + v2) / 2.0;
+        } else {
+            out = (I == J && a == b) ? 1.0 : 0.0;
+        }
+        Kr[p * BB + ab] = out;
+    }
+}
+
+// (K + K')/2 on the BSR pattern (used once for the elastic matrix, like CONSTITUTIVE.m:429).
+template <int DIM>
+__global__ void k_symmetrize(int64_t n_blocks, const int32_t *__restrict__ tr, const double *__restrict__ K,
+                             double *__restrict__ Ks) {
+    constexpr int BB = DIM * DIM;
+    const int64_t total = n_blocks * BB;
+    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < total; t += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t p = t / BB;
+        const int ab = (int)(t - p * BB), a = ab / DIM, b = ab - a * DIM;
+        Ks[p * BB + ab] = (K[p * BB + ab] + K[(int64_t)tr[p] * BB + b * DIM + a]) / 2.0;
+    }
+}
+
+__global__ void k_gather(int64_t n, const int64_t *__restrict__ idx, const double *__restrict__ src,
+                         double *__restrict__ dst) {
+    for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < n; k += (int64_t)gridDim.x * blockDim.x)
+        dst[k] = src[idx[k]];
+}
+
+}  // namespace sg
+
+using namespace sg;
+
+extern "C" int sg_strain_dev(const sg_mesh *m, const double *U, double *E, void *stream) {
+    SG_CHECK_ARG(m && U && E, "null argument");
+    const cudaStream_t st = as_stream(stream);
+    if (m->dim == 3) k_strain<3><<<grid_for(m->n_int, 256), 256, 0, st>>>(m->d_elem, m->d_dphi, m->np, m->nq, m->n_int, U, E);
+    else k_strain<2><<<grid_for(m->n_int, 256), 256, 0, st>>>(m->d_elem, m->d_dphi, m->np, m->nq, m->n_int, U, E);
+    SG_CUDA(cudaGetLastError());
+    return SG_OK;
+}
+
+extern "C" int sg_force_dev(const sg_mesh *m, const double *S, int32_t s_rows, double *F, void *stream) {
+    SG_CHECK_ARG(m && S && F, "null argument");
+    SG_CHECK_ARG(s_rows >= m->ns, "s_rows smaller than the number of strain components");
+    const cudaStream_t st = as_stream(stream);
+    SG_CUDA(cudaMemsetAsync(F, 0, sizeof(double) * m->n_n * m->dim, st));
+    const int64_t work = m->n_e * m->np;
+    if (m->dim == 3) k_force<3><<<grid_for(work, 256), 256, 0, st>>>(m->d_elem, m->d_dphi, m->d_w, m->np, m->nq, m->n_e, S, s_rows, F);
+    else k_force<2><<<grid_for(work, 256), 256, 0, st>>>(m->d_elem, m->d_dphi, m->d_w, m->np, m->nq, m->n_e, S, s_rows, F);
+    SG_CUDA(cudaGetLastError());
+    return SG_OK;
+}
+
+extern "C" int sg_assemble_bsr_dev(const sg_mesh *m, const double *DS, double *K, void *stream) {
+    SG_CHECK_ARG(m && DS && K, "null argument");
+    const cudaStream_t st = as_stream(stream);
+    SG_CUDA(cudaMemsetAsync(K, 0, sizeof(double) * m->bsr.n_blocks * m->dim * m->dim, st));
+    const int64_t work = m->n_e * m->dim * m->np;
+    if (m->dim == 3 && m->np == 10)
+        k_assemble_bsr<3, 10><<<grid_for(work, 128, 16), 128, 0, st>>>(m->d_pair_blk, m->d_dphi, m->d_w, m->nq, m->n_e, DS, K);
+    else if (m->dim == 2 && m->np == 6)
+        k_assemble_bsr<2, 6><<<grid_for(work, 128, 16), 128, 0, st>>>(m->d_pair_blk, m->d_dphi, m->d_w, m->nq, m->n_e, DS, K);
+    else if (m->dim == 3 && m->np == 4)
+        k_assemble_bsr<3, 4><<<grid_for(work, 128, 16), 128, 0, st>>>(m->d_pair_blk, m->d_dphi, m->d_w, m->nq, m->n_e, DS, K);
+    else if (m->dim == 2 && m->np == 3)
+        k_assemble_bsr<2, 3><<<grid_for(work, 128, 16), 128, 0, st>>>(m->d_pair_blk, m->d_dphi, m->d_w, m->nq, m->n_e, DS, K);
+    else
+        return set_error(SG_ERR_ARG, "BSR assembly supports P1/P2 triangles and tetrahedra");
+    SG_CUDA(cudaGetLastError());
+    return SG_OK;
+}
+
+extern "C" int sg_elastic_ds_dev(const sg_mesh *m, const double *shear, const double *bulk, double *DS, void *stream) {
+    SG_CHECK_ARG(m && shear && bulk && DS, "null argument");
+    const cudaStream_t st = as_stream(stream);
+    if (m->dim == 3) k_elastic_ds<6><<<grid_for(m->n_int, 256), 256, 0, st>>>(shear, bulk, m->n_int, DS);
+    else k_elastic_ds<3><<<grid_for(m->n_int, 256), 256, 0, st>>>(shear, bulk, m->n_int, DS);
+    SG_CUDA(cudaGetLastError());
+    return SG_OK;
+}
+
+
+extern "C" int sg_symmetrize_bsr_dev(const sg_mesh *m, const double *K, double *Ks, void *stream) {
+    SG_CHECK_ARG(m && K && Ks && K != Ks, "null or aliased argument");
+    const cudaStream_t st = as_stream(stream);
+    const int64_t work = m->bsr.n_blocks * m->dim * m->dim;
+    if (m->dim == 3) k_symmetrize<3><<<grid_for(work, 256), 256, 0, st>>>(m->bsr.n_blocks, m->bsr.d_transpose, K, Ks);
+    else k_symmetrize<2><<<grid_for(work, 256), 256, 0, st>>>(m->bsr.n_blocks, m->bsr.d_transpose, K, Ks);
+    SG_CUDA(cudaGetLastError());
+    return SG_OK;
+}
+
+extern "C" int sg_kr_blend_dev(const sg_mesh *m, double r, const double *Kel, const double *Kt, double *Kr,
+                               void *stream) {
+    SG_CHECK_ARG(m && Kt && Kr && Kt != Kr, "null or aliased argument");
+    const cudaStream_t st = as_stream(stream);
+    const int32_t *row_of = m->bsr.d_row_of;
+    const int64_t work = m->bsr.n_blocks * m->dim * m->dim;
+    if (m->dim == 3)
+        k_kr_blend<3><<<grid_for(work, 256), 256, 0, st>>>(m->bsr.n_blocks, row_of, m->bsr.d_col, m->bsr.d_transpose, m->d_mask, r, Kel, Kt, Kr);
+    else
+        k_kr_blend<2><<<grid_for(work, 256), 256, 0, st>>>(m->bsr.n_blocks, row_of, m->bsr.d_col, m->bsr.d_transpose, m->d_mask, r, Kel, Kt, Kr);
+    SG_CUDA(cudaGetLastError());
+    return SG_OK;
+}
+
+extern "C" int sg_bsr_to_ref_dev(sg_mesh *m, const double *K, double *V_ref, void *stream) {
+    SG_CHECK_ARG(m && K && V_ref, "null argument");
+    const cudaStream_t st = as_stream(stream);
+    if (!m->d_ref2bsr) {
+        // value index of K(ref_I, ref_J) for every pattern entry, built once per mesh
+        const int dim = m->dim;
+        std::vector<int32_t> tr(m->bsr.n_blocks);
+        SG_CUDA(cudaMemcpy(tr.data(), m->bsr.d_transpose, sizeof(int32_t) * tr.size(), cudaMemcpyDeviceToHost));
+        std::vector<int64_t> idx(m->nnz_ref);
+        int64_t k = 0;
+        const sg_bsr &B = m->bsr;
+        for (int64_t v = 0; v < m->n_n; ++v)
+            for (int a = 0; a < dim; ++a) {
+                if (m->dof2q[v * dim + a] < 0) continue;
+                for (int32_t p = B.row_ptr[v]; p < B.row_ptr[v + 1]; ++p) {
+                    const int64_t wn = B.col[p];
+                    for (int b = 0; b < dim; ++b) {
+                        if (m->dof2q[wn * dim + b] < 0) continue;
+                        // entry (row q(v,a), col q(wn,b)) holds K(ref_I = q(wn,b), ref_J = q(v,a))
+                        idx[k++] = (int64_t)tr[p] * dim * dim + b * dim + a;
+                    }
+                }
+            }
+        SG_CUDA(cudaMalloc(&m->d_ref2bsr, sizeof(int64_t) * (idx.size() ? idx.size() : 1)));
+        SG_CUDA(cudaMemcpy(m->d_ref2bsr, idx.data(), sizeof(int64_t) * idx.size(), cudaMemcpyHostToDevice));
+    }
+    k_gather<<<grid_for(m->nnz_ref, 256), 256, 0, st>>>(m->nnz_ref, m->d_ref2bsr, K, V_ref);
+    SG_CUDA(cudaGetLastError());
+    return SG_OK;
+}

@@ -1,0 +1,294 @@
+// (c2) Node-block BSR SpMV and (c1, c3) Krylov vector kernels.
+//
+// SpMV: a group of G threads per block row; the group's lanes read consecutive blocks of the
+// row (contiguous b*b-value runs), accumulate b partial sums and combine them with warp
+// shuffles.  Rows are assigned in warp-uniform slots so the shuffles never diverge.
+// Dot products use a fixed two-stage tree (per-block partials, then one ordered pass), so
+// results are bitwise reproducible from run to run.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+
+#include "linalg.cuh"
+#include "sg_common.cuh"
+
+namespace sg {
+
+template <typename T> struct Acc { using type = double; };
+template <> struct Acc<float> { using type = float; };
+
+template <int BR, int BC, int G, typename VT, typename XT>
+__global__ void __launch_bounds__(256) k_bsr_spmv(int64_t nrows, const int32_t *__restrict__ rp,
+                                                  const int32_t *__restrict__ col, const VT *__restrict__ vals,
+                                                  const XT *__restrict__ x, XT *__restrict__ y, double alpha,
+                                                  double beta, const XT *__restrict__ bvec, int mode) {
+    using A = typename Acc<XT>::type;
+    constexpr int GPW = 32 / G;  // groups per warp
+    const int lane = threadIdx.x & 31, g = lane / G, gl = lane - g * G;
+    const int64_t warp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+    const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    for (int64_t base = warp * GPW; base < nrows; base += nwarps * GPW) {
+        const int64_t row = base + g;
+        A acc[BR];
+#pragma unroll
+        for (int a = 0; a < BR; ++a) acc[a] = 0;
+        if (row < nrows) {
+            const int32_t p1 = rp[row + 1];
+            for (int32_t p = rp[row] + gl; p < p1; p += G) {
+                const int64_t j = col[p];
+                A xj[BC];
+#pragma unroll
+                for (int b = 0; b < BC; ++b) xj[b] = (A)x[j * BC + b];
+                const VT *v = vals + (int64_t)p * BR * BC;
+#pragma unroll
+                for (int a = 0; a < BR; ++a)
+#pragma unroll
+                    for (int b = 0; b < BC; ++b) acc[a] += (A)v[a * BC + b] * xj[b];
+            }
+        }
+#pragma unroll
+        for (int off = G / 2; off > 0; off >>= 1)
+#pragma unroll
+            for (int a = 0; a < BR; ++a) acc[a] += __shfl_xor_sync(0xffffffffu, acc[a], off);
+        if (row < nrows && gl == 0) {
+#pragma unroll
+            for (int a = 0; a < BR; ++a) {
+                const int64_t k = row * BR + a;
+                if (mode == 1) y[k] = (XT)((A)bvec[k] - acc[a]);
+                else if (beta == 0.0) y[k] = (XT)(alpha * acc[a]);
+                else y[k] = (XT)(alpha * acc[a] + beta * (A)y[k]);
+            }
+        }
+    }
+}
+
+template <int BR, int BC, typename VT, typename XT>
+static void spmv_launch(int64_t nrows, const int32_t *rp, const int32_t *col, const VT *vals, const XT *x, XT *y,
+                        double alpha, double beta, const XT *bvec, int mode, cudaStream_t st) {
+    constexpr int G = (BR * BC >= 9) ? 8 : 4;
+    const int64_t threads = nrows * G;
+    k_bsr_spmv<BR, BC, G, VT, XT><<<grid_for(threads, 256, 16), 256, 0, st>>>(nrows, rp, col, vals, x, y, alpha, beta,
+                                                                               bvec, mode);
+}
+
+template <typename VT, typename XT>
+int rect_spmv(int br, int bc, int64_t nrows, const int32_t *rp, const int32_t *col, const VT *vals, const XT *x,
+              XT *y, double alpha, double beta, const XT *bvec, int mode, cudaStream_t st) {
+#define SG_SPMV_CASE(R, Cc) \
+    if (br == R && bc == Cc) { spmv_launch<R, Cc>(nrows, rp, col, vals, x, y, alpha, beta, bvec, mode, st); SG_CUDA(cudaGetLastError()); return SG_OK; }
+    SG_SPMV_CASE(1, 1) SG_SPMV_CASE(2, 2) SG_SPMV_CASE(3, 3) SG_SPMV_CASE(6, 6)
+    SG_SPMV_CASE(2, 3) SG_SPMV_CASE(3, 2) SG_SPMV_CASE(3, 6) SG_SPMV_CASE(6, 3)
+#undef SG_SPMV_CASE
+    return set_error(SG_ERR_ARG, "unsupported BSR block shape");
+}
+template int rect_spmv<double, double>(int, int, int64_t, const int32_t *, const int32_t *, const double *, const double *,
+                                       double *, double, double, const double *, int, cudaStream_t);
+template int rect_spmv<float, float>(int, int, int64_t, const int32_t *, const int32_t *, const float *, const float *,
+                                     float *, double, double, const float *, int, cudaStream_t);
+
+template <typename VT, typename XT>
+int bsr_spmv(const sg_bsr &A, const VT *vals, const XT *x, XT *y, double alpha, double beta, cudaStream_t st) {
+    return rect_spmv<VT, XT>(A.b, A.b, A.n_rows, A.d_row_ptr, A.d_col, vals, x, y, alpha, beta, nullptr, 0, st);
+}
+template <typename VT, typename XT>
+int bsr_residual(const sg_bsr &A, const VT *vals, const XT *x, const XT *b, XT *r, cudaStream_t st) {
+    return rect_spmv<VT, XT>(A.b, A.b, A.n_rows, A.d_row_ptr, A.d_col, vals, x, r, 1.0, 0.0, b, 1, st);
+}
+template int bsr_spmv<double, double>(const sg_bsr &, const double *, const double *, double *, double, double, cudaStream_t);
+template int bsr_spmv<float, float>(const sg_bsr &, const float *, const float *, float *, double, double, cudaStream_t);
+template int bsr_residual<double, double>(const sg_bsr &, const double *, const double *, const double *, double *, cudaStream_t);
+template int bsr_residual<float, float>(const sg_bsr &, const float *, const float *, const float *, float *, cudaStream_t);
+
+// ------------------------------------------------------------------ dots and GEMV
+
+__device__ __forceinline__ double block_sum(double v, double *sh) {
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) v += __shfl_xor_sync(0xffffffffu, v, off);
+    const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+    __syncthreads();
+    if (l == 0) sh[w] = v;
+    __syncthreads();
+    double t = 0.0;
+    if (threadIdx.x < 32) {
+        t = (l < (int)(blockDim.x >> 5)) ? sh[l] : 0.0;
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1) t += __shfl_xor_sync(0xffffffffu, t, off);
+    }
+    return t;  // valid in thread 0
+}
+
+// partial[i * gridDim.x + block] = sum over this block's row chunk of V(r, i) * w(r)
+__global__ void __launch_bounds__(DOT_THREADS) k_multidot(int64_t n, int m, const double *__restrict__ V, int64_t ldv,
+                                                          const double *__restrict__ w, double *__restrict__ partial) {
+    __shared__ double sh[32];
+    const int64_t chunk = (n + gridDim.x - 1) / gridDim.x;
+    const int64_t r0 = blockIdx.x * chunk, r1 = min(n, r0 + chunk);
+    int i = 0;
+    for (; i + 4 <= m; i += 4) {
+        double s0 = 0, s1 = 0, s2 = 0, s3 = 0;
+        for (int64_t r = r0 + threadIdx.x; r < r1; r += blockDim.x) {
+            const double wr = w[r];
+            s0 += V[(i + 0) * ldv + r] * wr;
+            s1 += V[(i + 1) * ldv + r] * wr;
+            s2 += V[(i + 2) * ldv + r] * wr;
+            s3 += V[(i + 3) * ldv + r] * wr;
+        }
+        s0 = block_sum(s0, sh);
+        if (threadIdx.x == 0) partial[(i + 0) * gridDim.x + blockIdx.x] = s0;
+        s1 = block_sum(s1, sh);
+        if (threadIdx.x == 0) partial[(i + 1) * gridDim.x + blockIdx.x] = s1;
+        s2 = block_sum(s2, sh);
+        if (threadIdx.x == 0) partial[(i + 2) * gridDim.x + blockIdx.x] = s2;
+        s3 = block_sum(s3, sh);
+        if (threadIdx.x == 0) partial[(i + 3) * gridDim.x + blockIdx.x] = s3;
+    }
+    for (; i < m; ++i) {
+        double s = 0;
+        for (int64_t r = r0 + threadIdx.x; r < r1; r += blockDim.x) s += V[i * ldv + r] * w[r];
+        s = block_sum(s, sh);
+        if (threadIdx.x == 0) partial[i * gridDim.x + blockIdx.x] = s;
+    }
+}
+
+// out[i] = sum_b partial[i * nb + b]   (one block per column, fixed order)
+__global__ void k_reduce_partials(int m, int nb, const double *__restrict__ partial, double *__restrict__ out) {
+    __shared__ double sh[32];
+    for (int i = blockIdx.x; i < m; i += gridDim.x) {
+        double s = 0;
+        for (int b = threadIdx.x; b < nb; b += blockDim.x) s += partial[(int64_t)i * nb + b];
+        s = block_sum(s, sh);
+        if (threadIdx.x == 0) out[i] = s;
+    }
+}
+
+int multidot(int64_t n, int m, const double *V, int64_t ldv, const double *w, double *partial, double *out,
+             cudaStream_t st) {
+    if (m <= 0) return SG_OK;
+    k_multidot<<<DOT_BLOCKS, DOT_THREADS, 0, st>>>(n, m, V, ldv, w, partial);
+    k_reduce_partials<<<std::min(m, 1024), 256, 0, st>>>(m, DOT_BLOCKS, partial, out);
+    SG_CUDA(cudaGetLastError());
+    return SG_OK;
+}
+
+template <int SIGN>
+__global__ void k_gemv(int64_t n, int m, const double *__restrict__ V, int64_t ldv, const double *__restrict__ h,
+                       double *__restrict__ w) {
+    extern __shared__ double hs[];
+    for (int i = threadIdx.x; i < m; i += blockDim.x) hs[i] = h[i];
+    __syncthreads();
+    for (int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; r < n; r += (int64_t)gridDim.x * blockDim.x) {
+        double s = 0;
+        for (int i = 0; i < m; ++i) s += hs[i] * V[i * ldv + r];
+        w[r] = SIGN > 0 ? w[r] + s : w[r] - s;
+    }
+}
+
+int gemv_sub(int64_t n, int m, const double *V, int64_t ldv, const double *h, double *w, cudaStream_t st) {
+    if (m <= 0) return SG_OK;
+    k_gemv<-1><<<grid_for(n, 256, 8), 256, sizeof(double) * m, st>>>(n, m, V, ldv, h, w);
+    SG_CUDA(cudaGetLastError());
+    return SG_OK;
+}
+
+int gemv_add(int64_t n, int m, const double *V, int64_t ldv, const double *y, double *x, cudaStream_t st) {
+    if (m <= 0) return SG_OK;
+    k_gemv<1><<<grid_for(n, 256, 8), 256, sizeof(double) * m, st>>>(n, m, V, ldv, y, x);
+    SG_CUDA(cudaGetLastError());
+    return SG_OK;
+}
+
+__global__ void k_axpby(int64_t n, double a, const double *__restrict__ x, double b, double *__restrict__ y) {
+    for (int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; r < n; r += (int64_t)gridDim.x * blockDim.x)
+        y[r] = (b == 0.0) ? a * x[r] : a * x[r] + b * y[r];
+}
+
+int axpby(int64_t n, double a, const double *x, double b, double *y, cudaStream_t st) {
+    k_axpby<<<grid_for(n, 256, 8), 256, 0, st>>>(n, a, x, b, y);
+    SG_CUDA(cudaGetLastError());
+    return SG_OK;
+}
+
+// y = x * s, s = num[0] (invert: 1 / num[0])
+__global__ void k_scale(int64_t n, const double *__restrict__ x, const double *__restrict__ num, int invert,
+                        double *__restrict__ y) {
+    const double s = invert ? 1.0 / num[0] : num[0];
+    for (int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; r < n; r += (int64_t)gridDim.x * blockDim.x)
+        y[r] = x[r] * s;
+}
+
+int scale_dev(int64_t n, const double *x, const double *num, int invert, double *y, cudaStream_t st) {
+    k_scale<<<grid_for(n, 256, 8), 256, 0, st>>>(n, x, num, invert, y);
+    SG_CUDA(cudaGetLastError());
+    return SG_OK;
+}
+
+// sum mask * (a - b)^2 partials (Newton residual over the free DOFs)
+__global__ void __launch_bounds__(DOT_THREADS) k_masked_diff2(int64_t n, const double *__restrict__ a,
+                                                              const double *__restrict__ b,
+                                                              const double *__restrict__ mask,
+                                                              double *__restrict__ partial) {
+    __shared__ double sh[32];
+    const int64_t chunk = (n + gridDim.x - 1) / gridDim.x;
+    const int64_t r0 = blockIdx.x * chunk, r1 = min(n, r0 + chunk);
+    double s = 0;
+    for (int64_t r = r0 + threadIdx.x; r < r1; r += blockDim.x) {
+        const double d = (a[r] - (b ? b[r] : 0.0)) * (mask ? mask[r] : 1.0);
+        s += d * d;
+    }
+    s = block_sum(s, sh);
+    if (threadIdx.x == 0) partial[blockIdx.x] = s;
+}
+
+}  // namespace sg
+
+using namespace sg;
+
+extern "C" int sg_bsr_spmv_dev(const sg_bsr *A, const double *vals, const double *x, double *y, void *stream) {
+    SG_CHECK_ARG(A && vals && x && y, "null argument");
+    return bsr_spmv<double, double>(*A, vals, x, y, 1.0, 0.0, as_stream(stream));
+}
+
+extern "C" int sg_bsr_info(const sg_bsr *A, int64_t *info) {
+    SG_CHECK_ARG(A && info, "null argument");
+    info[0] = A->b;
+    info[1] = A->n_rows;
+    info[2] = A->n_blocks;
+    return SG_OK;
+}
+
+// Host-visible reductions (synchronise `stream`).
+extern "C" int sg_dot_dev(int64_t n, const double *x, const double *y, double *result, void *stream) {
+    SG_CHECK_ARG(x && y && result && n >= 0, "bad argument");
+    static thread_local Scratch ws;
+    int rc = ws.reserve(sizeof(double) * (DOT_BLOCKS + 8));
+    if (rc) return rc;
+    double *part = (double *)ws.ptr, *out = part + DOT_BLOCKS;
+    const cudaStream_t st = as_stream(stream);
+    rc = multidot(n, 1, x, n, y, part, out, st);
+    if (rc) return rc;
+    SG_CUDA(cudaMemcpyAsync(result, out, sizeof(double), cudaMemcpyDeviceToHost, st));
+    SG_CUDA(cudaStreamSynchronize(st));
+    return SG_OK;
+}
+
+// result = sum_r mask[r] * (a[r] - b[r])^2   (b, mask nullable)
+extern "C" int sg_masked_diff_norm2_dev(int64_t n, const double *a, const double *b, const double *mask,
+                                        double *result, void *stream) {
+    SG_CHECK_ARG(a && result && n >= 0, "bad argument");
+    static thread_local Scratch ws;
+    int rc = ws.reserve(sizeof(double) * (DOT_BLOCKS + 8));
+    if (rc) return rc;
+    double *part = (double *)ws.ptr, *out = part + DOT_BLOCKS;
+    const cudaStream_t st = as_stream(stream);
+    k_masked_diff2<<<DOT_BLOCKS, DOT_THREADS, 0, st>>>(n, a, b, mask, part);
+    k_reduce_partials<<<1, 256, 0, st>>>(1, DOT_BLOCKS, part, out);
+    SG_CUDA(cudaGetLastError());
+    SG_CUDA(cudaMemcpyAsync(result, out, sizeof(double), cudaMemcpyDeviceToHost, st));
+    SG_CUDA(cudaStreamSynchronize(st));
+    return SG_OK;
+}
+
+extern "C" int sg_axpby_dev(int64_t n, double a, const double *x, double b, double *y, void *stream) {
+    SG_CHECK_ARG(x && y && n >= 0, "bad argument");
+    return axpby(n, a, x, b, y, as_stream(stream));
+}

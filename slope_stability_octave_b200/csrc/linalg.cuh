@@ -1,0 +1,40 @@
+// Device linear-algebra building blocks for the Krylov solver and the AMG V-cycle.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "mesh.h"
+
+namespace sg {
+
+// y = alpha * A x + beta * y  (BSR, b x b blocks, values of type VT, vectors of type XT)
+template <typename VT, typename XT>
+int bsr_spmv(const sg_bsr &A, const VT *vals, const XT *x, XT *y, double alpha, double beta, cudaStream_t st);
+// r = b - A x
+template <typename VT, typename XT>
+int bsr_residual(const sg_bsr &A, const VT *vals, const XT *x, const XT *b, XT *r, cudaStream_t st);
+
+// Rectangular-block row SpMV: y = alpha * M x + beta * y (mode 0) or y = bvec - M x (mode 1),
+// M with br x bc blocks.  Supported shapes: 1x1 2x2 3x3 6x6 2x3 3x2 3x6 6x3.
+template <typename VT, typename XT>
+int rect_spmv(int br, int bc, int64_t nrows, const int32_t *rp, const int32_t *col, const VT *vals, const XT *x,
+              XT *y, double alpha, double beta, const XT *bvec, int mode, cudaStream_t st);
+
+// Reduction workspace for dot products: partial sums of `nblk` blocks per column.
+constexpr int DOT_BLOCKS = 296;  // 2 x 148 SMs
+constexpr int DOT_THREADS = 256;
+
+// out[i] = V(:, i)' w for i < m (V column-major, leading dimension ldv); deterministic.
+int multidot(int64_t n, int m, const double *V, int64_t ldv, const double *w, double *partial, double *out,
+             cudaStream_t st);
+// w -= V(:, 0:m) h      (h on the device)
+int gemv_sub(int64_t n, int m, const double *V, int64_t ldv, const double *h, double *w, cudaStream_t st);
+// x += V(:, 0:m) y      (y on the device)
+int gemv_add(int64_t n, int m, const double *V, int64_t ldv, const double *y, double *x, cudaStream_t st);
+// y = a x + b y
+int axpby(int64_t n, double a, const double *x, double b, double *y, cudaStream_t st);
+// y = x * s where s = *num / *den on the device (den may be null -> s = *num)
+int scale_dev(int64_t n, const double *x, const double *num, int invert, double *y, cudaStream_t st);
+
+}  // namespace sg

@@ -70,9 +70,21 @@ def classify3d(E, c_bar, sin_phi, shear, lame):
     margin = np.abs(f) / scale_f
     for a, b in ((ls, gsl), (ls, gsr), (gsl, gsr), (ll, gsl), (ll, gla), (lr, gsr), (lr, gra)):
         margin = np.minimum(margin, rel(a, b))
-    spread = np.abs(e1) + np.abs(e3) + 1e-300
-    margin = np.minimum(margin, np.minimum(e1 - e2, e2 - e3) / spread)
     return br, margin
+
+
+def separation3d(E, branch):
+    """Relative separation of the principal strains that the branch's tangent formula divides
+    by (smooth: all three; left edge: e3 from e1, e2; right edge: e1 from e2, e3); inf for
+    the elastic and apex branches, whose tangents do not depend on the eigen-projections."""
+    e1, e2, e3, _ = _principal(E)
+    spread = np.abs(e1) + np.abs(e2) + np.abs(e3) + 1e-300
+    sep = np.full(E.shape[0], np.inf)
+    sm, lf, rt = branch == 1, branch == 2, branch == 3
+    sep[sm] = (np.minimum(e1 - e2, e2 - e3) / spread)[sm]
+    sep[lf] = ((e2 - e3) / spread)[lf]
+    sep[rt] = ((e1 - e2) / spread)[rt]
+    return sep
 
 
 def _random_rotations(rng, n):
@@ -91,8 +103,12 @@ _PROPOSALS = {0: (-1.0, 0.3, 0.0, 1.0), 1: (-2.0, 2.0, 0.0, 4.0), 2: (-2.0, 2.0,
 
 
 def constitutive_points(n, seed=20261203, fractions=(0.2, 0.2, 0.2, 0.2, 0.2), margin=1e-8,
-                        young=40000.0, poisson=0.3, sort_by_branch=False):
-    """Seeded per-point inputs for the constitutive kernels (config 1 draws)."""
+                        young=40000.0, poisson=0.3, sort_by_branch=False, separation=1e-4):
+    """Seeded per-point inputs for the constitutive kernels (config 1 draws).
+
+    ``separation``: minimum relative gap of the principal strains entering the branch's
+    tangent (``separation3d``); nearly coincident principal strains make the reference's
+    own tangent sensitive to 1-ulp input changes, so they are excluded from seeded sets."""
     rng = np.random.default_rng(seed)
     c0 = rng.uniform(5.0, 15.0, n)
     phi_deg = rng.uniform(25.0, 45.0, n)
@@ -123,7 +139,7 @@ def constitutive_points(n, seed=20261203, fractions=(0.2, 0.2, 0.2, 0.2, 0.2), m
         Ed = np.zeros((k, 6))
         Ed[:, :3] = e
         br, mg = classify3d(Ed, c_bar[todo], sin_phi[todo], mat["shear"][todo], mat["lame"][todo])
-        ok = (br == t) & (mg >= margin)
+        ok = (br == t) & (mg >= margin) & (separation3d(Ed, br) >= separation)
         prin[todo[ok]] = e[ok]
         todo = todo[~ok]
     if todo.size:
@@ -134,7 +150,7 @@ def constitutive_points(n, seed=20261203, fractions=(0.2, 0.2, 0.2, 0.2, 0.2), m
     # the rotation perturbs the principal values by rounding: re-check and re-draw the few
     # points whose margin fell below the threshold (keeps the guarantee exact)
     br, mg = classify3d(E, c_bar, sin_phi, mat["shear"], mat["lame"])
-    bad = np.nonzero((br != target) | (mg < margin))[0]
+    bad = np.nonzero((br != target) | (mg < margin) | (separation3d(E, br) < separation))[0]
     if bad.size:
         E[bad] = 0.0
         E[bad, :3] = prin[bad]

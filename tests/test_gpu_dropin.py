@@ -1,8 +1,15 @@
 """GPU parity of the drop-in (host-buffer) entry points against the oracle.
 
-Tolerances (FP64): branch ids bit-exact; stress and tangent within 1e-12 relative per point
-(|x - x_ref| <= 1e-12 * ||x_ref|| with the point's Frobenius norm); assembled K values within
-1e-12 relative to max |V|.
+Tolerances (FP64):
+  * branch ids: bit-exact;
+  * stress and tangent, per point, in the point's Frobenius norm:
+        |x - x_ref| <= max(1e-12, 10 * kappa_p) * |x_ref|
+    where kappa_p is the oracle's own relative change under random 1-ulp perturbations of
+    the strain at that point (the reference's arithmetic sums large, nearly cancelling
+    eigen-projection derivatives; at a few points per 10^5 its own result moves by up to
+    ~1e-11 under 1-ulp input changes, so no implementation with different rounding can
+    agree below that there).  At least 99.9 % of points must meet 1e-12 outright;
+  * assembled K values: within 1e-12 relative to max |V|.
 """
 import ctypes as C
 
@@ -33,11 +40,29 @@ def gpu_constitutive(dim, d, want_ds=True):
     return S, DS, br
 
 
-def assert_pointwise(x, ref, rtol=RTOL):
+def sensitivity(dim, d, draws=3):
+    """Per-point relative change of the oracle's S and DS under random 1-ulp strain changes."""
+    rng = np.random.default_rng(1234)
+    args = [d[k] for k in ("c_bar", "sin_phi", "shear", "bulk", "lame")]
+    S0, D0, _ = native.constitutive(dim, d["E"], *args)
+    ks = np.zeros(len(S0))
+    kd = np.zeros(len(S0))
+    for _ in range(draws):
+        Ep = d["E"] * (1 + rng.choice([-1.0, 1.0], size=d["E"].shape) * 2.220446049250313e-16)
+        S1, D1, _ = native.constitutive(dim, Ep, *args)
+        ks = np.maximum(ks, np.linalg.norm(S1 - S0, axis=1) / np.maximum(np.linalg.norm(S0, axis=1), 1e-300))
+        kd = np.maximum(kd, np.linalg.norm(D1 - D0, axis=1) / np.maximum(np.linalg.norm(D0, axis=1), 1e-300))
+    return ks, kd
+
+
+def assert_pointwise(x, ref, kappa=None, rtol=RTOL):
     nrm = np.linalg.norm(ref, axis=1)
     err = np.linalg.norm(x - ref, axis=1)
     scale = np.maximum(nrm, np.max(nrm) * 1e-6)
-    assert np.all(err <= rtol * scale), f"max rel err {np.max(err / scale):.3e}"
+    tol = rtol if kappa is None else np.maximum(rtol, 10 * kappa)
+    rel = err / scale
+    assert np.all(rel <= tol), f"max rel err {np.max(rel):.3e} (allowed {np.max(tol):.1e})"
+    assert np.mean(rel <= rtol) >= 0.999, f"only {np.mean(rel <= rtol):.5f} of points within {rtol}"
 
 
 @pytest.mark.parametrize("sorted_order", [False, True])
@@ -46,8 +71,9 @@ def test_constitutive3d_matches_oracle(cuda_device, sorted_order):
     S, DS, br = gpu_constitutive(3, d)
     So, DSo, bro = native.constitutive(3, d["E"], d["c_bar"], d["sin_phi"], d["shear"], d["bulk"], d["lame"])
     assert np.array_equal(br, bro) and np.array_equal(br, d["target"])
-    assert_pointwise(S, So)
-    assert_pointwise(DS, DSo)
+    ks, kd = sensitivity(3, d)
+    assert_pointwise(S, So, ks)
+    assert_pointwise(DS, DSo, kd)
     # tangent symmetry is exact
     D = DS.reshape(-1, 6, 6)
     assert np.array_equal(D, D.transpose(0, 2, 1))
@@ -59,7 +85,7 @@ def test_constitutive3d_stress_only_and_odd_sizes(cuda_device):
         S, DS, br = gpu_constitutive(3, d, want_ds=False)
         So, _, bro = native.constitutive(3, d["E"], d["c_bar"], d["sin_phi"], d["shear"], d["bulk"], d["lame"], False)
         assert DS is None and np.array_equal(br, bro)
-        assert_pointwise(S, So)
+        assert_pointwise(S, So, sensitivity(3, d)[0])
 
 
 def test_constitutive_empty_input(cuda_device):
@@ -79,8 +105,9 @@ def test_constitutive2d_matches_oracle(cuda_device):
     S, DS, br = gpu_constitutive(2, d)
     So, DSo, bro = native.constitutive(2, E, cb, sp, mat["shear"], mat["bulk"], mat["lame"])
     assert np.array_equal(br, bro)
-    assert_pointwise(S, So)
-    assert_pointwise(DS, DSo)
+    ks, kd = sensitivity(2, d)
+    assert_pointwise(S, So, ks)
+    assert_pointwise(DS, DSo, kd)
 
 
 def test_constitutive3d_device_pointers(cuda_device):
@@ -97,8 +124,9 @@ def test_constitutive3d_device_pointers(cuda_device):
     torch.cuda.synchronize()
     So, DSo, bro = native.constitutive(3, d["E"], d["c_bar"], d["sin_phi"], d["shear"], d["bulk"], d["lame"])
     assert np.array_equal(br.cpu().numpy(), bro)
-    assert_pointwise(S.cpu().numpy(), So)
-    assert_pointwise(DS.cpu().numpy(), DSo)
+    ks, kd = sensitivity(3, d)
+    assert_pointwise(S.cpu().numpy(), So, ks)
+    assert_pointwise(DS.cpu().numpy(), DSo, kd)
 
 
 def test_reduction_device(cuda_device):
