@@ -151,6 +151,46 @@ int sg_masked_diff_norm2_dev(int64_t n, const double *a, const double *b, const 
 /* y = a x + b y */
 int sg_axpby_dev(int64_t n, double a, const double *x, double b, double *y, void *stream);
 
+/* ------------------------------------------------------------------------------
+ * (d1, d2) AMG preconditioner.  Takes the role of the BoomerAMG instance of
+ * +LINEAR_SOLVERS/mex/hypre_boomeramg_mex.cpp (commands setup_ijv :1013-1146,
+ * update_values :1151-1213, apply :751-796, clear): one V-cycle per apply, numeric
+ * set-up redone on every value update.  Smoothed aggregation on the node blocks with a
+ * near-null space (near_null_space_elasticity_3D.m: 6 rigid-body modes in 3D), Chebyshev
+ * smoothing, FP64 or FP32 cycle.
+ *   nullspace  (n_rows*b) x nns column-major host array; fixed: per-DOF 1 = Dirichlet (host)
+ *   opts       [max_levels, coarse_size, cheb_degree, cheb_ratio, power_its, mixed(0/1),
+ *               omega_scale]; entries <= 0 keep the defaults (10, 1200, 2, 30, 10, 0, 4/3)
+ * ---------------------------------------------------------------------------- */
+typedef struct sg_amg sg_amg;
+int sg_amg_create(const sg_bsr *A, const double *nullspace, int32_t nns, const uint8_t *fixed,
+                  const double *opts, int32_t n_opts, sg_amg **out);
+int sg_amg_destroy(sg_amg *amg);
+/* numeric set-up from device values of A (kept by reference until the next update) */
+int sg_amg_update(sg_amg *amg, const double *A_vals, void *stream);
+/* z = V-cycle(r), device vectors of n_rows*b entries */
+int sg_amg_apply(sg_amg *amg, const double *r, double *z, void *stream);
+/* info[0] levels, info[1] coarsest dense size, then (block size, block rows, blocks) per level */
+int sg_amg_info(const sg_amg *amg, int64_t *info, int32_t cap);
+/* host copies of level l's A pattern/values and P pattern/values (any pointer may be NULL) */
+int sg_amg_export(const sg_amg *amg, int32_t level, int32_t *A_rp, int32_t *A_col, double *A_vals,
+                  int32_t *P_rp, int32_t *P_col, double *P_vals);
+
+/* ------------------------------------------------------------------------------
+ * (c1, c3) Deflated FGMRES and A-orthogonalisation.
+ *   sg_dfgmres_solve     +LINEAR_SOLVERS/dfgmres_solver.m:1-181 (DFGMRES.solve, DFGMRES.m:134-147)
+ *   sg_a_orthogonalize   +LINEAR_SOLVERS/A_orthogonalize.m:1-58 (DFGMRES.A_orthogonalize)
+ * Device vectors of n entries; the deflation basis W is n x k column-major (device).
+ * ---------------------------------------------------------------------------- */
+typedef struct sg_krylov sg_krylov;
+int sg_krylov_create(int64_t n, int32_t maxit, sg_krylov **out);
+int sg_krylov_destroy(sg_krylov *ws);
+int sg_dfgmres_solve(sg_krylov *ws, const sg_bsr *A, const double *A_vals, sg_amg *M, const double *W,
+                     int32_t k, const double *b, double *x, double tol, int32_t maxit, int32_t *iters,
+                     double *relres, double *res_hist, void *stream);
+int sg_a_orthogonalize(sg_krylov *ws, const sg_bsr *A, const double *A_vals, double *W, int32_t k,
+                       double eps_add, int32_t *k_out, void *stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -50,6 +50,18 @@ SIGNATURES = {
     "sg_dot_dev": [i64, vp, vp, vp, vp],
     "sg_masked_diff_norm2_dev": [i64, vp, vp, vp, vp, vp],
     "sg_axpby_dev": [i64, f64, vp, f64, vp, vp],
+    # AMG
+    "sg_amg_create": [vp, vp, i32, vp, vp, i32, vp],
+    "sg_amg_destroy": [vp],
+    "sg_amg_update": [vp, vp, vp],
+    "sg_amg_apply": [vp, vp, vp, vp],
+    "sg_amg_info": [vp, vp, i32],
+    "sg_amg_export": [vp, i32, vp, vp, vp, vp, vp, vp],
+    # Krylov
+    "sg_krylov_create": [i64, i32, vp],
+    "sg_krylov_destroy": [vp],
+    "sg_dfgmres_solve": [vp, vp, vp, vp, vp, i32, vp, vp, f64, i32, vp, vp, vp, vp],
+    "sg_a_orthogonalize": [vp, vp, vp, vp, i32, f64, vp, vp],
 }
 _RESTYPES = {"sg_last_error": C.c_char_p}
 

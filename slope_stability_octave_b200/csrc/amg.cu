@@ -756,6 +756,8 @@ static int build_hierarchy(sg_amg *h, const sg_bsr *A0, const double *nullspace,
         if (!last) na = aggregate(n, rp, col, active, L.agg);
         if (last || na == 0 || na * nns >= ndof * 3 / 4) {
             std::vector<int32_t>().swap(L.agg);
+            if (ndof > 12000)
+                return set_error(SG_ERR_NUMERIC, "AMG coarsening stalled: coarsest level too large for a dense inverse");
             h->nc_dense = ndof;
             rc = dalloc(&h->Ainv, (size_t)ndof * ndof);
             if (!rc) rc = dalloc(&h->colk, ndof);

@@ -1,0 +1,209 @@
+"""Device mirror of the reference's LINEAR_SOLVERS package (DFGMRES with an AMG V-cycle).
+
+  near_null_space_elasticity   +LINEAR_SOLVERS/near_null_space_elasticity_3D.m:1-108
+                               (rigid-body modes on centred coordinates; 3 modes in 2D)
+  AMG                          the BoomerAMG instance of hypre_boomeramg_mex.cpp
+                               (setup_ijv / update_values / apply / clear), here a
+                               smoothed-aggregation hierarchy built once per pattern
+  DFGMRES                      +LINEAR_SOLVERS/DFGMRES.m:1-223 (deflation basis,
+                               preconditioner hooks, copy semantics)
+  set_linear_solver            +LINEAR_SOLVERS/set_linear_solver.m:1-71 (solver tokens)
+
+Vectors are flat device tensors over all dim*n_n DOFs; Dirichlet DOFs carry zeros (the
+block matrix has identity rows there), which leaves every inner product identical to the
+reference's K(Q,Q) formulation.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import time
+
+import numpy as np
+import torch
+
+from . import _lib
+from .device import DeviceMesh, F64, cur_stream, hptr, ptr
+
+
+def near_null_space_elasticity(coord, Q=None, center=True):
+    """Rigid-body modes (n_dof x nns, node-major rows), zero on Dirichlet DOFs when Q is given."""
+    coord = np.asarray(coord, np.float64)
+    dim, n_n = coord.shape
+    X = coord - coord.mean(axis=1, keepdims=True) if center else coord
+    if dim == 3:
+        x, y, z = X
+        modes = np.zeros((6, n_n, 3))
+        modes[0, :, 0] = 1
+        modes[1, :, 1] = 1
+        modes[2, :, 2] = 1
+        modes[3, :, 1], modes[3, :, 2] = -z, y
+        modes[4, :, 0], modes[4, :, 2] = z, -x
+        modes[5, :, 0], modes[5, :, 1] = -y, x
+    else:
+        x, y = X
+        modes = np.zeros((3, n_n, 2))
+        modes[0, :, 0] = 1
+        modes[1, :, 1] = 1
+        modes[2, :, 0], modes[2, :, 1] = -y, x
+    Z = modes.reshape(modes.shape[0], -1).T.copy()          # (n_dof, nns), node-major rows
+    if Q is not None:
+        Z[~np.asarray(Q, bool).T.ravel()] = 0.0
+    return Z
+
+
+class AMG:
+    """Device AMG preconditioner bound to a mesh's block pattern."""
+
+    def __init__(self, dmesh: DeviceMesh, coord=None, mixed=False, max_levels=10, coarse_size=1200,
+                 cheb_degree=2, cheb_ratio=30.0, power_its=10):
+        self.dmesh = dmesh
+        coord = dmesh.mesh.coord if coord is None else coord
+        Z = near_null_space_elasticity(coord, dmesh.mesh.Q)
+        nns = Z.shape[1]
+        Zc = np.ascontiguousarray(Z.T)                      # column-major n_dof x nns
+        fixed = np.ascontiguousarray((~dmesh.mesh.Q.T.ravel()).astype(np.uint8))
+        opts = np.array([max_levels, coarse_size, cheb_degree, cheb_ratio, power_its, 1.0 if mixed else 0.0, 0.0])
+        h = C.c_void_p()
+        t0 = time.perf_counter()
+        _lib.call("sg_amg_create", dmesh.bsr, hptr(Zc), nns, hptr(fixed), hptr(opts), len(opts), C.byref(h))
+        self.setup_time = time.perf_counter() - t0
+        self.handle = h
+        self.mixed = mixed
+        self._A = None
+
+    def __del__(self):
+        h = getattr(self, "handle", None)
+        if h is not None and h.value:
+            try:
+                _lib.lib().sg_amg_destroy(h)
+            except Exception:
+                pass
+            self.handle = None
+
+    def update(self, K):
+        self._A = K     # keep the values alive: the hierarchy references them
+        _lib.call("sg_amg_update", self.handle, ptr(K), cur_stream())
+
+    def apply(self, r, z):
+        _lib.call("sg_amg_apply", self.handle, ptr(r), ptr(z), cur_stream())
+
+    def info(self):
+        buf = np.zeros(32, np.int64)
+        _lib.call("sg_amg_info", self.handle, hptr(buf), 32)
+        nl = int(buf[0])
+        levels = [dict(block=int(buf[2 + 3 * i]), rows=int(buf[3 + 3 * i]), blocks=int(buf[4 + 3 * i])) for i in range(nl)]
+        return dict(levels=levels, coarse_dense=int(buf[1]))
+
+
+class _Workspace:
+    def __init__(self, n, maxit):
+        h = C.c_void_p()
+        _lib.call("sg_krylov_create", int(n), int(maxit), C.byref(h))
+        self.handle = h
+
+    def __del__(self):
+        h = getattr(self, "handle", None)
+        if h is not None and h.value:
+            try:
+                _lib.lib().sg_krylov_destroy(h)
+            except Exception:
+                pass
+
+
+class DFGMRES:
+    """Deflated FGMRES with an AMG preconditioner (DFGMRES.m).  ``copy()`` shares the AMG
+    instance and the Krylov workspace and copies the deflation basis, like the reference
+    (copies share the closed-over HYPRE instance id, keep their own basis)."""
+
+    def __init__(self, dmesh: DeviceMesh, tolerance, max_iterations, tolerance_deflation_basis, verbose=0,
+                 amg: AMG | None = None, _ws=None):
+        self.dmesh = dmesh
+        self.tolerance = float(tolerance)
+        self.max_iterations = int(max_iterations)
+        self.tolerance_deflation_basis = float(tolerance_deflation_basis)
+        self.verbose = verbose
+        self.preconditioner = amg
+        self.n = dmesh.n_dof
+        self._ws = _ws if _ws is not None else _Workspace(self.n, self.max_iterations)
+        self.basis = torch.empty((0, self.n), dtype=F64, device=dmesh.device)   # rows = columns of W
+        self.profiler = None
+        self.last_iterations = 0
+        self.last_relres = 0.0
+
+    @property
+    def k(self):
+        return self.basis.shape[0]
+
+    def _time(self, name, t0):
+        if self.profiler is not None:
+            torch.cuda.synchronize()
+            self.profiler.add_time(name, time.perf_counter() - t0)
+
+    def setup_preconditioner(self, K):
+        t0 = time.perf_counter()
+        if self.preconditioner is not None:
+            self.preconditioner.update(K)
+        self._time("DFGMRES.update_preconditioner", t0)
+
+    # the reference's IJV hooks map onto the same update on the device pattern
+    setup_preconditioner_ijv = setup_preconditioner
+    update_preconditioner_values = setup_preconditioner
+
+    def A_orthogonalize(self, K):
+        t0 = time.perf_counter()
+        k = self.k
+        if k > 0:
+            B = self.basis.contiguous()
+            kout = C.c_int32()
+            _lib.call("sg_a_orthogonalize", self._ws.handle, self.dmesh.bsr, ptr(K), ptr(B), k,
+                      self.tolerance_deflation_basis, C.byref(kout), cur_stream())
+            self.basis = B[: kout.value]
+        self._time("DFGMRES.A_orthogonalize", t0)
+
+    def solve(self, K, b):
+        """x, nit = solve(K, b) on device vectors (dfgmres_solver.m)."""
+        t0 = time.perf_counter()
+        x = torch.empty_like(b)
+        it = C.c_int32()
+        rr = C.c_double()
+        B = self.basis
+        M = self.preconditioner.handle if self.preconditioner is not None else None
+        _lib.call("sg_dfgmres_solve", self._ws.handle, self.dmesh.bsr, ptr(K), M, ptr(B) if self.k else None,
+                  self.k, ptr(b), ptr(x), self.tolerance, self.max_iterations, C.byref(it), C.byref(rr), None,
+                  cur_stream())
+        self.last_iterations = it.value
+        self.last_relres = rr.value
+        self._time("DFGMRES.solve", t0)
+        return x, it.value
+
+    def expand_deflation_basis(self, v):
+        t0 = time.perf_counter()
+        v = v.reshape(1, -1).to(F64)
+        self.basis = torch.cat([self.basis, v], 0)
+        self._time("DFGMRES.expand_deflation_basis", t0)
+
+    def copy(self):
+        new = DFGMRES(self.dmesh, self.tolerance, self.max_iterations, self.tolerance_deflation_basis, self.verbose,
+                      amg=self.preconditioner, _ws=self._ws)
+        new.basis = self.basis.clone()
+        new.profiler = self.profiler
+        return new
+
+
+def set_linear_solver(solver_type, linear_solver_tolerance, linear_solver_maxit, deflation_basis_tolerance,
+                      linear_solver_printing, dmesh: DeviceMesh, coord=None, amg_opts=None):
+    """Solver factory (set_linear_solver.m).  Tokens: 'DFGMRES_B200' (FP64 AMG V-cycle),
+    'DFGMRES_B200_MIXED' (FP32 V-cycle inside the FP64 FGMRES), 'DFGMRES_NONE' (no
+    preconditioner)."""
+    tok = str(solver_type).upper()
+    opts = dict(amg_opts or {})
+    if tok in ("DFGMRES_B200", "DFGMRES_HYPRE_BOOMERAMG", "DFGMRES_BOOMERAMG", "BOOMERAMG", "HYPRE_BOOMERAMG"):
+        amg = AMG(dmesh, coord, mixed=False, **opts)
+    elif tok == "DFGMRES_B200_MIXED":
+        amg = AMG(dmesh, coord, mixed=True, **opts)
+    elif tok == "DFGMRES_NONE":
+        amg = None
+    else:
+        raise ValueError(f"Bad choice of solver type: {solver_type}")
+    return DFGMRES(dmesh, linear_solver_tolerance, linear_solver_maxit, deflation_basis_tolerance,
+                   linear_solver_printing, amg=amg)

@@ -1,0 +1,113 @@
+"""Problem set-up for the benchmark configurations (host inputs + device objects).
+
+Config 0   2D homogeneous slope, P2 triangles, h = 0.5 (slope_stability_2D_homo_SSR.m:30-48)
+Config 2   3D homogeneous slope, P2 tets: the 2D profile extruded 40 m, mesh_P2_3D(N_h = 1,
+           15, 10, 15, 10, 10, 40) (slope_stability_3D_homo_SSR.m parameters)
+Config 3   3D slope with horizontal material layers (heterogeneous), see ``layered_material_ids``
+
+Material rows are (c0 [kPa], phi [deg], psi [deg], E [kPa], nu, gamma_sat, gamma_unsat).
+"""
+from __future__ import annotations
+
+from dataclasses import dataclass
+
+import numpy as np
+import torch
+
+from . import fem
+from .constitutive import CONSTITUTIVE
+from .device import DeviceMesh, F64
+from .linear_solvers import set_linear_solver
+
+HOMO = [6.0, 45.0, 0.0, 40000.0, 0.3, 20.0, 20.0]
+
+# continuation parameters of the reference drivers
+SSR_3D = dict(lambda_init=0.9, d_lambda_init=0.1, d_lambda_min=1e-3, d_lambda_diff_scaled_min=1e-3,
+              step_max=100, omega_max_stop=3000.0, it_newt_max=100, it_damp_max=10, tol=1e-4, r_min=1e-4)
+SSR_2D = dict(lambda_init=0.9, d_lambda_init=0.05, d_lambda_min=1e-5, d_lambda_diff_scaled_min=1e-3,
+              step_max=100, omega_max_stop=5e3, it_newt_max=30, it_damp_max=10, tol=1e-4, r_min=1e-4)
+
+
+@dataclass
+class Problem:
+    mesh: fem.Mesh
+    dphi: tuple
+    weight: np.ndarray
+    hat: np.ndarray
+    n_q: int
+    mat: dict
+    f: np.ndarray           # (dim, n_n)
+    Davis_type: str = "B"
+    dmesh: DeviceMesh = None
+    cons: CONSTITUTIVE = None
+
+    @property
+    def dim(self):
+        return self.mesh.dim
+
+    def to_device(self):
+        self.dmesh = DeviceMesh(self.mesh, self.dphi, self.weight, self.n_q)
+        m = self.mat
+        self.cons = CONSTITUTIVE(self.dmesh, m["c0"], m["phi"], m["psi"], self.Davis_type, m["shear"], m["bulk"],
+                                 m["lame"])
+        return self
+
+    def f_device(self):
+        return torch.from_numpy(np.ascontiguousarray(self.f.T).ravel()).to(self.dmesh.device)
+
+    def solver(self, solver_type="DFGMRES_B200", tol=1e-1, maxit=100, defl_tol=1e-3, amg_opts=None):
+        return set_linear_solver(solver_type, tol, maxit, defl_tol, 0, self.dmesh, self.mesh.coord, amg_opts)
+
+
+def _assemble_problem(mesh, mat_ids, table, davis="B"):
+    if mesh.dim == 3:
+        xi, wf = fem.quadrature_p2_tet()
+        hat, d1, d2, d3 = fem.local_basis_p2_tet(xi)
+        D1, D2, D3, W = fem.geometry_3d(mesh, d1, d2, d3, wf)
+        dphi = (D1, D2, D3)
+    else:
+        xi, wf = fem.quadrature_p2_tri()
+        hat, d1, d2 = fem.local_basis_p2_tri(xi)
+        D1, D2, W = fem.geometry_2d(mesh, d1, d2, wf)
+        dphi = (D1, D2)
+    n_q = wf.size
+    mat = fem.materials(mat_ids, n_q, table)
+    f = fem.gravity_load(mesh, hat, W, mat["gamma"])
+    return Problem(mesh, dphi, W, hat, n_q, mat, f, davis)
+
+
+def slope_2d(h=0.5, mat=HOMO):
+    x1, x3, y1, y2 = 15.0, 15.0, 10.0, 10.0
+    x2 = y2 / np.tan(45 * np.pi / 180)
+    mesh = fem.mesh_p2_2d(h, x1, x2, x3, y1, y2)
+    return _assemble_problem(mesh, np.zeros(mesh.n_e, int), mat)
+
+
+def slope_3d(N_h=1, dims=(15, 10, 15, 10, 10, 40), mat=HOMO):
+    mesh = fem.mesh_p2_3d(N_h, *dims)
+    return _assemble_problem(mesh, np.zeros(mesh.n_e, int), mat)
+
+
+# four horizontal layers, thicknesses 5/5/10/20 m measured from the crest (y = 20 m)
+# downward and clipped at the base (y = 0): the body is 20 m high, so the two lower layers
+# of the listed four fall below the base and only the first three (plus the clipped 10 m one)
+# carry material.  Rows: (c0, phi, psi, E, nu, gamma, gamma).
+LAYERS_CFG3 = [[15.0, 30.0, 0.0, 50000.0, 0.30, 19.0, 19.0],
+               [10.0, 35.0, 0.0, 40000.0, 0.30, 20.0, 20.0],
+               [18.0, 25.0, 0.0, 60000.0, 0.30, 21.0, 21.0],
+               [6.0, 45.0, 0.0, 40000.0, 0.30, 20.0, 20.0]]
+LAYER_THICKNESS_CFG3 = (5.0, 5.0, 10.0, 20.0)
+
+
+def layered_material_ids(mesh, top=20.0, thickness=LAYER_THICKNESS_CFG3):
+    """Layer index of every element by the depth of its centroid below ``top``."""
+    yc = mesh.coord[1, mesh.elem[:4]].mean(axis=0)
+    depth = top - yc
+    bounds = np.cumsum(thickness)
+    return np.minimum(np.searchsorted(bounds, depth, side="right"), len(thickness) - 1)
+
+
+def slope_3d_layered(N_h=1, dims=(15, 10, 15, 10, 10, 40)):
+    mesh = fem.mesh_p2_3d(N_h, *dims)
+    ids = layered_material_ids(mesh, top=dims[3] + dims[4])
+    return _assemble_problem(mesh, ids, LAYERS_CFG3)
