@@ -158,13 +158,16 @@ int sg_axpby_dev(int64_t n, double a, const double *x, double b, double *y, void
  * set-up redone on every value update.  Smoothed aggregation on the node blocks with a
  * near-null space (near_null_space_elasticity_3D.m: 6 rigid-body modes in 3D), Chebyshev
  * smoothing, FP64 or FP32 cycle.
+ *   A_vals     device values of A used for the strength graph of every level (NULL: whole
+ *              block graph); the numeric set-up runs during creation when given
  *   nullspace  (n_rows*b) x nns column-major host array; fixed: per-DOF 1 = Dirichlet (host)
  *   opts       [max_levels, coarse_size, cheb_degree, cheb_ratio, power_its, mixed(0/1),
- *               omega_scale]; entries <= 0 keep the defaults (10, 1200, 2, 30, 10, 0, 4/3)
+ *               omega_scale, theta]; entries <= 0 keep the defaults (10, 1200, 2, 30, 10, 0,
+ *               4/3, 0.05) except theta, where 0 selects the whole block graph
  * ---------------------------------------------------------------------------- */
 typedef struct sg_amg sg_amg;
-int sg_amg_create(const sg_bsr *A, const double *nullspace, int32_t nns, const uint8_t *fixed,
-                  const double *opts, int32_t n_opts, sg_amg **out);
+int sg_amg_create(const sg_bsr *A, const double *A_vals, const double *nullspace, int32_t nns,
+                  const uint8_t *fixed, const double *opts, int32_t n_opts, sg_amg **out, void *stream);
 int sg_amg_destroy(sg_amg *amg);
 /* numeric set-up from device values of A (kept by reference until the next update) */
 int sg_amg_update(sg_amg *amg, const double *A_vals, void *stream);
@@ -190,6 +193,16 @@ int sg_dfgmres_solve(sg_krylov *ws, const sg_bsr *A, const double *A_vals, sg_am
                      double *relres, double *res_hist, void *stream);
 int sg_a_orthogonalize(sg_krylov *ws, const sg_bsr *A, const double *A_vals, double *W, int32_t k,
                        double eps_add, int32_t *k_out, void *stream);
+
+/* ------------------------------------------------------------------------------
+ * Live kernel timing (no reference counterpart: profiling support in the spirit of the
+ * reference's PROFILING.Profiler).  When enabled, every `sample`-th launch of the fine-level
+ * SpMV, the return mapping and the assembly is bracketed by CUDA events on its stream.
+ * Kinds: 0 SpMV FP64, 1 SpMV FP32, 2 return mapping + tangent, 3 return mapping (stress),
+ * 4 assembly.  sg_instr_read synchronises the device and resets the counters.
+ * ---------------------------------------------------------------------------- */
+int sg_instr_enable(int on, int sample);
+int sg_instr_read(double *ms, int64_t *timed, int64_t *launches, int32_t cap);
 
 #ifdef __cplusplus
 }

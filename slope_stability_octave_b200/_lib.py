@@ -51,7 +51,7 @@ SIGNATURES = {
     "sg_masked_diff_norm2_dev": [i64, vp, vp, vp, vp, vp],
     "sg_axpby_dev": [i64, f64, vp, f64, vp, vp],
     # AMG
-    "sg_amg_create": [vp, vp, i32, vp, vp, i32, vp],
+    "sg_amg_create": [vp, vp, vp, i32, vp, vp, i32, vp, vp],
     "sg_amg_destroy": [vp],
     "sg_amg_update": [vp, vp, vp],
     "sg_amg_apply": [vp, vp, vp, vp],
@@ -62,6 +62,9 @@ SIGNATURES = {
     "sg_krylov_destroy": [vp],
     "sg_dfgmres_solve": [vp, vp, vp, vp, vp, i32, vp, vp, f64, i32, vp, vp, vp, vp],
     "sg_a_orthogonalize": [vp, vp, vp, vp, i32, f64, vp, vp],
+    # live kernel timing
+    "sg_instr_enable": [cint, cint],
+    "sg_instr_read": [vp, vp, vp, i32],
 }
 _RESTYPES = {"sg_last_error": C.c_char_p}
 

@@ -84,6 +84,7 @@ struct AmgOptions {
     int power_its = 10;
     int mixed = 0;            // 1: FP32 V-cycle
     double omega_scale = 4.0 / 3.0;
+    double theta = 0.05;      // strength threshold (0: whole block graph)
 };
 
 }  // namespace sg
@@ -702,92 +703,9 @@ static int setup_transfer(Level &L, const std::vector<int32_t> &rp, const std::v
     return rc;
 }
 
-static int build_hierarchy(sg_amg *h, const sg_bsr *A0, const double *nullspace, int nns, const uint8_t *fixed) {
-    const AmgOptions &o = h->opt;
-    h->L.reserve(o.max_levels + 1);
-    std::vector<int32_t> rp = A0->row_ptr, col = A0->col;
-    int b = A0->b;
-    int64_t n = A0->n_rows;
-    std::vector<double> B((size_t)n * b * nns);
-    std::vector<uint8_t> active(n, 0), dead;
-    for (int64_t i = 0; i < n; ++i)
-        for (int a = 0; a < b; ++a) {
-            const int64_t row = i * b + a;
-            const bool fx = fixed && fixed[row];
-            for (int c = 0; c < nns; ++c) B[(size_t)row * nns + c] = fx ? 0.0 : nullspace[(size_t)c * n * b + row];
-            if (!fx) active[i] = 1;
-        }
-    for (int lev = 0;; ++lev) {
-        h->L.emplace_back();
-        Level &L = h->L.back();
-        L.b = b;
-        L.n = n;
-        int rc = SG_OK;
-        if (lev == 0) {
-            L.Aext = A0;
-            L.d_Arp = A0->d_row_ptr;
-            L.d_Acol = A0->d_col;
-            L.d_Adiag = A0->d_diag;
-            L.Anblk = A0->n_blocks;
-        } else {
-            L.Aown.nrows = n;
-            L.Aown.ncols = n;
-            L.Aown.rp = rp;
-            L.Aown.col = col;
-            L.Aown.nblk = rp[n];
-            rc = upload_pattern(L.Aown);
-            std::vector<int32_t> diag(n, -1);
-            for (int64_t i = 0; i < n; ++i)
-                for (int32_t p = rp[i]; p < rp[i + 1]; ++p)
-                    if (col[p] == i) diag[i] = p;
-            if (!rc) rc = dup(&L.d_diag_own, diag);
-            if (!rc) rc = dalloc(&L.Aown_vals, (size_t)L.Aown.nblk * b * b);
-            if (!rc) rc = dup(&L.d_dead, dead);
-            L.d_Arp = L.Aown.d_rp;
-            L.d_Acol = L.Aown.d_col;
-            L.d_Adiag = L.d_diag_own;
-            L.Anblk = L.Aown.nblk;
-        }
-        if (!rc) rc = alloc_level_buffers(L, o.mixed);
-        if (rc) return rc;
-        const int64_t ndof = n * b;
-        int64_t na = 0;
-        const bool last = (ndof <= o.coarse_size) || (lev + 1 >= o.max_levels);
-        if (!last) na = aggregate(n, rp, col, active, L.agg);
-        if (last || na == 0 || na * nns >= ndof * 3 / 4) {
-            std::vector<int32_t>().swap(L.agg);
-            if (ndof > 12000)
-                return set_error(SG_ERR_NUMERIC, "AMG coarsening stalled: coarsest level too large for a dense inverse");
-            h->nc_dense = ndof;
-            rc = dalloc(&h->Ainv, (size_t)ndof * ndof);
-            if (!rc) rc = dalloc(&h->colk, ndof);
-            if (!rc) rc = dalloc(&h->rowk, ndof);
-            if (!rc && o.mixed) rc = dalloc(&h->Ainv32, (size_t)ndof * ndof);
-            return rc;
-        }
-        Pattern Ac;
-        std::vector<double> Bc;
-        std::vector<uint8_t> dead_c;
-        rc = setup_transfer(L, rp, col, B, nns, na, Ac, Bc, dead_c, o.mixed);
-        if (rc) return rc;
-        rp = std::move(Ac.rp);
-        col = std::move(Ac.col);
-        b = nns;
-        n = na;
-        B = std::move(Bc);
-        dead = std::move(dead_c);
-        active.assign(n, 0);
-        for (int64_t i = 0; i < n; ++i)
-            for (int c = 0; c < b; ++c) active[i] |= !dead[(size_t)i * b + c];
-    }
-}
-
 // ------------------------------------------------------------------ numeric set-up
 
-static int level_values(Level &L, const double **vals) {
-    *vals = L.Aext ? L.Avals : L.Aown_vals;
-    return SG_OK;
-}
+static const double *level_values(const Level &L) { return L.Aext ? L.Avals : L.Aown_vals; }
 
 static int power_lmax(sg_amg *h, Level &L, const double *A, cudaStream_t st) {
     const int64_t nd = L.n * L.b;
@@ -805,54 +723,210 @@ static int power_lmax(sg_amg *h, Level &L, const double *A, cudaStream_t st) {
     return rc;
 }
 
-static int numeric_update(sg_amg *h, cudaStream_t st) {
-    const int nl = (int)h->L.size();
-    for (int l = 0; l < nl; ++l) {
-        Level &L = h->L[l];
-        const double *A;
-        level_values(L, &A);
-        SG_B_DISPATCH(L.b, (k_block_diag_inv<BB><<<grid_for(L.n, 128), 128, 0, st>>>(L.n, L.d_Adiag, A, L.Dinv, L.Dinv32)));
-        SG_CUDA(cudaGetLastError());
-        if (h->opt.mixed) {
-            const int64_t nv = L.Anblk * L.b * L.b;
-            k_to_float<<<grid_for(nv, 256), 256, 0, st>>>(nv, A, L.A32);
-        }
-        if (l == nl - 1) {
-            // coarsest: dense Gauss-Jordan inverse
-            const int64_t N = h->nc_dense;
-            SG_CUDA(cudaMemsetAsync(h->Ainv, 0, sizeof(double) * N * N, st));
-            SG_B_DISPATCH(L.b, (k_bsr_to_dense<BB><<<grid_for(L.n, 128), 128, 0, st>>>(L.n, L.d_Arp, L.d_Acol, A, N, h->Ainv)));
-            for (int64_t k = 0; k < N; ++k) {
-                k_gj_save<<<grid_for(N, 256), 256, 0, st>>>(N, k, h->Ainv, h->colk, h->rowk);
-                k_gj_update<<<grid_for(N * N, 256, 16), 256, 0, st>>>(N, k, h->Ainv, h->colk, h->rowk);
-            }
-            if (h->opt.mixed) k_to_float<<<grid_for(N * N, 256), 256, 0, st>>>(N * N, h->Ainv, h->Ainv32);
-            SG_CUDA(cudaGetLastError());
-            break;
-        }
-        int rc = power_lmax(h, L, A, st);
-        if (rc) return rc;
-        Level &C = h->L[l + 1];
-        SG_BBC_DISPATCH(L.b, L.bc, ({
-            k_smooth_prolongator<BB, BC><<<grid_for(L.n, 128), 128, 0, st>>>(
-                L.n, L.P.d_rp, L.P.d_col, L.at_plan.d_ptr, L.at_plan.d_a, L.d_Acol, A, L.T, L.d_agg, L.Dinv, L.lmax,
-                h->opt.omega_scale, L.Pv);
-            k_transpose_blocks<BB, BC><<<grid_for(L.P.nblk * BB * BC, 256), 256, 0, st>>>(L.P.nblk, L.d_R_from_P, L.Pv, L.Rv);
-            k_gather_AP<BB, BC><<<grid_for(L.AP.nblk, 128), 128, 0, st>>>(L.AP.nblk, L.ap_plan.d_ptr, L.ap_plan.d_a,
-                                                                          L.ap_plan.d_b, A, L.Pv, L.APv);
-            k_gather_Ac<BB, BC><<<grid_for(C.n, 64), 64, 0, st>>>(C.n, C.d_Arp, C.d_Acol, L.ac_plan.d_ptr,
-                                                                  L.ac_plan.d_a, L.ac_plan.d_b, L.Pv, L.APv, C.d_dead,
-                                                                  C.Aown_vals);
-        }));
-        SG_CUDA(cudaGetLastError());
-        if (h->opt.mixed) {
-            const int64_t np_ = L.P.nblk * L.b * L.bc;
-            k_to_float<<<grid_for(np_, 256), 256, 0, st>>>(np_, L.Pv, L.P32);
-            k_to_float<<<grid_for(np_, 256), 256, 0, st>>>(np_, L.Rv, L.R32);
-        }
+// Block-Jacobi inverse of level l (and the FP32 copy of its matrix).
+static int numeric_smoother(sg_amg *h, int l, cudaStream_t st) {
+    Level &L = h->L[l];
+    const double *A = level_values(L);
+    SG_B_DISPATCH(L.b, (k_block_diag_inv<BB><<<grid_for(L.n, 128), 128, 0, st>>>(L.n, L.d_Adiag, A, L.Dinv, L.Dinv32)));
+    SG_CUDA(cudaGetLastError());
+    if (h->opt.mixed) {
+        const int64_t nv = L.Anblk * L.b * L.b;
+        k_to_float<<<grid_for(nv, 256), 256, 0, st>>>(nv, A, L.A32);
     }
+    return SG_OK;
+}
+
+// lambda_max, prolongator, restriction and the next level's Galerkin matrix.
+static int numeric_transfer(sg_amg *h, int l, cudaStream_t st) {
+    Level &L = h->L[l];
+    Level &C = h->L[l + 1];
+    const double *A = level_values(L);
+    int rc = power_lmax(h, L, A, st);
+    if (rc) return rc;
+    SG_BBC_DISPATCH(L.b, L.bc, ({
+        k_smooth_prolongator<BB, BC><<<grid_for(L.n, 128), 128, 0, st>>>(
+            L.n, L.P.d_rp, L.P.d_col, L.at_plan.d_ptr, L.at_plan.d_a, L.d_Acol, A, L.T, L.d_agg, L.Dinv, L.lmax,
+            h->opt.omega_scale, L.Pv);
+        k_transpose_blocks<BB, BC><<<grid_for(L.P.nblk * BB * BC, 256), 256, 0, st>>>(L.P.nblk, L.d_R_from_P, L.Pv, L.Rv);
+        k_gather_AP<BB, BC><<<grid_for(L.AP.nblk, 128), 128, 0, st>>>(L.AP.nblk, L.ap_plan.d_ptr, L.ap_plan.d_a,
+                                                                      L.ap_plan.d_b, A, L.Pv, L.APv);
+        k_gather_Ac<BB, BC><<<grid_for(C.n, 64), 64, 0, st>>>(C.n, C.d_Arp, C.d_Acol, L.ac_plan.d_ptr, L.ac_plan.d_a,
+                                                              L.ac_plan.d_b, L.Pv, L.APv, C.d_dead, C.Aown_vals);
+    }));
+    SG_CUDA(cudaGetLastError());
+    if (h->opt.mixed) {
+        const int64_t np_ = L.P.nblk * L.b * L.bc;
+        k_to_float<<<grid_for(np_, 256), 256, 0, st>>>(np_, L.Pv, L.P32);
+        k_to_float<<<grid_for(np_, 256), 256, 0, st>>>(np_, L.Rv, L.R32);
+    }
+    return SG_OK;
+}
+
+static int numeric_coarsest(sg_amg *h, cudaStream_t st) {
+    Level &L = h->L.back();
+    const double *A = level_values(L);
+    const int64_t N = h->nc_dense;
+    SG_CUDA(cudaMemsetAsync(h->Ainv, 0, sizeof(double) * N * N, st));
+    SG_B_DISPATCH(L.b, (k_bsr_to_dense<BB><<<grid_for(L.n, 128), 128, 0, st>>>(L.n, L.d_Arp, L.d_Acol, A, N, h->Ainv)));
+    for (int64_t k = 0; k < N; ++k) {
+        k_gj_save<<<grid_for(N, 256), 256, 0, st>>>(N, k, h->Ainv, h->colk, h->rowk);
+        k_gj_update<<<grid_for(N * N, 256, 16), 256, 0, st>>>(N, k, h->Ainv, h->colk, h->rowk);
+    }
+    if (h->opt.mixed) k_to_float<<<grid_for(N * N, 256), 256, 0, st>>>(N * N, h->Ainv, h->Ainv32);
     SG_CUDA(cudaGetLastError());
     return SG_OK;
+}
+
+static int numeric_update(sg_amg *h, cudaStream_t st) {
+    const int nl = (int)h->L.size();
+    int rc = SG_OK;
+    for (int l = 0; l < nl && !rc; ++l) {
+        rc = numeric_smoother(h, l, st);
+        if (rc) break;
+        rc = (l == nl - 1) ? numeric_coarsest(h, st) : numeric_transfer(h, l, st);
+    }
+    return rc;
+}
+
+// ------------------------------------------------------------------ hierarchy structure
+
+// Strength graph: keep block (i, j) when ||A_ij||_F >= theta sqrt(||A_ii||_F ||A_jj||_F), and i == j.
+static void strength_graph(int64_t n, int b, const std::vector<int32_t> &rp, const std::vector<int32_t> &col,
+                           const std::vector<double> &vals, double theta, std::vector<int32_t> &srp,
+                           std::vector<int32_t> &scol) {
+    const int64_t nb = rp[n];
+    std::vector<double> nrm(nb), dg(n, 0.0);
+#pragma omp parallel for schedule(static)
+    for (int64_t p = 0; p < nb; ++p) {
+        double s = 0.0;
+        for (int t = 0; t < b * b; ++t) s += vals[(size_t)p * b * b + t] * vals[(size_t)p * b * b + t];
+        nrm[p] = std::sqrt(s);
+    }
+    for (int64_t i = 0; i < n; ++i)
+        for (int32_t p = rp[i]; p < rp[i + 1]; ++p)
+            if (col[p] == i) dg[i] = nrm[p];
+    srp.assign(n + 1, 0);
+    scol.clear();
+    scol.reserve(nb);
+    for (int64_t i = 0; i < n; ++i) {
+        for (int32_t p = rp[i]; p < rp[i + 1]; ++p) {
+            const int32_t j = col[p];
+            if (j == i || nrm[p] >= theta * std::sqrt(dg[i] * dg[j])) scol.push_back(j);
+        }
+        srp[i + 1] = (int32_t)scol.size();
+    }
+}
+
+static int make_level(sg_amg *h, const sg_bsr *A0, const std::vector<int32_t> &rp, const std::vector<int32_t> &col,
+                      int b, int64_t n, const std::vector<uint8_t> &dead) {
+    h->L.emplace_back();
+    Level &L = h->L.back();
+    L.b = b;
+    L.n = n;
+    int rc = SG_OK;
+    if (A0) {
+        L.Aext = A0;
+        L.d_Arp = A0->d_row_ptr;
+        L.d_Acol = A0->d_col;
+        L.d_Adiag = A0->d_diag;
+        L.Anblk = A0->n_blocks;
+    } else {
+        L.Aown.nrows = n;
+        L.Aown.ncols = n;
+        L.Aown.rp = rp;
+        L.Aown.col = col;
+        L.Aown.nblk = rp[n];
+        rc = upload_pattern(L.Aown);
+        std::vector<int32_t> diag(n, -1);
+        for (int64_t i = 0; i < n; ++i)
+            for (int32_t p = rp[i]; p < rp[i + 1]; ++p)
+                if (col[p] == i) diag[i] = p;
+        if (!rc) rc = dup(&L.d_diag_own, diag);
+        if (!rc) rc = dalloc(&L.Aown_vals, (size_t)L.Aown.nblk * b * b);
+        if (!rc) rc = dup(&L.d_dead, dead);
+        L.d_Arp = L.Aown.d_rp;
+        L.d_Acol = L.Aown.d_col;
+        L.d_Adiag = L.d_diag_own;
+        L.Anblk = L.Aown.nblk;
+    }
+    if (!rc) rc = alloc_level_buffers(L, h->opt.mixed);
+    return rc;
+}
+
+// Builds the hierarchy structure.  With A0vals (device values of the fine matrix) and
+// theta > 0, every level's aggregation runs on its strength graph; the numeric set-up of a
+// level is then done as soon as its transfer exists, so the next level's values are known.
+static int build_hierarchy(sg_amg *h, const sg_bsr *A0, const double *A0vals, const double *nullspace, int nns,
+                           const uint8_t *fixed, cudaStream_t st) {
+    const AmgOptions &o = h->opt;
+    h->L.reserve(o.max_levels + 2);
+    std::vector<int32_t> rp = A0->row_ptr, col = A0->col;
+    int b = A0->b;
+    int64_t n = A0->n_rows;
+    std::vector<double> B((size_t)n * b * nns);
+    std::vector<uint8_t> active(n, 0), dead;
+    for (int64_t i = 0; i < n; ++i)
+        for (int a = 0; a < b; ++a) {
+            const int64_t row = i * b + a;
+            const bool fx = fixed && fixed[row];
+            for (int c = 0; c < nns; ++c) B[(size_t)row * nns + c] = fx ? 0.0 : nullspace[(size_t)c * n * b + row];
+            if (!fx) active[i] = 1;
+        }
+    const bool with_values = A0vals != nullptr && o.theta > 0.0;
+    int rc = make_level(h, A0, rp, col, b, n, dead);
+    if (rc) return rc;
+    if (A0vals) h->L[0].Avals = A0vals;
+    for (int lev = 0;; ++lev) {
+        Level &L = h->L[lev];
+        const int64_t ndof = n * b;
+        const bool last = (ndof <= o.coarse_size) || (lev + 1 >= o.max_levels);
+        int64_t na = 0;
+        if (!last) {
+            if (with_values) {
+                std::vector<double> vals((size_t)rp[n] * b * b);
+                SG_CUDA(cudaMemcpyAsync(vals.data(), level_values(L), sizeof(double) * vals.size(),
+                                        cudaMemcpyDeviceToHost, st));
+                SG_CUDA(cudaStreamSynchronize(st));
+                std::vector<int32_t> srp, scol;
+                strength_graph(n, b, rp, col, vals, o.theta, srp, scol);
+                na = aggregate(n, srp, scol, active, L.agg);
+            } else {
+                na = aggregate(n, rp, col, active, L.agg);
+            }
+        }
+        if (last || na == 0 || na * nns >= ndof * 3 / 4) {
+            std::vector<int32_t>().swap(L.agg);
+            if (ndof > 12000)
+                return set_error(SG_ERR_NUMERIC, "AMG coarsening stalled: coarsest level too large for a dense inverse");
+            h->nc_dense = ndof;
+            rc = dalloc(&h->Ainv, (size_t)ndof * ndof);
+            if (!rc) rc = dalloc(&h->colk, ndof);
+            if (!rc) rc = dalloc(&h->rowk, ndof);
+            if (!rc && o.mixed) rc = dalloc(&h->Ainv32, (size_t)ndof * ndof);
+            return rc;
+        }
+        Pattern Ac;
+        std::vector<double> Bc;
+        std::vector<uint8_t> dead_c;
+        rc = setup_transfer(L, rp, col, B, nns, na, Ac, Bc, dead_c, o.mixed);
+        if (rc) return rc;
+        rc = make_level(h, nullptr, Ac.rp, Ac.col, nns, na, dead_c);
+        if (rc) return rc;
+        if (with_values) {
+            rc = numeric_smoother(h, lev, st);
+            if (!rc) rc = numeric_transfer(h, lev, st);
+            if (rc) return rc;
+        }
+        rp = std::move(Ac.rp);
+        col = std::move(Ac.col);
+        b = nns;
+        n = na;
+        B = std::move(Bc);
+        dead = std::move(dead_c);
+        active.assign(n, 0);
+        for (int64_t i = 0; i < n; ++i)
+            for (int c = 0; c < b; ++c) active[i] |= !dead[(size_t)i * b + c];
+    }
 }
 
 // ------------------------------------------------------------------ V-cycle
@@ -917,8 +991,9 @@ static int vcycle(sg_amg *h, int l, cudaStream_t st) {
 
 using namespace sg;
 
-extern "C" int sg_amg_create(const sg_bsr *A, const double *nullspace, int32_t nns, const uint8_t *fixed,
-                             const double *opts, int32_t n_opts, sg_amg **out) {
+extern "C" int sg_amg_create(const sg_bsr *A, const double *A_vals, const double *nullspace, int32_t nns,
+                             const uint8_t *fixed, const double *opts, int32_t n_opts, sg_amg **out,
+                             void *stream) {
     SG_CHECK_ARG(out, "null output handle");
     *out = nullptr;
     SG_CHECK_ARG(A && nullspace, "null pattern or near-null space");
@@ -937,9 +1012,10 @@ extern "C" int sg_amg_create(const sg_bsr *A, const double *nullspace, int32_t n
         if (n_opts > 4 && opts[4] > 0) h->opt.power_its = (int)opts[4];
         if (n_opts > 5) h->opt.mixed = opts[5] != 0.0;
         if (n_opts > 6 && opts[6] > 0) h->opt.omega_scale = opts[6];
+        if (n_opts > 7 && opts[7] >= 0) h->opt.theta = opts[7];
     }
     int rc = dalloc(&h->dots, DOT_BLOCKS + 64);
-    if (!rc) rc = build_hierarchy(h, A, nullspace, nns, fixed);
+    if (!rc) rc = build_hierarchy(h, A, A_vals, nullspace, nns, fixed, as_stream(stream));
     if (rc) {
         for (auto &L : h->L) free_level(L);
         cudaFree(h->Ainv); cudaFree(h->Ainv32); cudaFree(h->colk); cudaFree(h->rowk); cudaFree(h->dots);

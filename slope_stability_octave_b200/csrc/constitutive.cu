@@ -8,6 +8,7 @@
 
 #include <algorithm>
 
+#include "instr.cuh"
 #include "mc_point.cuh"
 #include "sg_common.cuh"
 
@@ -131,6 +132,7 @@ int launch_constitutive(int dim, bool fused, const double *E, const double *m0, 
                         int64_t n, double *S, double *DS, uint8_t *branch, cudaStream_t st) {
     if (n <= 0) return SG_OK;
     const unsigned grid = grid_for(n, MC_BLOCK, 16);
+    const InstrToken tk = instr_begin(DS ? IK_CONST_SDS : IK_CONST_S, st);
     if (dim == 3) {
         const size_t sm = sizeof(double) * MC_WARPS * 32 * (DS3_PITCH + S3_PITCH);
         if (DS) {
@@ -150,6 +152,7 @@ int launch_constitutive(int dim, bool fused, const double *E, const double *m0, 
             else k_mc2d<false, false><<<grid, MC_BLOCK, sm, st>>>(E, m0, m1, psi, shear, lame, lambda, davis, n, S, DS, branch);
         }
     }
+    instr_end(tk, st);
     SG_CUDA(cudaGetLastError());
     return SG_OK;
 }

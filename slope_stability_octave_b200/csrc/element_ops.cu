@@ -14,6 +14,7 @@
 
 #include <vector>
 
+#include "instr.cuh"
 #include "mesh.h"
 #include "sg_common.cuh"
 
@@ -257,6 +258,12 @@ extern "C" int sg_assemble_bsr_dev(const sg_mesh *m, const double *DS, double *K
     const cudaStream_t st = as_stream(stream);
     SG_CUDA(cudaMemsetAsync(K, 0, sizeof(double) * m->bsr.n_blocks * m->dim * m->dim, st));
     const int64_t work = m->n_e * m->dim * m->np;
+    const InstrToken tk = instr_begin(IK_ASSEMBLY, st);
+    struct End {
+        const InstrToken &t;
+        cudaStream_t s;
+        ~End() { instr_end(t, s); }
+    } end_guard{tk, st};
     if (m->dim == 3 && m->np == 10)
         k_assemble_bsr<3, 10><<<grid_for(work, 128, 16), 128, 0, st>>>(m->d_pair_blk, m->d_dphi, m->d_w, m->nq, m->n_e, DS, K);
     else if (m->dim == 2 && m->np == 6)

@@ -1,0 +1,26 @@
+// Sampled CUDA-event timing of selected kernel kinds (see instr.cu).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace sg {
+
+enum InstrKind {
+    IK_SPMV3_F64 = 0,    // node-block (3x3 or 2x2) SpMV, FP64 values
+    IK_SPMV3_F32 = 1,    // the same, FP32 values (mixed-precision V-cycle)
+    IK_CONST_SDS = 2,    // return mapping with tangent
+    IK_CONST_S = 3,      // return mapping, stress only
+    IK_ASSEMBLY = 4,     // tangent assembly into the block pattern
+    IK_COUNT = 8
+};
+
+struct InstrToken {
+    int kind = -1;
+    cudaEvent_t a = nullptr, b = nullptr;
+};
+
+InstrToken instr_begin(int kind, cudaStream_t st);
+void instr_end(const InstrToken &t, cudaStream_t st);
+
+}  // namespace sg

@@ -9,6 +9,7 @@
 
 #include <algorithm>
 
+#include "instr.cuh"
 #include "linalg.cuh"
 #include "sg_common.cuh"
 
@@ -67,8 +68,13 @@ static void spmv_launch(int64_t nrows, const int32_t *rp, const int32_t *col, co
                         double alpha, double beta, const XT *bvec, int mode, cudaStream_t st) {
     constexpr int G = (BR * BC >= 9) ? 8 : 4;
     const int64_t threads = nrows * G;
+    // the node-block shapes of the fine level are the ones timed for the roofline report
+    constexpr bool fine = (BR == BC) && (BR == 3 || BR == 2);
+    InstrToken tk;
+    if (fine) tk = instr_begin(sizeof(VT) == 8 ? IK_SPMV3_F64 : IK_SPMV3_F32, st);
     k_bsr_spmv<BR, BC, G, VT, XT><<<grid_for(threads, 256, 16), 256, 0, st>>>(nrows, rp, col, vals, x, y, alpha, beta,
                                                                                bvec, mode);
+    if (fine) instr_end(tk, st);
 }
 
 template <typename VT, typename XT>

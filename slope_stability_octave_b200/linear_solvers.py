@@ -52,24 +52,34 @@ def near_null_space_elasticity(coord, Q=None, center=True):
 
 
 class AMG:
-    """Device AMG preconditioner bound to a mesh's block pattern."""
+    """Device AMG preconditioner bound to a mesh's block pattern.
+
+    The hierarchy's structure (aggregates on each level's strength graph) is built at the
+    first value update, from those values, and reused for later updates, which redo only the
+    numeric set-up on the device (the pattern is fixed per mesh)."""
 
     def __init__(self, dmesh: DeviceMesh, coord=None, mixed=False, max_levels=10, coarse_size=1200,
-                 cheb_degree=2, cheb_ratio=30.0, power_its=10):
+                 cheb_degree=2, cheb_ratio=30.0, power_its=10, theta=0.05):
         self.dmesh = dmesh
         coord = dmesh.mesh.coord if coord is None else coord
         Z = near_null_space_elasticity(coord, dmesh.mesh.Q)
-        nns = Z.shape[1]
-        Zc = np.ascontiguousarray(Z.T)                      # column-major n_dof x nns
-        fixed = np.ascontiguousarray((~dmesh.mesh.Q.T.ravel()).astype(np.uint8))
-        opts = np.array([max_levels, coarse_size, cheb_degree, cheb_ratio, power_its, 1.0 if mixed else 0.0, 0.0])
-        h = C.c_void_p()
-        t0 = time.perf_counter()
-        _lib.call("sg_amg_create", dmesh.bsr, hptr(Zc), nns, hptr(fixed), hptr(opts), len(opts), C.byref(h))
-        self.setup_time = time.perf_counter() - t0
-        self.handle = h
+        self._nns = Z.shape[1]
+        self._Z = np.ascontiguousarray(Z.T)                  # column-major n_dof x nns
+        self._fixed = np.ascontiguousarray((~dmesh.mesh.Q.T.ravel()).astype(np.uint8))
+        self._opts = np.array([max_levels, coarse_size, cheb_degree, cheb_ratio, power_its, 1.0 if mixed else 0.0,
+                               0.0, theta], dtype=np.float64)
+        self.handle = None
+        self.setup_time = 0.0
         self.mixed = mixed
         self._A = None
+
+    def _create(self, K):
+        h = C.c_void_p()
+        t0 = time.perf_counter()
+        _lib.call("sg_amg_create", self.dmesh.bsr, ptr(K), hptr(self._Z), self._nns, hptr(self._fixed),
+                  hptr(self._opts), len(self._opts), C.byref(h), cur_stream())
+        self.setup_time = time.perf_counter() - t0
+        self.handle = h
 
     def __del__(self):
         h = getattr(self, "handle", None)
@@ -82,6 +92,8 @@ class AMG:
 
     def update(self, K):
         self._A = K     # keep the values alive: the hierarchy references them
+        if self.handle is None:
+            self._create(K)
         _lib.call("sg_amg_update", self.handle, ptr(K), cur_stream())
 
     def apply(self, r, z):
