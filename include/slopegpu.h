@@ -188,11 +188,15 @@ int sg_amg_export(const sg_amg *amg, int32_t level, int32_t *A_rp, int32_t *A_co
 typedef struct sg_krylov sg_krylov;
 int sg_krylov_create(int64_t n, int32_t maxit, sg_krylov **out);
 int sg_krylov_destroy(sg_krylov *ws);
+/* AW = A W (optional, may be NULL): as produced by sg_a_orthogonalize; when given, the
+ * projection w - W (W' (A w)) is evaluated as w - W ((A W)' w) (A symmetric), saving one
+ * SpMV per iteration. */
 int sg_dfgmres_solve(sg_krylov *ws, const sg_bsr *A, const double *A_vals, sg_amg *M, const double *W,
-                     int32_t k, const double *b, double *x, double tol, int32_t maxit, int32_t *iters,
-                     double *relres, double *res_hist, void *stream);
-int sg_a_orthogonalize(sg_krylov *ws, const sg_bsr *A, const double *A_vals, double *W, int32_t k,
-                       double eps_add, int32_t *k_out, void *stream);
+                     const double *AW, int32_t k, const double *b, double *x, double tol, int32_t maxit,
+                     int32_t *iters, double *relres, double *res_hist, void *stream);
+/* AW (optional, may be NULL): receives A times the kept columns of W, in W's output order. */
+int sg_a_orthogonalize(sg_krylov *ws, const sg_bsr *A, const double *A_vals, double *W, double *AW,
+                       int32_t k, double eps_add, int32_t *k_out, void *stream);
 
 /* ------------------------------------------------------------------------------
  * Live kernel timing (no reference counterpart: profiling support in the spirit of the
@@ -203,6 +207,8 @@ int sg_a_orthogonalize(sg_krylov *ws, const sg_bsr *A, const double *A_vals, dou
  * ---------------------------------------------------------------------------- */
 int sg_instr_enable(int on, int sample);
 int sg_instr_read(double *ms, int64_t *timed, int64_t *launches, int32_t cap);
+/* number of kernels the library launched since the last reset (reset != 0 clears it) */
+int64_t sg_launch_count(int reset);
 
 #ifdef __cplusplus
 }

@@ -126,6 +126,31 @@ def tentative(agg, na, B, b, k):
     return T, Bc, dead
 
 
+def _filtered(A, b, rp, col):
+    """A with the blocks outside the strength graph (rp, col) removed and their row sums
+    added to the diagonal block's diagonal (so A_F keeps A's action on constants)."""
+    Ab = sp.bsr_matrix(A, blocksize=(b, b))
+    Ab.sort_indices()
+    n = Ab.shape[0] // b
+    data = Ab.data.copy()
+    for i in range(n):
+        keep = set(col[rp[i]:rp[i + 1]].tolist())
+        dpos = None
+        lump = np.zeros(b)
+        for p in range(Ab.indptr[i], Ab.indptr[i + 1]):
+            j = Ab.indices[p]
+            if j == i:
+                dpos = p
+            elif j not in keep:
+                lump += data[p].sum(axis=1)
+                data[p] = 0.0
+        if dpos is not None:
+            data[dpos] += np.diag(lump)
+    F = sp.bsr_matrix((data, Ab.indices, Ab.indptr), shape=Ab.shape).tocsr()
+    F.eliminate_zeros()
+    return F
+
+
 def _block_dinv(A, b):
     n = A.shape[0] // b
     D = np.zeros((n, b, b))
@@ -150,7 +175,7 @@ def _init_vec(n):
 
 class Hierarchy:
     def __init__(self, A, B, b, fixed=None, coarse_size=1200, max_levels=10, cheb_degree=2, cheb_ratio=30.0,
-                 power_its=10, omega_scale=4.0 / 3.0, theta=0.0, theta_coarse=None):
+                 power_its=10, omega_scale=4.0 / 3.0, theta=0.0, theta_coarse=None, filtered_smoothing=False):
         self.deg, self.ratio = cheb_degree, cheb_ratio
         A = sp.csr_matrix(A)
         n = A.shape[0] // b
@@ -189,7 +214,10 @@ class Hierarchy:
                 v = w / lmax
             lev["lmax"] = lmax
             Ts = T
-            AT = A @ Ts
+            As = A
+            if filtered_smoothing and th > 0:
+                As = _filtered(A, b, rp, col)
+            AT = As @ Ts
             P = Ts - (oscale := omega_scale / lmax) * self._dinv_mat(lev, AT)
             lev["P"] = sp.csr_matrix(P)
             Ac = (P.T @ A @ P).tocsr()

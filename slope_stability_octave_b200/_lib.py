@@ -60,13 +60,14 @@ SIGNATURES = {
     # Krylov
     "sg_krylov_create": [i64, i32, vp],
     "sg_krylov_destroy": [vp],
-    "sg_dfgmres_solve": [vp, vp, vp, vp, vp, i32, vp, vp, f64, i32, vp, vp, vp, vp],
-    "sg_a_orthogonalize": [vp, vp, vp, vp, i32, f64, vp, vp],
+    "sg_dfgmres_solve": [vp, vp, vp, vp, vp, vp, i32, vp, vp, f64, i32, vp, vp, vp, vp],
+    "sg_a_orthogonalize": [vp, vp, vp, vp, vp, i32, f64, vp, vp],
     # live kernel timing
     "sg_instr_enable": [cint, cint],
     "sg_instr_read": [vp, vp, vp, i32],
+    "sg_launch_count": [cint],
 }
-_RESTYPES = {"sg_last_error": C.c_char_p}
+_RESTYPES = {"sg_last_error": C.c_char_p, "sg_launch_count": C.c_int64}
 
 
 class SlopeGPUError(RuntimeError):

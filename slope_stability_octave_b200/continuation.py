@@ -3,12 +3,14 @@
   init_phase_SSR_indirect_continuation   +CONTINUATION/init_phase_SSR_indirect_continuation.m:1-143
   SSR_indirect_continuation              +CONTINUATION/SSR_indirect_continuation.m:1-237
 
+``SSRIndirectStepper`` is the same loop split into ``init()`` and ``step()`` (one accepted
+continuation step per call, including its rejected attempts), so that a caller can time,
+checkpoint or drive individual steps; ``SSR_indirect_continuation`` runs it to the end.
 The per-step statistics follow SSR_indirect_continuation.m:53-72,134-195: one accepted step
 is the sum of its attempts' wall times (``step_wall_time``), which is the benchmark metric.
 """
 from __future__ import annotations
 
-import math
 import time
 
 import numpy as np
@@ -61,111 +63,150 @@ def init_phase_SSR_indirect_continuation(lambda_init, d_lambda_init, d_lambda_mi
     return U1, U2, omega1, omega2, lambda1, lambda2, its
 
 
+class SSRIndirectStepper:
+    """SSR_indirect_continuation.m split into init() and step().  Parameters as the reference
+    function (``p`` holds lambda_init, d_lambda_init, d_lambda_min, d_lambda_diff_scaled_min,
+    step_max, omega_max_stop, it_newt_max, it_damp_max, tol, r_min)."""
+
+    def __init__(self, p, Q, f, cons, solver, K_elast=None, verbose=False):
+        self.p, self.Q, self.f, self.cons, self.solver = dict(p), Q, f, cons, solver
+        self.K_elast = K_elast
+        self.verbose = verbose
+        self.fQ = f * Q
+        self.stats = dict(init_newton_iterations=[], attempt_step=[], attempt_success=[], attempt_wall_time=[],
+                          attempt_newton_iterations=[], attempt_newton_flag=[], attempt_newton_relres_end=[],
+                          attempt_omega_target=[], attempt_lambda_before=[], attempt_lambda_after=[],
+                          attempt_linear_iterations=[], step_index=[], step_attempt_count=[], step_wall_time=[],
+                          step_newton_iterations=[], step_newton_iterations_total=[], step_newton_relres_end=[],
+                          step_lambda=[], step_omega=[], step_linear_iterations=[])
+        self.finished = False
+        self.stop_reason = ""
+
+    def _umax(self, V):
+        return float(torch.sqrt((V.reshape(-1, self.cons.dim) ** 2).sum(1)).max())
+
+    def init(self):
+        p = self.p
+        t0 = time.perf_counter()
+        (self.U_old, self.U, self.omega_old, self.omega, lambda_old, self.lam, its) = \
+            init_phase_SSR_indirect_continuation(p["lambda_init"], p["d_lambda_init"], p["d_lambda_min"],
+                                                 p["it_newt_max"], p["it_damp_max"], p["tol"], p["r_min"],
+                                                 self.K_elast, self.Q, self.f, self.cons, self.solver.copy(),
+                                                 self.verbose)
+        self.stats["init_wall_time"] = time.perf_counter() - t0
+        self.stats["init_newton_iterations"] = its
+        self.solver.expand_deflation_basis(self.U_old)
+        self.lambda_hist = [lambda_old, self.lam]
+        self.omega_hist = [self.omega_old, self.omega]
+        self.Umax_hist = [self._umax(self.U_old), self._umax(self.U)]
+        self.d_omega = self.omega - self.omega_old
+        if p["omega_max_stop"] < self.omega + self.d_omega:
+            raise ContinuationError("Too small value of omega_max_stop.")
+        self.step_no = 2
+        self.n_omega = 0
+        return self
+
+    def step(self):
+        """Attempts until one is accepted (or the run stops).  Returns the accepted step's
+        statistics, or None if the continuation stopped without accepting a step."""
+        p, st = self.p, self.stats
+        wall_acc, it_acc, cnt_acc, lin_acc = 0.0, 0, 0, 0
+        while not self.finished:
+            omega_it = min(self.omega + self.d_omega, p["omega_max_stop"])
+            self.d_omega = omega_it - self.omega
+            U_ini = self.d_omega * (self.U - self.U_old) / (self.omega - self.omega_old) + self.U
+            torch.cuda.synchronize()
+            t_att = time.perf_counter()
+            U_it, lambda_it, flag, it_newt, hist = newton_ind_SSR(
+                U_ini, omega_it, self.lam, p["it_newt_max"], p["it_damp_max"], p["tol"], p["r_min"], self.K_elast,
+                self.Q, self.f, self.cons, self.solver.copy(), self.verbose)
+            torch.cuda.synchronize()
+            att_wall = time.perf_counter() - t_att
+            relres = hist["residual"][-1] if hist["residual"] else float("nan")
+            lin_total = hist["linear_iters_W_total"] + hist["linear_iters_V_total"]
+            st["attempt_step"].append(self.step_no + 1)
+            st["attempt_success"].append(flag == 0)
+            st["attempt_wall_time"].append(att_wall)
+            st["attempt_newton_iterations"].append(it_newt)
+            st["attempt_newton_flag"].append(flag)
+            st["attempt_newton_relres_end"].append(relres)
+            st["attempt_omega_target"].append(omega_it)
+            st["attempt_lambda_before"].append(self.lam)
+            st["attempt_lambda_after"].append(lambda_it if flag == 0 else float("nan"))
+            st["attempt_linear_iterations"].append(lin_total)
+            wall_acc += att_wall
+            it_acc += it_newt
+            cnt_acc += 1
+            lin_acc += lin_total
+            if self.verbose:
+                print(f"Step {self.step_no + 1}: omega={omega_it:.6g} flag={flag} lambda={lambda_it:.8f} "
+                      f"newton_it={it_newt} lin_it={lin_total} wall={att_wall:.3f}s")
+            accepted = None
+            if flag == 1:
+                self.d_omega = self.d_omega / 2
+                self.n_omega += 1
+            else:
+                self.step_no += 1
+                step = self.step_no
+                self.U_old, self.U = self.U, U_it
+                self.solver.expand_deflation_basis(self.U)
+                self.omega_old, self.omega = self.omega, omega_it
+                d_lambda = lambda_it - self.lam
+                self.lam = lambda_it
+                self.n_omega = 0
+                self.omega_hist.append(self.omega)
+                self.lambda_hist.append(self.lam)
+                self.Umax_hist.append(self._umax(self.U))
+                accepted = dict(step=step, wall=wall_acc, attempts=cnt_acc, newton_iterations=it_newt,
+                                newton_iterations_total=it_acc, linear_iterations=lin_acc, relres=relres,
+                                lam=self.lam, omega=self.omega)
+                st["step_index"].append(step)
+                st["step_attempt_count"].append(cnt_acc)
+                st["step_wall_time"].append(wall_acc)
+                st["step_newton_iterations"].append(it_newt)
+                st["step_newton_iterations_total"].append(it_acc)
+                st["step_newton_relres_end"].append(relres)
+                st["step_lambda"].append(self.lam)
+                st["step_omega"].append(self.omega)
+                st["step_linear_iterations"].append(lin_acc)
+                lh, oh = self.lambda_hist, self.omega_hist
+                if (d_lambda / self.d_omega) * (oh[step - 1] - oh[0]) < p["d_lambda_diff_scaled_min"]:
+                    self.finished, self.stop_reason = True, "minimal increase of lambda"
+                elif self.omega >= p["omega_max_stop"]:
+                    self.finished, self.stop_reason = True, "maximal omega"
+                elif (lh[step - 1] - lh[step - 2]) < 0.9 * (lh[step - 2] - lh[step - 3]):
+                    self.d_omega = 2 * self.d_omega
+            if self.n_omega >= 5:
+                self.finished, self.stop_reason = True, "impossible to increase omega"
+            elif self.step_no >= p["step_max"]:
+                self.finished, self.stop_reason = True, "maximal number of steps"
+            if accepted is not None:
+                return accepted
+        return None
+
+
 def SSR_indirect_continuation(lambda_init, d_lambda_init, d_lambda_min, d_lambda_diff_scaled_min, step_max,
                               omega_max_stop, it_newt_max, it_damp_max, tol, r_min, K_elast, Q, f, cons, solver,
                               verbose=False, max_steps_after_init=None, on_step=None):
     """Returns (U, lambda_hist, omega_hist, Umax_hist, stats).  ``max_steps_after_init``
     optionally stops after that many accepted continuation steps (bounded benchmarks)."""
     t_total = time.perf_counter()
-    fQ = f * Q
-    stats = dict(init_newton_iterations=[], attempt_step=[], attempt_success=[], attempt_wall_time=[],
-                 attempt_newton_iterations=[], attempt_newton_flag=[], attempt_newton_relres_end=[],
-                 attempt_omega_target=[], attempt_lambda_before=[], attempt_lambda_after=[],
-                 attempt_linear_iterations=[], step_index=[], step_attempt_count=[], step_wall_time=[],
-                 step_newton_iterations=[], step_newton_iterations_total=[], step_newton_relres_end=[],
-                 step_lambda=[], step_omega=[], step_linear_iterations=[])
-    t_init = time.perf_counter()
-    U_old, U, omega_old, omega, lambda_old, lam, its = init_phase_SSR_indirect_continuation(
-        lambda_init, d_lambda_init, d_lambda_min, it_newt_max, it_damp_max, tol, r_min, K_elast, Q, f, cons,
-        solver.copy(), verbose)
-    stats["init_wall_time"] = time.perf_counter() - t_init
-    stats["init_newton_iterations"] = its
-    solver.expand_deflation_basis(U_old)
-    lambda_hist = [lambda_old, lam]
-    omega_hist = [omega_old, omega]
-    umax = lambda V: float(torch.sqrt((V.reshape(-1, cons.dim) ** 2).sum(1)).max())
-    Umax_hist = [umax(U_old), umax(U)]
-    d_omega = omega - omega_old
-    if omega_max_stop < omega + d_omega:
-        raise ContinuationError("Too small value of omega_max_stop.")
-    step = 2
-    n_omega, n_omega_max = 0, 5
-    wall_acc, it_acc, cnt_acc, lin_acc = 0.0, 0, 0, 0
-    n_accepted = 0
-    stop_reason = ""
-    while True:
-        omega_it = min(omega + d_omega, omega_max_stop)
-        d_omega = omega_it - omega
-        U_ini = d_omega * (U - U_old) / (omega - omega_old) + U
-        torch.cuda.synchronize()
-        t_att = time.perf_counter()
-        U_it, lambda_it, flag, it_newt, hist = newton_ind_SSR(U_ini, omega_it, lam, it_newt_max, it_damp_max, tol,
-                                                              r_min, K_elast, Q, f, cons, solver.copy(), verbose)
-        torch.cuda.synchronize()
-        att_wall = time.perf_counter() - t_att
-        relres = hist["residual"][-1] if hist["residual"] else float("nan")
-        lin_total = hist["linear_iters_W_total"] + hist["linear_iters_V_total"]
-        stats["attempt_step"].append(step + 1)
-        stats["attempt_success"].append(flag == 0)
-        stats["attempt_wall_time"].append(att_wall)
-        stats["attempt_newton_iterations"].append(it_newt)
-        stats["attempt_newton_flag"].append(flag)
-        stats["attempt_newton_relres_end"].append(relres)
-        stats["attempt_omega_target"].append(omega_it)
-        stats["attempt_lambda_before"].append(lam)
-        stats["attempt_lambda_after"].append(lambda_it if flag == 0 else float("nan"))
-        stats["attempt_linear_iterations"].append(lin_total)
-        wall_acc += att_wall
-        it_acc += it_newt
-        cnt_acc += 1
-        lin_acc += lin_total
-        if verbose:
-            print(f"Step {step + 1}: omega={omega_it:.6g} flag={flag} lambda={lambda_it:.8f} newton_it={it_newt} "
-                  f"lin_it={lin_total} wall={att_wall:.3f}s")
-        if flag == 1:
-            d_omega = d_omega / 2
-            n_omega += 1
-        else:
-            step += 1
-            U_old, U = U, U_it
-            solver.expand_deflation_basis(U)
-            omega_old, omega = omega, omega_it
-            d_lambda = lambda_it - lam
-            lam = lambda_it
-            n_omega = 0
-            omega_hist.append(omega)
-            lambda_hist.append(lam)
-            Umax_hist.append(umax(U))
-            stats["step_index"].append(step)
-            stats["step_attempt_count"].append(cnt_acc)
-            stats["step_wall_time"].append(wall_acc)
-            stats["step_newton_iterations"].append(it_newt)
-            stats["step_newton_iterations_total"].append(it_acc)
-            stats["step_newton_relres_end"].append(relres)
-            stats["step_lambda"].append(lam)
-            stats["step_omega"].append(omega)
-            stats["step_linear_iterations"].append(lin_acc)
-            wall_acc, it_acc, cnt_acc, lin_acc = 0.0, 0, 0, 0
-            n_accepted += 1
-            if on_step is not None:
-                on_step(step, lam, omega)
-            if (d_lambda / d_omega) * (omega_hist[step - 1] - omega_hist[0]) < d_lambda_diff_scaled_min:
-                stop_reason = "minimal increase of lambda"
-                break
-            if omega >= omega_max_stop:
-                stop_reason = "maximal omega"
-                break
-            if (lambda_hist[step - 1] - lambda_hist[step - 2]) < 0.9 * (lambda_hist[step - 2] - lambda_hist[step - 3]):
-                d_omega = 2 * d_omega
-            if max_steps_after_init is not None and n_accepted >= max_steps_after_init:
-                stop_reason = "step budget"
-                break
-        if n_omega >= n_omega_max:
-            stop_reason = "impossible to increase omega"
+    p = dict(lambda_init=lambda_init, d_lambda_init=d_lambda_init, d_lambda_min=d_lambda_min,
+             d_lambda_diff_scaled_min=d_lambda_diff_scaled_min, step_max=step_max, omega_max_stop=omega_max_stop,
+             it_newt_max=it_newt_max, it_damp_max=it_damp_max, tol=tol, r_min=r_min)
+    run = SSRIndirectStepper(p, Q, f, cons, solver, K_elast, verbose).init()
+    n = 0
+    while not run.finished:
+        acc = run.step()
+        if acc is None:
             break
-        if step >= step_max:
-            stop_reason = "maximal number of steps"
+        n += 1
+        if on_step is not None:
+            on_step(acc["step"], acc["lam"], acc["omega"])
+        if max_steps_after_init is not None and n >= max_steps_after_init:
+            run.stop_reason = "step budget"
             break
-    stats["stop_reason"] = stop_reason
-    stats["total_wall_time"] = time.perf_counter() - t_total
-    return U, np.array(lambda_hist), np.array(omega_hist), np.array(Umax_hist), stats
+    st = run.stats
+    st["stop_reason"] = run.stop_reason
+    st["total_wall_time"] = time.perf_counter() - t_total
+    return run.U, np.array(run.lambda_hist), np.array(run.omega_hist), np.array(run.Umax_hist), st

@@ -37,7 +37,7 @@ namespace sg {
 struct Pattern {  // CSR of blocks (rectangular)
     int64_t nrows = 0, ncols = 0, nblk = 0;
     std::vector<int32_t> rp, col;
-    int32_t *d_rp = nullptr, *d_col = nullptr;
+    int32_t *d_rp = nullptr, *d_col = nullptr, *d_row = nullptr;  // d_row: block row of every block
 };
 
 struct Plan {  // for every output block: a list of (first, second) input block indices
@@ -95,7 +95,8 @@ struct sg_amg {
     int64_t nc_dense = 0;      // coarsest dense size (DOFs)
     double *Ainv = nullptr;    // dense inverse, nc_dense^2
     float *Ainv32 = nullptr;
-    double *colk = nullptr, *rowk = nullptr;
+    double *colk = nullptr, *rowk = nullptr;   // Gauss-Jordan column block (N x NB) and row block (NB x N)
+    double *gj_pinv = nullptr;                 // inverse of the current pivot block (NB x NB)
     double *dots = nullptr;    // reduction scratch
     int device = 0;
     int updated = 0;
@@ -269,8 +270,12 @@ static void build_product(int64_t nrows, Pattern &out, Plan &plan, F collect) {
 }
 
 static int upload_pattern(Pattern &p) {
+    std::vector<int32_t> row(p.col.size());
+    for (int64_t i = 0; i < (int64_t)p.rp.size() - 1; ++i)
+        for (int32_t q = p.rp[i]; q < p.rp[i + 1]; ++q) row[q] = (int32_t)i;
     int rc = dup(&p.d_rp, p.rp);
     if (!rc) rc = dup(&p.d_col, p.col);
+    if (!rc) rc = dup(&p.d_row, row);
     return rc;
 }
 static int upload_plan(Plan &p) {
@@ -380,16 +385,18 @@ __global__ void k_cheb(int64_t n, int k, double ratio, const double *__restrict_
 }
 
 // P block (i,J) = [agg(i) == J] T_i - omega Dinv_i sum_{p in list} A_p T_{col(p)},  omega = s / lmax
+// One thread per P block.
 template <int B, int BC>
-__global__ void k_smooth_prolongator(int64_t n, const int32_t *__restrict__ Prp, const int32_t *__restrict__ Pcol,
+__global__ void k_smooth_prolongator(int64_t nblk, const int32_t *__restrict__ Prow, const int32_t *__restrict__ Pcol,
                                      const int64_t *__restrict__ lptr, const int32_t *__restrict__ la,
                                      const int32_t *__restrict__ Acol, const double *__restrict__ A,
                                      const double *__restrict__ T, const int32_t *__restrict__ agg,
                                      const double *__restrict__ Dinv, const double *__restrict__ lmax, double oscale,
                                      double *__restrict__ P) {
     const double omega = oscale / lmax[0];
-    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
-        for (int32_t q = Prp[i]; q < Prp[i + 1]; ++q) {
+    for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q < nblk; q += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t i = Prow[q];
+        {
             double acc[B * BC];
 #pragma unroll
             for (int t = 0; t < B * BC; ++t) acc[t] = 0.0;
@@ -460,15 +467,17 @@ __global__ void k_gather_AP(int64_t nblk, const int64_t *__restrict__ lptr, cons
     }
 }
 
-// Ac block (I,J) = sum over plan pairs P_a' (BC x B) * AP_b (B x BC); dead DOFs get identity
+// Ac block (I,J) = sum over plan pairs P_a' (BC x B) * AP_b (B x BC); dead DOFs get identity.
+// One thread per coarse block.
 template <int B, int BC>
-__global__ void k_gather_Ac(int64_t nrows, const int32_t *__restrict__ rp, const int32_t *__restrict__ col,
+__global__ void k_gather_Ac(int64_t nblk, const int32_t *__restrict__ row, const int32_t *__restrict__ col,
                             const int64_t *__restrict__ lptr, const int32_t *__restrict__ la,
                             const int32_t *__restrict__ lb, const double *__restrict__ P,
                             const double *__restrict__ AP, const uint8_t *__restrict__ dead,
                             double *__restrict__ Ac) {
-    for (int64_t I = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; I < nrows; I += (int64_t)gridDim.x * blockDim.x) {
-        for (int32_t q = rp[I]; q < rp[I + 1]; ++q) {
+    for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q < nblk; q += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t I = row[q];
+        {
             const int64_t J = col[q];
             double acc[BC * BC];
 #pragma unroll
@@ -567,6 +576,82 @@ __global__ void k_gj_update(int64_t N, int64_t k, double *__restrict__ D, const 
     }
 }
 
+// Blocked Gauss-Jordan inversion (SPD, no pivoting) with NB x NB pivot blocks:
+//   1. k_gjb_pivot : invert the pivot block in shared memory (one CTA) -> Pinv
+//   2. k_gjb_save  : keep the pivot column block C = D(:, K) and the scaled row block
+//                    Rw = Pinv D(K, :)
+//   3. k_gjb_update: D(K,K) = Pinv, D(K,j) = Rw(:,j), D(i,K) = -C(i,:) Pinv,
+//                    D(i,j) -= C(i,:) Rw(:,j)
+constexpr int GJ_NB = 32;
+
+__global__ void __launch_bounds__(GJ_NB * GJ_NB) k_gjb_pivot(int64_t N, int64_t k0, int nb, const double *__restrict__ D,
+                                                             double *__restrict__ Pinv) {
+    __shared__ double m[GJ_NB][2 * GJ_NB + 1];
+    const int r = threadIdx.x / GJ_NB, c = threadIdx.x % GJ_NB;
+    if (r < nb && c < nb) {
+        m[r][c] = D[(k0 + r) * N + k0 + c];
+        m[r][GJ_NB + c] = (r == c) ? 1.0 : 0.0;
+    }
+    __syncthreads();
+    for (int k = 0; k < nb; ++k) {
+        // every thread owns entries (r, c) and (r, c + NB); all reads happen before the barrier,
+        // all writes after it
+        double n0 = 0.0, n1 = 0.0;
+        if (r < nb) {
+            const double piv = m[k][k];
+            const double ip = piv != 0.0 ? 1.0 / piv : 0.0;
+            const double fk = m[r][k];
+            const double rk0 = m[k][c] * ip, rk1 = m[k][c + GJ_NB] * ip;
+            n0 = (r == k) ? rk0 : m[r][c] - fk * rk0;
+            n1 = (r == k) ? rk1 : m[r][c + GJ_NB] - fk * rk1;
+        }
+        __syncthreads();
+        if (r < nb) {
+            m[r][c] = n0;
+            m[r][c + GJ_NB] = n1;
+        }
+        __syncthreads();
+    }
+    if (r < nb && c < nb) Pinv[r * GJ_NB + c] = m[r][GJ_NB + c];
+}
+
+__global__ void k_gjb_save(int64_t N, int64_t k0, int nb, const double *__restrict__ D,
+                           const double *__restrict__ Pinv, double *__restrict__ C, double *__restrict__ Rw) {
+    const int64_t total = N * nb;
+    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < total; t += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t i = t / nb;
+        const int c = (int)(t - i * nb);
+        C[i * GJ_NB + c] = D[i * N + k0 + c];                // column block
+        double s = 0.0;                                      // Rw(c, j = i) = sum_m Pinv(c, m) D(k0 + m, i)
+        for (int m = 0; m < nb; ++m) s += Pinv[c * GJ_NB + m] * D[(k0 + m) * N + i];
+        Rw[c * N + i] = s;
+    }
+}
+
+__global__ void k_gjb_update(int64_t N, int64_t k0, int nb, double *__restrict__ D, const double *__restrict__ Pinv,
+                             const double *__restrict__ C, const double *__restrict__ Rw) {
+    const int64_t total = N * N;
+    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < total; t += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t i = t / N, j = t - i * N;
+        const bool ik = (i >= k0 && i < k0 + nb), jk = (j >= k0 && j < k0 + nb);
+        double v;
+        if (ik && jk) {
+            v = Pinv[(i - k0) * GJ_NB + (j - k0)];
+        } else if (ik) {
+            v = Rw[(i - k0) * N + j];
+        } else if (jk) {
+            double s = 0.0;
+            for (int m = 0; m < nb; ++m) s += C[i * GJ_NB + m] * Pinv[m * GJ_NB + (j - k0)];
+            v = -s;
+        } else {
+            double s = 0.0;
+            for (int m = 0; m < nb; ++m) s += C[i * GJ_NB + m] * Rw[m * N + j];
+            v = D[t] - s;
+        }
+        D[t] = v;
+    }
+}
+
 template <typename T>
 __global__ void k_dense_gemv(int64_t N, const T *__restrict__ M, const T *__restrict__ x, T *__restrict__ y) {
     // one warp per row
@@ -604,6 +689,7 @@ static int free_level(Level &l) {
     F(l.Aown.d_rp); F(l.Aown.d_col); F(l.d_diag_own); F(l.Aown_vals); F(l.A32); F(l.Dinv); F(l.Dinv32);
     F(l.lmax); F(l.d_dead); F(l.d_agg); F(l.T); F(l.P.d_rp); F(l.P.d_col); F(l.R.d_rp); F(l.R.d_col);
     F(l.AP.d_rp); F(l.AP.d_col); F(l.d_R_from_P);
+    F(l.Aown.d_row); F(l.P.d_row); F(l.R.d_row); F(l.AP.d_row);
     for (Plan *p : {&l.at_plan, &l.ap_plan, &l.ac_plan}) { F(p->d_ptr); F(p->d_a); F(p->d_b); }
     F(l.Pv); F(l.Rv); F(l.APv); F(l.P32); F(l.R32);
     F(l.x); F(l.rhs); F(l.r); F(l.d); F(l.t); F(l.x32); F(l.rhs32); F(l.r32); F(l.d32);
@@ -712,7 +798,7 @@ static int power_lmax(sg_amg *h, Level &L, const double *A, cudaStream_t st) {
     k_init_vec<<<grid_for(nd, 256), 256, 0, st>>>(nd, L.d);
     int rc = SG_OK;
     for (int it = 0; it < h->opt.power_its && !rc; ++it) {
-        rc = rect_spmv<double, double>(L.b, L.b, L.n, L.d_Arp, L.d_Acol, A, L.d, L.t, 1.0, 0.0, nullptr, 0, st);
+        rc = rect_spmv<double, double>(L.b, L.b, L.n, L.d_Arp, L.d_Acol, A, L.d, L.t, 1.0, 0.0, nullptr, 0, st, L.Anblk);
         if (rc) break;
         SG_B_DISPATCH(L.b, (k_dinv_apply<BB, double><<<grid_for(L.n, 256), 256, 0, st>>>(L.n, L.Dinv, L.t, L.r)));
         rc = multidot(nd, 1, L.r, nd, L.r, h->dots, h->dots + DOT_BLOCKS, st);
@@ -744,14 +830,15 @@ static int numeric_transfer(sg_amg *h, int l, cudaStream_t st) {
     int rc = power_lmax(h, L, A, st);
     if (rc) return rc;
     SG_BBC_DISPATCH(L.b, L.bc, ({
-        k_smooth_prolongator<BB, BC><<<grid_for(L.n, 128), 128, 0, st>>>(
-            L.n, L.P.d_rp, L.P.d_col, L.at_plan.d_ptr, L.at_plan.d_a, L.d_Acol, A, L.T, L.d_agg, L.Dinv, L.lmax,
+        k_smooth_prolongator<BB, BC><<<grid_for(L.P.nblk, 128), 128, 0, st>>>(
+            L.P.nblk, L.P.d_row, L.P.d_col, L.at_plan.d_ptr, L.at_plan.d_a, L.d_Acol, A, L.T, L.d_agg, L.Dinv, L.lmax,
             h->opt.omega_scale, L.Pv);
         k_transpose_blocks<BB, BC><<<grid_for(L.P.nblk * BB * BC, 256), 256, 0, st>>>(L.P.nblk, L.d_R_from_P, L.Pv, L.Rv);
         k_gather_AP<BB, BC><<<grid_for(L.AP.nblk, 128), 128, 0, st>>>(L.AP.nblk, L.ap_plan.d_ptr, L.ap_plan.d_a,
                                                                       L.ap_plan.d_b, A, L.Pv, L.APv);
-        k_gather_Ac<BB, BC><<<grid_for(C.n, 64), 64, 0, st>>>(C.n, C.d_Arp, C.d_Acol, L.ac_plan.d_ptr, L.ac_plan.d_a,
-                                                              L.ac_plan.d_b, L.Pv, L.APv, C.d_dead, C.Aown_vals);
+        k_gather_Ac<BB, BC><<<grid_for(C.Anblk, 128), 128, 0, st>>>(C.Anblk, C.Aown.d_row, C.d_Acol, L.ac_plan.d_ptr,
+                                                                    L.ac_plan.d_a, L.ac_plan.d_b, L.Pv, L.APv,
+                                                                    C.d_dead, C.Aown_vals);
     }));
     SG_CUDA(cudaGetLastError());
     if (h->opt.mixed) {
@@ -768,9 +855,12 @@ static int numeric_coarsest(sg_amg *h, cudaStream_t st) {
     const int64_t N = h->nc_dense;
     SG_CUDA(cudaMemsetAsync(h->Ainv, 0, sizeof(double) * N * N, st));
     SG_B_DISPATCH(L.b, (k_bsr_to_dense<BB><<<grid_for(L.n, 128), 128, 0, st>>>(L.n, L.d_Arp, L.d_Acol, A, N, h->Ainv)));
-    for (int64_t k = 0; k < N; ++k) {
-        k_gj_save<<<grid_for(N, 256), 256, 0, st>>>(N, k, h->Ainv, h->colk, h->rowk);
-        k_gj_update<<<grid_for(N * N, 256, 16), 256, 0, st>>>(N, k, h->Ainv, h->colk, h->rowk);
+    for (int64_t k0 = 0; k0 < N; k0 += GJ_NB) {
+        const int nb = (int)std::min<int64_t>(GJ_NB, N - k0);
+        count_launch();
+        k_gjb_pivot<<<1, GJ_NB * GJ_NB, 0, st>>>(N, k0, nb, h->Ainv, h->gj_pinv);
+        k_gjb_save<<<grid_for(N * nb, 256), 256, 0, st>>>(N, k0, nb, h->Ainv, h->gj_pinv, h->colk, h->rowk);
+        k_gjb_update<<<grid_for(N * N, 256, 16), 256, 0, st>>>(N, k0, nb, h->Ainv, h->gj_pinv, h->colk, h->rowk);
     }
     if (h->opt.mixed) k_to_float<<<grid_for(N * N, 256), 256, 0, st>>>(N * N, h->Ainv, h->Ainv32);
     SG_CUDA(cudaGetLastError());
@@ -900,8 +990,9 @@ static int build_hierarchy(sg_amg *h, const sg_bsr *A0, const double *A0vals, co
                 return set_error(SG_ERR_NUMERIC, "AMG coarsening stalled: coarsest level too large for a dense inverse");
             h->nc_dense = ndof;
             rc = dalloc(&h->Ainv, (size_t)ndof * ndof);
-            if (!rc) rc = dalloc(&h->colk, ndof);
-            if (!rc) rc = dalloc(&h->rowk, ndof);
+            if (!rc) rc = dalloc(&h->colk, (size_t)ndof * GJ_NB);
+            if (!rc) rc = dalloc(&h->rowk, (size_t)ndof * GJ_NB);
+            if (!rc) rc = dalloc(&h->gj_pinv, (size_t)GJ_NB * GJ_NB);
             if (!rc && o.mixed) rc = dalloc(&h->Ainv32, (size_t)ndof * ndof);
             return rc;
         }
@@ -955,7 +1046,7 @@ static int smooth(sg_amg *h, Level &L, LevelView<T> &v, bool x_zero, cudaStream_
     for (int k = 0; k < deg && !rc; ++k) {
         const T *r = v.rhs;
         if (!(x_zero && k == 0)) {
-            rc = rect_spmv<T, T>(L.b, L.b, L.n, L.d_Arp, L.d_Acol, v.A, v.x, v.r, 1.0, 0.0, v.rhs, 1, st);
+            rc = rect_spmv<T, T>(L.b, L.b, L.n, L.d_Arp, L.d_Acol, v.A, v.x, v.r, 1.0, 0.0, v.rhs, 1, st, L.Anblk);
             if (rc) return rc;
             r = v.r;
         }
@@ -979,10 +1070,10 @@ static int vcycle(sg_amg *h, int l, cudaStream_t st) {
     Level &C = h->L[l + 1];
     LevelView<T> c = view<T>(C);
     int rc = smooth<T>(h, L, v, true, st);
-    if (!rc) rc = rect_spmv<T, T>(L.b, L.b, L.n, L.d_Arp, L.d_Acol, v.A, v.x, v.r, 1.0, 0.0, v.rhs, 1, st);
-    if (!rc) rc = rect_spmv<T, T>(L.bc, L.b, C.n, L.R.d_rp, L.R.d_col, v.R, v.r, c.rhs, 1.0, 0.0, nullptr, 0, st);
+    if (!rc) rc = rect_spmv<T, T>(L.b, L.b, L.n, L.d_Arp, L.d_Acol, v.A, v.x, v.r, 1.0, 0.0, v.rhs, 1, st, L.Anblk);
+    if (!rc) rc = rect_spmv<T, T>(L.bc, L.b, C.n, L.R.d_rp, L.R.d_col, v.R, v.r, c.rhs, 1.0, 0.0, nullptr, 0, st, L.R.nblk);
     if (!rc) rc = vcycle<T>(h, l + 1, st);
-    if (!rc) rc = rect_spmv<T, T>(L.b, L.bc, L.n, L.P.d_rp, L.P.d_col, v.P, c.x, v.x, 1.0, 1.0, nullptr, 0, st);
+    if (!rc) rc = rect_spmv<T, T>(L.b, L.bc, L.n, L.P.d_rp, L.P.d_col, v.P, c.x, v.x, 1.0, 1.0, nullptr, 0, st, L.P.nblk);
     if (!rc) rc = smooth<T>(h, L, v, false, st);
     return rc;
 }
@@ -1019,6 +1110,7 @@ extern "C" int sg_amg_create(const sg_bsr *A, const double *A_vals, const double
     if (rc) {
         for (auto &L : h->L) free_level(L);
         cudaFree(h->Ainv); cudaFree(h->Ainv32); cudaFree(h->colk); cudaFree(h->rowk); cudaFree(h->dots);
+        cudaFree(h->gj_pinv);
         delete h;
         return rc;
     }
@@ -1037,6 +1129,7 @@ extern "C" int sg_amg_destroy(sg_amg *h) {
     cudaFree(h->colk);
     cudaFree(h->rowk);
     cudaFree(h->dots);
+    cudaFree(h->gj_pinv);
     cudaSetDevice(cur);
     delete h;
     return SG_OK;

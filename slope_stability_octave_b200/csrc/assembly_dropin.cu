@@ -105,6 +105,7 @@ static int launch_general(int dim, const double *D1, const double *D2, const dou
     if (ne <= 0) return SG_OK;
     const size_t sm = general_smem(dim, np, nq);
     const unsigned grid = (unsigned)std::min<int64_t>(ne, (int64_t)sm_count() * 16);
+    count_launch();
     if (dim == 3) {
         if (sm > 48 * 1024) SG_CUDA(cudaFuncSetAttribute(k_assemble_general<3>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
         k_assemble_general<3><<<grid, 256, sm, st>>>(D1, D2, D3, DS, W, smap, np, nq, ne, nnz, V, flag);

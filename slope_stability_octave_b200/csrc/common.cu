@@ -1,6 +1,7 @@
 // Library-wide helpers: error capture, device queries, scratch buffers.
 #include <cuda_runtime.h>
 
+#include <atomic>
 #include <cstdio>
 #include <string>
 
@@ -9,6 +10,9 @@
 namespace sg {
 
 static thread_local std::string g_last_error;
+static std::atomic<int64_t> g_launches{0};
+
+void count_launch(int n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
 
 int set_error(int code, const std::string &msg) {
     g_last_error = msg;
@@ -65,6 +69,13 @@ Scratch::~Scratch() {
 }  // namespace sg
 
 extern "C" int sg_abi_version(void) { return 1; }
+
+// Kernel launches issued by the library since the last reset.
+extern "C" int64_t sg_launch_count(int reset) {
+    const int64_t v = sg::g_launches.load();
+    if (reset) sg::g_launches.store(0);
+    return v;
+}
 
 extern "C" const char *sg_last_error(void) { return sg::g_last_error.c_str(); }
 

@@ -35,6 +35,8 @@ struct sg_krylov {
     double *hdev = nullptr;     // 2 * (maxit + 2) + 4 scalars
     double *hd = nullptr;       // kcap coefficients for the deflation projection
     double *Worth = nullptr;    // n * kcap
+    double *AWorth = nullptr;   // n * kcap
+    double *nt = nullptr, *sig = nullptr;  // kcap A-norms^2 and signs
     int64_t kcap = 0;
     double *hpin = nullptr;     // pinned host mirror of hdev
     int device = 0;
@@ -45,17 +47,26 @@ namespace sg {
 static int ensure_kcap(sg_krylov *ws, int64_t k) {
     if (k <= ws->kcap) return SG_OK;
     const int64_t cap = std::max<int64_t>(k, ws->kcap * 2 + 16);
-    double *part = nullptr, *hd = nullptr, *Wo = nullptr;
+    double *part = nullptr, *hd = nullptr, *Wo = nullptr, *AWo = nullptr, *nt = nullptr, *sig = nullptr;
     const int64_t rows = std::max<int64_t>(cap, ws->maxit + 2);
     SG_CUDA(cudaMalloc(&part, sizeof(double) * DOT_BLOCKS * rows));
     SG_CUDA(cudaMalloc(&hd, sizeof(double) * (cap + 8)));
     SG_CUDA(cudaMalloc(&Wo, sizeof(double) * ws->n * cap));
+    SG_CUDA(cudaMalloc(&AWo, sizeof(double) * ws->n * cap));
+    SG_CUDA(cudaMalloc(&nt, sizeof(double) * (cap + 8)));
+    SG_CUDA(cudaMalloc(&sig, sizeof(double) * (cap + 8)));
     cudaFree(ws->part);
     cudaFree(ws->hd);
     cudaFree(ws->Worth);
+    cudaFree(ws->AWorth);
+    cudaFree(ws->nt);
+    cudaFree(ws->sig);
     ws->part = part;
     ws->hd = hd;
     ws->Worth = Wo;
+    ws->AWorth = AWo;
+    ws->nt = nt;
+    ws->sig = sig;
     ws->kcap = cap;
     return SG_OK;
 }
@@ -68,6 +79,20 @@ __global__ void k_scale_host(int64_t n, double s, const double *__restrict__ x, 
 // c[j] *= norms[j] (norms = +-1 signature of the A-orthogonal basis)
 __global__ void k_mul_sign(int m, double *__restrict__ c, const double *__restrict__ sign) {
     for (int j = threadIdx.x; j < m; j += blockDim.x) c[j] *= sign[j];
+}
+
+// Keep a column when |nt| > eps: u = tmp / sqrt|nt|, A u = atmp / sqrt|nt|, sign = sign(nt);
+// otherwise u = A u = 0 (A_orthogonalize.m:40-52).
+__global__ void k_anorm_scale(int64_t n, const double *__restrict__ ntp, double eps, const double *__restrict__ tmp,
+                              double *__restrict__ col, double *__restrict__ acol, double *__restrict__ sgn) {
+    const double nt = ntp[0];
+    const bool keep = fabs(nt) > eps;
+    const double s = keep ? 1.0 / sqrt(fabs(nt)) : 0.0;
+    if (blockIdx.x == 0 && threadIdx.x == 0) sgn[0] = (keep && nt < 0.0) ? -1.0 : 1.0;
+    for (int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; r < n; r += (int64_t)gridDim.x * blockDim.x) {
+        col[r] = tmp[r] * s;
+        acol[r] = acol[r] * s;
+    }
 }
 
 }  // namespace sg
@@ -105,7 +130,8 @@ extern "C" int sg_krylov_destroy(sg_krylov *ws) {
     cudaGetDevice(&cur);
     cudaSetDevice(ws->device);
     cudaFree(ws->V); cudaFree(ws->Z); cudaFree(ws->w); cudaFree(ws->t); cudaFree(ws->hdev);
-    cudaFree(ws->part); cudaFree(ws->hd); cudaFree(ws->Worth);
+    cudaFree(ws->part); cudaFree(ws->hd); cudaFree(ws->Worth); cudaFree(ws->AWorth); cudaFree(ws->nt);
+    cudaFree(ws->sig);
     if (ws->hpin) cudaFreeHost(ws->hpin);
     cudaSetDevice(cur);
     delete ws;
@@ -113,11 +139,12 @@ extern "C" int sg_krylov_destroy(sg_krylov *ws) {
 }
 
 // Solve A x = b.  M: AMG preconditioner or NULL (identity).  Wd: n x k deflation basis
-// (A-orthonormal, may be NULL with k = 0).  x is overwritten.  res_hist (optional, host,
+// (A-orthonormal, may be NULL with k = 0); AWd: A Wd or NULL (then one extra SpMV per
+// iteration forms A z for the projection).  x is overwritten.  res_hist (optional, host,
 // maxit + 1 entries) receives the relative residual estimates.
 extern "C" int sg_dfgmres_solve(sg_krylov *ws, const sg_bsr *A, const double *Avals, sg_amg *M, const double *Wd,
-                                int32_t k, const double *b, double *x, double tol, int32_t maxit, int32_t *iters,
-                                double *relres, double *res_hist, void *stream) {
+                                const double *AWd, int32_t k, const double *b, double *x, double tol, int32_t maxit,
+                                int32_t *iters, double *relres, double *res_hist, void *stream) {
     SG_CHECK_ARG(ws && A && Avals && b && x, "null argument");
     SG_CHECK_ARG(maxit > 0 && maxit <= ws->maxit, "maxit exceeds the workspace");
     SG_CHECK_ARG(k >= 0 && (k == 0 || Wd), "bad deflation basis");
@@ -163,10 +190,14 @@ extern "C" int sg_dfgmres_solve(sg_krylov *ws, const sg_bsr *A, const double *Av
         } else {
             SG_CUDA(cudaMemcpyAsync(zj, vj, sizeof(double) * n, cudaMemcpyDeviceToDevice, st));
         }
-        // z = z - Wd (Wd' (A z))
+        // z = z - Wd (Wd' (A z)); with AWd = A Wd given, Wd' (A z) = AWd' z (A symmetric)
         if (k > 0) {
-            if ((rc = bsr_spmv<double, double>(*A, Avals, zj, ws->t, 1.0, 0.0, st))) return rc;
-            if ((rc = multidot(n, k, Wd, n, ws->t, part, ws->hd, st))) return rc;
+            if (AWd) {
+                if ((rc = multidot(n, k, AWd, n, zj, part, ws->hd, st))) return rc;
+            } else {
+                if ((rc = bsr_spmv<double, double>(*A, Avals, zj, ws->t, 1.0, 0.0, st))) return rc;
+                if ((rc = multidot(n, k, Wd, n, ws->t, part, ws->hd, st))) return rc;
+            }
             if ((rc = gemv_sub(n, k, Wd, n, ws->hd, zj, st))) return rc;
         }
         // u = A z ; CGS2 against v_0..v_j
@@ -226,61 +257,56 @@ extern "C" int sg_dfgmres_solve(sg_krylov *ws, const sg_bsr *A, const double *Av
 }
 
 // A-orthonormalise the n x k basis W in place (column-major, ld = n); returns the number of
-// kept columns in *k_out (W's first *k_out columns hold the result).
-extern "C" int sg_a_orthogonalize(sg_krylov *ws, const sg_bsr *A, const double *Avals, double *W, int32_t k,
-                                  double eps_add, int32_t *k_out, void *stream) {
+// kept columns in *k_out (W's first *k_out columns hold the result).  AW (optional, n x k)
+// receives A times the kept columns, in the same order, for the solve's projection.
+extern "C" int sg_a_orthogonalize(sg_krylov *ws, const sg_bsr *A, const double *Avals, double *W, double *AW,
+                                  int32_t k, double eps_add, int32_t *k_out, void *stream) {
     SG_CHECK_ARG(ws && A && Avals && k_out && k >= 0 && (k == 0 || W), "bad argument");
     const int64_t n = ws->n;
     const cudaStream_t st = as_stream(stream);
     if (k == 0) { *k_out = 0; return SG_OK; }
     int rc = ensure_kcap(ws, k);
     if (rc) return rc;
-    double *Wo = ws->Worth, *At = ws->t, *tmp = ws->w, *part = ws->part, *c = ws->hd, *hdev = ws->hdev;
-    std::vector<double> sign(k, 1.0);
-    std::vector<char> keep(k, 0);
-    double *dsign = hdev + 4;  // reuse the scalar buffer tail for the signature (k <= 2*maxit)
-    std::vector<double> signs_dev_host;
-    double *dsig = nullptr;
-    SG_CUDA(cudaMallocAsync(&dsig, sizeof(double) * (k + 1), st));
-    (void)dsign;
+    // Wo, AWo: the A-orthonormalised columns and A times them, in processing order; nt[i] is
+    // column i's A-norm^2 and sig[i] its sign (kept, scaled and signed on the device, so the
+    // loop needs no host round trip; dropped columns are left as zeros).
+    double *Wo = ws->Worth, *AWo = ws->AWorth, *At = ws->t, *tmp = ws->w, *part = ws->part, *c = ws->hd;
+    double *nt = ws->nt, *sig = ws->sig;
     const unsigned gb = grid_for(n, 256, 8);
-    for (int i = 0; i < k; ++i) {
+    for (int i = 0; i < k && !rc; ++i) {
         const double *src = W + (int64_t)(k - 1 - i) * n;
+        double *col_i = Wo + (int64_t)i * n, *acol_i = AWo + (int64_t)i * n;
         if ((rc = bsr_spmv<double, double>(*A, Avals, src, At, 1.0, 0.0, st))) break;
         SG_CUDA(cudaMemcpyAsync(tmp, src, sizeof(double) * n, cudaMemcpyDeviceToDevice, st));
+        SG_CUDA(cudaMemcpyAsync(acol_i, At, sizeof(double) * n, cudaMemcpyDeviceToDevice, st));
         if (i > 0) {
+            // c_j = sig_j (A src)' u_j ;  tmp -= sum c_j u_j ;  A tmp = A src - sum c_j A u_j
             if ((rc = multidot(n, i, Wo, n, At, part, c, st))) break;
-            k_mul_sign<<<1, 256, 0, st>>>(i, c, dsig);
+            count_launch();
+            k_mul_sign<<<1, 256, 0, st>>>(i, c, sig);
             if ((rc = gemv_sub(n, i, Wo, n, c, tmp, st))) break;
+            if ((rc = gemv_sub(n, i, AWo, n, c, acol_i, st))) break;
         }
-        if ((rc = multidot(n, 1, tmp, n, At, part, hdev, st))) break;
-        double nt = 0.0;
-        SG_CUDA(cudaMemcpyAsync(&ws->hpin[0], hdev, sizeof(double), cudaMemcpyDeviceToHost, st));
-        SG_CUDA(cudaStreamSynchronize(st));
-        nt = ws->hpin[0];
-        double* col_i = Wo + (int64_t)i * n;
-        if (std::fabs(nt) > eps_add) {
-            if (nt < 0) sign[i] = -1.0;
-            k_scale_host<<<gb, 256, 0, st>>>(n, 1.0 / std::sqrt(std::fabs(nt)), tmp, col_i);
-            keep[i] = 1;
-        } else {
-            SG_CUDA(cudaMemsetAsync(col_i, 0, sizeof(double) * n, st));
-        }
-        SG_CUDA(cudaMemcpyAsync(dsig + i, &sign[i], sizeof(double), cudaMemcpyHostToDevice, st));
-        SG_CUDA(cudaStreamSynchronize(st));
+        if ((rc = multidot(n, 1, tmp, n, At, part, nt + i, st))) break;
+        k_anorm_scale<<<gb, 256, 0, st>>>(n, nt + i, eps_add, tmp, col_i, acol_i, sig + i);
+        SG_CUDA(cudaGetLastError());
     }
-    if (!rc) {
-        // kept columns, reversed: output column o = kept column in reverse processing order
-        int o = 0;
-        for (int i = k - 1; i >= 0; --i) {
-            if (!keep[i]) continue;
-            SG_CUDA(cudaMemcpyAsync(W + (int64_t)o * n, Wo + (int64_t)i * n, sizeof(double) * n,
-                                    cudaMemcpyDeviceToDevice, st));
-            ++o;
-        }
-        *k_out = o;
-    }
-    cudaFreeAsync(dsig, st);
+    if (rc) return rc;
+    std::vector<double> nth(k);
+    SG_CUDA(cudaMemcpyAsync(nth.data(), nt, sizeof(double) * k, cudaMemcpyDeviceToHost, st));
     SG_CUDA(cudaStreamSynchronize(st));
-    return rc;
+    // kept columns, reversed: output column o = kept column in reverse processing order
+    int o = 0;
+    for (int i = k - 1; i >= 0; --i) {
+        if (!(std::fabs(nth[i]) > eps_add)) continue;
+        SG_CUDA(cudaMemcpyAsync(W + (int64_t)o * n, Wo + (int64_t)i * n, sizeof(double) * n,
+                                cudaMemcpyDeviceToDevice, st));
+        if (AW)
+            SG_CUDA(cudaMemcpyAsync(AW + (int64_t)o * n, AWo + (int64_t)i * n, sizeof(double) * n,
+                                    cudaMemcpyDeviceToDevice, st));
+        ++o;
+    }
+    *k_out = o;
+    SG_CUDA(cudaStreamSynchronize(st));
+    return SG_OK;
 }

@@ -63,42 +63,51 @@ __global__ void __launch_bounds__(256) k_bsr_spmv(int64_t nrows, const int32_t *
     }
 }
 
+// Group width: enough lanes per row to cover the row's blocks in a few passes (fine level,
+// ~28 blocks per row: 8 lanes; coarse 6x6 levels, ~100 blocks per row: a full warp).
 template <int BR, int BC, typename VT, typename XT>
-static void spmv_launch(int64_t nrows, const int32_t *rp, const int32_t *col, const VT *vals, const XT *x, XT *y,
-                        double alpha, double beta, const XT *bvec, int mode, cudaStream_t st) {
-    constexpr int G = (BR * BC >= 9) ? 8 : 4;
+static void spmv_launch(int64_t nrows, int64_t nblk, const int32_t *rp, const int32_t *col, const VT *vals,
+                        const XT *x, XT *y, double alpha, double beta, const XT *bvec, int mode, cudaStream_t st) {
+    const double avg = nblk > 0 && nrows > 0 ? (double)nblk / (double)nrows : 8.0;
+    const int G = avg >= 64 ? 32 : (avg >= 24 ? ((BR * BC >= 9) ? 8 : 16) : (avg >= 10 ? 8 : 4));
     const int64_t threads = nrows * G;
     // the node-block shapes of the fine level are the ones timed for the roofline report
     constexpr bool fine = (BR == BC) && (BR == 3 || BR == 2);
     InstrToken tk;
     if (fine) tk = instr_begin(sizeof(VT) == 8 ? IK_SPMV3_F64 : IK_SPMV3_F32, st);
-    k_bsr_spmv<BR, BC, G, VT, XT><<<grid_for(threads, 256, 16), 256, 0, st>>>(nrows, rp, col, vals, x, y, alpha, beta,
-                                                                               bvec, mode);
+    const unsigned grid = grid_for(threads, 256, 16);
+    switch (G) {
+        case 32: k_bsr_spmv<BR, BC, 32, VT, XT><<<grid, 256, 0, st>>>(nrows, rp, col, vals, x, y, alpha, beta, bvec, mode); break;
+        case 16: k_bsr_spmv<BR, BC, 16, VT, XT><<<grid, 256, 0, st>>>(nrows, rp, col, vals, x, y, alpha, beta, bvec, mode); break;
+        case 8: k_bsr_spmv<BR, BC, 8, VT, XT><<<grid, 256, 0, st>>>(nrows, rp, col, vals, x, y, alpha, beta, bvec, mode); break;
+        default: k_bsr_spmv<BR, BC, 4, VT, XT><<<grid, 256, 0, st>>>(nrows, rp, col, vals, x, y, alpha, beta, bvec, mode); break;
+    }
     if (fine) instr_end(tk, st);
 }
 
 template <typename VT, typename XT>
 int rect_spmv(int br, int bc, int64_t nrows, const int32_t *rp, const int32_t *col, const VT *vals, const XT *x,
-              XT *y, double alpha, double beta, const XT *bvec, int mode, cudaStream_t st) {
+              XT *y, double alpha, double beta, const XT *bvec, int mode, cudaStream_t st, int64_t nblk) {
 #define SG_SPMV_CASE(R, Cc) \
-    if (br == R && bc == Cc) { spmv_launch<R, Cc>(nrows, rp, col, vals, x, y, alpha, beta, bvec, mode, st); SG_CUDA(cudaGetLastError()); return SG_OK; }
+    if (br == R && bc == Cc) { spmv_launch<R, Cc>(nrows, nblk, rp, col, vals, x, y, alpha, beta, bvec, mode, st); SG_CUDA(cudaGetLastError()); return SG_OK; }
     SG_SPMV_CASE(1, 1) SG_SPMV_CASE(2, 2) SG_SPMV_CASE(3, 3) SG_SPMV_CASE(6, 6)
     SG_SPMV_CASE(2, 3) SG_SPMV_CASE(3, 2) SG_SPMV_CASE(3, 6) SG_SPMV_CASE(6, 3)
 #undef SG_SPMV_CASE
     return set_error(SG_ERR_ARG, "unsupported BSR block shape");
 }
 template int rect_spmv<double, double>(int, int, int64_t, const int32_t *, const int32_t *, const double *, const double *,
-                                       double *, double, double, const double *, int, cudaStream_t);
+                                       double *, double, double, const double *, int, cudaStream_t, int64_t);
 template int rect_spmv<float, float>(int, int, int64_t, const int32_t *, const int32_t *, const float *, const float *,
-                                     float *, double, double, const float *, int, cudaStream_t);
+                                     float *, double, double, const float *, int, cudaStream_t, int64_t);
 
 template <typename VT, typename XT>
 int bsr_spmv(const sg_bsr &A, const VT *vals, const XT *x, XT *y, double alpha, double beta, cudaStream_t st) {
-    return rect_spmv<VT, XT>(A.b, A.b, A.n_rows, A.d_row_ptr, A.d_col, vals, x, y, alpha, beta, nullptr, 0, st);
+    return rect_spmv<VT, XT>(A.b, A.b, A.n_rows, A.d_row_ptr, A.d_col, vals, x, y, alpha, beta, nullptr, 0, st,
+                             A.n_blocks);
 }
 template <typename VT, typename XT>
 int bsr_residual(const sg_bsr &A, const VT *vals, const XT *x, const XT *b, XT *r, cudaStream_t st) {
-    return rect_spmv<VT, XT>(A.b, A.b, A.n_rows, A.d_row_ptr, A.d_col, vals, x, r, 1.0, 0.0, b, 1, st);
+    return rect_spmv<VT, XT>(A.b, A.b, A.n_rows, A.d_row_ptr, A.d_col, vals, x, r, 1.0, 0.0, b, 1, st, A.n_blocks);
 }
 template int bsr_spmv<double, double>(const sg_bsr &, const double *, const double *, double *, double, double, cudaStream_t);
 template int bsr_spmv<float, float>(const sg_bsr &, const float *, const float *, float *, double, double, cudaStream_t);
@@ -170,6 +179,7 @@ __global__ void k_reduce_partials(int m, int nb, const double *__restrict__ part
 int multidot(int64_t n, int m, const double *V, int64_t ldv, const double *w, double *partial, double *out,
              cudaStream_t st) {
     if (m <= 0) return SG_OK;
+    count_launch(2);
     k_multidot<<<DOT_BLOCKS, DOT_THREADS, 0, st>>>(n, m, V, ldv, w, partial);
     k_reduce_partials<<<std::min(m, 1024), 256, 0, st>>>(m, DOT_BLOCKS, partial, out);
     SG_CUDA(cudaGetLastError());
@@ -286,6 +296,7 @@ extern "C" int sg_masked_diff_norm2_dev(int64_t n, const double *a, const double
     if (rc) return rc;
     double *part = (double *)ws.ptr, *out = part + DOT_BLOCKS;
     const cudaStream_t st = as_stream(stream);
+    count_launch(2);
     k_masked_diff2<<<DOT_BLOCKS, DOT_THREADS, 0, st>>>(n, a, b, mask, part);
     k_reduce_partials<<<1, 256, 0, st>>>(1, DOT_BLOCKS, part, out);
     SG_CUDA(cudaGetLastError());

@@ -17,9 +17,10 @@ int bsr_residual(const sg_bsr &A, const VT *vals, const XT *x, const XT *b, XT *
 
 // Rectangular-block row SpMV: y = alpha * M x + beta * y (mode 0) or y = bvec - M x (mode 1),
 // M with br x bc blocks.  Supported shapes: 1x1 2x2 3x3 6x6 2x3 3x2 3x6 6x3.
+// nblk (total blocks, -1 if unknown) selects the number of lanes per row.
 template <typename VT, typename XT>
 int rect_spmv(int br, int bc, int64_t nrows, const int32_t *rp, const int32_t *col, const VT *vals, const XT *x,
-              XT *y, double alpha, double beta, const XT *bvec, int mode, cudaStream_t st);
+              XT *y, double alpha, double beta, const XT *bvec, int mode, cudaStream_t st, int64_t nblk = -1);
 
 // Reduction workspace for dot products: partial sums of `nblk` blocks per column.
 constexpr int DOT_BLOCKS = 296;  // 2 x 148 SMs

@@ -25,10 +25,15 @@ int cuda_error(cudaError_t e, const char *what);
         if (!(cond)) return sg::set_error(SG_ERR_ARG, msg);    \
     } while (0)
 
+// Number of kernel launches issued by the library (every launch computes its grid through
+// grid_for or calls count_launch), read by sg_launch_count for benchmark reporting.
+void count_launch(int n = 1);
+
 // Launch shape: grid sized in multiples of the SM count (148 on B200) for
 // grid-stride kernels, capped by the work.
 int sm_count();
 inline unsigned grid_for(int64_t work, int block, int per_sm = 8) {
+    count_launch();
     int64_t need = (work + block - 1) / block;
     int64_t cap = (int64_t)sm_count() * per_sm;
     if (need < 1) need = 1;

@@ -36,6 +36,19 @@ def require_cuda():
         raise _lib.SlopeGPUError("a CUDA device is required (no CPU fallback)")
 
 
+# Bumped by every DeviceMesh operation that writes matrix values, so that cached products of
+# a matrix (A W of the deflation basis) can tell whether the values changed since.
+_matrix_generation = [0]
+
+
+def matrix_generation() -> int:
+    return _matrix_generation[0]
+
+
+def _bump():
+    _matrix_generation[0] += 1
+
+
 class DeviceMesh:
     """Owns an ``sg_mesh``: element data, gradients, weights and sparsity patterns on the GPU.
 
@@ -117,15 +130,19 @@ class DeviceMesh:
         _lib.call("sg_force_dev", self.handle, ptr(S), int(s_rows), ptr(F), cur_stream())
 
     def assemble(self, DS, K):
+        _bump()
         _lib.call("sg_assemble_bsr_dev", self.handle, ptr(DS), ptr(K), cur_stream())
 
     def elastic_ds(self, shear, bulk, DS):
+        _bump()
         _lib.call("sg_elastic_ds_dev", self.handle, ptr(shear), ptr(bulk), ptr(DS), cur_stream())
 
     def symmetrize(self, K, Ks):
+        _bump()
         _lib.call("sg_symmetrize_bsr_dev", self.handle, ptr(K), ptr(Ks), cur_stream())
 
     def kr_blend(self, r, Kel, Kt, Kr):
+        _bump()
         _lib.call("sg_kr_blend_dev", self.handle, float(r), ptr(Kel), ptr(Kt), ptr(Kr), cur_stream())
 
     def spmv(self, K, x, y):

@@ -22,7 +22,7 @@ import numpy as np
 import torch
 
 from . import _lib
-from .device import DeviceMesh, F64, cur_stream, hptr, ptr
+from .device import DeviceMesh, F64, cur_stream, hptr, matrix_generation, ptr
 
 
 def near_null_space_elasticity(coord, Q=None, center=True):
@@ -138,6 +138,10 @@ class DFGMRES:
         self.n = dmesh.n_dof
         self._ws = _ws if _ws is not None else _Workspace(self.n, self.max_iterations)
         self.basis = torch.empty((0, self.n), dtype=F64, device=dmesh.device)   # rows = columns of W
+        # A W of the current basis and the matrix it was formed with ((data_ptr, generation)):
+        # the solve uses it for the projection only while both still hold
+        self.AW = None
+        self._aw_key = None
         self.profiler = None
         self.last_iterations = 0
         self.last_relres = 0.0
@@ -164,12 +168,16 @@ class DFGMRES:
     def A_orthogonalize(self, K):
         t0 = time.perf_counter()
         k = self.k
+        self.AW, self._aw_key = None, None
         if k > 0:
             B = self.basis.contiguous()
+            AW = torch.empty_like(B)
             kout = C.c_int32()
-            _lib.call("sg_a_orthogonalize", self._ws.handle, self.dmesh.bsr, ptr(K), ptr(B), k,
+            _lib.call("sg_a_orthogonalize", self._ws.handle, self.dmesh.bsr, ptr(K), ptr(B), ptr(AW), k,
                       self.tolerance_deflation_basis, C.byref(kout), cur_stream())
             self.basis = B[: kout.value]
+            self.AW = AW[: kout.value]
+            self._aw_key = (K.data_ptr(), matrix_generation())
         self._time("DFGMRES.A_orthogonalize", t0)
 
     def solve(self, K, b):
@@ -180,9 +188,10 @@ class DFGMRES:
         rr = C.c_double()
         B = self.basis
         M = self.preconditioner.handle if self.preconditioner is not None else None
+        aw_ok = self.k > 0 and self.AW is not None and self._aw_key == (K.data_ptr(), matrix_generation())
         _lib.call("sg_dfgmres_solve", self._ws.handle, self.dmesh.bsr, ptr(K), M, ptr(B) if self.k else None,
-                  self.k, ptr(b), ptr(x), self.tolerance, self.max_iterations, C.byref(it), C.byref(rr), None,
-                  cur_stream())
+                  ptr(self.AW) if aw_ok else None, self.k, ptr(b), ptr(x), self.tolerance, self.max_iterations,
+                  C.byref(it), C.byref(rr), None, cur_stream())
         self.last_iterations = it.value
         self.last_relres = rr.value
         self._time("DFGMRES.solve", t0)
@@ -192,12 +201,15 @@ class DFGMRES:
         t0 = time.perf_counter()
         v = v.reshape(1, -1).to(F64)
         self.basis = torch.cat([self.basis, v], 0)
+        self.AW, self._aw_key = None, None
         self._time("DFGMRES.expand_deflation_basis", t0)
 
     def copy(self):
         new = DFGMRES(self.dmesh, self.tolerance, self.max_iterations, self.tolerance_deflation_basis, self.verbose,
                       amg=self.preconditioner, _ws=self._ws)
         new.basis = self.basis.clone()
+        if self.AW is not None:
+            new.AW, new._aw_key = self.AW.clone(), self._aw_key
         new.profiler = self.profiler
         return new
 
