@@ -10,11 +10,16 @@ Newton tol 1e-4 (the reference scripts' settings).  Synthetic, seeded, no datase
 A step is one accepted step of SSR_indirect_continuation (the sum of its attempts, as
 stats.step_wall_time).  The init phase is untimed, W warm-up steps run untimed, then exactly
 K steps are timed with CUDA events (barrier + synchronize on both sides; max over ranks).
-``value`` excludes the per-step host<->device state copies; ``e2e`` includes them: every timed
-step starts by copying its input state (U, U_old) from pinned host memory and ends by reading
-the new state back.  The working set (K_r 441 MB, Krylov bases ~1 GB) exceeds the 126 MB L2.
+Two forms run back to back on the same workload from the same start: ``plain`` (FP64
+throughout) and ``mixed`` (FP32 V-cycle inside the FP64 FGMRES; return mapping, Newton
+residual, Arnoldi and the lambda update in FP64).  ``value`` is the mixed form's s/step (the
+form the metric names), the plain form's figures and the lambda error between the forms at
+equal step index are in ``config``.  ``value`` excludes the per-step host<->device state copies;
+``e2e`` includes them: every timed step starts by copying its input state (U, U_old) from
+pinned host memory and ends by reading the new state back.  The working set (K_r 441 MB,
+Krylov bases ~1 GB) exceeds the 126 MB L2, so no flush is needed between steps.
 
-  python bench.py [--gpus N] [--steps K] [--warmup W] [--form plain|mixed] [--impl reference]
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--form both|plain|mixed] [--impl reference]
 
 Multi-GPU: replicas only (each rank runs the same continuation; no collective on the path).
 """
@@ -35,7 +40,10 @@ sys.path.insert(0, ROOT)
 
 METRIC = "s per SSR continuation step, 3D P2 (mixed+learned vs plain FP64 GPU) at equal λ"
 UNIT = "s/step"
-WORKLOAD = "3D homogeneous slope SSR, mesh_P2_3D(N_h=1, 15,10,15,10,10, z=40): 156,000 P2 tets, 631,380 free DOFs"
+WORKLOAD = ("3D homogeneous slope SSR, mesh_P2_3D(N_h=1, 15,10,15,10,10, z=40): 156,000 P2 tets, "
+            "220,401 nodes, 631,380 free DOFs, 1,716,000 integration points")
+COUNTS_FILE = os.path.join(ROOT, "profiles", "ssr3d_z40_step_counts.json")
+N_INSTR = 8
 
 
 def parse():
@@ -44,7 +52,7 @@ def parse():
     ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    ap.add_argument("--form", default="plain", choices=["plain", "mixed"])
+    ap.add_argument("--form", default="both", choices=["both", "plain", "mixed"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     return ap.parse_args()
 
@@ -69,6 +77,7 @@ class ClockSampler:
             self.t.start()
         except OSError:
             self.proc = None
+        return self
 
     def _read(self):
         for line in self.proc.stdout:
@@ -108,42 +117,37 @@ def traffic_per_spmv():
         return None
 
 
-def run_b200(args, rank, world):
+def run_form(args, form, P, rank, world):
+    """One continuation of the workload in ``form``: init, W warm-up steps, K timed steps."""
     import numpy as np
     import torch
 
     from slope_stability_octave_b200 import _lib, problems
     from slope_stability_octave_b200.continuation import SSRIndirectStepper
 
-    torch.cuda.set_device(rank % max(torch.cuda.device_count(), 1))
-    dev = torch.device("cuda", torch.cuda.current_device())
-    t_setup = time.perf_counter()
-    P = problems.slope_3d(1).to_device()
-    solver = P.solver("DFGMRES_B200_MIXED" if args.form == "mixed" else "DFGMRES_B200", tol=1e-1, maxit=100)
+    t0 = time.perf_counter()
+    solver = P.solver("DFGMRES_B200_MIXED" if form == "mixed" else "DFGMRES_B200", tol=1e-1, maxit=100)
     f = P.f_device()
-    Q = P.dmesh.mask
-    run = SSRIndirectStepper(problems.SSR_3D_EXTRUDED, Q, f, P.cons, solver).init()
-    t_init = time.perf_counter() - t_setup
+    run = SSRIndirectStepper(problems.SSR_3D_EXTRUDED, P.dmesh.mask, f, P.cons, solver).init()
+    t_init = time.perf_counter() - t0
     for _ in range(args.warmup):
         if run.step() is None:
-            raise RuntimeError("continuation stopped during warm-up")
-    # host-resident state for the e2e measurement
+            raise RuntimeError(f"continuation stopped during warm-up ({run.stop_reason})")
+    # host-resident state for the end-to-end measurement
     U_h = torch.empty_like(run.U, device="cpu").pin_memory()
     Uo_h = torch.empty_like(run.U_old, device="cpu").pin_memory()
     U_h.copy_(run.U)
     Uo_h.copy_(run.U_old)
-    torch.cuda.synchronize()
-    if world > 1:
-        torch.distributed.barrier()
-    clocks = ClockSampler(torch.cuda.current_device())
-    clocks.start()
-    _lib.call("sg_instr_enable", 1, 4)
-    _lib.lib().sg_launch_count(1)
     ev = [[torch.cuda.Event(enable_timing=True) for _ in range(4)] for _ in range(args.steps)]
-    steps = []
+    steps, basis = [], []
+    clocks = ClockSampler(torch.cuda.current_device()).start()
+    _lib.call("sg_instr_enable", 1, 4)
     torch.cuda.synchronize()
     if world > 1:
         torch.distributed.barrier()
+    torch.cuda.synchronize()
+    _lib.lib().sg_launch_count(1)
+    torch.cuda.nvtx.range_push("timed_step")
     for k in range(args.steps):
         e0, e1, e2, e3 = ev[k]
         e0.record()
@@ -156,95 +160,101 @@ def run_b200(args, rank, world):
         Uo_h.copy_(run.U_old, non_blocking=True)
         e3.record()
         if acc is None:
-            raise RuntimeError("continuation stopped inside the timed region")
+            raise RuntimeError(f"continuation stopped inside the timed region ({run.stop_reason})")
         steps.append(acc)
+        basis.append(solver.k)
     torch.cuda.synchronize()
+    torch.cuda.nvtx.range_pop()
+    if world > 1:
+        torch.distributed.barrier()
     launches = int(_lib.lib().sg_launch_count(1))
-    ms = np.zeros(8)
-    nt = np.zeros(8, np.int64)
-    nl = np.zeros(8, np.int64)
+    ms = np.zeros(N_INSTR)
+    nt = np.zeros(N_INSTR, np.int64)
+    nl = np.zeros(N_INSTR, np.int64)
     _lib.call("sg_instr_read", ms.ctypes.data_as(C.c_void_p), nt.ctypes.data_as(C.c_void_p),
-              nl.ctypes.data_as(C.c_void_p), 8)
+              nl.ctypes.data_as(C.c_void_p), N_INSTR)
     _lib.call("sg_instr_enable", 0, 1)
     clk = clocks.stop()
     t_dev = sum(ev[k][1].elapsed_time(ev[k][2]) for k in range(args.steps)) / 1e3
     t_e2e = sum(ev[k][0].elapsed_time(ev[k][3]) for k in range(args.steps)) / 1e3
     if world > 1:
-        t = torch.tensor([t_dev, t_e2e], dtype=torch.float64, device=dev)
+        t = torch.tensor([t_dev, t_e2e], dtype=torch.float64, device="cuda")
         torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
         t_dev, t_e2e = t.tolist()
-    n_dof = P.dmesh.n_dof
-    res = dict(t_dev=t_dev, t_e2e=t_e2e, steps=steps, launches=launches, instr=(ms, nt, nl), clocks=clk,
-               n_dof=n_dof, n_blocks=P.dmesh.n_blocks, n_rows=P.dmesh.n_n, t_init=t_init,
-               lam=[s["lam"] for s in steps], amg=solver.preconditioner.info())
-    return res, P
+    res = dict(t_dev=t_dev, t_e2e=t_e2e, steps=steps, basis=basis, launches=launches, instr=(ms, nt, nl),
+               clocks=clk, t_init=t_init, lam=[s["lam"] for s in steps], amg=solver.preconditioner.info(),
+               lam_init=list(run.lambda_hist[: 2 + args.warmup]))
+    del run, solver
+    torch.cuda.empty_cache()
+    return res
 
 
-def cpu_baseline_sample(P, counts, threads, log=print):
-    """Reference C kernels (OpenMP) + oracle port on a z = 4 m slice of the workload (1/10 of
-    its points, elements and DOFs), unit costs scaled by the size ratio, weighted by the counts
-    of the timed steps."""
-    import numpy as np
+def step_counts(res):
+    """Per-step operation counts of the timed steps (drive the CPU-baseline model)."""
+    steps = res["steps"]
+    n = len(steps)
+    newton = sum(s["newton_iterations_total"] for s in steps) / n
+    lin = sum(s["linear_iterations"] for s in steps) / n
+    return dict(newton=newton, linear=lin, damping=newton, deflation=sum(res["basis"]) / n,
+                krylov_j=max(1.0, lin / max(2 * newton, 1) / 2),
+                branch_mix=(0.8, 0.1, 0.04, 0.04, 0.02))
 
-    from oracle.cpu_baseline import CPUSample, step_seconds
+
+def cpu_sample(log=lambda *a: None):
+    """The CPU path's unit costs are timed on a z = 4 m slice of the workload (1/10 of its
+    points, elements and DOFs) and scaled by the size ratio."""
+    from oracle.cpu_baseline import CPUSample
     from slope_stability_octave_b200 import problems, workloads
     from slope_stability_octave_b200.linear_solvers import near_null_space_elasticity
 
     S = problems.slope_3d(1, dims=(15, 10, 15, 10, 10, 4))
-    # per-point strains with the branch mix of the timed steps (seeded)
-    pts = workloads.constitutive_points(S.weight.size, seed=7, fractions=tuple(counts.get("branch_mix", (0.2,) * 5)))
+    pts = workloads.constitutive_points(S.weight.size, seed=7, fractions=(0.8, 0.1, 0.04, 0.04, 0.02))
     smp = CPUSample(S.mesh, S.dphi, S.weight, S.n_q, S.mat, pts, log=log)
     Z = near_null_space_elasticity(S.mesh.coord, S.mesh.Q)
     smp.build_amg(Z, ~S.mesh.Q.T.ravel(), log=log)
+    return S, smp
+
+
+def cpu_step_seconds(S, smp, counts, n_int_full, n_dof_full):
+    from oracle.cpu_baseline import step_seconds
     c = smp.unit_costs()
-    scale = P.dmesh.n_int / S.weight.size
+    scale = n_int_full / S.weight.size
     cs = {k: v * scale for k, v in c.items()}
-    cs["dot"] = c["dot"] * P.dmesh.n_dof / (S.mesh.n_n * 3)
-    cs["axpy"] = c["axpy"] * P.dmesh.n_dof / (S.mesh.n_n * 3)
-    return step_seconds(cs, counts), dict(unit_costs_sample=c, scale=scale)
+    cs["dot"] = c["dot"] * n_dof_full / (S.mesh.n_n * 3)
+    cs["axpy"] = c["axpy"] * n_dof_full / (S.mesh.n_n * 3)
+    return step_seconds(cs, counts), c
 
 
-def step_counts(steps, amg_info, branch_mix=None):
-    n = len(steps)
-    newton = sum(s["newton_iterations_total"] for s in steps) / n
-    lin = sum(s["linear_iterations"] for s in steps) / n
-    return dict(newton=newton, linear=lin, damping=newton, deflation=2 * newton + 3,
-                krylov_j=max(1.0, lin / max(2 * newton, 1) / 2), amg_setup_factor=3.0,
-                branch_mix=branch_mix or (0.8, 0.1, 0.04, 0.04, 0.02))
+CPU_SAMPLE_TEXT = ("one modelled continuation step: unit costs of every Newton-iteration operation timed on a "
+                   "z=4 m slice of the workload (1/10 of its points/elements/DOFs) and scaled by size, weighted by "
+                   "the timed GPU steps' Newton/Krylov/deflation counts; return mapping and tangent assembly are "
+                   "the reference's own C (MEX sources compiled with -O2 -fopenmp, all host threads), B*U, B'S, "
+                   "SpMV, Gram-Schmidt, deflation and the AMG set-up/V-cycle are the NumPy/SciPy port (the "
+                   "reference's Octave/sparsersb/HYPRE layer is not installable)")
 
 
 def reference_arm(args, rank, world):
     if rank != 0:
         return None
+    import numpy as np
     threads = os.cpu_count() or 1
     os.environ.setdefault("OMP_NUM_THREADS", str(threads))
-    import numpy as np
-    counts_path = os.path.join(ROOT, "profiles", "cfg2_step_counts.json")
-    with open(counts_path) as fh:
+    with open(COUNTS_FILE) as fh:
         counts = json.load(fh)
-
-    class _P:  # sizes of the full workload
-        pass
-    from slope_stability_octave_b200 import problems
-    full = problems.slope_3d(1)
-
-    class _D:
-        n_int = full.weight.size
-        n_dof = full.mesh.n_n * 3
-    _P.dmesh = _D
+    S, smp = cpu_sample()
     vals = []
     for i in range(args.warmup + args.steps):
-        v, info = cpu_baseline_sample(_P, counts, threads, log=lambda *a: None)
+        v, _ = cpu_step_seconds(S, smp, counts, counts["n_int"], counts["n_dof"])
         if i >= args.warmup:
             vals.append(v)
-    value = float(np.median(vals))
+    value = float(np.mean(vals))
     line = dict(metric=METRIC, value=value, unit=UNIT, n_gpus=args.gpus, steps=args.steps, warmup=args.warmup,
                 ms_per_step=value * 1e3, higher_is_better=False, scaling="weak", vs_baseline=None, dtype="f64",
                 data="synthetic", impl="reference",
-                config=dict(workload=WORKLOAD, form="reference CPU path", parallelism="replicas"),
-                cpu_baseline=dict(value=value, unit=UNIT, cores=threads, kind="reference",
-                                  sample="reference MEX kernels (OpenMP) + oracle port, z=4 m slice scaled x10, "
-                                         "weighted by committed per-step counts"),
+                config=dict(workload=WORKLOAD, form="reference CPU path (plain FP64)", parallelism="replicas",
+                            counts=counts),
+                cpu_baseline=dict(value=value, unit=UNIT, cores=int(os.environ["OMP_NUM_THREADS"]), kind="port",
+                                  sample=CPU_SAMPLE_TEXT),
                 e2e=dict(value=value, unit=UNIT, h2d_bytes_per_step=0, d2h_bytes_per_step=0))
     print(json.dumps(line))
     return line
@@ -254,57 +264,81 @@ def main():
     args = parse()
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
-    if world > 1:
-        import datetime
-
-        import torch
-        torch.distributed.init_process_group("nccl" if args.impl == "b200" else "gloo",
-                                             timeout=datetime.timedelta(seconds=600))
     if args.impl == "reference":
         reference_arm(args, rank, world)
         return
-    res, P = run_b200(args, rank, world)
+    import datetime
+
+    import torch
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local % max(torch.cuda.device_count(), 1))
+    if world > 1:
+        torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                             device_id=torch.device("cuda", torch.cuda.current_device()))
+    from slope_stability_octave_b200 import problems
+    P = problems.slope_3d(1).to_device()
+    forms = ["plain", "mixed"] if args.form == "both" else [args.form]
+    out = {form: run_form(args, form, P, rank, world) for form in forms}
+    if world > 1:
+        torch.distributed.destroy_process_group()
     if rank != 0:
         return
+    head = out["mixed"] if "mixed" in out else out["plain"]
     K = args.steps
-    value_step = res["t_dev"] / K
-    e2e_step = res["t_e2e"] / K
-    ms, nt, nl = res["instr"]
+    value_step = head["t_dev"] / K
+    e2e_step = head["t_e2e"] / K
+    ms, nt, nl = head["instr"]
     peak, peak_kind = peaks()
-    spmv_bytes = res["n_blocks"] * (72 + 4) + (res["n_rows"] + 1) * 4 + 2 * 8 * res["n_dof"]
+    n_dof, n_blocks, n_rows = P.dmesh.n_dof, P.dmesh.n_blocks, P.dmesh.n_n
+    # fine-level 3x3 BSR SpMV: 72 B of values + 4 B column index per block, row pointers,
+    # x read once and y written once
+    spmv_bytes = n_blocks * (72 + 4) + (n_rows + 1) * 4 + 2 * 8 * n_dof
     spmv_ms = ms[0] / nt[0] if nt[0] else None
     achieved = spmv_bytes / (spmv_ms * 1e-3) / 1e9 if spmv_ms else None
-    counts = step_counts(res["steps"], res["amg"])
+    base = out["plain"] if "plain" in out else head
+    counts = step_counts(base)
+    counts.update(n_int=P.dmesh.n_int, n_dof=n_dof)
     cpu = None
     if not args.no_cpu_baseline and args.gpus == 1:
         try:
-            v, info = cpu_baseline_sample(P, counts, os.cpu_count() or 1, log=lambda *a: None)
+            S, smp = cpu_sample()
+            v, _ = cpu_step_seconds(S, smp, counts, P.dmesh.n_int, n_dof)
             cpu = dict(value=v, unit=UNIT, cores=int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1)),
-                       kind="reference",
-                       sample="reference MEX kernels (OpenMP, all cores) + oracle port for B*U, B'S, SpMV, MGS, "
-                              "AMG V-cycle; unit costs on a z=4 m slice (1/10 of the workload) scaled by size, "
-                              "weighted by the timed steps' Newton/Krylov counts")
+                       kind="port", sample=CPU_SAMPLE_TEXT)
         except Exception as exc:  # the CPU leg must not hide the GPU result
-            cpu = dict(value=None, unit=UNIT, cores=None, kind="reference", sample=f"failed: {exc}")
-    h2d = 2 * 8 * res["n_dof"]
-    d2h = 2 * 8 * res["n_dof"]
+            cpu = dict(value=None, unit=UNIT, cores=None, kind="port", sample=f"failed: {exc}")
+    h2d = 2 * 8 * n_dof
+    d2h = 2 * 8 * n_dof
+    forms_cfg = {}
+    for form, r in out.items():
+        forms_cfg[form] = dict(
+            s_per_step=r["t_dev"] / K, e2e_s_per_step=r["t_e2e"] / K, lambdas=r["lam"],
+            newton_iterations=[s["newton_iterations_total"] for s in r["steps"]],
+            linear_iterations=[s["linear_iterations"] for s in r["steps"]],
+            attempts=[s["attempts"] for s in r["steps"]], deflation_basis=r["basis"], init_s=round(r["t_init"], 2),
+            gpu_launches=r["launches"], amg_levels=[(l["rows"], l["block"]) for l in r["amg"]["levels"]])
+    if "plain" in out and "mixed" in out:
+        lp, lm = out["plain"]["lam"], out["mixed"]["lam"]
+        forms_cfg["lambda_rel_err_mixed_vs_plain"] = max(abs(a - b) / abs(a) for a, b in zip(lp, lm))
+        forms_cfg["speedup_mixed_vs_plain"] = out["plain"]["t_dev"] / out["mixed"]["t_dev"]
     line = dict(
         metric=METRIC, value=value_step, unit=UNIT, n_gpus=args.gpus, steps=K, warmup=args.warmup,
         ms_per_step=value_step * 1e3, higher_is_better=False, scaling="weak", vs_baseline=None,
-        dtype="f64" if args.form == "plain" else "f64 outer / f32 V-cycle", data="synthetic",
-        config=dict(workload=WORKLOAD, form=args.form, parallelism=f"replicas x{args.gpus}",
-                    solver="DFGMRES tol 1e-1 + AMG V-cycle", l2="working set > L2 (no flush needed)",
-                    lambdas=[round(x, 8) for x in res["lam"]],
-                    newton_iterations=[s["newton_iterations_total"] for s in res["steps"]],
-                    linear_iterations=[s["linear_iterations"] for s in res["steps"]],
-                    init_s=round(res["t_init"], 2)),
+        dtype="f64" if "mixed" not in out else "f64 (f32 V-cycle)", data="synthetic (seeded mesh and material)",
+        config=dict(workload=WORKLOAD, form="mixed" if "mixed" in out else "plain",
+                    parallelism=f"replicas x{args.gpus}", solver="DFGMRES tol 1e-1 + AMG V-cycle, Newton tol 1e-4",
+                    l2="working set > L2 (no flush needed)", forms=forms_cfg),
         e2e=dict(value=e2e_step, unit=UNIT, h2d_bytes_per_step=h2d, d2h_bytes_per_step=d2h),
-        gpu_launches=res["launches"],
-        clocks=res["clocks"],
-        roofline=dict(kernel="k_bsr_spmv<3,3> fine-level SpMV (FGMRES + V-cycle)", bound="hbm",
-                      achieved=achieved, peak=peak, unit="GB/s", frac=(achieved / peak if achieved else None),
-                      peak_kind=peak_kind, traffic=traffic_per_spmv(), algorithmic_bytes=spmv_bytes,
-                      launches=int(nl[0]), timed_launches=int(nt[0]), avg_ms=spmv_ms),
+        gpu_launches=head["launches"],
+        clocks=head["clocks"],
+        roofline=dict(kernel="k_bsr_spmv 3x3 FP64, fine level (Arnoldi, projection, smoother, residual)",
+                      bound="hbm", achieved=achieved, peak=peak, unit="GB/s",
+                      frac=(achieved / peak if achieved else None), peak_kind=peak_kind,
+                      traffic=traffic_per_spmv(), algorithmic_bytes_per_launch=spmv_bytes,
+                      launches=int(nl[0]), timed_launches=int(nt[0]), avg_ms=spmv_ms,
+                      other_kernels={name: dict(launches=int(nl[i]), avg_ms=(ms[i] / nt[i] if nt[i] else None))
+                                     for i, name in enumerate(["spmv3_f64", "spmv3_f32", "constitutive_S_DS",
+                                                               "constitutive_S", "assembly"]) if nl[i]}),
         cpu_baseline=cpu,
         counts=counts,
     )

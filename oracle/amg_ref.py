@@ -205,6 +205,8 @@ class Hierarchy:
                 break
             T, Bc, dead = tentative(agg, na, B, b, nns)
             lev["agg"] = agg
+            lev["T"] = T
+            lev["dead_next"] = dead
             # lambda_max(D^-1 A) by power iteration
             v = _init_vec(ndof)
             lmax = 1.0
@@ -262,7 +264,7 @@ class Hierarchy:
     def _dinv_mat(self, lev, M):
         b = lev["b"]
         n = lev["A"].shape[0] // b
-        D = sp.block_diag([lev["Dinv"][i] for i in range(n)], format="csr")
+        D = sp.bsr_matrix((lev["Dinv"], np.arange(n), np.arange(n + 1)), shape=(n * b, n * b)).tocsr()
         return D @ M
 
     def smooth(self, lev, x, rhs, x_zero):

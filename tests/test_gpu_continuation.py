@@ -1,0 +1,56 @@
+"""End-to-end parity of the device Newton/continuation path (n1 with a1-a6, b1-b4, c1-c3, d1).
+
+  * SSR indirect continuation on the GPU (DFGMRES + AMG at a linear tolerance of 1e-10, so
+    lambda carries no Krylov error) against the oracle's histories computed with a sparse
+    direct solver (tests/golden/ssr_oracle.npz, made by make_continuation_golden.py):
+    lambda and omega within 1e-6 relative, Newton iteration counts equal;
+  * the reference's stored run of slope_stability_2D_homo_SSR.ipynb (2D homogeneous slope,
+    h = 1/4, 83,280 unknowns, HYPRE-preconditioned DFGMRES at tolerance 1e-1, Newton 1e-4):
+    omega_init = 425.2321 and the final lambda 1.16411213 (both as printed there).  The Krylov
+    solves stop at 1e-1, so the AMG difference enters lambda at the 1e-5 level: the test
+    bound is 1e-4 relative.
+"""
+import os
+
+import numpy as np
+import pytest
+
+from slope_stability_octave_b200 import continuation, problems
+
+pytestmark = pytest.mark.gpu
+
+GOLDEN = os.path.join(os.path.dirname(__file__), "golden", "ssr_oracle.npz")
+
+CASES = {
+    "cfg0": (lambda: problems.slope_2d(0.5), problems.SSR_2D),
+    "small3d": (lambda: problems.slope_3d(1, dims=(15, 10, 15, 10, 10, 1)), problems.SSR_3D),
+}
+
+
+def run_gpu(P, params, tol, steps=None, solver_type="DFGMRES_B200"):
+    P.to_device()
+    solver = P.solver(solver_type, tol=tol, maxit=100)
+    p = params
+    U, lh, oh, um, st = continuation.SSR_indirect_continuation(
+        p["lambda_init"], p["d_lambda_init"], p["d_lambda_min"], p["d_lambda_diff_scaled_min"], p["step_max"],
+        p["omega_max_stop"], p["it_newt_max"], p["it_damp_max"], p["tol"], p["r_min"], None, P.dmesh.mask,
+        P.f_device(), P.cons, solver, max_steps_after_init=steps)
+    return np.asarray(lh), np.asarray(oh), st
+
+
+@pytest.mark.parametrize("case", sorted(CASES))
+def test_ssr_continuation_matches_oracle(cuda_device, case):
+    g = np.load(GOLDEN)
+    make, params = CASES[case]
+    lam_ref, om_ref, its_ref = g[f"{case}_lambda"], g[f"{case}_omega"], g[f"{case}_newton"]
+    lh, oh, st = run_gpu(make(), params, 1e-10, steps=len(its_ref))
+    assert lh.shape == lam_ref.shape
+    assert np.max(np.abs(lh - lam_ref) / np.abs(lam_ref)) <= 1e-6
+    assert np.max(np.abs(oh - om_ref) / np.abs(om_ref)) <= 1e-6
+    assert list(st["step_newton_iterations"]) == list(its_ref)
+
+
+def test_ssr_2d_reproduces_reference_notebook_run(cuda_device):
+    lh, oh, st = run_gpu(problems.slope_2d(0.25), problems.SSR_2D, 1e-1)
+    assert abs(oh[0] - 425.2321) / 425.2321 <= 1e-4
+    assert abs(lh[-1] - 1.16411213) / 1.16411213 <= 1e-4

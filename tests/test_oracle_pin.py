@@ -132,3 +132,16 @@ def test_reduction_matches_host_restatement():
             cb2, sp2 = fem.davis_reduction(c0, phi, psi, lam, davis)
             np.testing.assert_allclose(cb, cb2, rtol=1e-14)
             np.testing.assert_allclose(sp, sp2, rtol=1e-14)
+
+
+def test_oracle_continuation_reproduces_fixture():
+    """The oracle's 2D SSR continuation (direct solver) reproduces ssr_oracle.npz."""
+    import sys
+    sys.path.insert(0, os.path.join(os.path.dirname(__file__), "golden"))
+    from make_continuation_golden import cases, run_case
+    g = np.load(os.path.join(os.path.dirname(__file__), "golden", "ssr_oracle.npz"))
+    make, params = cases()["cfg0"]
+    lh, oh, its = run_case(make, params)
+    np.testing.assert_allclose(lh, g["cfg0_lambda"], rtol=1e-10)
+    np.testing.assert_allclose(oh, g["cfg0_omega"], rtol=1e-10)
+    assert list(its) == list(g["cfg0_newton"])
