@@ -66,6 +66,18 @@ int sg_constitutive2d_dev(const double *E, const double *c_bar, const double *si
                           const double *shear, const double *bulk, const double *lame,
                           int64_t n_int, double *S, double *DS, uint8_t *branch, void *stream);
 
+/* Allocation-free variant of sg_constitutive3d (no counterpart in the reference).  Same
+ * arguments and outputs; stages through a fixed array in the library's device image instead
+ * of cudaMalloc'd memory, on the legacy default stream, for callers that must not allocate
+ * device memory after start-up.  At most SG_NOALLOC_MAX_POINTS points per call (larger n_int
+ * returns SG_ERR_ARG with nothing launched).  The first call on a device sets up the array's
+ * address and should come before any stream capture starts.  One array per device: calls
+ * that overlap in time on the same device race on it and must be serialised by the caller. */
+#define SG_NOALLOC_MAX_POINTS 16384
+int sg_constitutive3d_noalloc(const double *E, const double *c_bar, const double *sin_phi,
+                              const double *shear, const double *bulk, const double *lame,
+                              int64_t n_int, double *S, double *DS, uint8_t *branch);
+
 /* (a4) Davis strength reduction, +CONSTITUTIVE_PROBLEM/reduction.m:25-58 (types 'A','B','C';
  * type 'C' is applied point-wise).  Device pointers. */
 int sg_reduction_dev(const double *c0, const double *phi, const double *psi, double lambda,
