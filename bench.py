@@ -331,7 +331,7 @@ def main():
         e2e=dict(value=e2e_step, unit=UNIT, h2d_bytes_per_step=h2d, d2h_bytes_per_step=d2h),
         gpu_launches=head["launches"],
         clocks=head["clocks"],
-        roofline=dict(kernel="k_bsr_spmv 3x3 FP64, fine level (Arnoldi, projection, smoother, residual)",
+        roofline=dict(kernel="k_spmv_blk 3x3 FP64, fine level (Arnoldi, projection, smoother, residual)",
                       bound="hbm", achieved=achieved, peak=peak, unit="GB/s",
                       frac=(achieved / peak if achieved else None), peak_kind=peak_kind,
                       traffic=traffic_per_spmv(), algorithmic_bytes_per_launch=spmv_bytes,

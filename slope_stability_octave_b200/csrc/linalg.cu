@@ -1,8 +1,8 @@
 // (c2) Node-block BSR SpMV and (c1, c3) Krylov vector kernels.
 //
-// SpMV: a group of G threads per block row; the group's lanes read consecutive blocks of the
-// row (contiguous b*b-value runs), accumulate b partial sums and combine them with warp
-// shuffles.  Rows are assigned in warp-uniform slots so the shuffles never diverge.
+// SpMV: a group of lanes per block row of the matrix (two lane mappings, see k_spmv_blk and
+// k_spmv_row); the lanes' partial sums are combined with warp shuffles.  Rows are assigned in
+// warp-uniform slots so the shuffles never diverge.
 // Dot products use a fixed two-stage tree (per-block partials, then one ordered pass), so
 // results are bitwise reproducible from run to run.
 #include <cuda_runtime.h>
@@ -18,13 +18,24 @@ namespace sg {
 template <typename T> struct Acc { using type = double; };
 template <> struct Acc<float> { using type = float; };
 
+// Two lane mappings, chosen per block shape from measurements on the SSR slope hierarchy
+// (fine 3x3, coarse 6x6, transfer 3x6 / 6x3):
+//
+// k_spmv_blk: G lanes per block row of the matrix, one block per lane per step (the lane reads
+//   the block's br*bc contiguous values).  Best for 3x3 (G = 32 at ~28 blocks per row:
+//   4.8 TB/s) and the short rows of P.
+// k_spmv_row: LPR lanes per block row of the matrix, BR lanes per block: lane (slot, a) reads
+//   row a of the group's slot-th block, so a warp's loads walk one contiguous run of SLOTS
+//   blocks; U steps are loaded before the first product.  Best for wide blocks (6x6: 2.3x
+//   the lane-per-block mapping, whose 288-byte lane stride spreads each load over 32 lines).
+// Both sum in a fixed order (reproducible bitwise from run to run).
 template <int BR, int BC, int G, typename VT, typename XT>
-__global__ void __launch_bounds__(256) k_bsr_spmv(int64_t nrows, const int32_t *__restrict__ rp,
+__global__ void __launch_bounds__(256) k_spmv_blk(int64_t nrows, const int32_t *__restrict__ rp,
                                                   const int32_t *__restrict__ col, const VT *__restrict__ vals,
                                                   const XT *__restrict__ x, XT *__restrict__ y, double alpha,
                                                   double beta, const XT *__restrict__ bvec, int mode) {
     using A = typename Acc<XT>::type;
-    constexpr int GPW = 32 / G;  // groups per warp
+    constexpr int GPW = 32 / G;  // rows per warp
     const int lane = threadIdx.x & 31, g = lane / G, gl = lane - g * G;
     const int64_t warp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
     const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
@@ -63,24 +74,93 @@ __global__ void __launch_bounds__(256) k_bsr_spmv(int64_t nrows, const int32_t *
     }
 }
 
-// Group width: enough lanes per row to cover the row's blocks in a few passes (fine level,
-// ~28 blocks per row: 8 lanes; coarse 6x6 levels, ~100 blocks per row: a full warp).
+template <int BR, int BC, int LPR, int U, typename VT, typename XT>
+__global__ void __launch_bounds__(256) k_spmv_row(int64_t nrows, const int32_t *__restrict__ rp,
+                                                  const int32_t *__restrict__ col, const VT *__restrict__ vals,
+                                                  const XT *__restrict__ x, XT *__restrict__ y, double alpha,
+                                                  double beta, const XT *__restrict__ bvec, int mode) {
+    using A = typename Acc<XT>::type;
+    constexpr int BB = BR * BC, SLOTS = LPR / BR, RPW = 32 / LPR;  // rows per warp
+    const int lane = threadIdx.x & 31, rg = lane / LPR, li = lane - rg * LPR;
+    const int slot = li / BR, a = li - slot * BR;
+    const bool active = slot < SLOTS;
+    const int64_t warp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+    const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    for (int64_t base = warp * RPW; base < nrows; base += nwarps * RPW) {
+        const int64_t row = base + rg;
+        A acc = 0;
+        if (row < nrows && active) {
+            const int32_t p0 = rp[row] + slot, p1 = rp[row + 1];
+            for (int32_t p = p0; p < p1; p += U * SLOTS) {
+                int64_t c[U];
+#pragma unroll
+                for (int u = 0; u < U; ++u) {
+                    const int32_t q = p + u * SLOTS;
+                    c[u] = q < p1 ? col[q] : -1;
+                }
+                A vv[U][BC], xv[U][BC];
+#pragma unroll
+                for (int u = 0; u < U; ++u) {
+                    const VT *v = vals + (int64_t)(p + u * SLOTS) * BB + a * BC;
+                    const XT *xc = x + (c[u] < 0 ? 0 : c[u]) * BC;
+                    if (c[u] >= 0) {
+#pragma unroll
+                        for (int b = 0; b < BC; ++b) {
+                            vv[u][b] = (A)__ldg(v + b);
+                            xv[u][b] = (A)__ldg(xc + b);
+                        }
+                    } else {
+#pragma unroll
+                        for (int b = 0; b < BC; ++b) vv[u][b] = xv[u][b] = 0;
+                    }
+                }
+#pragma unroll
+                for (int u = 0; u < U; ++u)
+#pragma unroll
+                    for (int b = 0; b < BC; ++b) acc += vv[u][b] * xv[u][b];
+            }
+        }
+        // sum over the group's slots for component a (all lanes take part in the shuffles)
+        A tot = 0;
+        const int g0 = rg * LPR;
+#pragma unroll
+        for (int sl = 0; sl < SLOTS; ++sl) tot += __shfl_sync(0xffffffffu, acc, g0 + sl * BR + (active ? a : 0));
+        if (row < nrows && active && slot == 0) {
+            const int64_t k = row * BR + a;
+            if (mode == 1) y[k] = (XT)((A)bvec[k] - tot);
+            else if (beta == 0.0) y[k] = (XT)(alpha * tot);
+            else y[k] = (XT)(alpha * tot + beta * (A)y[k]);
+        }
+    }
+}
+
 template <int BR, int BC, typename VT, typename XT>
 static void spmv_launch(int64_t nrows, int64_t nblk, const int32_t *rp, const int32_t *col, const VT *vals,
                         const XT *x, XT *y, double alpha, double beta, const XT *bvec, int mode, cudaStream_t st) {
     const double avg = nblk > 0 && nrows > 0 ? (double)nblk / (double)nrows : 8.0;
-    const int G = avg >= 64 ? 32 : (avg >= 24 ? ((BR * BC >= 9) ? 8 : 16) : (avg >= 10 ? 8 : 4));
-    const int64_t threads = nrows * G;
     // the node-block shapes of the fine level are the ones timed for the roofline report
     constexpr bool fine = (BR == BC) && (BR == 3 || BR == 2);
     InstrToken tk;
     if (fine) tk = instr_begin(sizeof(VT) == 8 ? IK_SPMV3_F64 : IK_SPMV3_F32, st);
-    const unsigned grid = grid_for(threads, 256, 16);
-    switch (G) {
-        case 32: k_bsr_spmv<BR, BC, 32, VT, XT><<<grid, 256, 0, st>>>(nrows, rp, col, vals, x, y, alpha, beta, bvec, mode); break;
-        case 16: k_bsr_spmv<BR, BC, 16, VT, XT><<<grid, 256, 0, st>>>(nrows, rp, col, vals, x, y, alpha, beta, bvec, mode); break;
-        case 8: k_bsr_spmv<BR, BC, 8, VT, XT><<<grid, 256, 0, st>>>(nrows, rp, col, vals, x, y, alpha, beta, bvec, mode); break;
-        default: k_bsr_spmv<BR, BC, 4, VT, XT><<<grid, 256, 0, st>>>(nrows, rp, col, vals, x, y, alpha, beta, bvec, mode); break;
+    constexpr bool wide = BR == 6 && BC == 6;
+    constexpr bool tall_f64 = BR == 6 && BC == 3 && sizeof(VT) == 8;
+    if (wide || tall_f64) {
+        const int lpr = avg >= 48.0 ? 32 : 16;
+        const unsigned grid = grid_for(nrows * lpr, 256, 16);
+        if (lpr == 32) {
+            if (wide) k_spmv_row<BR, BC, 32, 1, VT, XT><<<grid, 256, 0, st>>>(nrows, rp, col, vals, x, y, alpha, beta, bvec, mode);
+            else k_spmv_row<BR, BC, 32, 3, VT, XT><<<grid, 256, 0, st>>>(nrows, rp, col, vals, x, y, alpha, beta, bvec, mode);
+        } else {
+            k_spmv_row<BR, BC, 16, 2, VT, XT><<<grid, 256, 0, st>>>(nrows, rp, col, vals, x, y, alpha, beta, bvec, mode);
+        }
+    } else {
+        const int G = avg >= 16.0 ? 32 : (avg >= 8.0 ? 16 : 8);
+        const unsigned grid = grid_for(nrows * G, 256, 16);
+        switch (G) {
+            case 32: k_spmv_blk<BR, BC, 32, VT, XT><<<grid, 256, 0, st>>>(nrows, rp, col, vals, x, y, alpha, beta, bvec, mode); break;
+            case 16: k_spmv_blk<BR, BC, 16, VT, XT><<<grid, 256, 0, st>>>(nrows, rp, col, vals, x, y, alpha, beta, bvec, mode); break;
+            default: k_spmv_blk<BR, BC, 8, VT, XT><<<grid, 256, 0, st>>>(nrows, rp, col, vals, x, y, alpha, beta, bvec, mode); break;
+        }
     }
     if (fine) instr_end(tk, st);
 }
