@@ -103,7 +103,7 @@ class CPUSample:
         E = sp.csr_matrix((np.ones(self.nQ), (self.q, np.arange(self.nQ))), shape=(n, self.nQ))
         Kfull = (E @ self.K @ E.T + sp.diags(fixed.astype(float))).tocsr()
         self.amg_matrix = Kfull
-        self.amg = Hierarchy(Kfull, B_nullspace, self.dim, fixed=fixed, theta=0.05)
+        self.amg = Hierarchy(Kfull, B_nullspace, self.dim, fixed=fixed, theta=0.02)
         log(f"cpu AMG restatement built {time.perf_counter() - t0:.1f}s")
 
     def amg_numeric_resetup(self, A):

@@ -60,7 +60,7 @@ def elastic_problem():
     return P, K
 
 
-@pytest.mark.parametrize("theta", [0.05, 0.0])
+@pytest.mark.parametrize("theta", [0.02, 0.0])
 def test_amg_hierarchy_and_vcycle_match_restatement(cuda_device, theta):
     P, K = elastic_problem()
     amg = AMG(P.dmesh, theta=theta)
