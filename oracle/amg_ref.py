@@ -174,7 +174,7 @@ def _init_vec(n):
 
 
 class Hierarchy:
-    def __init__(self, A, B, b, fixed=None, coarse_size=1200, max_levels=10, cheb_degree=2, cheb_ratio=10.0,
+    def __init__(self, A, B, b, fixed=None, coarse_size=1200, max_levels=10, cheb_degree=3, cheb_ratio=10.0,
                  power_its=10, omega_scale=4.0 / 3.0, theta=0.0, theta_coarse=None, filtered_smoothing=False):
         self.deg, self.ratio = cheb_degree, cheb_ratio
         A = sp.csr_matrix(A)
@@ -234,7 +234,7 @@ class Hierarchy:
             active = ~dead.reshape(na, nns).all(axis=1)
 
     @classmethod
-    def from_levels(cls, mats, prolongators, blocks, cheb_degree=2, cheb_ratio=10.0, power_its=10):
+    def from_levels(cls, mats, prolongators, blocks, cheb_degree=3, cheb_ratio=10.0, power_its=10):
         """V-cycle on a given hierarchy: mats[l] (level matrices), prolongators[l] (l < L-1);
         smoother data (block inverse, lambda_max) recomputed the same way as the device."""
         self = cls.__new__(cls)

@@ -12,12 +12,13 @@
 //   numerics (device, every update)      block-Jacobi inverse, lambda_max(D^-1 A) by power
 //       iteration, P = T - omega D^-1 A T (omega = 4 / (3 lambda_max)), R = P', A P,
 //       A_c = P' (A P); coarsest level: dense Gauss-Jordan inverse
-//   apply (device)                       V(1,1) cycle with degree-2 Chebyshev smoothing on
+//   apply (device)                       V(1,1) cycle with degree-3 Chebyshev smoothing on
 //       D^-1 A over [lambda_max / 10, 1.1 lambda_max], in FP64 or FP32 (mixed precision)
 //
-// Defaults (strength threshold 0.02 on every level, Chebyshev interval ratio 10) were chosen
-// on the SSR continuation of the 40 m slope: against threshold 0.05 and ratio 30 they cut the
-// FGMRES iterations per continuation step from ~265 to ~51 and the step time 3.5x.
+// Defaults (strength threshold 0.02 on every level, Chebyshev degree 3 on the interval ratio
+// 10) were chosen on the SSR continuation of the 40 m slope: against threshold 0.05, degree 2
+// and ratio 30 they cut the FGMRES iterations per continuation step from ~265 to ~36 and the
+// step time about 4x.
 //
 // Every product is a gather over a precomputed list, so the numeric set-up uses no atomics
 // and is deterministic.
@@ -83,7 +84,7 @@ struct Level {
 struct AmgOptions {
     int max_levels = 10;
     int coarse_size = 1200;   // stop coarsening at this many DOFs
-    int cheb_degree = 2;
+    int cheb_degree = 3;
     double cheb_ratio = 10.0; // smoothing interval [lmax / ratio, 1.1 lmax]
     int power_its = 10;
     int mixed = 0;            // 1: FP32 V-cycle

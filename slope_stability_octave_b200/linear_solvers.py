@@ -59,7 +59,7 @@ class AMG:
     numeric set-up on the device (the pattern is fixed per mesh)."""
 
     def __init__(self, dmesh: DeviceMesh, coord=None, mixed=False, max_levels=10, coarse_size=1200,
-                 cheb_degree=2, cheb_ratio=10.0, power_its=10, theta=0.02):
+                 cheb_degree=3, cheb_ratio=10.0, power_its=10, theta=0.02):
         self.dmesh = dmesh
         coord = dmesh.mesh.coord if coord is None else coord
         Z = near_null_space_elasticity(coord, dmesh.mesh.Q)
