@@ -54,13 +54,22 @@ __device__ __forceinline__ void sylvester(const double tsq[6], const double t[6]
     for (int i = 3; i < 6; ++i) P[i] = scale * (tsq[i] - bc_sum * t[i]);
 }
 
-// Writes S[6]; when ds != nullptr writes the 6x6 tangent at ds[i + 6*j] (column-major).
-template <bool WANT_DS>
-__device__ __forceinline__ int mc3d_point(const double E[6], double c_bar, double sin_phi,
-                                          double shear, double lame, double S[6], double *ds) {
+// Quantities shared by every branch: the stress-representation strain t, t^2, I1, the
+// ordered principal strains e1 >= e2 >= e3 and the trial yield value.
+struct MC3Pre {
+    double t[6], tsq[6], I1, e1, e2, e3, f_tr;
+};
+
+__device__ __forceinline__ void mc3d_prefix(const double E[6], double c_bar, double sin_phi, double shear,
+                                            double lame, MC3Pre &q) {
     const double sp = sin_phi;
-    const double t[6] = {E[0], E[1], E[2], 0.5 * E[3], 0.5 * E[4], 0.5 * E[5]};
-    double tsq[6];
+    double *t = q.t, *tsq = q.tsq;
+    t[0] = E[0];
+    t[1] = E[1];
+    t[2] = E[2];
+    t[3] = 0.5 * E[3];
+    t[4] = 0.5 * E[4];
+    t[5] = 0.5 * E[5];
     tsq[0] = t[0] * t[0] + t[3] * t[3] + t[5] * t[5];
     tsq[1] = t[1] * t[1] + t[3] * t[3] + t[4] * t[4];
     tsq[2] = t[2] * t[2] + t[4] * t[4] + t[5] * t[5];
@@ -87,7 +96,49 @@ __device__ __forceinline__ int mc3d_point(const double E[6], double c_bar, doubl
     const double e3 = -2.0 * rq * cos(theta) + I1 / 3.0;
 
     const double f_tr = 2.0 * shear * ((1.0 + sp) * e1 - (1.0 - sp) * e3) + 2.0 * lame * sp * I1 - c_bar;
-    if (f_tr <= 0.0) {
+    q.I1 = I1;
+    q.e1 = e1;
+    q.e2 = e2;
+    q.e3 = e3;
+    q.f_tr = f_tr;
+}
+
+// The branch the reference's kernel takes for this point (its tests, in its order).
+__device__ __forceinline__ int mc3d_classify(const MC3Pre &q, double c_bar, double sp, double shear, double lame) {
+    if (q.f_tr <= 0.0) return BR_ELASTIC;
+    const double e1 = q.e1, e2 = q.e2, e3 = q.e3, I1 = q.I1;
+    const double g_sl = (e1 - e2) / (1.0 + sp);
+    const double g_sr = (e2 - e3) / (1.0 - sp);
+    const double den_s = 4.0 * lame * sp * sp + 4.0 * shear * (1.0 + sp * sp);
+    const double dl_s = q.f_tr / den_s;
+    if (dl_s <= g_sl && dl_s <= g_sr) return BR_SMOOTH;
+    if (g_sl < g_sr) {
+        const double den_l = 4.0 * lame * sp * sp + shear * (1.0 + sp) * (1.0 + sp) +
+                             2.0 * shear * (1.0 - sp) * (1.0 - sp);
+        const double dl_l =
+            (shear * ((1.0 + sp) * (e1 + e2) - 2.0 * (1.0 - sp) * e3) + 2.0 * lame * sp * I1 - c_bar) / den_l;
+        const double g_la = (e1 + e2 - 2.0 * e3) / (3.0 - sp);
+        if (dl_l >= g_sl && dl_l <= g_la) return BR_LEFT;
+    }
+    if (g_sl > g_sr) {
+        const double den_r = 4.0 * lame * sp * sp + 2.0 * shear * (1.0 + sp) * (1.0 + sp) +
+                             shear * (1.0 - sp) * (1.0 - sp);
+        const double dl_r =
+            (shear * (2.0 * (1.0 + sp) * e1 - (1.0 - sp) * (e2 + e3)) + 2.0 * lame * sp * I1 - c_bar) / den_r;
+        const double g_ra = (2.0 * e1 - e2 - e3) / (3.0 + sp);
+        if (dl_r >= g_sr && dl_r <= g_ra) return BR_RIGHT;
+    }
+    return BR_APEX;
+}
+
+// Stress (and tangent when WANT_DS) of branch `br` from the shared quantities; writes S[6] and
+// ds[i + 6*j] (column-major).  The formulas are those of the reference's branch code.
+template <bool WANT_DS>
+__device__ __forceinline__ void mc3d_finish(const MC3Pre &q, int br, double c_bar, double sp, double shear,
+                                            double lame, double S[6], double *ds) {
+    const double *t = q.t, *tsq = q.tsq;
+    const double I1 = q.I1, e1 = q.e1, e2 = q.e2, e3 = q.e3, f_tr = q.f_tr;
+    if (br == BR_ELASTIC) {
         const double v = lame * I1, g2 = 2.0 * shear;
         S[0] = v + g2 * t[0];
         S[1] = v + g2 * t[1];
@@ -102,15 +153,11 @@ __device__ __forceinline__ int mc3d_point(const double E[6], double c_bar, doubl
                 for (int i = 0; i < 6; ++i)
                     ds[i + 6 * j] = (i < 3 && j < 3 ? lame : 0.0) + (i == j ? (i < 3 ? g2 : shear) : 0.0);
         }
-        return BR_ELASTIC;
+        return;
     }
-
-    const double g_sl = (e1 - e2) / (1.0 + sp);
-    const double g_sr = (e2 - e3) / (1.0 - sp);
-    const double den_s = 4.0 * lame * sp * sp + 4.0 * shear * (1.0 + sp * sp);
-    const double dl_s = f_tr / den_s;
-
-    if (dl_s <= g_sl && dl_s <= g_sr) {
+    if (br == BR_SMOOTH) {
+        const double den_s = 4.0 * lame * sp * sp + 4.0 * shear * (1.0 + sp * sp);
+        const double dl_s = f_tr / den_s;
         const double k1 = 1.0 / ((e1 - e2) * (e1 - e3));
         const double k2 = 1.0 / ((e2 - e1) * (e2 - e3));
         const double k3 = 1.0 / ((e3 - e1) * (e3 - e2));
@@ -147,16 +194,14 @@ __device__ __forceinline__ int mc3d_point(const double E[6], double c_bar, doubl
                     ds[j + 6 * i] = v;
                 }
         }
-        return BR_SMOOTH;
+        return;
     }
-
-    if (g_sl < g_sr) {
+    if (br == BR_LEFT) {
         const double den_l = 4.0 * lame * sp * sp + shear * (1.0 + sp) * (1.0 + sp) +
                              2.0 * shear * (1.0 - sp) * (1.0 - sp);
         const double dl_l =
             (shear * ((1.0 + sp) * (e1 + e2) - 2.0 * (1.0 - sp) * e3) + 2.0 * lame * sp * I1 - c_bar) / den_l;
-        const double g_la = (e1 + e2 - 2.0 * e3) / (3.0 - sp);
-        if (dl_l >= g_sl && dl_l <= g_la) {
+        {
             const double k3 = 1.0 / ((e3 - e1) * (e3 - e2));
             double P3[6], P12[6];
             sylvester(tsq, t, e1 + e2, e1 * e2, k3, P3);
@@ -187,17 +232,15 @@ __device__ __forceinline__ int mc3d_point(const double E[6], double c_bar, doubl
                         ds[j + 6 * i] = v;
                     }
             }
-            return BR_LEFT;
+            return;
         }
     }
-
-    if (g_sl > g_sr) {
+    if (br == BR_RIGHT) {
         const double den_r = 4.0 * lame * sp * sp + 2.0 * shear * (1.0 + sp) * (1.0 + sp) +
                              shear * (1.0 - sp) * (1.0 - sp);
         const double dl_r =
             (shear * (2.0 * (1.0 + sp) * e1 - (1.0 - sp) * (e2 + e3)) + 2.0 * lame * sp * I1 - c_bar) / den_r;
-        const double g_ra = (2.0 * e1 - e2 - e3) / (3.0 + sp);
-        if (dl_r >= g_sr && dl_r <= g_ra) {
+        {
             const double k1 = 1.0 / ((e1 - e2) * (e1 - e3));
             double P1[6], P23[6];
             sylvester(tsq, t, e2 + e3, e2 * e3, k1, P1);
@@ -228,10 +271,10 @@ __device__ __forceinline__ int mc3d_point(const double E[6], double c_bar, doubl
                         ds[j + 6 * i] = v;
                     }
             }
-            return BR_RIGHT;
+            return;
         }
     }
-
+    // apex
     const double sa = c_bar / (2.0 * sp);
     S[0] = sa;
     S[1] = sa;
@@ -243,7 +286,17 @@ __device__ __forceinline__ int mc3d_point(const double E[6], double c_bar, doubl
 #pragma unroll
         for (int k = 0; k < 36; ++k) ds[k] = 0.0;
     }
-    return BR_APEX;
+}
+
+// Writes S[6]; when ds != nullptr writes the 6x6 tangent at ds[i + 6*j] (column-major).
+template <bool WANT_DS>
+__device__ __forceinline__ int mc3d_point(const double E[6], double c_bar, double sin_phi,
+                                          double shear, double lame, double S[6], double *ds) {
+    MC3Pre q;
+    mc3d_prefix(E, c_bar, sin_phi, shear, lame, q);
+    const int br = mc3d_classify(q, c_bar, sin_phi, shear, lame);
+    mc3d_finish<WANT_DS>(q, br, c_bar, sin_phi, shear, lame, S, ds);
+    return br;
 }
 
 // 2D plane-strain variant.  E = (e11, e22, g12); S = (s11, s22, s12, s33); ds 3x3 column-major.
