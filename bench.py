@@ -54,6 +54,8 @@ def parse():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--form", default="both", choices=["both", "plain", "mixed"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--workload", default="ssr", choices=["ssr", "box"],
+                    help="ssr: the SSR continuation step (headline); box: the return-map microbenchmark")
     return ap.parse_args()
 
 
@@ -260,12 +262,127 @@ def reference_arm(args, rank, world):
     return line
 
 
+BOX_METRIC = "ms per return-map pass (S and DS), structured box 80x40x40 m, 8,448,000 points"
+BOX_WORKLOAD = ("box 80x40x40 m, 6 P2 tets per unit cell (768,000 tets), 11-point rule: 8,448,000 points; "
+                "seeded strains with the five return-map branches at 20 % each in random order; c ~ U[5,15] kPa, "
+                "phi ~ U[25,45] deg, psi = 0, E = 40 MPa, nu = 0.3")
+BOX_SAMPLE = 1 << 20
+
+
+def box_cpu_ms(n_full, threads, reps=3):
+    """The reference's own return-map MEX (oracle/_ref, OpenMP on all host threads) on the
+    first 2^20 points of the same seeded set, scaled to the full point count."""
+    from oracle import native
+    from slope_stability_octave_b200 import workloads
+    d = workloads.constitutive_points(BOX_SAMPLE, seed=20261203)
+    args = (d["E"], d["c_bar"], d["sin_phi"], d["shear"], d["bulk"], d["lame"])
+    native.ref_constitutive(3, *args, want_ds=True)
+    best = float("inf")
+    for _ in range(reps):
+        t0 = time.perf_counter()
+        native.ref_constitutive(3, *args, want_ds=True)
+        best = min(best, time.perf_counter() - t0)
+    return best * 1e3 * n_full / BOX_SAMPLE
+
+
+def run_box(args, rank):
+    """Return-map microbenchmark: S and DS for every point of the box, inputs resident
+    (value), and through the host-buffer drop-in entry point with the copies (e2e)."""
+    import numpy as np
+    import torch
+
+    from slope_stability_octave_b200 import _lib
+    from slope_stability_octave_b200.device import cur_stream, ptr
+    from slope_stability_octave_b200.kernel_bench import points_on_device
+
+    n = 8448000
+    dev = torch.device("cuda", torch.cuda.current_device())
+    pts = points_on_device(n, "shuffled", dev)
+    S = torch.empty((n, 6), dtype=torch.float64, device=dev)
+    DS = torch.empty((n, 36), dtype=torch.float64, device=dev)
+    L = _lib.lib()
+    st = cur_stream()
+    cargs = [ptr(pts[k]) for k in ("E", "c_bar", "sin_phi", "shear", "bulk", "lame")]
+
+    def sds():
+        _lib.check(L.sg_constitutive3d_dev(*cargs, n, ptr(S), ptr(DS), None, st), "sg_constitutive3d_dev")
+
+    for _ in range(args.warmup):
+        sds()
+    torch.cuda.synchronize()
+    clocks = ClockSampler(torch.cuda.current_device()).start()
+    L.sg_launch_count(1)
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+    ev[0].record()
+    for _ in range(args.steps):
+        sds()
+    ev[1].record()
+    torch.cuda.synchronize()
+    launches = int(L.sg_launch_count(1))
+    clk = clocks.stop()
+    ms = ev[0].elapsed_time(ev[1]) / args.steps
+    # e2e: the drop-in host-buffer entry point (the MEX arguments), copies included
+    host = {k: pts[k].cpu().numpy() for k in pts}
+    Sh = np.empty((n, 6))
+    DSh = np.empty((n, 36))
+    hargs = [host[k].ctypes.data_as(C.c_void_p) for k in ("E", "c_bar", "sin_phi", "shear", "bulk", "lame")]
+    _lib.call("sg_constitutive3d", *hargs, n, Sh.ctypes.data_as(C.c_void_p), DSh.ctypes.data_as(C.c_void_p), None)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        _lib.call("sg_constitutive3d", *hargs, n, Sh.ctypes.data_as(C.c_void_p), DSh.ctypes.data_as(C.c_void_p),
+                  None)
+    e2e_ms = (time.perf_counter() - t0) * 1e3 / args.steps
+    peak, peak_kind = peaks()
+    nbytes = n * 416
+    achieved = nbytes / (ms * 1e-3) / 1e9
+    cpu = None
+    if not args.no_cpu_baseline:
+        threads = os.cpu_count() or 1
+        os.environ.setdefault("OMP_NUM_THREADS", str(threads))
+        cpu = dict(value=box_cpu_ms(n, threads), unit="ms/pass", cores=int(os.environ["OMP_NUM_THREADS"]),
+                   kind="reference",
+                   sample="reference constitutive_problem_3D_SDS_mex (its C sources compiled with -O2 -fopenmp) "
+                          "on the first 2^20 points of the seeded set, best of 3, scaled to 8,448,000 points")
+    line = dict(metric=BOX_METRIC, value=ms, unit="ms/pass", n_gpus=args.gpus, steps=args.steps,
+                warmup=args.warmup, ms_per_step=ms, higher_is_better=False, scaling="weak", vs_baseline=None,
+                dtype="f64", data="synthetic (seeded points)",
+                config=dict(workload=BOX_WORKLOAD, l2="3.5 GB per pass > L2 (no flush needed)"),
+                e2e=dict(value=e2e_ms, unit="ms/pass", h2d_bytes_per_step=n * 80, d2h_bytes_per_step=n * 336),
+                gpu_launches=launches, clocks=clk,
+                roofline=dict(kernel="k_mc3d<S and DS>", bound="hbm", achieved=achieved, peak=peak, unit="GB/s",
+                              frac=achieved / peak, peak_kind=peak_kind, traffic=None,
+                              algorithmic_bytes_per_launch=nbytes),
+                cpu_baseline=cpu)
+    print(json.dumps(line))
+
+
+def box_reference_arm(args, rank):
+    if rank != 0:
+        return
+    threads = os.cpu_count() or 1
+    os.environ.setdefault("OMP_NUM_THREADS", str(threads))
+    vals = [box_cpu_ms(8448000, threads, reps=1) for _ in range(args.warmup + args.steps)][args.warmup:]
+    value = sum(vals) / len(vals)
+    line = dict(metric=BOX_METRIC, value=value, unit="ms/pass", n_gpus=args.gpus, steps=args.steps,
+                warmup=args.warmup, ms_per_step=value, higher_is_better=False, scaling="weak", vs_baseline=None,
+                dtype="f64", data="synthetic (seeded points)", impl="reference",
+                config=dict(workload=BOX_WORKLOAD),
+                cpu_baseline=dict(value=value, unit="ms/pass", cores=int(os.environ["OMP_NUM_THREADS"]),
+                                  kind="reference",
+                                  sample="constitutive_problem_3D_SDS_mex on 2^20 points, scaled to 8,448,000"),
+                e2e=dict(value=value, unit="ms/pass", h2d_bytes_per_step=0, d2h_bytes_per_step=0))
+    print(json.dumps(line))
+
+
 def main():
     args = parse()
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     if args.impl == "reference":
-        reference_arm(args, rank, world)
+        if args.workload == "box":
+            box_reference_arm(args, rank)
+        else:
+            reference_arm(args, rank, world)
         return
     import datetime
 
@@ -275,6 +392,11 @@ def main():
     if world > 1:
         torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
                                              device_id=torch.device("cuda", torch.cuda.current_device()))
+    if args.workload == "box":
+        run_box(args, rank)
+        if world > 1:
+            torch.distributed.destroy_process_group()
+        return
     from slope_stability_octave_b200 import problems
     P = problems.slope_3d(1).to_device()
     forms = ["plain", "mixed"] if args.form == "both" else [args.form]
