@@ -74,6 +74,11 @@ class OracleConstitutive:
         self._stress(U, True)
         return self.build_F()
 
+    def elastic_K(self):
+        """K_elast(Q, Q) (the elastic values of init_K_r_pattern, CONSTITUTIVE.m:393-464)."""
+        n = self.pat.n_Q
+        return sp.csc_matrix((self.pat.V_elast, (self.pat.ref_I - 1, self.pat.ref_J - 1)), shape=(n, n))
+
     def build_K_r_QQ_vals(self, r):
         d3 = self.dphi[2] if self.dim == 3 else None
         Vt = native.assemble(self.dim, self.dphi[0], self.dphi[1], d3, self.DS, self.pat.weight, self.smap, self.n_q,
@@ -385,3 +390,113 @@ def SSR_indirect_continuation(p, Q, f, cons, solver, max_steps_after_init=None):
         if n_omega >= 5 or step >= p["step_max"]:
             break
     return np.array(lambda_hist), np.array(omega_hist), newton_its, U
+
+
+# ---------------------------------------------------------------------------- limit load
+
+
+def newton_ind_LL(U_ini, t_ini, omega, it_newt_max, it_damp_max, tol, r_min, Q, f, cons, solver):
+    """newton_ind_LL.m:55-167: F(U) = t f with f(Q)' U(Q) = omega; returns (U, t, flag, it)."""
+    U = U_ini.copy()
+    t = float(t_ini)
+    fQ = f[Q]
+    norm_f = np.linalg.norm(fQ)
+    r, it, flag, compute = r_min, 0, 0, True
+    F = None
+    while True:
+        it += 1
+        if compute:
+            F = cons.build_F_and_DS_reduced(U)
+        criterion = np.linalg.norm(F[Q] - t * fQ)
+        rel = criterion / norm_f
+        if criterion < tol * norm_f and it > 1:
+            break
+        K = cons.build_K_r_QQ_vals(r)
+        solver.setup_preconditioner(K)
+        solver.A_orthogonalize(K)
+        W, _ = _solveQ(solver, K, f, Q)
+        V, _ = _solveQ(solver, K, t * f - F, Q)
+        d_t = -(fQ @ V[Q]) / (fQ @ W[Q])
+        dU = V + d_t * W
+        alpha = damping(it_damp_max, U, dU, F, F * 0, cons)   # newton_ind_LL.m:134 passes f = 0
+        compute = True
+        if alpha < 1e-1:
+            if alpha == 0:
+                compute = False
+                r *= 2
+            else:
+                r *= 2 ** 0.25
+        else:
+            solver.expand_deflation_basis(W[Q])
+            solver.expand_deflation_basis(V[Q])
+            if alpha > 0.5:
+                r = max(r / math.sqrt(2), r_min)
+        if alpha == 0 and r > 1:
+            flag = 1
+            break
+        U = U + alpha * dU
+        U = omega * U / (fQ @ U[Q])
+        t = t + d_t
+        if math.isnan(rel) or it == it_newt_max:
+            flag = 1
+            break
+    return U, t, flag, it
+
+
+def LL_elastic_start(Q, f, cons, solver):
+    """The LL scripts' start (slope_stability_3D_homo_LL.m:121-129): elastic solution at
+    lambda = 1, omega increment one fifth of its work, U_elast scaled by 1/5."""
+    cons.reduction(1.0)
+    K = cons.elastic_K()
+    solver.setup_preconditioner(K)
+    U, _ = _solveQ(solver, K, f, Q)
+    solver.expand_deflation_basis(U[Q])
+    omega_el = f[Q] @ U[Q]
+    return U / 5, omega_el / 5
+
+
+def LL_indirect_continuation(d_omega_ini, d_t_min, step_max, omega_max, it_newt_max, it_damp_max, tol, r_min,
+                             U_elast, Q, f, cons, solver, max_steps=None):
+    """LL_indirect_continuation.m:47-158; returns (t_hist, omega_hist, newton_its, U) with the
+    reference's leading zero entries."""
+    omega = omega_old = 0.0
+    d_omega = d_omega_ini
+    t = 0.0
+    U = U_elast.copy()
+    U_old = U.copy()
+    U_ini = U.copy()
+    n_omega, step, accepted = 0, 1, 0
+    t_hist, omega_hist, its = [0.0], [0.0], []
+    while True:
+        omega_it = omega + d_omega
+        if omega_it > omega_max:
+            omega_it = omega_max
+            d_omega = omega_it - omega
+        if step > 1:
+            U_ini = d_omega * (U - U_old) / (omega - omega_old) + U
+        U_it, t_it, flag, nit = newton_ind_LL(U_ini, t, omega_it, it_newt_max, it_damp_max, tol, r_min, Q, f, cons,
+                                              solver.copy())
+        if flag == 1:
+            d_omega /= 2
+            n_omega += 1
+        else:
+            step += 1
+            accepted += 1
+            U_old, U = U, U_it
+            solver.expand_deflation_basis(U[Q])
+            omega_old, omega = omega, omega_it
+            d_t = t_it - t
+            t = t_it
+            n_omega = 0
+            omega_hist.append(omega)
+            t_hist.append(t)
+            its.append(nit)
+            if d_t < d_t_min:
+                break
+            if nit < 20 and step > 2 and (t_hist[step - 1] - t_hist[step - 2]) < 0.9 * (t_hist[step - 2] - t_hist[step - 3]):
+                d_omega = 2 * d_omega
+            if max_steps is not None and accepted >= max_steps:
+                break
+        if n_omega >= 5 or omega >= omega_max or step >= step_max:
+            break
+    return np.array(t_hist), np.array(omega_hist), its, U

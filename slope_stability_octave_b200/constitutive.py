@@ -160,6 +160,16 @@ class CONSTITUTIVE:
         self.pattern_initialized = True
         return self
 
+    def elastic_K_QQ(self):
+        """K_elast(Q, Q) on the device pattern, Dirichlet rows and columns replaced by the
+        identity (the matrix the LL scripts solve for the elastic start)."""
+        if not self.pattern_initialized:
+            self.init_K_r_pattern()
+        if getattr(self, "K_elQ", None) is None:
+            self.K_elQ = self.m.new_block_values()
+            self.m.kr_blend(1.0, self.K_el, self.K_el, self.K_elQ)
+        return self.K_elQ
+
     def build_K_tangent_QQ_vals(self):
         with _Timer(self.profiler, "CONSTITUTIVE.build_K_tangent_QQ_vals"):
             self.m.assemble(self.DS, self.K_t)

@@ -1,7 +1,9 @@
-"""Indirect SSR continuation (device mirror of +CONTINUATION).
+"""Indirect SSR and limit-load continuation (device mirror of +CONTINUATION).
 
   init_phase_SSR_indirect_continuation   +CONTINUATION/init_phase_SSR_indirect_continuation.m:1-143
   SSR_indirect_continuation              +CONTINUATION/SSR_indirect_continuation.m:1-237
+  LL_elastic_start                       the LL scripts' start, slope_stability_3D_homo_LL.m:121-129
+  LL_indirect_continuation               +CONTINUATION/LL_indirect_continuation.m:1-160
 
 ``SSRIndirectStepper`` is the same loop split into ``init()`` and ``step()`` (one accepted
 continuation step per call, including its rejected attempts), so that a caller can time,
@@ -17,7 +19,7 @@ import numpy as np
 import torch
 
 from .device import dot
-from .newton import newton, newton_ind_SSR
+from .newton import newton, newton_ind_LL, newton_ind_SSR
 
 
 class ContinuationError(RuntimeError):
@@ -210,3 +212,92 @@ def SSR_indirect_continuation(lambda_init, d_lambda_init, d_lambda_min, d_lambda
     st["stop_reason"] = run.stop_reason
     st["total_wall_time"] = time.perf_counter() - t_total
     return run.U, np.array(run.lambda_hist), np.array(run.omega_hist), np.array(run.Umax_hist), st
+
+
+def LL_elastic_start(Q, f, cons, solver):
+    """Elastic solution at lambda = 1 as the start of the limit-load continuation: returns
+    (U_elast / 5, omega_el / 5) with omega_el = f(Q)' U_elast(Q) (the LL scripts' set-up,
+    slope_stability_3D_homo_LL.m:121-129); the solution joins the deflation basis."""
+    cons.reduction(1.0)
+    K = cons.elastic_K_QQ()
+    solver.setup_preconditioner(K)
+    U, _ = solver.solve(K, f * Q)
+    solver.expand_deflation_basis(U)
+    omega_el = dot(f * Q, U)
+    return U / 5, omega_el / 5
+
+
+def LL_indirect_continuation(d_omega_ini, d_t_min, step_max, omega_max, it_newt_max, it_damp_max, tol, r_min,
+                             K_elast, U_elast, Q, f, cons, solver, verbose=False, max_steps=None):
+    """Returns (U, t_hist, omega_hist, Umax_hist, stats); the histories start with the
+    reference's leading zero entry.  ``max_steps`` optionally stops after that many accepted
+    steps (bounded runs)."""
+    t_total = time.perf_counter()
+    omega = omega_old = 0.0
+    d_omega = float(d_omega_ini)
+    t = 0.0
+    U = U_elast.clone()
+    U_old = U.clone()
+    U_ini = U.clone()
+    n_omega, step, accepted = 0, 1, 0
+    t_hist, omega_hist, umax_hist = [0.0], [0.0], [0.0]
+    stats = dict(step_newton_iterations=[], step_wall_time=[], step_linear_iterations=[], attempts=[])
+    attempts, wall = 0, 0.0
+    stop = ""
+    dim = cons.dim
+    while True:
+        omega_it = omega + d_omega
+        if omega_it > omega_max:
+            omega_it = omega_max
+            d_omega = omega_it - omega
+        if step > 1:
+            U_ini = d_omega * (U - U_old) / (omega - omega_old) + U
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        U_it, t_it, flag, nit, hist = newton_ind_LL(U_ini, t, omega_it, it_newt_max, it_damp_max, tol, r_min,
+                                                    K_elast, Q, f, cons, solver.copy(), verbose)
+        torch.cuda.synchronize()
+        wall += time.perf_counter() - t0
+        attempts += 1
+        if flag == 1:
+            d_omega = d_omega / 2
+            n_omega += 1
+        else:
+            step += 1
+            accepted += 1
+            U_old, U = U, U_it
+            solver.expand_deflation_basis(U)
+            omega_old, omega = omega, omega_it
+            d_t = t_it - t
+            t = t_it
+            n_omega = 0
+            omega_hist.append(omega)
+            t_hist.append(t)
+            umax_hist.append(float(torch.sqrt((U.reshape(-1, dim) ** 2).sum(1)).max()))
+            stats["step_newton_iterations"].append(nit)
+            stats["step_wall_time"].append(wall)
+            stats["step_linear_iterations"].append(hist["linear_iters_W_total"] + hist["linear_iters_V_total"])
+            stats["attempts"].append(attempts)
+            attempts, wall = 0, 0.0
+            if verbose:
+                print(f"  accepted: t={t:.8g} d_t={d_t:.6g} omega={omega:.6g} newton_it={nit}")
+            if d_t < d_t_min:
+                stop = "minimal increment of t"
+                break
+            if nit < 20 and step > 2 and (t_hist[step - 1] - t_hist[step - 2]) < 0.9 * (t_hist[step - 2] - t_hist[step - 3]):
+                d_omega = 2 * d_omega
+            if max_steps is not None and accepted >= max_steps:
+                stop = "step budget"
+                break
+        if n_omega >= 5:
+            stop = "impossible to increase omega further"
+            break
+        if omega >= omega_max:
+            stop = "maximal omega"
+            break
+        if step >= step_max:
+            stop = "maximal number of steps"
+            break
+    stats["stop_reason"] = stop
+    stats["total_wall_time"] = time.perf_counter() - t_total
+    return U, np.array(t_hist), np.array(omega_hist), np.array(umax_hist), stats

@@ -218,3 +218,83 @@ def newton_ind_SSR(U_ini, omega, lambda_ini, it_newt_max, it_damp_max, tol, r_mi
     hist["linear_iters_W_total"] = int(sum(hist["linear_iters_W"]))
     hist["linear_iters_V_total"] = int(sum(hist["linear_iters_V"]))
     return U_it, lambda_it, flag, it, hist
+
+
+def newton_ind_LL(U_ini, t_ini, omega, it_newt_max, it_damp_max, tol, r_min, K_elast, Q, f, cons, solver,
+                  verbose=False):
+    """F(U) = t f with f(Q)' U(Q) = omega fixed (+NEWTON/newton_ind_LL.m:55-167).  Returns
+    (U, t, flag, it, hist)."""
+    U_it = U_ini.clone()
+    t_it = float(t_ini)
+    fQ = f * Q
+    norm_f = _norm_masked(f, Q)
+    flag = 0
+    compute_diffs = True
+    r = r_min
+    it = 0
+    if not cons.pattern_initialized:
+        cons.init_K_r_pattern()
+    hist = dict(residual=[], r=[], alpha=[], linear_iters_W=[], linear_iters_V=[])
+    rel_resid = float("nan")
+    status = "unknown"
+    ijv_init = False
+    t0 = time.perf_counter()
+    F = None
+    while True:
+        it += 1
+        if compute_diffs:
+            F = cons.build_F_and_DS_reduced(U_it)
+        criterion = masked_diff_norm(F, t_it * f, Q)
+        rel_resid = criterion / norm_f
+        hist["residual"].append(rel_resid)
+        if criterion < tol * norm_f and it > 1:
+            status = "converged"
+            break
+        hist["r"].append(r)
+        K = cons.build_K_r_QQ_vals(r)
+        if not ijv_init:
+            solver.setup_preconditioner_ijv(K)
+            ijv_init = True
+        else:
+            solver.update_preconditioner_values(K)
+        solver.A_orthogonalize(K)
+        W, lin_w = solver.solve(K, fQ)
+        V, lin_v = solver.solve(K, t_it * fQ - F * Q)
+        hist["linear_iters_W"].append(lin_w)
+        hist["linear_iters_V"].append(lin_v)
+        d_t = -dot(fQ, V) / dot(fQ, W)
+        dU = V + d_t * W
+        # newton_ind_LL.m:134 passes F_int * 0 as the load of the line search
+        alpha = damping(it_damp_max, U_it, dU, F, torch.zeros_like(F), cons)
+        hist["alpha"].append(alpha)
+        compute_diffs = True
+        if alpha < 1e-1:
+            if alpha == 0:
+                compute_diffs = False
+                r = r * 2
+            else:
+                r = r * 2 ** 0.25
+        else:
+            solver.expand_deflation_basis(W)
+            solver.expand_deflation_basis(V)
+            if alpha > 0.5:
+                r = max(r / math.sqrt(2), r_min)
+        if alpha == 0 and r > 1:
+            status = "stalled_regularization"
+            flag = 1
+            break
+        U_it = U_it + alpha * dU
+        U_it = omega * U_it / dot(fQ, U_it)
+        t_it = t_it + d_t
+        if verbose:
+            print(f"  newton_ind_LL it={it} rel_resid={rel_resid:.2e} alpha={alpha:.2f} r={r:.3g} "
+                  f"lin_it=[W:{lin_w},V:{lin_v}] t={t_it:.8f}")
+        if math.isnan(rel_resid) or it == it_newt_max:
+            flag = 1
+            status = "nan_residual" if math.isnan(rel_resid) else "max_iterations"
+            break
+    hist["status"] = status
+    hist["wall_time"] = time.perf_counter() - t0
+    hist["linear_iters_W_total"] = int(sum(hist["linear_iters_W"]))
+    hist["linear_iters_V_total"] = int(sum(hist["linear_iters_V"]))
+    return U_it, t_it, flag, it, hist

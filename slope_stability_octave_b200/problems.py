@@ -30,6 +30,10 @@ SSR_2D = dict(lambda_init=0.9, d_lambda_init=0.05, d_lambda_min=1e-5, d_lambda_d
 # reference 3D driver's omega_max_stop = 3000 (chosen for its own smaller mesh) would stop at
 # once, so the bound is lifted to the 2D script's 7e7 and the lambda-increment test stops.
 SSR_3D_EXTRUDED = dict(SSR_3D, omega_max_stop=7e7)
+# limit-load continuation parameters of slope_stability_3D_homo_LL.m:82-96 and
+# slope_stability_2D_homo_LL.m:154-163
+LL_3D = dict(d_t_min=1e-3, step_max=100, omega_max=5100.0, it_newt_max=200, it_damp_max=10, tol=1e-4, r_min=1e-4)
+LL_2D = dict(d_t_min=1e-3, step_max=100, omega_max=2000.0, it_newt_max=100, it_damp_max=10, tol=1e-4, r_min=1e-4)
 
 
 @dataclass

@@ -1,4 +1,5 @@
-"""Generate ssr_oracle.npz: the oracle's SSR indirect continuation histories.
+"""Generate ssr_oracle.npz and ll_oracle.npz: the oracle's SSR and limit-load (LL) indirect
+continuation histories.
 
     python tests/golden/make_continuation_golden.py
 
@@ -11,6 +12,8 @@ AMG error.  Cases (three accepted steps after the two-step init phase):
           parameters of slope_stability_2D_homo_SSR.m
   small3d the 3D homogeneous slope mesh_P2_3D(N_h = 1, 15, 10, 15, 10, 10, z = 1),
           parameters of slope_stability_3D_homo_SSR.m
+and, for LL_indirect_continuation.m / newton_ind_LL.m (seven accepted steps from the scripts'
+elastic start), the same two meshes with the parameters of slope_stability_{2D,3D}_homo_LL.m.
 """
 from __future__ import annotations
 
@@ -23,7 +26,8 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, os.path.dirname(os.path.dirname(HERE)))
 
-from oracle.drivers import DirectSolver, OracleConstitutive, SSR_indirect_continuation  # noqa: E402
+from oracle.drivers import (DirectSolver, LL_elastic_start, LL_indirect_continuation,  # noqa: E402
+                            OracleConstitutive, SSR_indirect_continuation)
 from slope_stability_octave_b200 import problems  # noqa: E402
 
 STEPS = 3
@@ -44,6 +48,28 @@ def run_case(make, params, steps=STEPS):
     return np.asarray(lh), np.asarray(oh), np.asarray(its, np.int64)
 
 
+LL_STEPS = 7
+
+
+def ll_cases():
+    return {
+        "cfg0": (lambda: problems.slope_2d(0.5), problems.LL_2D),
+        "small3d": (lambda: problems.slope_3d(1, dims=(15, 10, 15, 10, 10, 1)), problems.LL_3D),
+    }
+
+
+def run_ll_case(make, p, steps=LL_STEPS):
+    P = make()
+    cons = OracleConstitutive(P.mesh, P.dphi, P.weight, P.n_q, P.mat)
+    f = np.ascontiguousarray(P.f.T).ravel()
+    solver = DirectSolver()
+    U0, d_omega = LL_elastic_start(cons.Q, f, cons, solver)
+    th, oh, its, _ = LL_indirect_continuation(d_omega, p["d_t_min"], p["step_max"], p["omega_max"], p["it_newt_max"],
+                                              p["it_damp_max"], p["tol"], p["r_min"], U0, cons.Q, f, cons,
+                                              solver.copy(), max_steps=steps)
+    return th, oh, np.asarray(its, np.int64)
+
+
 def main():
     out = {}
     for name, (make, params) in cases().items():
@@ -52,6 +78,13 @@ def main():
         out[f"{name}_lambda"], out[f"{name}_omega"], out[f"{name}_newton"] = lh, oh, its
         print(name, f"{time.perf_counter() - t0:.1f}s", "lambda", lh, "omega", oh, "newton", its)
     np.savez(os.path.join(HERE, "ssr_oracle.npz"), **out)
+    out = {}
+    for name, (make, params) in ll_cases().items():
+        t0 = time.perf_counter()
+        th, oh, its = run_ll_case(make, params)
+        out[f"{name}_t"], out[f"{name}_omega"], out[f"{name}_newton"] = th, oh, its
+        print("LL", name, f"{time.perf_counter() - t0:.1f}s", "t", th, "omega", oh, "newton", its)
+    np.savez(os.path.join(HERE, "ll_oracle.npz"), **out)
 
 
 if __name__ == "__main__":

@@ -4,6 +4,9 @@
     lambda carries no Krylov error) against the oracle's histories computed with a sparse
     direct solver (tests/golden/ssr_oracle.npz, made by make_continuation_golden.py):
     lambda and omega within 1e-6 relative, Newton iteration counts equal;
+  * limit-load (LL) indirect continuation from the scripts' elastic start, seven accepted
+    steps, against the oracle's (tests/golden/ll_oracle.npz): load factor t and omega within
+    1e-6 relative, Newton iteration counts equal;
   * the reference's stored run of slope_stability_2D_homo_SSR.ipynb (2D homogeneous slope,
     h = 1/4, 83,280 unknowns, HYPRE-preconditioned DFGMRES at tolerance 1e-1, Newton 1e-4):
     omega_init = 425.2321 and the final lambda 1.16411213 (both as printed there).  The Krylov
@@ -20,6 +23,7 @@ from slope_stability_octave_b200 import continuation, problems
 pytestmark = pytest.mark.gpu
 
 GOLDEN = os.path.join(os.path.dirname(__file__), "golden", "ssr_oracle.npz")
+GOLDEN_LL = os.path.join(os.path.dirname(__file__), "golden", "ll_oracle.npz")
 
 CASES = {
     "cfg0": (lambda: problems.slope_2d(0.5), problems.SSR_2D),
@@ -47,6 +51,31 @@ def test_ssr_continuation_matches_oracle(cuda_device, case):
     assert lh.shape == lam_ref.shape
     assert np.max(np.abs(lh - lam_ref) / np.abs(lam_ref)) <= 1e-6
     assert np.max(np.abs(oh - om_ref) / np.abs(om_ref)) <= 1e-6
+    assert list(st["step_newton_iterations"]) == list(its_ref)
+
+
+LL_CASES = {
+    "cfg0": (lambda: problems.slope_2d(0.5), problems.LL_2D),
+    "small3d": (lambda: problems.slope_3d(1, dims=(15, 10, 15, 10, 10, 1)), problems.LL_3D),
+}
+
+
+@pytest.mark.parametrize("case", sorted(LL_CASES))
+def test_ll_continuation_matches_oracle(cuda_device, case):
+    g = np.load(GOLDEN_LL)
+    make, p = LL_CASES[case]
+    t_ref, om_ref, its_ref = g[f"{case}_t"], g[f"{case}_omega"], g[f"{case}_newton"]
+    P = make().to_device()
+    solver = P.solver("DFGMRES_B200", tol=1e-10, maxit=100)
+    f = P.f_device()
+    Q = P.dmesh.mask
+    U0, d_omega = continuation.LL_elastic_start(Q, f, P.cons, solver)
+    U, th, oh, um, st = continuation.LL_indirect_continuation(
+        d_omega, p["d_t_min"], p["step_max"], p["omega_max"], p["it_newt_max"], p["it_damp_max"], p["tol"],
+        p["r_min"], None, U0, Q, f, P.cons, solver.copy(), max_steps=len(its_ref))
+    assert th.shape == t_ref.shape
+    assert np.max(np.abs(th[1:] - t_ref[1:]) / np.abs(t_ref[1:])) <= 1e-6
+    assert np.max(np.abs(oh[1:] - om_ref[1:]) / np.abs(om_ref[1:])) <= 1e-6
     assert list(st["step_newton_iterations"]) == list(its_ref)
 
 
