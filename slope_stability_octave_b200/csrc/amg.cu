@@ -74,6 +74,7 @@ struct Level {
     Pattern P, R, AP;
     int32_t *d_R_from_P = nullptr;
     Plan at_plan, ap_plan, ac_plan;  // at: (A block) per P block; ap: (A, P); ac: (P, AP)
+    int64_t ap_pairs = 0, ac_pairs = 0;  // plan lengths (pairs of input blocks)
     double *Pv = nullptr, *Rv = nullptr, *APv = nullptr;
     float *P32 = nullptr, *R32 = nullptr;
     // vectors
@@ -446,6 +447,24 @@ __global__ void k_transpose_blocks(int64_t nblk, const int32_t *__restrict__ fro
     }
 }
 
+// Block of N doubles into registers: pairs of 16-byte loads when N is even (blocks of such
+// arrays then start on 16-byte boundaries), single loads otherwise.
+template <int N>
+__device__ __forceinline__ void load_block(const double *__restrict__ src, double *dst) {
+    if constexpr (N % 2 == 0) {
+        const double2 *s2 = reinterpret_cast<const double2 *>(src);
+#pragma unroll
+        for (int t = 0; t < N / 2; ++t) {
+            const double2 w = __ldg(s2 + t);
+            dst[2 * t] = w.x;
+            dst[2 * t + 1] = w.y;
+        }
+    } else {
+#pragma unroll
+        for (int t = 0; t < N; ++t) dst[t] = __ldg(src + t);
+    }
+}
+
 // AP block = sum over plan pairs A_a (B x B) * P_b (B x BC)
 template <int B, int BC>
 __global__ void k_gather_AP(int64_t nblk, const int64_t *__restrict__ lptr, const int32_t *__restrict__ la,
@@ -457,14 +476,15 @@ __global__ void k_gather_AP(int64_t nblk, const int64_t *__restrict__ lptr, cons
         for (int t = 0; t < B * BC; ++t) acc[t] = 0.0;
         for (int64_t l = lptr[q]; l < lptr[q + 1]; ++l) {
             const double *a = A + (int64_t)la[l] * B * B;
-            const double *p = P + (int64_t)lb[l] * B * BC;
+            double pv[B * BC];
+            load_block<B * BC>(P + (int64_t)lb[l] * B * BC, pv);
 #pragma unroll
             for (int r = 0; r < B; ++r)
 #pragma unroll
                 for (int m = 0; m < B; ++m) {
                     const double av = a[r * B + m];
 #pragma unroll
-                    for (int c = 0; c < BC; ++c) acc[r * BC + c] += av * p[m * BC + c];
+                    for (int c = 0; c < BC; ++c) acc[r * BC + c] += av * pv[m * BC + c];
                 }
         }
 #pragma unroll
@@ -488,8 +508,9 @@ __global__ void k_gather_Ac(int64_t nblk, const int32_t *__restrict__ row, const
 #pragma unroll
             for (int t = 0; t < BC * BC; ++t) acc[t] = 0.0;
             for (int64_t l = lptr[q]; l < lptr[q + 1]; ++l) {
-                const double *p = P + (int64_t)la[l] * B * BC;
-                const double *ap = AP + (int64_t)lb[l] * B * BC;
+                double p[B * BC], ap[B * BC];
+                load_block<B * BC>(P + (int64_t)la[l] * B * BC, p);
+                load_block<B * BC>(AP + (int64_t)lb[l] * B * BC, ap);
 #pragma unroll
                 for (int m = 0; m < B; ++m)
 #pragma unroll
@@ -499,6 +520,82 @@ __global__ void k_gather_Ac(int64_t nblk, const int32_t *__restrict__ row, const
                         for (int c = 0; c < BC; ++c) acc[r * BC + c] += pv * ap[m * BC + c];
                     }
             }
+#pragma unroll
+            for (int r = 0; r < BC; ++r)
+#pragma unroll
+                for (int c = 0; c < BC; ++c) {
+                    double v = acc[r * BC + c];
+                    if (dead[I * BC + r] || dead[J * BC + c]) v = (I == J && r == c) ? 1.0 : 0.0;
+                    Ac[(int64_t)q * BC * BC + r * BC + c] = v;
+                }
+        }
+    }
+}
+
+// Warp-per-output-block variants of the two gathers for the small coarse levels, where a few
+// hundred output blocks each sum thousands of pairs and one thread per block leaves the GPU
+// idle: the lanes split the block's pairs and the partial sums are combined by a fixed
+// shuffle tree (deterministic).
+template <int B, int BC>
+__global__ void k_gather_AP_warp(int64_t nblk, const int64_t *__restrict__ lptr, const int32_t *__restrict__ la,
+                                 const int32_t *__restrict__ lb, const double *__restrict__ A,
+                                 const double *__restrict__ P, double *__restrict__ AP) {
+    const int lane = threadIdx.x & 31;
+    const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    for (int64_t q = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5; q < nblk; q += nw) {
+        double acc[B * BC];
+#pragma unroll
+        for (int t = 0; t < B * BC; ++t) acc[t] = 0.0;
+        for (int64_t l = lptr[q] + lane; l < lptr[q + 1]; l += 32) {
+            double a[B * B], p[B * BC];
+            load_block<B * B>(A + (int64_t)la[l] * B * B, a);
+            load_block<B * BC>(P + (int64_t)lb[l] * B * BC, p);
+#pragma unroll
+            for (int r = 0; r < B; ++r)
+#pragma unroll
+                for (int m = 0; m < B; ++m)
+#pragma unroll
+                    for (int c = 0; c < BC; ++c) acc[r * BC + c] += a[r * B + m] * p[m * BC + c];
+        }
+#pragma unroll
+        for (int t = 0; t < B * BC; ++t)
+#pragma unroll
+            for (int off = 16; off > 0; off >>= 1) acc[t] += __shfl_xor_sync(0xffffffffu, acc[t], off);
+        if (lane == 0)
+#pragma unroll
+            for (int t = 0; t < B * BC; ++t) AP[q * B * BC + t] = acc[t];
+    }
+}
+
+template <int B, int BC>
+__global__ void k_gather_Ac_warp(int64_t nblk, const int32_t *__restrict__ row, const int32_t *__restrict__ col,
+                                 const int64_t *__restrict__ lptr, const int32_t *__restrict__ la,
+                                 const int32_t *__restrict__ lb, const double *__restrict__ P,
+                                 const double *__restrict__ AP, const uint8_t *__restrict__ dead,
+                                 double *__restrict__ Ac) {
+    const int lane = threadIdx.x & 31;
+    const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    for (int64_t q = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5; q < nblk; q += nw) {
+        double acc[BC * BC];
+#pragma unroll
+        for (int t = 0; t < BC * BC; ++t) acc[t] = 0.0;
+        for (int64_t l = lptr[q] + lane; l < lptr[q + 1]; l += 32) {
+            double p[B * BC], ap[B * BC];
+            load_block<B * BC>(P + (int64_t)la[l] * B * BC, p);
+            load_block<B * BC>(AP + (int64_t)lb[l] * B * BC, ap);
+#pragma unroll
+            for (int m = 0; m < B; ++m)
+#pragma unroll
+                for (int r = 0; r < BC; ++r)
+#pragma unroll
+                    for (int c = 0; c < BC; ++c) acc[r * BC + c] += p[m * BC + r] * ap[m * BC + c];
+        }
+#pragma unroll
+        for (int t = 0; t < BC * BC; ++t)
+#pragma unroll
+            for (int off = 16; off > 0; off >>= 1) acc[t] += __shfl_xor_sync(0xffffffffu, acc[t], off);
+        if (lane == 0) {
+            const int64_t I = row[q], J = col[q];
 #pragma unroll
             for (int r = 0; r < BC; ++r)
 #pragma unroll
@@ -786,6 +883,8 @@ static int setup_transfer(Level &L, const std::vector<int32_t> &rp, const std::v
     if (!rc) rc = dalloc(&L.APv, (size_t)L.AP.nblk * b * bc);
     if (!rc && mixed) rc = dalloc(&L.P32, (size_t)L.P.nblk * b * bc);
     if (!rc && mixed) rc = dalloc(&L.R32, (size_t)L.P.nblk * b * bc);
+    L.ap_pairs = (int64_t)L.ap_plan.a.size();
+    L.ac_pairs = (int64_t)L.ac_plan.a.size();
     for (Plan *pl : {&L.at_plan, &L.ap_plan, &L.ac_plan}) {  // host copies no longer needed
         std::vector<int64_t>().swap(pl->ptr);
         std::vector<int32_t>().swap(pl->a);
@@ -839,11 +938,27 @@ static int numeric_transfer(sg_amg *h, int l, cudaStream_t st) {
             L.P.nblk, L.P.d_row, L.P.d_col, L.at_plan.d_ptr, L.at_plan.d_a, L.d_Acol, A, L.T, L.d_agg, L.Dinv, L.lmax,
             h->opt.omega_scale, L.Pv);
         k_transpose_blocks<BB, BC><<<grid_for(L.P.nblk * BB * BC, 256), 256, 0, st>>>(L.P.nblk, L.d_R_from_P, L.Pv, L.Rv);
-        k_gather_AP<BB, BC><<<grid_for(L.AP.nblk, 128), 128, 0, st>>>(L.AP.nblk, L.ap_plan.d_ptr, L.ap_plan.d_a,
-                                                                      L.ap_plan.d_b, A, L.Pv, L.APv);
-        k_gather_Ac<BB, BC><<<grid_for(C.Anblk, 128), 128, 0, st>>>(C.Anblk, C.Aown.d_row, C.d_Acol, L.ac_plan.d_ptr,
-                                                                    L.ac_plan.d_a, L.ac_plan.d_b, L.Pv, L.APv,
-                                                                    C.d_dead, C.Aown_vals);
+        // one thread per output block, or a warp per block where blocks are few or each sums
+        // many pairs (measured on the SSR hierarchy: fine-level A P, ~15 pairs per block, is
+        // faster per thread; P'(A P), ~63 pairs per block, 1.3x faster per warp; the small
+        // coarse levels 10-20x faster per warp)
+        auto per_warp = [](int64_t nblk, int64_t pairs) { return nblk < 32768 || pairs >= 24 * nblk; };
+        if (!per_warp(L.AP.nblk, L.ap_pairs))
+            k_gather_AP<BB, BC><<<grid_for(L.AP.nblk, 128), 128, 0, st>>>(L.AP.nblk, L.ap_plan.d_ptr,
+                                                                          L.ap_plan.d_a, L.ap_plan.d_b, A, L.Pv,
+                                                                          L.APv);
+        else
+            k_gather_AP_warp<BB, BC><<<grid_for(L.AP.nblk * 32, 128), 128, 0, st>>>(
+                L.AP.nblk, L.ap_plan.d_ptr, L.ap_plan.d_a, L.ap_plan.d_b, A, L.Pv, L.APv);
+        if (!per_warp(C.Anblk, L.ac_pairs))
+            k_gather_Ac<BB, BC><<<grid_for(C.Anblk, 128), 128, 0, st>>>(C.Anblk, C.Aown.d_row, C.d_Acol,
+                                                                        L.ac_plan.d_ptr, L.ac_plan.d_a,
+                                                                        L.ac_plan.d_b, L.Pv, L.APv, C.d_dead,
+                                                                        C.Aown_vals);
+        else
+            k_gather_Ac_warp<BB, BC><<<grid_for(C.Anblk * 32, 128), 128, 0, st>>>(
+                C.Anblk, C.Aown.d_row, C.d_Acol, L.ac_plan.d_ptr, L.ac_plan.d_a, L.ac_plan.d_b, L.Pv, L.APv,
+                C.d_dead, C.Aown_vals);
     }));
     SG_CUDA(cudaGetLastError());
     if (h->opt.mixed) {
