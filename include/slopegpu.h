@@ -83,6 +83,15 @@ int sg_constitutive3d_noalloc(const double *E, const double *c_bar, const double
 int sg_reduction_dev(const double *c0, const double *phi, const double *psi, double lambda,
                      char davis_type, int64_t n, double *c_bar, double *sin_phi, void *stream);
 
+/* Integrated elastoplastic potential sum_p WEIGHT_p * Psi(E_p), CONSTITUTIVE.potential_energy
+ * (+CONSTITUTIVE_PROBLEM/CONSTITUTIVE.m:363-387, Psi of potential_3D.m / potential_2D.m), the
+ * energy of the SSR direct continuation (omega_SSR_direct_continuation.m:45-66).  E is the
+ * strain (6 x n_int in 3D, 3 x n_int in 2D, engineering shears); device arrays; the sum is
+ * returned to the host. */
+int sg_potential_dev(int dim, const double *E, const double *c_bar, const double *sin_phi,
+                     const double *shear, const double *bulk, const double *lame, const double *weight,
+                     int64_t n_int, double *result, void *stream);
+
 /* ------------------------------------------------------------------------------
  * (b3, b5) Element-level tangent assembly.  Replaces assemble_K_tangent_vals /
  * assemble_K_tangent_vals_2D (+ASSEMBLY/mex/assemble_K_tangent_vals.c:38-172,

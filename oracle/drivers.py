@@ -74,6 +74,13 @@ class OracleConstitutive:
         self._stress(U, True)
         return self.build_F()
 
+    def potential_energy(self, U):
+        """CONSTITUTIVE.m:363-387: integrated potential WEIGHT * Psi(B U)."""
+        E = self.pat.strain(U.reshape(-1, self.dim).T)
+        psi = potential(self.dim, E, self.c_bar, self.sin_phi, self.mat["shear"], self.mat["bulk"],
+                        self.mat["lame"])
+        return float(self.pat.weight @ psi)
+
     def elastic_K(self):
         """K_elast(Q, Q) (the elastic values of init_K_r_pattern, CONSTITUTIVE.m:393-464)."""
         n = self.pat.n_Q
@@ -500,3 +507,142 @@ def LL_indirect_continuation(d_omega_ini, d_t_min, step_max, omega_max, it_newt_
         if n_omega >= 5 or omega >= omega_max or step >= step_max:
             break
     return np.array(t_hist), np.array(omega_hist), its, U
+
+
+# ---------------------------------------------------------------------------- SSR direct
+
+
+def potential(dim, E, c_bar, sin_phi, shear, bulk, lame):
+    """Per-point elastoplastic potential Psi of the trial strain: potential_3D.m:36-123 and
+    potential_2D.m:26-95 (E is (n, 6) in 3D, (n, 3) in 2D; engineering shears)."""
+    sp = sin_phi
+    if dim == 3:
+        t = E.copy()
+        t[:, 3:] *= 0.5
+        I1 = t[:, 0] + t[:, 1] + t[:, 2]
+        I2 = t[:, 0] * t[:, 1] + t[:, 0] * t[:, 2] + t[:, 1] * t[:, 2] - t[:, 3] ** 2 - t[:, 4] ** 2 - t[:, 5] ** 2
+        I3 = (t[:, 0] * t[:, 1] * t[:, 2] - t[:, 2] * t[:, 3] ** 2 - t[:, 1] * t[:, 5] ** 2 - t[:, 0] * t[:, 4] ** 2
+              + 2 * t[:, 3] * t[:, 4] * t[:, 5])
+        Q = np.maximum(0.0, (1 / 9) * (I1 ** 2 - 3 * I2))
+        R = (1 / 54) * (-2 * I1 ** 3 + 9 * (I1 * I2) - 27 * I3)
+        th0 = np.zeros_like(Q)
+        pos = Q > 0
+        th0[pos] = R[pos] / np.sqrt(Q[pos] ** 3)
+        th = np.arccos(np.clip(th0, -1, 1)) / 3
+        e1 = -2 * np.sqrt(Q) * np.cos(th + 2 * np.pi / 3) + I1 / 3
+        e2 = -2 * np.sqrt(Q) * np.cos(th - 2 * np.pi / 3) + I1 / 3
+        e3 = -2 * np.sqrt(Q) * np.cos(th) + I1 / 3
+        f_tr = 2 * shear * ((1 + sp) * e1 - (1 - sp) * e3) + 2 * (lame * sp) * I1 - c_bar
+        den_s = 4 * lame * sp ** 2 + 4 * shear * (1 + sp ** 2)
+    else:
+        I1 = E[:, 0] + E[:, 1]
+        I2 = np.sqrt((E[:, 0] - E[:, 1]) ** 2 + E[:, 2] ** 2)
+        a, b, c = (I1 + I2) / 2, (I1 - I2) / 2, np.zeros_like(I1)
+        e1, e2, e3 = a.copy(), b.copy(), c.copy()
+        t2 = (a >= c) & (c > b)
+        e2[t2], e3[t2] = c[t2], b[t2]
+        t3 = c > a
+        e1[t3], e2[t3], e3[t3] = c[t3], a[t3], b[t3]
+        I1 = e1 + e2 + e3
+        f_tr = 2 * shear * ((1 + sp) * e1 - (1 - sp) * e3) + 2 * lame * sp * I1 - c_bar
+        den_s = 4 * lame * sp ** 2 + 2 * shear * (1 + sp) ** 2 + 2 * shear * (1 - sp) ** 2
+    g_sl = (e1 - e2) / (1 + sp)
+    g_sr = (e2 - e3) / (1 - sp)
+    g_la = (e1 + e2 - 2 * e3) / (3 - sp)
+    g_ra = (2 * e1 - e2 - e3) / (3 + sp)
+    den_l = 4 * lame * sp ** 2 + shear * (1 + sp) ** 2 + 2 * shear * (1 - sp) ** 2
+    den_r = 4 * lame * sp ** 2 + 2 * shear * (1 + sp) ** 2 + shear * (1 - sp) ** 2
+    den_a = 4 * bulk * sp ** 2
+    tr = e1 + e2 + e3
+    l_s = f_tr / den_s
+    l_l = (shear * ((1 + sp) * (e1 + e2) - 2 * (1 - sp) * e3) + 2 * lame * sp * tr - c_bar) / den_l
+    l_r = (shear * (2 * (1 + sp) * e1 - (1 - sp) * (e2 + e3)) + 2 * lame * sp * tr - c_bar) / den_r
+    l_a = (2 * bulk * sp * tr - c_bar) / den_a
+    el_part = 0.5 * lame * tr ** 2
+    psi = np.zeros_like(tr)
+    t_el = f_tr <= 0
+    psi[t_el] = (el_part + shear * (e1 ** 2 + e2 ** 2 + e3 ** 2))[t_el]
+    t_s = (l_s <= np.minimum(g_sl, g_sr)) & ~t_el
+    psi[t_s] = (el_part + shear * (e1 ** 2 + e2 ** 2 + e3 ** 2) - 0.5 * den_s * l_s ** 2)[t_s]
+    t_l = (g_sl < g_sr) & (l_l >= g_sl) & (l_l <= g_la) & ~(t_el | t_s)
+    psi[t_l] = (el_part + shear * (e3 ** 2 + 0.5 * (e1 + e2) ** 2) - 0.5 * den_l * l_l ** 2)[t_l]
+    t_r = (g_sl > g_sr) & (l_r >= g_sr) & (l_r <= g_ra) & ~(t_el | t_s)
+    psi[t_r] = (el_part + shear * (e1 ** 2 + 0.5 * (e2 + e3) ** 2) - 0.5 * den_r * l_r ** 2)[t_r]
+    t_a = ~(t_el | t_s | t_l | t_r)
+    psi[t_a] = (0.5 * bulk * tr ** 2 - 0.5 * den_a * l_a ** 2)[t_a]
+    return psi
+
+
+def omega_SSR_direct(lambda_ini, U_ini, eps, d_lambda, it_newt_max, it_damp_max, tol, r_min, Q, f, cons, solver):
+    """omega_SSR_direct_continuation.m:32-68: U at lambda, omega = dJ/dlambda by a backward
+    difference of the energy J = Psi - f'U over eps."""
+    cons.reduction(lambda_ini)
+    U, flag, _ = newton(U_ini, tol, it_newt_max, it_damp_max, r_min, Q, f, cons, solver)
+    if flag:
+        return U, 0.0, 1
+    J = cons.potential_energy(U) - f[Q] @ U[Q]
+    beta = min(1.0, eps / d_lambda)
+    U_beta = beta * U_ini + (1 - beta) * U
+    cons.reduction(lambda_ini - eps)
+    U_eps, flag, _ = newton(U_beta, tol, it_newt_max, it_damp_max, r_min, Q, f, cons, solver)
+    if flag:
+        return U, 0.0, 1
+    J_eps = cons.potential_energy(U_eps) - f[Q] @ U_eps[Q]
+    return U, (J_eps - J) / eps, 0
+
+
+def SSR_direct_continuation(p, Q, f, cons, solver, max_steps_after_init=None):
+    """init_phase_SSR_direct_continuation.m + SSR_direct_continuation.m:52-150; returns
+    (lambda_hist, omega_hist)."""
+    tol = p["tol"]
+    eps = tol * 100
+    args = (p["it_newt_max"], p["it_damp_max"], tol, p["r_min"], Q, f, cons)
+    U1, omega1, flag = omega_SSR_direct(p["lambda_init"], np.zeros_like(f), eps, 1000, *args, solver.copy())
+    if flag:
+        raise RuntimeError("Initial choice of lambda seems to be too large.")
+    d_lambda, lambda1 = p["d_lambda_init"], p["lambda_init"]
+    while True:
+        lam_it = lambda1 + d_lambda
+        solver.expand_deflation_basis(U1[Q])
+        U_it, omega_it, flag = omega_SSR_direct(lam_it, U1, eps, d_lambda, *args, solver.copy())
+        if flag:
+            d_lambda /= 2
+        else:
+            U2, omega2, lambda2 = U_it, omega_it, lam_it
+            if (omega2 - omega1) / max(1, omega1) < 1e-5:
+                U1, lambda1, omega1 = U2, lambda2, omega2
+            else:
+                break
+        if d_lambda < p["d_lambda_min"]:
+            raise RuntimeError("It seems that FoS is equal to lambda_init.")
+        if lambda1 > 10:
+            raise RuntimeError("It seems that the FoS is greater than 10.")
+    U, omega, lam = U2, omega2, lambda2
+    solver.expand_deflation_basis(U[Q])
+    lambda_hist, omega_hist = [lambda1, lam], [omega1, omega]
+    d_omega = omega - omega1
+    d_lambda = lam - p["lambda_init"]
+    step, accepted = 2, 0
+    while True:
+        lam_it = lam + d_lambda
+        U_it, omega_it, flag = omega_SSR_direct(lam_it, U, eps, d_lambda, *args, solver.copy())
+        d_omega_test = omega_it - omega_hist[step - 1]
+        if flag or d_omega_test < 0:
+            d_lambda /= 2
+        else:
+            U, omega, lam = U_it, omega_it, lam_it
+            step += 1
+            accepted += 1
+            lambda_hist.append(lam)
+            omega_hist.append(omega)
+            solver.expand_deflation_basis(U[Q])
+            if (d_lambda / d_omega_test) * (omega_hist[step - 1] - omega_hist[0]) < p["d_lambda_diff_scaled_min"]:
+                break
+            if d_omega_test > 1.5 * d_omega:
+                d_lambda /= 2
+            d_omega = d_omega_test
+            if max_steps_after_init is not None and accepted >= max_steps_after_init:
+                break
+        if d_lambda < p["d_lambda_min"] or step >= p["step_max"]:
+            break
+    return np.array(lambda_hist), np.array(omega_hist)

@@ -27,6 +27,7 @@ SIGNATURES = {
     "sg_constitutive2d_dev": [vp] * 6 + [i64, vp, vp, vp, vp],
     "sg_constitutive3d_noalloc": [vp] * 6 + [i64, vp, vp, vp],
     "sg_reduction_dev": [vp, vp, vp, f64, ch, i64, vp, vp, vp],
+    "sg_potential_dev": [cint] + [vp] * 7 + [i64, vp, vp],
     "sg_assemble_ktangent3d": [vp] * 6 + [i32, i64, i64, i32, i64, vp],
     "sg_assemble_ktangent2d": [vp] * 5 + [i32, i64, i64, i32, i64, vp],
     "sg_assemble_ktangent_dev": [cint] + [vp] * 6 + [i32, i64, i32, i64, vp, vp],

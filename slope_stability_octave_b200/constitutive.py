@@ -19,6 +19,7 @@ column-major layout).  K values live in the mesh's node-block pattern.
 """
 from __future__ import annotations
 
+import ctypes as C
 import time
 
 import numpy as np
@@ -104,6 +105,15 @@ class CONSTITUTIVE:
         _lib.call(fn, ptr(self.E), ptr(self.c_bar), ptr(self.sin_phi), ptr(self.shear), ptr(self.bulk),
                   ptr(self.lame), self.n_int, ptr(self.S), ptr(self.DS) if with_ds else None, ptr(self.branch),
                   cur_stream())
+
+    def potential_energy(self, U):
+        """Integrated potential WEIGHT * Psi(B U) at the current reduction (CONSTITUTIVE.m:363-387)."""
+        with _Timer(self.profiler, "CONSTITUTIVE.potential"):
+            self.m.strain(U, self.E)
+            out = C.c_double()
+            _lib.call("sg_potential_dev", self.dim, ptr(self.E), ptr(self.c_bar), ptr(self.sin_phi), ptr(self.shear),
+                      ptr(self.bulk), ptr(self.lame), ptr(self.m.weight), self.n_int, C.byref(out), cur_stream())
+        return out.value
 
     def constitutive_problem_stress(self, U):
         with _Timer(self.profiler, "CONSTITUTIVE.stress"):

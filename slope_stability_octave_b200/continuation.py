@@ -4,6 +4,9 @@
   SSR_indirect_continuation              +CONTINUATION/SSR_indirect_continuation.m:1-237
   LL_elastic_start                       the LL scripts' start, slope_stability_3D_homo_LL.m:121-129
   LL_indirect_continuation               +CONTINUATION/LL_indirect_continuation.m:1-160
+  omega_SSR_direct_continuation          +CONTINUATION/omega_SSR_direct_continuation.m:1-68
+  init_phase_SSR_direct_continuation     +CONTINUATION/init_phase_SSR_direct_continuation.m:1-110
+  SSR_direct_continuation                +CONTINUATION/SSR_direct_continuation.m:1-150
 
 ``SSRIndirectStepper`` is the same loop split into ``init()`` and ``step()`` (one accepted
 continuation step per call, including its rejected attempts), so that a caller can time,
@@ -301,3 +304,122 @@ def LL_indirect_continuation(d_omega_ini, d_t_min, step_max, omega_max, it_newt_
     stats["stop_reason"] = stop
     stats["total_wall_time"] = time.perf_counter() - t_total
     return U, np.array(t_hist), np.array(omega_hist), np.array(umax_hist), stats
+
+
+def omega_SSR_direct_continuation(lambda_ini, U_ini, eps, d_lambda, it_newt_max, it_damp_max, tol, r_min, K_elast, Q,
+                                  f, cons, solver, verbose=False):
+    """U at strength reduction lambda and omega = dJ/dlambda, J = Psi(U) - f(Q)'U(Q), by a
+    backward difference over eps (+CONTINUATION/omega_SSR_direct_continuation.m:32-68).
+    Returns (U, omega, flag); omega = 0 when a Newton solve failed (flag 1)."""
+    fQ = f * Q
+    cons.reduction(lambda_ini)
+    U, flag, _, _ = newton(U_ini, tol, it_newt_max, it_damp_max, r_min, K_elast, Q, f, cons, solver, verbose)
+    if flag == 1:
+        return U, 0.0, 1
+    J = cons.potential_energy(U) - dot(fQ, U)
+    beta = min(1.0, eps / d_lambda)
+    U_beta = beta * U_ini + (1 - beta) * U
+    cons.reduction(lambda_ini - eps)
+    U_eps, flag, _, _ = newton(U_beta, tol, it_newt_max, it_damp_max, r_min, K_elast, Q, f, cons, solver, verbose)
+    if flag == 1:
+        return U, 0.0, 1
+    J_eps = cons.potential_energy(U_eps) - dot(fQ, U_eps)
+    return U, (J_eps - J) / eps, 0
+
+
+def init_phase_SSR_direct_continuation(lambda_init, d_lambda_init, d_lambda_min, it_newt_max, it_damp_max, tol, eps,
+                                       r_min, K_elast, Q, f, cons, solver, verbose=False):
+    """+CONTINUATION/init_phase_SSR_direct_continuation.m:43-110: the first two points."""
+    args = (it_newt_max, it_damp_max, tol, r_min, K_elast, Q, f, cons)
+    U1, omega1, flag = omega_SSR_direct_continuation(lambda_init, torch.zeros_like(f), eps, 1000, *args,
+                                                     solver.copy(), verbose)
+    if flag == 1:
+        raise ContinuationError("Initial choice of lambda seems to be too large.")
+    d_lambda, lambda1 = d_lambda_init, lambda_init
+    while True:
+        lambda_it = lambda1 + d_lambda
+        solver.expand_deflation_basis(U1)
+        U_it, omega_it, flag = omega_SSR_direct_continuation(lambda_it, U1, eps, d_lambda, *args, solver.copy(),
+                                                             verbose)
+        if flag == 1:
+            d_lambda = d_lambda / 2
+        else:
+            U2, omega2, lambda2 = U_it, omega_it, lambda_it
+            if (omega2 - omega1) / max(1, omega1) < 1e-5:
+                U1, lambda1, omega1 = U2, lambda2, omega2
+            else:
+                break
+        if d_lambda < d_lambda_min:
+            raise ContinuationError("It seems that FoS is equal to lambda_init.")
+        if lambda1 > 10:
+            raise ContinuationError("It seems that the FoS is greater than 10.")
+    return U1, U2, omega1, omega2, lambda1, lambda2
+
+
+def SSR_direct_continuation(lambda_init, d_lambda_init, d_lambda_min, d_lambda_diff_scaled_min, step_max,
+                            it_newt_max, it_damp_max, tol, r_min, K_elast, Q, f, cons, solver, verbose=False,
+                            max_steps_after_init=None):
+    """+CONTINUATION/SSR_direct_continuation.m:52-150 (lambda is the control parameter, omega is
+    measured).  Returns (U, lambda_hist, omega_hist, Umax_hist, work_hist, stats)."""
+    t_total = time.perf_counter()
+    eps = tol * 100
+    dim = cons.dim
+    umax = lambda V: float(torch.sqrt((V.reshape(-1, dim) ** 2).sum(1)).max())
+    U_old, U, omega_old, omega, lambda_old, lam = init_phase_SSR_direct_continuation(
+        lambda_init, d_lambda_init, d_lambda_min, it_newt_max, it_damp_max, tol, eps, r_min, K_elast, Q, f, cons,
+        solver, verbose)
+    solver.expand_deflation_basis(U)
+    lambda_hist, omega_hist = [lambda_old, lam], [omega_old, omega]
+    Umax_hist = [umax(U), umax(U)]
+    work_hist = [dot(U_old, f), dot(U, f)]
+    d_omega = omega - omega_old
+    d_lambda = lam - lambda_init
+    step, accepted = 2, 0
+    stats = dict(step_wall_time=[], attempts=[])
+    attempts, wall = 0, 0.0
+    stop = ""
+    args = (it_newt_max, it_damp_max, tol, r_min, K_elast, Q, f, cons)
+    while True:
+        lambda_it = lam + d_lambda
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        U_it, omega_it, flag = omega_SSR_direct_continuation(lambda_it, U, eps, d_lambda, *args, solver.copy(),
+                                                             verbose)
+        torch.cuda.synchronize()
+        wall += time.perf_counter() - t0
+        attempts += 1
+        d_omega_test = omega_it - omega_hist[step - 1]
+        if flag == 1 or d_omega_test < 0:
+            d_lambda = d_lambda / 2
+        else:
+            U, omega, lam = U_it, omega_it, lambda_it
+            step += 1
+            accepted += 1
+            lambda_hist.append(lam)
+            omega_hist.append(omega)
+            Umax_hist.append(umax(U))
+            work_hist.append(dot(U, f))
+            solver.expand_deflation_basis(U)
+            stats["step_wall_time"].append(wall)
+            stats["attempts"].append(attempts)
+            attempts, wall = 0, 0.0
+            if verbose:
+                print(f"  accepted: lambda={lam:.8g} d_lambda={d_lambda:.6g} omega={omega:.6g}")
+            if (d_lambda / d_omega_test) * (omega_hist[step - 1] - omega_hist[0]) < d_lambda_diff_scaled_min:
+                stop = "minimal increase of lambda"
+                break
+            if d_omega_test > 1.5 * d_omega:
+                d_lambda = d_lambda / 2
+            d_omega = d_omega_test
+            if max_steps_after_init is not None and accepted >= max_steps_after_init:
+                stop = "step budget"
+                break
+        if d_lambda < d_lambda_min:
+            stop = "minimal increment of lambda"
+            break
+        if step >= step_max:
+            stop = "maximal number of steps"
+            break
+    stats["stop_reason"] = stop
+    stats["total_wall_time"] = time.perf_counter() - t_total
+    return U, np.array(lambda_hist), np.array(omega_hist), np.array(Umax_hist), np.array(work_hist), stats

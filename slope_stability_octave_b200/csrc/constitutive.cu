@@ -255,6 +255,36 @@ extern "C" int sg_constitutive2d_dev(const double *E, const double *c_bar, const
                                as_stream(stream));
 }
 
+// Per-block partial sums of weight * Psi; the host adds them in block order (deterministic).
+template <int DIM>
+__global__ void __launch_bounds__(256) k_potential(const double *__restrict__ E, const double *__restrict__ c_bar,
+                                                   const double *__restrict__ sin_phi,
+                                                   const double *__restrict__ shear, const double *__restrict__ bulk,
+                                                   const double *__restrict__ lame,
+                                                   const double *__restrict__ weight, int64_t n,
+                                                   double *__restrict__ part) {
+    constexpr int NS = DIM == 3 ? 6 : 3;
+    __shared__ double sh[256 / 32];
+    double acc = 0.0;
+    for (int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; p < n; p += (int64_t)gridDim.x * blockDim.x) {
+        double e[NS];
+#pragma unroll
+        for (int c = 0; c < NS; ++c) e[c] = E[NS * p + c];
+        const double psi = DIM == 3 ? potential3d(e, c_bar[p], sin_phi[p], shear[p], bulk[p], lame[p])
+                                    : potential2d(e, c_bar[p], sin_phi[p], shear[p], bulk[p], lame[p]);
+        acc += weight[p] * psi;
+    }
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, off);
+    if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = acc;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double t = 0.0;
+        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) t += sh[w];
+        part[blockIdx.x] = t;
+    }
+}
+
 extern "C" int sg_reduction_dev(const double *c0, const double *phi, const double *psi, double lambda,
                                 char davis_type, int64_t n, double *c_bar, double *sin_phi, void *stream) {
     SG_CHECK_ARG(n >= 0, "n must be >= 0");
@@ -264,5 +294,34 @@ extern "C" int sg_reduction_dev(const double *c0, const double *phi, const doubl
     SG_CHECK_ARG(c0 && phi && psi && c_bar && sin_phi, "null device pointer");
     k_reduction<<<grid_for(n, 256), 256, 0, as_stream(stream)>>>(c0, phi, psi, lambda, davis_type, n, c_bar, sin_phi);
     SG_CUDA(cudaGetLastError());
+    return SG_OK;
+}
+
+// Integrated potential sum_p weight[p] * Psi(E_p) (CONSTITUTIVE.m:363-387 with potential_3D.m /
+// potential_2D.m).  Device arrays; the result is returned to the host (synchronises stream).
+extern "C" int sg_potential_dev(int dim, const double *E, const double *c_bar, const double *sin_phi,
+                                const double *shear, const double *bulk, const double *lame, const double *weight,
+                                int64_t n_int, double *result, void *stream) {
+    SG_CHECK_ARG(dim == 2 || dim == 3, "dim must be 2 or 3");
+    SG_CHECK_ARG(n_int >= 0 && result, "bad argument");
+    *result = 0.0;
+    if (n_int == 0) return SG_OK;
+    SG_CHECK_ARG(E && c_bar && sin_phi && shear && bulk && lame && weight, "null device pointer");
+    constexpr int NBLK = 296;
+    static thread_local Scratch ws;
+    int rc = ws.reserve(sizeof(double) * NBLK);
+    if (rc) return rc;
+    const cudaStream_t st = as_stream(stream);
+    const unsigned grid = (unsigned)std::min<int64_t>(NBLK, (n_int + 255) / 256);
+    count_launch();
+    if (dim == 3) k_potential<3><<<grid, 256, 0, st>>>(E, c_bar, sin_phi, shear, bulk, lame, weight, n_int, (double *)ws.ptr);
+    else k_potential<2><<<grid, 256, 0, st>>>(E, c_bar, sin_phi, shear, bulk, lame, weight, n_int, (double *)ws.ptr);
+    SG_CUDA(cudaGetLastError());
+    double part[NBLK];
+    SG_CUDA(cudaMemcpyAsync(part, ws.ptr, sizeof(double) * grid, cudaMemcpyDeviceToHost, st));
+    SG_CUDA(cudaStreamSynchronize(st));
+    double t = 0.0;
+    for (unsigned b = 0; b < grid; ++b) t += part[b];
+    *result = t;
     return SG_OK;
 }

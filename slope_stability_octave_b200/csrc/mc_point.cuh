@@ -457,6 +457,68 @@ __device__ __forceinline__ int mc2d_point(const double E[3], double c_bar, doubl
 }
 
 // Davis strength reduction (+CONSTITUTIVE_PROBLEM/reduction.m:25-58), point-wise.
+// Elastoplastic potential of the trial strain at one point (the integrand of the SSR direct
+// method's energy): +CONSTITUTIVE_PROBLEM/potential_3D.m:36-123 (3D, E with engineering
+// shears) and potential_2D.m:26-95 (2D, E = e11, e22, g12).  The branch tests and formulas
+// follow those files, including their own eigenvalue formulas (R / sqrt(Q^3), Q > 0).
+__device__ __forceinline__ double potential_branches(double e1, double e2, double e3, double f_tr, double den_s,
+                                                     double c_bar, double sp, double shear, double bulk,
+                                                     double lame) {
+    const double g_sl = (e1 - e2) / (1.0 + sp);
+    const double g_sr = (e2 - e3) / (1.0 - sp);
+    const double g_la = (e1 + e2 - 2.0 * e3) / (3.0 - sp);
+    const double g_ra = (2.0 * e1 - e2 - e3) / (3.0 + sp);
+    const double den_l = 4.0 * lame * sp * sp + shear * (1.0 + sp) * (1.0 + sp) + 2.0 * shear * (1.0 - sp) * (1.0 - sp);
+    const double den_r = 4.0 * lame * sp * sp + 2.0 * shear * (1.0 + sp) * (1.0 + sp) + shear * (1.0 - sp) * (1.0 - sp);
+    const double den_a = 4.0 * bulk * sp * sp;
+    const double tr = e1 + e2 + e3;
+    const double el = 0.5 * lame * tr * tr;
+    if (f_tr <= 0.0) return el + shear * (e1 * e1 + e2 * e2 + e3 * e3);
+    const double l_s = f_tr / den_s;
+    if (l_s <= fmin(g_sl, g_sr)) return el + shear * (e1 * e1 + e2 * e2 + e3 * e3) - 0.5 * den_s * l_s * l_s;
+    const double l_l = (shear * ((1.0 + sp) * (e1 + e2) - 2.0 * (1.0 - sp) * e3) + 2.0 * lame * sp * tr - c_bar) / den_l;
+    if (g_sl < g_sr && l_l >= g_sl && l_l <= g_la)
+        return el + shear * (e3 * e3 + 0.5 * (e1 + e2) * (e1 + e2)) - 0.5 * den_l * l_l * l_l;
+    const double l_r = (shear * (2.0 * (1.0 + sp) * e1 - (1.0 - sp) * (e2 + e3)) + 2.0 * lame * sp * tr - c_bar) / den_r;
+    if (g_sl > g_sr && l_r >= g_sr && l_r <= g_ra)
+        return el + shear * (e1 * e1 + 0.5 * (e2 + e3) * (e2 + e3)) - 0.5 * den_r * l_r * l_r;
+    const double l_a = (2.0 * bulk * sp * tr - c_bar) / den_a;
+    return 0.5 * bulk * tr * tr - 0.5 * den_a * l_a * l_a;
+}
+
+__device__ __forceinline__ double potential3d(const double E[6], double c_bar, double sp, double shear, double bulk,
+                                              double lame) {
+    const double t0 = E[0], t1 = E[1], t2 = E[2], t3 = 0.5 * E[3], t4 = 0.5 * E[4], t5 = 0.5 * E[5];
+    const double I1 = t0 + t1 + t2;
+    const double I2 = t0 * t1 + t0 * t2 + t1 * t2 - t3 * t3 - t4 * t4 - t5 * t5;
+    const double I3 = t0 * t1 * t2 - t2 * t3 * t3 - t1 * t5 * t5 - t0 * t4 * t4 + 2.0 * t3 * t4 * t5;
+    const double Q = fmax(0.0, (1.0 / 9.0) * (I1 * I1 - 3.0 * I2));
+    const double R = (1.0 / 54.0) * (-2.0 * (I1 * I1 * I1) + 9.0 * (I1 * I2) - 27.0 * I3);
+    const double th0 = Q > 0.0 ? R / sqrt(Q * Q * Q) : 0.0;
+    const double th = acos(fmin(fmax(th0, -1.0), 1.0)) / 3.0;
+    const double pi = 3.14159265358979323846, sq = sqrt(Q);
+    const double e1 = -2.0 * sq * cos(th + 2.0 * pi / 3.0) + I1 / 3.0;
+    const double e2 = -2.0 * sq * cos(th - 2.0 * pi / 3.0) + I1 / 3.0;
+    const double e3 = -2.0 * sq * cos(th) + I1 / 3.0;
+    const double f_tr = 2.0 * shear * ((1.0 + sp) * e1 - (1.0 - sp) * e3) + 2.0 * (lame * sp) * I1 - c_bar;
+    const double den_s = 4.0 * lame * sp * sp + 4.0 * shear * (1.0 + sp * sp);
+    return potential_branches(e1, e2, e3, f_tr, den_s, c_bar, sp, shear, bulk, lame);
+}
+
+__device__ __forceinline__ double potential2d(const double E[3], double c_bar, double sp, double shear, double bulk,
+                                              double lame) {
+    const double I1 = E[0] + E[1];
+    const double I2 = sqrt((E[0] - E[1]) * (E[0] - E[1]) + E[2] * E[2]);
+    const double a = (I1 + I2) / 2.0, b = (I1 - I2) / 2.0, c = 0.0;
+    double e1 = a, e2 = b, e3 = c;
+    if (a >= c && c > b) { e2 = c; e3 = b; }
+    if (c > a) { e1 = c; e2 = a; e3 = b; }
+    const double tr = e1 + e2 + e3;
+    const double f_tr = 2.0 * shear * ((1.0 + sp) * e1 - (1.0 - sp) * e3) + 2.0 * lame * sp * tr - c_bar;
+    const double den_s = 4.0 * lame * sp * sp + 2.0 * shear * (1.0 + sp) * (1.0 + sp) + 2.0 * shear * (1.0 - sp) * (1.0 - sp);
+    return potential_branches(e1, e2, e3, f_tr, den_s, c_bar, sp, shear, bulk, lame);
+}
+
 __device__ __forceinline__ void davis_reduce(double c0, double phi, double psi, double lambda, char type,
                                              double &c_bar, double &sin_phi) {
     double beta, c_l, phi_l;

@@ -1,5 +1,5 @@
-"""Generate ssr_oracle.npz and ll_oracle.npz: the oracle's SSR and limit-load (LL) indirect
-continuation histories.
+"""Generate ssr_oracle.npz, ssr_direct_oracle.npz and ll_oracle.npz: the oracle's SSR
+(indirect and direct) and limit-load (LL) continuation histories.
 
     python tests/golden/make_continuation_golden.py
 
@@ -12,7 +12,9 @@ AMG error.  Cases (three accepted steps after the two-step init phase):
           parameters of slope_stability_2D_homo_SSR.m
   small3d the 3D homogeneous slope mesh_P2_3D(N_h = 1, 15, 10, 15, 10, 10, z = 1),
           parameters of slope_stability_3D_homo_SSR.m
-and, for LL_indirect_continuation.m / newton_ind_LL.m (seven accepted steps from the scripts'
+SSR direct continuation (SSR_direct_continuation.m with omega from the potential energy,
+four accepted steps after the init phase) on the same two meshes, and, for
+LL_indirect_continuation.m / newton_ind_LL.m (seven accepted steps from the scripts'
 elastic start), the same two meshes with the parameters of slope_stability_{2D,3D}_homo_LL.m.
 """
 from __future__ import annotations
@@ -27,7 +29,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, os.path.dirname(os.path.dirname(HERE)))
 
 from oracle.drivers import (DirectSolver, LL_elastic_start, LL_indirect_continuation,  # noqa: E402
-                            OracleConstitutive, SSR_indirect_continuation)
+                            OracleConstitutive, SSR_direct_continuation, SSR_indirect_continuation)
 from slope_stability_octave_b200 import problems  # noqa: E402
 
 STEPS = 3
@@ -70,6 +72,16 @@ def run_ll_case(make, p, steps=LL_STEPS):
     return th, oh, np.asarray(its, np.int64)
 
 
+DIRECT_STEPS = 4
+
+
+def run_direct_case(make, params, steps=DIRECT_STEPS):
+    P = make()
+    cons = OracleConstitutive(P.mesh, P.dphi, P.weight, P.n_q, P.mat)
+    f = np.ascontiguousarray(P.f.T).ravel()
+    return SSR_direct_continuation(params, cons.Q, f, cons, DirectSolver(), max_steps_after_init=steps)
+
+
 def main():
     out = {}
     for name, (make, params) in cases().items():
@@ -85,6 +97,13 @@ def main():
         out[f"{name}_t"], out[f"{name}_omega"], out[f"{name}_newton"] = th, oh, its
         print("LL", name, f"{time.perf_counter() - t0:.1f}s", "t", th, "omega", oh, "newton", its)
     np.savez(os.path.join(HERE, "ll_oracle.npz"), **out)
+    out = {}
+    for name, (make, params) in cases().items():
+        t0 = time.perf_counter()
+        lh, oh = run_direct_case(make, params)
+        out[f"{name}_lambda"], out[f"{name}_omega"] = lh, oh
+        print("direct", name, f"{time.perf_counter() - t0:.1f}s", "lambda", lh, "omega", oh)
+    np.savez(os.path.join(HERE, "ssr_direct_oracle.npz"), **out)
 
 
 if __name__ == "__main__":

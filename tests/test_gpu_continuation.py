@@ -7,9 +7,15 @@
   * limit-load (LL) indirect continuation from the scripts' elastic start, seven accepted
     steps, against the oracle's (tests/golden/ll_oracle.npz): load factor t and omega within
     1e-6 relative, Newton iteration counts equal;
+  * SSR direct continuation (lambda controlled, omega from the integrated potential by a
+    backward difference) against the oracle's (tests/golden/ssr_direct_oracle.npz): lambda
+    and omega within 1e-6 relative over four steps after the init phase; the device
+    potential against the oracle's restatement of potential_3D.m / potential_2D.m within
+    1e-12 relative;
   * the reference's stored run of slope_stability_2D_homo_SSR.ipynb (2D homogeneous slope,
     h = 1/4, 83,280 unknowns, HYPRE-preconditioned DFGMRES at tolerance 1e-1, Newton 1e-4):
-    omega_init = 425.2321 and the final lambda 1.16411213 (both as printed there).  The Krylov
+    omega_init = 425.2321 and the final lambda 1.16411213 of the indirect run, the final lambda
+    1.16406250 of the direct run (as printed there).  The Krylov
     solves stop at 1e-1, so the AMG difference enters lambda at the 1e-5 level: the test
     bound is 1e-4 relative.
 """
@@ -24,6 +30,7 @@ pytestmark = pytest.mark.gpu
 
 GOLDEN = os.path.join(os.path.dirname(__file__), "golden", "ssr_oracle.npz")
 GOLDEN_LL = os.path.join(os.path.dirname(__file__), "golden", "ll_oracle.npz")
+GOLDEN_DIRECT = os.path.join(os.path.dirname(__file__), "golden", "ssr_direct_oracle.npz")
 
 CASES = {
     "cfg0": (lambda: problems.slope_2d(0.5), problems.SSR_2D),
@@ -83,3 +90,48 @@ def test_ssr_2d_reproduces_reference_notebook_run(cuda_device):
     lh, oh, st = run_gpu(problems.slope_2d(0.25), problems.SSR_2D, 1e-1)
     assert abs(oh[0] - 425.2321) / 425.2321 <= 1e-4
     assert abs(lh[-1] - 1.16411213) / 1.16411213 <= 1e-4
+
+
+def run_direct(P, p, tol, steps=None):
+    P.to_device()
+    solver = P.solver("DFGMRES_B200", tol=tol, maxit=100)
+    U, lh, oh, um, wh, st = continuation.SSR_direct_continuation(
+        p["lambda_init"], p["d_lambda_init"], p["d_lambda_min"], p["d_lambda_diff_scaled_min"], p["step_max"],
+        p["it_newt_max"], p["it_damp_max"], p["tol"], p["r_min"], None, P.dmesh.mask, P.f_device(), P.cons, solver,
+        max_steps_after_init=steps)
+    return lh, oh
+
+
+@pytest.mark.parametrize("case", sorted(CASES))
+def test_ssr_direct_continuation_matches_oracle(cuda_device, case):
+    g = np.load(GOLDEN_DIRECT)
+    make, p = CASES[case]
+    lam_ref, om_ref = g[f"{case}_lambda"], g[f"{case}_omega"]
+    lh, oh = run_direct(make(), p, 1e-10, steps=len(lam_ref) - 2)
+    assert lh.shape == lam_ref.shape
+    assert np.max(np.abs(lh - lam_ref) / np.abs(lam_ref)) <= 1e-12
+    assert np.max(np.abs(oh - om_ref) / np.abs(om_ref)) <= 1e-6
+
+
+def test_potential_matches_restatement(cuda_device):
+    import torch
+    from oracle.drivers import potential
+    from slope_stability_octave_b200 import _lib, workloads
+    from slope_stability_octave_b200.device import ptr
+    d = workloads.constitutive_points(20000, seed=11)
+    rng = np.random.default_rng(2)
+    w = rng.uniform(0.1, 1.0, d["E"].shape[0])
+    ref = float(w @ potential(3, d["E"], d["c_bar"], d["sin_phi"], d["shear"], d["bulk"], d["lame"]))
+    dev = {k: torch.from_numpy(np.ascontiguousarray(v)).to(cuda_device)
+           for k, v in dict(E=d["E"], c_bar=d["c_bar"], sin_phi=d["sin_phi"], shear=d["shear"], bulk=d["bulk"],
+                            lame=d["lame"], w=w).items()}
+    import ctypes as C
+    out = C.c_double()
+    _lib.call("sg_potential_dev", 3, *[ptr(dev[k]) for k in ("E", "c_bar", "sin_phi", "shear", "bulk", "lame", "w")],
+              d["E"].shape[0], C.byref(out), None)
+    assert abs(out.value - ref) <= 1e-12 * abs(ref)
+
+
+def test_ssr_direct_2d_reproduces_reference_notebook_run(cuda_device):
+    lh, oh = run_direct(problems.slope_2d(0.25), problems.SSR_2D, 1e-1)
+    assert abs(lh[-1] - 1.1640625) / 1.1640625 <= 1e-4
