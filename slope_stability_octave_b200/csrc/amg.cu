@@ -10,7 +10,8 @@
 //       prolongator T from the near-null space (6 rigid-body modes in 3D, 3 in 2D) by a
 //       per-aggregate QR, and fixed-pattern product plans for A T, A P and P' (A P)
 //   numerics (device, every update)      block-Jacobi inverse, lambda_max(D^-1 A) by power
-//       iteration, P = T - omega D^-1 A T (omega = 4 / (3 lambda_max)), R = P', A P,
+//       iteration (10 steps from a fixed vector at set-up and first update, then 3 more from
+//       the previous vector at each later update), P = T - omega D^-1 A T (omega = 4 / (3 lambda_max)), R = P', A P,
 //       A_c = P' (A P); coarsest level: dense Gauss-Jordan inverse
 //   apply (device)                       V(1,1) cycle with degree-3 Chebyshev smoothing on
 //       D^-1 A over [lambda_max / 10, 1.1 lambda_max], in FP64 or FP32 (mixed precision)
@@ -79,6 +80,8 @@ struct Level {
     float *P32 = nullptr, *R32 = nullptr;
     // vectors
     double *x = nullptr, *rhs = nullptr, *r = nullptr, *d = nullptr, *t = nullptr;
+    double *pv = nullptr;          // power-iteration vector, kept between updates
+    int power_warm = 0;            // numeric passes done on this level (warm start from the third)
     float *x32 = nullptr, *rhs32 = nullptr, *r32 = nullptr, *d32 = nullptr;
 };
 
@@ -87,7 +90,8 @@ struct AmgOptions {
     int coarse_size = 1200;   // stop coarsening at this many DOFs
     int cheb_degree = 3;
     double cheb_ratio = 10.0; // smoothing interval [lmax / ratio, 1.1 lmax]
-    int power_its = 10;
+    int power_its = 10;       // first set-up; later updates continue from the last vector:
+    int power_its_warm = 3;   // lambda_max moves little between Newton iterations
     int mixed = 0;            // 1: FP32 V-cycle
     double omega_scale = 4.0 / 3.0;
     double theta = 0.02;      // strength threshold (0: whole block graph)
@@ -794,7 +798,7 @@ static int free_level(Level &l) {
     F(l.Aown.d_row); F(l.P.d_row); F(l.R.d_row); F(l.AP.d_row);
     for (Plan *p : {&l.at_plan, &l.ap_plan, &l.ac_plan}) { F(p->d_ptr); F(p->d_a); F(p->d_b); }
     F(l.Pv); F(l.Rv); F(l.APv); F(l.P32); F(l.R32);
-    F(l.x); F(l.rhs); F(l.r); F(l.d); F(l.t); F(l.x32); F(l.rhs32); F(l.r32); F(l.d32);
+    F(l.x); F(l.rhs); F(l.r); F(l.d); F(l.t); F(l.pv); F(l.x32); F(l.rhs32); F(l.r32); F(l.d32);
     return SG_OK;
 }
 
@@ -806,6 +810,7 @@ static int alloc_level_buffers(Level &L, int mixed) {
     if (!rc) rc = dalloc(&L.rhs, nb);
     if (!rc) rc = dalloc(&L.r, nb);
     if (!rc) rc = dalloc(&L.d, nb);
+    if (!rc) rc = dalloc(&L.pv, nb);
     if (!rc) rc = dalloc(&L.t, nb);
     if (!rc && mixed) {
         rc = dalloc(&L.Dinv32, nb * L.b);
@@ -899,15 +904,20 @@ static const double *level_values(const Level &L) { return L.Aext ? L.Avals : L.
 
 static int power_lmax(sg_amg *h, Level &L, const double *A, cudaStream_t st) {
     const int64_t nd = L.n * L.b;
-    k_init_vec<<<grid_for(nd, 256), 256, 0, st>>>(nd, L.d);
+    // cold (deterministic start vector, power_its steps) for the set-up inside sg_amg_create and
+    // for the first sg_amg_update, warm afterwards
+    const bool warm = L.power_warm >= 2;
+    if (!warm) k_init_vec<<<grid_for(nd, 256), 256, 0, st>>>(nd, L.pv);
+    ++L.power_warm;
     int rc = SG_OK;
-    for (int it = 0; it < h->opt.power_its && !rc; ++it) {
-        rc = rect_spmv<double, double>(L.b, L.b, L.n, L.d_Arp, L.d_Acol, A, L.d, L.t, 1.0, 0.0, nullptr, 0, st, L.Anblk);
+    const int its = warm ? h->opt.power_its_warm : h->opt.power_its;
+    for (int it = 0; it < its && !rc; ++it) {
+        rc = rect_spmv<double, double>(L.b, L.b, L.n, L.d_Arp, L.d_Acol, A, L.pv, L.t, 1.0, 0.0, nullptr, 0, st, L.Anblk);
         if (rc) break;
         SG_B_DISPATCH(L.b, (k_dinv_apply<BB, double><<<grid_for(L.n, 256), 256, 0, st>>>(L.n, L.Dinv, L.t, L.r)));
         rc = multidot(nd, 1, L.r, nd, L.r, h->dots, h->dots + DOT_BLOCKS, st);
         if (rc) break;
-        k_power_norm<<<grid_for(nd, 256), 256, 0, st>>>(nd, L.r, h->dots + DOT_BLOCKS, L.d, L.lmax);
+        k_power_norm<<<grid_for(nd, 256), 256, 0, st>>>(nd, L.r, h->dots + DOT_BLOCKS, L.pv, L.lmax);
     }
     SG_CUDA(cudaGetLastError());
     return rc;
