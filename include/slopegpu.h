@@ -196,7 +196,9 @@ int sg_amg_update(sg_amg *amg, const double *A_vals, void *stream);
 int sg_amg_apply(sg_amg *amg, const double *r, double *z, void *stream);
 /* info[0] levels, info[1] coarsest dense size, then (block size, block rows, blocks) per level */
 int sg_amg_info(const sg_amg *amg, int64_t *info, int32_t cap);
-/* host copies of level l's A pattern/values and P pattern/values (any pointer may be NULL) */
+/* host copies of level l's A pattern/values and P pattern/values (any pointer may be NULL);
+ * values are those of the FP64 numeric set-up: for a mixed-precision hierarchy (opts[5] != 0),
+ * whose value updates run in FP32, they are the values of its set-up in sg_amg_create */
 int sg_amg_export(const sg_amg *amg, int32_t level, int32_t *A_rp, int32_t *A_col, double *A_vals,
                   int32_t *P_rp, int32_t *P_col, double *P_vals);
 

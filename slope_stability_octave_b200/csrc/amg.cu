@@ -78,6 +78,7 @@ struct Level {
     int64_t ap_pairs = 0, ac_pairs = 0;  // plan lengths (pairs of input blocks)
     double *Pv = nullptr, *Rv = nullptr, *APv = nullptr;
     float *P32 = nullptr, *R32 = nullptr;
+    float *T32 = nullptr, *APv32 = nullptr;   // mixed form: FP32 numeric updates
     // vectors
     double *x = nullptr, *rhs = nullptr, *r = nullptr, *d = nullptr, *t = nullptr;
     double *pv = nullptr;          // power-iteration vector, kept between updates
@@ -328,14 +329,14 @@ __device__ __forceinline__ void inv_block(const double *a, double *out) {
         for (int j = 0; j < B; ++j) out[i * B + j] = m[i][B + j];
 }
 
-template <int B>
-__global__ void k_block_diag_inv(int64_t n, const int32_t *__restrict__ diag, const double *__restrict__ A,
+template <int B, typename V = double>
+__global__ void k_block_diag_inv(int64_t n, const int32_t *__restrict__ diag, const V *__restrict__ A,
                                  double *__restrict__ Dinv, float *__restrict__ Dinv32) {
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
         double a[B * B], o[B * B];
         const int64_t p = diag[i];
 #pragma unroll
-        for (int t = 0; t < B * B; ++t) a[t] = (p >= 0) ? A[p * B * B + t] : ((t % (B + 1)) == 0 ? 1.0 : 0.0);
+        for (int t = 0; t < B * B; ++t) a[t] = (p >= 0) ? (double)A[p * B * B + t] : ((t % (B + 1)) == 0 ? 1.0 : 0.0);
         inv_block<B>(a, o);
 #pragma unroll
         for (int t = 0; t < B * B; ++t) {
@@ -396,13 +397,13 @@ __global__ void k_cheb(int64_t n, int k, double ratio, const double *__restrict_
 
 // P block (i,J) = [agg(i) == J] T_i - omega Dinv_i sum_{p in list} A_p T_{col(p)},  omega = s / lmax
 // One thread per P block.
-template <int B, int BC>
+template <int B, int BC, typename V = double>
 __global__ void k_smooth_prolongator(int64_t nblk, const int32_t *__restrict__ Prow, const int32_t *__restrict__ Pcol,
                                      const int64_t *__restrict__ lptr, const int32_t *__restrict__ la,
-                                     const int32_t *__restrict__ Acol, const double *__restrict__ A,
-                                     const double *__restrict__ T, const int32_t *__restrict__ agg,
+                                     const int32_t *__restrict__ Acol, const V *__restrict__ A,
+                                     const V *__restrict__ T, const int32_t *__restrict__ agg,
                                      const double *__restrict__ Dinv, const double *__restrict__ lmax, double oscale,
-                                     double *__restrict__ P) {
+                                     V *__restrict__ P) {
     const double omega = oscale / lmax[0];
     for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q < nblk; q += (int64_t)gridDim.x * blockDim.x) {
         const int64_t i = Prow[q];
@@ -412,20 +413,20 @@ __global__ void k_smooth_prolongator(int64_t nblk, const int32_t *__restrict__ P
             for (int t = 0; t < B * BC; ++t) acc[t] = 0.0;
             for (int64_t l = lptr[q]; l < lptr[q + 1]; ++l) {
                 const int32_t p = la[l];
-                const double *a = A + (int64_t)p * B * B;
-                const double *tk = T + (int64_t)Acol[p] * B * BC;
+                const V *a = A + (int64_t)p * B * B;
+                const V *tk = T + (int64_t)Acol[p] * B * BC;
 #pragma unroll
                 for (int r = 0; r < B; ++r)
 #pragma unroll
                     for (int m = 0; m < B; ++m) {
-                        const double av = a[r * B + m];
+                        const double av = (double)a[r * B + m];
 #pragma unroll
-                        for (int c = 0; c < BC; ++c) acc[r * BC + c] += av * tk[m * BC + c];
+                        for (int c = 0; c < BC; ++c) acc[r * BC + c] += av * (double)tk[m * BC + c];
                     }
             }
             const double *di = Dinv + i * B * B;
             const bool own = agg[i] == Pcol[q];
-            const double *ti = T + i * B * BC;
+            const V *ti = T + i * B * BC;
 #pragma unroll
             for (int r = 0; r < B; ++r)
 #pragma unroll
@@ -433,16 +434,16 @@ __global__ void k_smooth_prolongator(int64_t nblk, const int32_t *__restrict__ P
                     double s = 0.0;
 #pragma unroll
                     for (int m = 0; m < B; ++m) s += di[r * B + m] * acc[m * BC + c];
-                    P[(int64_t)q * B * BC + r * BC + c] = (own ? ti[r * BC + c] : 0.0) - omega * s;
+                    P[(int64_t)q * B * BC + r * BC + c] = (V)((own ? (double)ti[r * BC + c] : 0.0) - omega * s);
                 }
         }
     }
 }
 
 // R block k = transpose of P block from[k]
-template <int B, int BC>
-__global__ void k_transpose_blocks(int64_t nblk, const int32_t *__restrict__ from, const double *__restrict__ P,
-                                   double *__restrict__ R) {
+template <int B, int BC, typename V = double>
+__global__ void k_transpose_blocks(int64_t nblk, const int32_t *__restrict__ from, const V *__restrict__ P,
+                                   V *__restrict__ R) {
     const int64_t total = nblk * B * BC;
     for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < total; t += (int64_t)gridDim.x * blockDim.x) {
         const int64_t k = t / (B * BC);
@@ -468,42 +469,58 @@ __device__ __forceinline__ void load_block(const double *__restrict__ src, doubl
         for (int t = 0; t < N; ++t) dst[t] = __ldg(src + t);
     }
 }
+// FP32 blocks (the mixed-precision set-up): pairs of 8-byte loads when N is even
+template <int N>
+__device__ __forceinline__ void load_block(const float *__restrict__ src, double *dst) {
+    if constexpr (N % 2 == 0) {
+        const float2 *s2 = reinterpret_cast<const float2 *>(src);
+#pragma unroll
+        for (int t = 0; t < N / 2; ++t) {
+            const float2 w = __ldg(s2 + t);
+            dst[2 * t] = w.x;
+            dst[2 * t + 1] = w.y;
+        }
+    } else {
+#pragma unroll
+        for (int t = 0; t < N; ++t) dst[t] = __ldg(src + t);
+    }
+}
 
 // AP block = sum over plan pairs A_a (B x B) * P_b (B x BC)
-template <int B, int BC>
+template <int B, int BC, typename V = double>
 __global__ void k_gather_AP(int64_t nblk, const int64_t *__restrict__ lptr, const int32_t *__restrict__ la,
-                            const int32_t *__restrict__ lb, const double *__restrict__ A, const double *__restrict__ P,
-                            double *__restrict__ AP) {
+                            const int32_t *__restrict__ lb, const V *__restrict__ A, const V *__restrict__ P,
+                            V *__restrict__ AP) {
     for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q < nblk; q += (int64_t)gridDim.x * blockDim.x) {
         double acc[B * BC];
 #pragma unroll
         for (int t = 0; t < B * BC; ++t) acc[t] = 0.0;
         for (int64_t l = lptr[q]; l < lptr[q + 1]; ++l) {
-            const double *a = A + (int64_t)la[l] * B * B;
+            const V *a = A + (int64_t)la[l] * B * B;
             double pv[B * BC];
             load_block<B * BC>(P + (int64_t)lb[l] * B * BC, pv);
 #pragma unroll
             for (int r = 0; r < B; ++r)
 #pragma unroll
                 for (int m = 0; m < B; ++m) {
-                    const double av = a[r * B + m];
+                    const double av = (double)a[r * B + m];
 #pragma unroll
                     for (int c = 0; c < BC; ++c) acc[r * BC + c] += av * pv[m * BC + c];
                 }
         }
 #pragma unroll
-        for (int t = 0; t < B * BC; ++t) AP[q * B * BC + t] = acc[t];
+        for (int t = 0; t < B * BC; ++t) AP[q * B * BC + t] = (V)acc[t];
     }
 }
 
 // Ac block (I,J) = sum over plan pairs P_a' (BC x B) * AP_b (B x BC); dead DOFs get identity.
 // One thread per coarse block.
-template <int B, int BC>
+template <int B, int BC, typename V = double>
 __global__ void k_gather_Ac(int64_t nblk, const int32_t *__restrict__ row, const int32_t *__restrict__ col,
                             const int64_t *__restrict__ lptr, const int32_t *__restrict__ la,
-                            const int32_t *__restrict__ lb, const double *__restrict__ P,
-                            const double *__restrict__ AP, const uint8_t *__restrict__ dead,
-                            double *__restrict__ Ac) {
+                            const int32_t *__restrict__ lb, const V *__restrict__ P,
+                            const V *__restrict__ AP, const uint8_t *__restrict__ dead,
+                            V *__restrict__ Ac) {
     for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q < nblk; q += (int64_t)gridDim.x * blockDim.x) {
         const int64_t I = row[q];
         {
@@ -530,7 +547,7 @@ __global__ void k_gather_Ac(int64_t nblk, const int32_t *__restrict__ row, const
                 for (int c = 0; c < BC; ++c) {
                     double v = acc[r * BC + c];
                     if (dead[I * BC + r] || dead[J * BC + c]) v = (I == J && r == c) ? 1.0 : 0.0;
-                    Ac[(int64_t)q * BC * BC + r * BC + c] = v;
+                    Ac[(int64_t)q * BC * BC + r * BC + c] = (V)v;
                 }
         }
     }
@@ -540,10 +557,10 @@ __global__ void k_gather_Ac(int64_t nblk, const int32_t *__restrict__ row, const
 // hundred output blocks each sum thousands of pairs and one thread per block leaves the GPU
 // idle: the lanes split the block's pairs and the partial sums are combined by a fixed
 // shuffle tree (deterministic).
-template <int B, int BC>
+template <int B, int BC, typename V = double>
 __global__ void k_gather_AP_warp(int64_t nblk, const int64_t *__restrict__ lptr, const int32_t *__restrict__ la,
-                                 const int32_t *__restrict__ lb, const double *__restrict__ A,
-                                 const double *__restrict__ P, double *__restrict__ AP) {
+                                 const int32_t *__restrict__ lb, const V *__restrict__ A,
+                                 const V *__restrict__ P, V *__restrict__ AP) {
     const int lane = threadIdx.x & 31;
     const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
     for (int64_t q = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5; q < nblk; q += nw) {
@@ -567,16 +584,16 @@ __global__ void k_gather_AP_warp(int64_t nblk, const int64_t *__restrict__ lptr,
             for (int off = 16; off > 0; off >>= 1) acc[t] += __shfl_xor_sync(0xffffffffu, acc[t], off);
         if (lane == 0)
 #pragma unroll
-            for (int t = 0; t < B * BC; ++t) AP[q * B * BC + t] = acc[t];
+            for (int t = 0; t < B * BC; ++t) AP[q * B * BC + t] = (V)acc[t];
     }
 }
 
-template <int B, int BC>
+template <int B, int BC, typename V = double>
 __global__ void k_gather_Ac_warp(int64_t nblk, const int32_t *__restrict__ row, const int32_t *__restrict__ col,
                                  const int64_t *__restrict__ lptr, const int32_t *__restrict__ la,
-                                 const int32_t *__restrict__ lb, const double *__restrict__ P,
-                                 const double *__restrict__ AP, const uint8_t *__restrict__ dead,
-                                 double *__restrict__ Ac) {
+                                 const int32_t *__restrict__ lb, const V *__restrict__ P,
+                                 const V *__restrict__ AP, const uint8_t *__restrict__ dead,
+                                 V *__restrict__ Ac) {
     const int lane = threadIdx.x & 31;
     const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
     for (int64_t q = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5; q < nblk; q += nw) {
@@ -606,7 +623,7 @@ __global__ void k_gather_Ac_warp(int64_t nblk, const int32_t *__restrict__ row, 
                 for (int c = 0; c < BC; ++c) {
                     double v = acc[r * BC + c];
                     if (dead[I * BC + r] || dead[J * BC + c]) v = (I == J && r == c) ? 1.0 : 0.0;
-                    Ac[(int64_t)q * BC * BC + r * BC + c] = v;
+                    Ac[(int64_t)q * BC * BC + r * BC + c] = (V)v;
                 }
         }
     }
@@ -643,9 +660,9 @@ __global__ void k_power_norm(int64_t n, const double *__restrict__ w, const doub
 }
 
 // dense coarsest matrix from the block pattern
-template <int B>
+template <int B, typename V = double>
 __global__ void k_bsr_to_dense(int64_t nrows, const int32_t *__restrict__ rp, const int32_t *__restrict__ col,
-                               const double *__restrict__ A, int64_t N, double *__restrict__ D) {
+                               const V *__restrict__ A, int64_t N, double *__restrict__ D) {
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < nrows; i += (int64_t)gridDim.x * blockDim.x)
         for (int32_t p = rp[i]; p < rp[i + 1]; ++p) {
             const int64_t j = col[p];
@@ -797,7 +814,7 @@ static int free_level(Level &l) {
     F(l.AP.d_rp); F(l.AP.d_col); F(l.d_R_from_P);
     F(l.Aown.d_row); F(l.P.d_row); F(l.R.d_row); F(l.AP.d_row);
     for (Plan *p : {&l.at_plan, &l.ap_plan, &l.ac_plan}) { F(p->d_ptr); F(p->d_a); F(p->d_b); }
-    F(l.Pv); F(l.Rv); F(l.APv); F(l.P32); F(l.R32);
+    F(l.Pv); F(l.Rv); F(l.APv); F(l.P32); F(l.R32); F(l.T32); F(l.APv32);
     F(l.x); F(l.rhs); F(l.r); F(l.d); F(l.t); F(l.pv); F(l.x32); F(l.rhs32); F(l.r32); F(l.d32);
     return SG_OK;
 }
@@ -888,6 +905,11 @@ static int setup_transfer(Level &L, const std::vector<int32_t> &rp, const std::v
     if (!rc) rc = dalloc(&L.APv, (size_t)L.AP.nblk * b * bc);
     if (!rc && mixed) rc = dalloc(&L.P32, (size_t)L.P.nblk * b * bc);
     if (!rc && mixed) rc = dalloc(&L.R32, (size_t)L.P.nblk * b * bc);
+    if (!rc && mixed) rc = dalloc(&L.APv32, (size_t)L.AP.nblk * b * bc);
+    if (!rc && mixed) {
+        std::vector<float> t32(T.begin(), T.end());
+        rc = dup(&L.T32, t32);
+    }
     L.ap_pairs = (int64_t)L.ap_plan.a.size();
     L.ac_pairs = (int64_t)L.ac_plan.a.size();
     for (Plan *pl : {&L.at_plan, &L.ap_plan, &L.ac_plan}) {  // host copies no longer needed
@@ -913,6 +935,27 @@ static int power_lmax(sg_amg *h, Level &L, const double *A, cudaStream_t st) {
     const int its = warm ? h->opt.power_its_warm : h->opt.power_its;
     for (int it = 0; it < its && !rc; ++it) {
         rc = rect_spmv<double, double>(L.b, L.b, L.n, L.d_Arp, L.d_Acol, A, L.pv, L.t, 1.0, 0.0, nullptr, 0, st, L.Anblk);
+        if (rc) break;
+        SG_B_DISPATCH(L.b, (k_dinv_apply<BB, double><<<grid_for(L.n, 256), 256, 0, st>>>(L.n, L.Dinv, L.t, L.r)));
+        rc = multidot(nd, 1, L.r, nd, L.r, h->dots, h->dots + DOT_BLOCKS, st);
+        if (rc) break;
+        k_power_norm<<<grid_for(nd, 256), 256, 0, st>>>(nd, L.r, h->dots + DOT_BLOCKS, L.pv, L.lmax);
+    }
+    SG_CUDA(cudaGetLastError());
+    return rc;
+}
+
+// lambda_max of D^-1 A from the FP32 level matrix (FP64 vectors), same start and step rules.
+static int power_lmax32(sg_amg *h, Level &L, cudaStream_t st) {
+    const int64_t nd = L.n * L.b;
+    const bool warm = L.power_warm >= 2;
+    if (!warm) k_init_vec<<<grid_for(nd, 256), 256, 0, st>>>(nd, L.pv);
+    ++L.power_warm;
+    int rc = SG_OK;
+    const int its = warm ? h->opt.power_its_warm : h->opt.power_its;
+    for (int it = 0; it < its && !rc; ++it) {
+        rc = rect_spmv<float, double>(L.b, L.b, L.n, L.d_Arp, L.d_Acol, L.A32, L.pv, L.t, 1.0, 0.0, nullptr, 0, st,
+                                      L.Anblk);
         if (rc) break;
         SG_B_DISPATCH(L.b, (k_dinv_apply<BB, double><<<grid_for(L.n, 256), 256, 0, st>>>(L.n, L.Dinv, L.t, L.r)));
         rc = multidot(nd, 1, L.r, nd, L.r, h->dots, h->dots + DOT_BLOCKS, st);
@@ -1006,6 +1049,69 @@ static int numeric_update(sg_amg *h, cudaStream_t st) {
         rc = (l == nl - 1) ? numeric_coarsest(h, st) : numeric_transfer(h, l, st);
     }
     return rc;
+}
+
+// Mixed form: the numeric update in FP32 for the FP32 V-cycle.  The level matrices, P, R and
+// A P are formed directly in FP32 (products accumulated in FP64 registers), the block
+// inverses and lambda_max in FP64 from the FP32 values; the coarsest dense inverse in FP64.
+// The set-up inside sg_amg_create keeps the FP64 path, so the mixed form has the same
+// hierarchy structure as the plain one.
+static int numeric_update32(sg_amg *h, cudaStream_t st) {
+    const int nl = (int)h->L.size();
+    for (int l = 0; l < nl; ++l) {
+        Level &L = h->L[l];
+        if (l == 0) {
+            const int64_t nv = L.Anblk * L.b * L.b;
+            k_to_float<<<grid_for(nv, 256), 256, 0, st>>>(nv, L.Avals, L.A32);
+        }
+        SG_B_DISPATCH(L.b, (k_block_diag_inv<BB, float><<<grid_for(L.n, 128), 128, 0, st>>>(L.n, L.d_Adiag, L.A32,
+                                                                                            L.Dinv, L.Dinv32)));
+        SG_CUDA(cudaGetLastError());
+        if (l == nl - 1) {
+            const int64_t N = h->nc_dense;
+            SG_CUDA(cudaMemsetAsync(h->Ainv, 0, sizeof(double) * N * N, st));
+            SG_B_DISPATCH(L.b, (k_bsr_to_dense<BB, float><<<grid_for(L.n, 128), 128, 0, st>>>(
+                                   L.n, L.d_Arp, L.d_Acol, L.A32, N, h->Ainv)));
+            for (int64_t k0 = 0; k0 < N; k0 += GJ_NB) {
+                const int nb = (int)std::min<int64_t>(GJ_NB, N - k0);
+                count_launch();
+                k_gjb_pivot<<<1, GJ_NB * GJ_NB, 0, st>>>(N, k0, nb, h->Ainv, h->gj_pinv);
+                k_gjb_save<<<grid_for(N * nb, 256), 256, 0, st>>>(N, k0, nb, h->Ainv, h->gj_pinv, h->colk, h->rowk);
+                k_gjb_update<<<grid_for(N * N, 256, 16), 256, 0, st>>>(N, k0, nb, h->Ainv, h->gj_pinv, h->colk,
+                                                                      h->rowk);
+            }
+            k_to_float<<<grid_for(N * N, 256), 256, 0, st>>>(N * N, h->Ainv, h->Ainv32);
+            SG_CUDA(cudaGetLastError());
+            break;
+        }
+        Level &C = h->L[l + 1];
+        int rc = power_lmax32(h, L, st);
+        if (rc) return rc;
+        SG_BBC_DISPATCH(L.b, L.bc, ({
+            k_smooth_prolongator<BB, BC, float><<<grid_for(L.P.nblk, 128), 128, 0, st>>>(
+                L.P.nblk, L.P.d_row, L.P.d_col, L.at_plan.d_ptr, L.at_plan.d_a, L.d_Acol, L.A32, L.T32, L.d_agg,
+                L.Dinv, L.lmax, h->opt.omega_scale, L.P32);
+            k_transpose_blocks<BB, BC, float><<<grid_for(L.P.nblk * BB * BC, 256), 256, 0, st>>>(
+                L.P.nblk, L.d_R_from_P, L.P32, L.R32);
+            auto per_warp = [](int64_t nblk, int64_t pairs) { return nblk < 32768 || pairs >= 24 * nblk; };
+            if (!per_warp(L.AP.nblk, L.ap_pairs))
+                k_gather_AP<BB, BC, float><<<grid_for(L.AP.nblk, 128), 128, 0, st>>>(
+                    L.AP.nblk, L.ap_plan.d_ptr, L.ap_plan.d_a, L.ap_plan.d_b, L.A32, L.P32, L.APv32);
+            else
+                k_gather_AP_warp<BB, BC, float><<<grid_for(L.AP.nblk * 32, 128), 128, 0, st>>>(
+                    L.AP.nblk, L.ap_plan.d_ptr, L.ap_plan.d_a, L.ap_plan.d_b, L.A32, L.P32, L.APv32);
+            if (!per_warp(C.Anblk, L.ac_pairs))
+                k_gather_Ac<BB, BC, float><<<grid_for(C.Anblk, 128), 128, 0, st>>>(
+                    C.Anblk, C.Aown.d_row, C.d_Acol, L.ac_plan.d_ptr, L.ac_plan.d_a, L.ac_plan.d_b, L.P32, L.APv32,
+                    C.d_dead, C.A32);
+            else
+                k_gather_Ac_warp<BB, BC, float><<<grid_for(C.Anblk * 32, 128), 128, 0, st>>>(
+                    C.Anblk, C.Aown.d_row, C.d_Acol, L.ac_plan.d_ptr, L.ac_plan.d_a, L.ac_plan.d_b, L.P32, L.APv32,
+                    C.d_dead, C.A32);
+        }));
+        SG_CUDA(cudaGetLastError());
+    }
+    return SG_OK;
 }
 
 // ------------------------------------------------------------------ hierarchy structure
@@ -1270,7 +1376,7 @@ extern "C" int sg_amg_destroy(sg_amg *h) {
 extern "C" int sg_amg_update(sg_amg *h, const double *Avals, void *stream) {
     SG_CHECK_ARG(h && Avals, "null argument");
     h->L[0].Avals = Avals;
-    int rc = numeric_update(h, as_stream(stream));
+    int rc = h->opt.mixed ? numeric_update32(h, as_stream(stream)) : numeric_update(h, as_stream(stream));
     if (!rc) h->updated = 1;
     return rc;
 }

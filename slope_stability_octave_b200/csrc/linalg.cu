@@ -179,6 +179,9 @@ template int rect_spmv<double, double>(int, int, int64_t, const int32_t *, const
                                        double *, double, double, const double *, int, cudaStream_t, int64_t);
 template int rect_spmv<float, float>(int, int, int64_t, const int32_t *, const int32_t *, const float *, const float *,
                                      float *, double, double, const float *, int, cudaStream_t, int64_t);
+template int rect_spmv<float, double>(int, int, int64_t, const int32_t *, const int32_t *, const float *,
+                                      const double *, double *, double, double, const double *, int, cudaStream_t,
+                                      int64_t);
 
 template <typename VT, typename XT>
 int bsr_spmv(const sg_bsr &A, const VT *vals, const XT *x, XT *y, double alpha, double beta, cudaStream_t st) {
