@@ -38,6 +38,8 @@ import time
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
+from slope_stability_octave_b200.replicas import barrier, max_over_ranks  # noqa: E402
+
 METRIC = "s per SSR continuation step, 3D P2 (mixed+learned vs plain FP64 GPU) at equal λ"
 UNIT = "s/step"
 WORKLOAD = ("3D homogeneous slope SSR, mesh_P2_3D(N_h=1, 15,10,15,10,10, z=40): 156,000 P2 tets, "
@@ -145,8 +147,7 @@ def run_form(args, form, P, rank, world):
     clocks = ClockSampler(torch.cuda.current_device()).start()
     _lib.call("sg_instr_enable", 1, 4)
     torch.cuda.synchronize()
-    if world > 1:
-        torch.distributed.barrier()
+    barrier(world)
     torch.cuda.synchronize()
     _lib.lib().sg_launch_count(1)
     torch.cuda.nvtx.range_push("timed_step")
@@ -167,8 +168,7 @@ def run_form(args, form, P, rank, world):
         basis.append(solver.k)
     torch.cuda.synchronize()
     torch.cuda.nvtx.range_pop()
-    if world > 1:
-        torch.distributed.barrier()
+    barrier(world)
     launches = int(_lib.lib().sg_launch_count(1))
     ms = np.zeros(N_INSTR)
     nt = np.zeros(N_INSTR, np.int64)
@@ -179,10 +179,7 @@ def run_form(args, form, P, rank, world):
     clk = clocks.stop()
     t_dev = sum(ev[k][1].elapsed_time(ev[k][2]) for k in range(args.steps)) / 1e3
     t_e2e = sum(ev[k][0].elapsed_time(ev[k][3]) for k in range(args.steps)) / 1e3
-    if world > 1:
-        t = torch.tensor([t_dev, t_e2e], dtype=torch.float64, device="cuda")
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        t_dev, t_e2e = t.tolist()
+    t_dev, t_e2e = max_over_ranks([t_dev, t_e2e], world, device="cuda")
     res = dict(t_dev=t_dev, t_e2e=t_e2e, steps=steps, basis=basis, launches=launches, instr=(ms, nt, nl),
                clocks=clk, t_init=t_init, lam=[s["lam"] for s in steps], amg=solver.preconditioner.info(),
                lam_init=list(run.lambda_hist[: 2 + args.warmup]))
@@ -307,9 +304,11 @@ def run_box(args, rank):
     def sds():
         _lib.check(L.sg_constitutive3d_dev(*cargs, n, ptr(S), ptr(DS), None, st), "sg_constitutive3d_dev")
 
+    world = int(os.environ.get("WORLD_SIZE", "1"))
     for _ in range(args.warmup):
         sds()
     torch.cuda.synchronize()
+    barrier(world)
     clocks = ClockSampler(torch.cuda.current_device()).start()
     L.sg_launch_count(1)
     ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
@@ -320,7 +319,10 @@ def run_box(args, rank):
     torch.cuda.synchronize()
     launches = int(L.sg_launch_count(1))
     clk = clocks.stop()
-    ms = ev[0].elapsed_time(ev[1]) / args.steps
+    barrier(world)
+    ms = max_over_ranks([ev[0].elapsed_time(ev[1]) / args.steps], world, device="cuda")[0]
+    if rank != 0:
+        return
     # e2e: the drop-in host-buffer entry point (the MEX arguments), copies included
     host = {k: pts[k].cpu().numpy() for k in pts}
     Sh = np.empty((n, 6))
