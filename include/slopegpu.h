@@ -222,6 +222,66 @@ int sg_a_orthogonalize(sg_krylov *ws, const sg_bsr *A, const double *A_vals, dou
                        int32_t k, double eps_add, int32_t *k_out, void *stream);
 
 /* ------------------------------------------------------------------------------
+ * Learned node-wise correction of the V-cycle (no counterpart in the reference, whose
+ * DFGMRES is preconditioned by one BoomerAMG V-cycle: hypre_boomeramg_mex.cpp:751-796).
+ * With a correction set, the preconditioner inside sg_dfgmres_solve becomes
+ *     z = V(r);   z += C (r - A z),   C_i = M_i G_i D_i^{-1}  (3 x 3 per node),
+ * G_i = MLP(phi_i), a per-node network 16 -> 64 -> 64 -> 9 (ReLU) run on the tensor cores
+ * (BF16 operands, FP32 accumulation) over node features phi from the matrix, the Newton
+ * residual and the constitutive state; D_i the node's diagonal block, M_i its free-DOF mask.
+ * Training minimises the mean of |rz - A M G D^{-1} rz|^2 / |rz|^2 over residual vectors
+ * rz = v - A V(v) of the plain preconditioner, collected from the Newton system; the last
+ * layer starts at zero, so the untrained correction is the plain V-cycle.
+ * ---------------------------------------------------------------------------- */
+#define SG_LEARNED_NPARAM 6288 /* W1[16][64] b1[64] W2[64][64] b2[64] W3[64][16] b3[16] (FP32) */
+/* z += C (r - A z) after every V-cycle; C: device n_rows x 9 (row-major 3 x 3), copied;
+ * NULL switches the correction off */
+int sg_amg_set_correction(sg_amg *amg, const double *C, void *stream);
+/* stateless network passes on device arrays: X is n_pad x 16 BF16 bit patterns (n_pad =
+ * 128*ceil(n/128), padding rows zero), G and dG n_pad x 16 FP32 (columns 9..15 unused);
+ * err: device int set to 1 when a tensor-core completion wait ran out (nothing then written) */
+int sg_mlp_forward_dev(const float *params, const uint16_t *X, int64_t n, float *G, int *err, void *stream);
+int64_t sg_mlp_part_size(int64_t n);
+int sg_mlp_backward_dev(const float *params, const uint16_t *X, const float *dG, int64_t n, float *grad,
+                        float *part, int *err, void *stream);
+
+typedef struct sg_learned sg_learned;
+/* coord: host 3 x n_n column-major node coordinates; max_vectors per slot; seed of the
+ * initial weights (He-uniform, last layer zero) */
+int sg_learned_create(const sg_mesh *mesh, const double *coord, int32_t max_vectors, uint64_t seed,
+                      sg_learned **out);
+int sg_learned_destroy(sg_learned *h);
+/* host copy of the NPARAM parameters (set != 0 writes them and resets the optimiser) */
+int sg_learned_params(sg_learned *h, float *host, int32_t set);
+/* features and diagonal-block inverses for matrix values A_vals (device, mesh pattern), the
+ * Newton residual res (device, dim*n_n), branch ids and reduced cohesion per integration
+ * point (device; either may be NULL) */
+int sg_learned_features(sg_learned *h, const double *A_vals, const double *res, const uint8_t *branch,
+                        const double *c_bar, void *stream);
+/* C from the current network; handed to amg when amg != NULL; copied to C_out when given */
+int sg_learned_correction(sg_learned *h, sg_amg *amg, double *C_out, void *stream);
+/* collect `count` residual vectors of the plain V-cycle on A x = b into slot 0 (training) or
+ * 1 (held out), replacing (append = 0) or appending; switches amg's correction off */
+int sg_learned_collect(sg_learned *h, sg_amg *amg, const sg_bsr *A, const double *A_vals, const double *b,
+                       int32_t count, int32_t slot, int32_t append, void *stream);
+/* mean relative corrected residual |rz - A d|^2/|rz|^2 over a slot's vectors */
+int sg_learned_loss(sg_learned *h, const sg_bsr *A, const double *A_vals, int32_t slot, double *loss,
+                    void *stream);
+/* gradient of that loss with respect to the parameters (host, NPARAM floats) */
+int sg_learned_gradient(sg_learned *h, const sg_bsr *A, const double *A_vals, int32_t slot, float *grad,
+                        double *loss, void *stream);
+/* `steps` full-batch Adam steps on slot 0; loss_hist (host, may be NULL) gets the loss
+ * before each step */
+int sg_learned_train(sg_learned *h, const sg_bsr *A, const double *A_vals, int32_t steps, double lr,
+                     double *loss_hist, void *stream);
+/* host copy, for checks: what 0 features (n_pad x 16 BF16 bits), 1 last network output G
+ * (n_pad x 16 FP32), 2 diagonal-block inverses (n_n x 9), 3 / 4 residual vector `index` of
+ * slot 0 / 1 (dim*n_n), 5 the correction C (n_n x 9) */
+int sg_learned_export(const sg_learned *h, int32_t what, int32_t index, void *host);
+/* info: [NPARAM, vectors in slot 0, vectors in slot 1, padded node count, Adam steps taken] */
+int sg_learned_info(const sg_learned *h, int64_t *info);
+
+/* ------------------------------------------------------------------------------
  * Live kernel timing (no reference counterpart: profiling support in the spirit of the
  * reference's PROFILING.Profiler).  When enabled, every `sample`-th launch of the fine-level
  * SpMV, the return mapping and the assembly is bracketed by CUDA events on its stream.

@@ -59,6 +59,22 @@ SIGNATURES = {
     "sg_amg_apply": [vp, vp, vp, vp],
     "sg_amg_info": [vp, vp, i32],
     "sg_amg_export": [vp, i32, vp, vp, vp, vp, vp, vp],
+    "sg_amg_set_correction": [vp, vp, vp],
+    # learned node-wise correction of the V-cycle
+    "sg_mlp_forward_dev": [vp, vp, i64, vp, vp, vp],
+    "sg_mlp_part_size": [i64],
+    "sg_mlp_backward_dev": [vp, vp, vp, i64, vp, vp, vp, vp],
+    "sg_learned_create": [vp, vp, i32, C.c_uint64, vp],
+    "sg_learned_destroy": [vp],
+    "sg_learned_params": [vp, vp, i32],
+    "sg_learned_features": [vp, vp, vp, vp, vp, vp],
+    "sg_learned_correction": [vp, vp, vp, vp],
+    "sg_learned_collect": [vp, vp, vp, vp, vp, i32, i32, i32, vp],
+    "sg_learned_loss": [vp, vp, vp, i32, vp, vp],
+    "sg_learned_gradient": [vp, vp, vp, i32, vp, vp, vp],
+    "sg_learned_train": [vp, vp, vp, i32, f64, vp, vp],
+    "sg_learned_export": [vp, i32, i32, vp],
+    "sg_learned_info": [vp, vp],
     # Krylov
     "sg_krylov_create": [i64, i32, vp],
     "sg_krylov_destroy": [vp],
@@ -69,7 +85,7 @@ SIGNATURES = {
     "sg_instr_read": [vp, vp, vp, i32],
     "sg_launch_count": [cint],
 }
-_RESTYPES = {"sg_last_error": C.c_char_p, "sg_launch_count": C.c_int64}
+_RESTYPES = {"sg_last_error": C.c_char_p, "sg_launch_count": C.c_int64, "sg_mlp_part_size": C.c_int64}
 
 
 class SlopeGPUError(RuntimeError):

@@ -109,6 +109,10 @@ struct sg_amg {
     double *colk = nullptr, *rowk = nullptr;   // Gauss-Jordan column block (N x NB) and row block (NB x N)
     double *gj_pinv = nullptr;                 // inverse of the current pivot block (NB x NB)
     double *dots = nullptr;    // reduction scratch
+    // optional node-wise correction after the cycle: z += C (r - A z), C n x 3 x 3 (3D only)
+    double *corrC = nullptr;
+    float *corrC32 = nullptr;
+    int corr_on = 0;
     int device = 0;
     int updated = 0;
 };
@@ -1256,6 +1260,18 @@ static int build_hierarchy(sg_amg *h, const sg_bsr *A0, const double *A0vals, co
     }
 }
 
+// x_i += C_i r_i for 3 x 3 node blocks C (row-major)
+template <typename T>
+__global__ void k_corr_apply(int64_t n, const T *__restrict__ Cb, const T *__restrict__ r, T *__restrict__ x) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        const T *c = Cb + i * 9;
+        const T r0 = r[3 * i], r1 = r[3 * i + 1], r2 = r[3 * i + 2];
+        x[3 * i] += c[0] * r0 + c[1] * r1 + c[2] * r2;
+        x[3 * i + 1] += c[3] * r0 + c[4] * r1 + c[5] * r2;
+        x[3 * i + 2] += c[6] * r0 + c[7] * r1 + c[8] * r2;
+    }
+}
+
 // ------------------------------------------------------------------ V-cycle
 
 template <typename T>
@@ -1366,6 +1382,8 @@ extern "C" int sg_amg_destroy(sg_amg *h) {
     cudaFree(h->rowk);
     cudaFree(h->dots);
     cudaFree(h->gj_pinv);
+    cudaFree(h->corrC);
+    cudaFree(h->corrC32);
     cudaSetDevice(cur);
     delete h;
     return SG_OK;
@@ -1392,14 +1410,50 @@ extern "C" int sg_amg_apply(sg_amg *h, const double *r, double *z, void *stream)
     if (h->opt.mixed) {
         k_to_float<<<grid_for(nd, 256), 256, 0, st>>>(nd, r, L.rhs32);
         rc = vcycle<float>(h, 0, st);
+        if (!rc && h->corr_on) {
+            rc = rect_spmv<float, float>(L.b, L.b, L.n, L.d_Arp, L.d_Acol, L.A32, L.x32, L.r32, 1.0, 0.0, L.rhs32, 1, st,
+                                         L.Anblk);
+            if (!rc) k_corr_apply<float><<<grid_for(L.n, 256), 256, 0, st>>>(L.n, h->corrC32, L.r32, L.x32);
+        }
         if (!rc) k_to_double<<<grid_for(nd, 256), 256, 0, st>>>(nd, L.x32, z);
     } else {
         SG_CUDA(cudaMemcpyAsync(L.rhs, r, sizeof(double) * nd, cudaMemcpyDeviceToDevice, st));
         rc = vcycle<double>(h, 0, st);
+        if (!rc && h->corr_on) {
+            LevelView<double> v = view<double>(L);
+            rc = rect_spmv<double, double>(L.b, L.b, L.n, L.d_Arp, L.d_Acol, v.A, L.x, L.r, 1.0, 0.0, L.rhs, 1, st,
+                                           L.Anblk);
+            if (!rc) k_corr_apply<double><<<grid_for(L.n, 256), 256, 0, st>>>(L.n, h->corrC, L.r, L.x);
+        }
         if (!rc) SG_CUDA(cudaMemcpyAsync(z, L.x, sizeof(double) * nd, cudaMemcpyDeviceToDevice, st));
     }
     SG_CUDA(cudaGetLastError());
     return rc;
+}
+
+// Node-wise correction after every cycle (no counterpart in the reference): with C set,
+// sg_amg_apply returns z + C (r - A z) for the cycle's z, C given as n_rows 3 x 3 row-major
+// blocks (device, FP64, copied; converted to FP32 for a mixed-precision hierarchy).  C = NULL
+// switches it off.
+extern "C" int sg_amg_set_correction(sg_amg *h, const double *Cb, void *stream) {
+    SG_CHECK_ARG(h, "null argument");
+    if (!Cb) {
+        h->corr_on = 0;
+        return SG_OK;
+    }
+    Level &L = h->L[0];
+    SG_CHECK_ARG(L.b == 3, "the node-wise correction needs 3 x 3 node blocks");
+    const cudaStream_t st = as_stream(stream);
+    const int64_t nv = L.n * 9;
+    if (!h->corrC) SG_CUDA(cudaMalloc(&h->corrC, sizeof(double) * nv));
+    SG_CUDA(cudaMemcpyAsync(h->corrC, Cb, sizeof(double) * nv, cudaMemcpyDeviceToDevice, st));
+    if (h->opt.mixed) {
+        if (!h->corrC32) SG_CUDA(cudaMalloc(&h->corrC32, sizeof(float) * nv));
+        k_to_float<<<grid_for(nv, 256), 256, 0, st>>>(nv, h->corrC, h->corrC32);
+        SG_CUDA(cudaGetLastError());
+    }
+    h->corr_on = 1;
+    return SG_OK;
 }
 
 // info: [levels, dense size, then per level: block size, block rows, blocks] (capacity 3 + 3*10)

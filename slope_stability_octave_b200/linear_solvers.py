@@ -145,6 +145,8 @@ class DFGMRES:
         self.profiler = None
         self.last_iterations = 0
         self.last_relres = 0.0
+        # optional learned node-wise correction of the V-cycle (learned.LearnedCorrection)
+        self.learned = None
 
     @property
     def k(self):
@@ -183,6 +185,21 @@ class DFGMRES:
     def solve(self, K, b):
         """x, nit = solve(K, b) on device vectors (dfgmres_solver.m)."""
         t0 = time.perf_counter()
+        amg = self.preconditioner
+        corrected = self.learned.before_solve(amg, K, b) if self.learned is not None else False
+        x, nit, rr = self._solve_core(K, b)
+        if corrected and not (rr <= self.tolerance):
+            # the corrected preconditioner did not reach the tolerance: plain V-cycle
+            self.learned.fallbacks += 1
+            self.learned.off(amg)
+            x, nit2, rr = self._solve_core(K, b)
+            nit += nit2
+        self.last_iterations = nit
+        self.last_relres = rr
+        self._time("DFGMRES.solve", t0)
+        return x, nit
+
+    def _solve_core(self, K, b):
         x = torch.empty_like(b)
         it = C.c_int32()
         rr = C.c_double()
@@ -192,10 +209,7 @@ class DFGMRES:
         _lib.call("sg_dfgmres_solve", self._ws.handle, self.dmesh.bsr, ptr(K), M, ptr(B) if self.k else None,
                   ptr(self.AW) if aw_ok else None, self.k, ptr(b), ptr(x), self.tolerance, self.max_iterations,
                   C.byref(it), C.byref(rr), None, cur_stream())
-        self.last_iterations = it.value
-        self.last_relres = rr.value
-        self._time("DFGMRES.solve", t0)
-        return x, it.value
+        return x, it.value, rr.value
 
     def expand_deflation_basis(self, v):
         t0 = time.perf_counter()
@@ -211,14 +225,17 @@ class DFGMRES:
         if self.AW is not None:
             new.AW, new._aw_key = self.AW.clone(), self._aw_key
         new.profiler = self.profiler
+        new.learned = self.learned
         return new
 
 
 def set_linear_solver(solver_type, linear_solver_tolerance, linear_solver_maxit, deflation_basis_tolerance,
-                      linear_solver_printing, dmesh: DeviceMesh, coord=None, amg_opts=None):
+                      linear_solver_printing, dmesh: DeviceMesh, coord=None, amg_opts=None, learned=None, cons=None):
     """Solver factory (set_linear_solver.m).  Tokens: 'DFGMRES_B200' (FP64 AMG V-cycle),
     'DFGMRES_B200_MIXED' (FP32 V-cycle inside the FP64 FGMRES), 'DFGMRES_NONE' (no
-    preconditioner)."""
+    preconditioner).  ``learned`` (a dict of LearnedCorrection options, or True) adds the
+    learned node-wise correction of the V-cycle; ``cons`` supplies its constitutive
+    features (branch ids, reduced cohesion)."""
     tok = str(solver_type).upper()
     opts = dict(amg_opts or {})
     if tok in ("DFGMRES_B200", "DFGMRES_HYPRE_BOOMERAMG", "DFGMRES_BOOMERAMG", "BOOMERAMG", "HYPRE_BOOMERAMG"):
@@ -229,5 +246,9 @@ def set_linear_solver(solver_type, linear_solver_tolerance, linear_solver_maxit,
         amg = None
     else:
         raise ValueError(f"Bad choice of solver type: {solver_type}")
-    return DFGMRES(dmesh, linear_solver_tolerance, linear_solver_maxit, deflation_basis_tolerance,
-                   linear_solver_printing, amg=amg)
+    solver = DFGMRES(dmesh, linear_solver_tolerance, linear_solver_maxit, deflation_basis_tolerance,
+                     linear_solver_printing, amg=amg)
+    if learned:
+        from .learned import LearnedCorrection
+        solver.learned = LearnedCorrection(dmesh, cons=cons, **(learned if isinstance(learned, dict) else {}))
+    return solver

@@ -1,0 +1,64 @@
+"""CPU checks of the learned-correction oracle (oracle/learned_ref.py), which the tensor-core
+kernels are compared against: BF16 rounding equals torch's round-to-nearest-even
+conversion, and the exact (FP64) backward pass and the loss gradient dL/dG agree with
+central finite differences."""
+import numpy as np
+import scipy.sparse as sp
+import torch
+
+from oracle import learned_ref as L
+
+
+def test_bf16_rounding_matches_torch():
+    rng = np.random.default_rng(0)
+    x = np.concatenate([rng.normal(size=4000) * 10.0 ** rng.integers(-6, 6, 4000), [0.0, -0.0, 1.0, 1.00390625,
+                                                                                    1.005859375, -3.0e38]])
+    x = x.astype(np.float32)
+    ref = torch.from_numpy(x).to(torch.bfloat16).to(torch.float32).numpy()
+    assert np.array_equal(L.bf16(x), ref)
+    bits = torch.from_numpy(x).to(torch.bfloat16).view(torch.int16).numpy().view(np.uint16)
+    assert np.array_equal(L.bf16_bits(x), bits)
+
+
+def test_mlp_backward_matches_finite_differences():
+    rng = np.random.default_rng(1)
+    p = L.init_params(3, zero_last=False).astype(np.float64)
+    n = 40
+    X = rng.normal(size=(n, L.NF))
+    dG = rng.normal(size=(n, L.NO))
+
+    def f(q):
+        Y, _ = L.mlp_forward(q, X, exact=True)
+        return float((Y * dG).sum())
+
+    g = L.mlp_backward(p, X, dG, exact=True)
+    idx = rng.choice(L.NPARAM, 60, replace=False)
+    h = 1e-5
+    for i in idx:
+        e = np.zeros_like(p)
+        e[i] = h
+        fd = (f(p + e) - f(p - e)) / (2 * h)
+        assert abs(fd - g[i]) <= 1e-5 * max(1.0, abs(fd)), (i, fd, g[i])
+
+
+def test_correction_loss_gradient_matches_finite_differences():
+    rng = np.random.default_rng(2)
+    n = 30
+    B = sp.random(3 * n, 3 * n, density=0.1, random_state=4)
+    A = (B @ B.T + sp.eye(3 * n) * 3.0).tocsr()
+    Kd = np.stack([A[3 * i:3 * i + 3, 3 * i:3 * i + 3].toarray() for i in range(n)])
+    Dinv = L.block_inv(Kd)
+    mask = np.ones((n, 3))
+    mask[0] = 0.0
+    rz = [rng.normal(size=3 * n) for _ in range(3)]
+    G = rng.normal(size=(n, L.NO)) * 0.3
+    loss, dG = L.correction_loss(G, Dinv, mask, A, rz)
+    h = 1e-6
+    for _ in range(40):
+        i, k = rng.integers(n), rng.integers(9)
+        Gp, Gm = G.copy(), G.copy()
+        Gp[i, k] += h
+        Gm[i, k] -= h
+        fd = (L.correction_loss(Gp, Dinv, mask, A, rz)[0] - L.correction_loss(Gm, Dinv, mask, A, rz)[0]) / (2 * h)
+        assert abs(fd - dG[i, k]) <= 1e-6 * max(1.0, abs(fd))
+    assert np.all(dG[:, 9:] == 0) and np.all(dG[0] == 0)
