@@ -10,16 +10,21 @@ Newton tol 1e-4 (the reference scripts' settings).  Synthetic, seeded, no datase
 A step is one accepted step of SSR_indirect_continuation (the sum of its attempts, as
 stats.step_wall_time).  The init phase is untimed, W warm-up steps run untimed, then exactly
 K steps are timed with CUDA events (barrier + synchronize on both sides; max over ranks).
-Two forms run back to back on the same workload from the same start: ``plain`` (FP64
-throughout) and ``mixed`` (FP32 V-cycle inside the FP64 FGMRES; return mapping, Newton
-residual, Arnoldi and the lambda update in FP64).  ``value`` is the mixed form's s/step (the
-form the metric names), the plain form's figures and the lambda error between the forms at
-equal step index are in ``config``.  ``value`` excludes the per-step host<->device state copies;
+Three forms run back to back on the same workload from the same start: ``plain`` (FP64
+throughout), ``mixed`` (FP32 V-cycle inside the FP64 FGMRES; return mapping, Newton
+residual, Arnoldi and the lambda update in FP64) and ``learned`` (mixed plus the learned
+node-wise correction of the V-cycle: a per-node BF16 network trained on the GPU during the
+init phase, on the residual vectors of the plain V-cycle for the init phase's fourth
+Newton system, then kept only if a trial solve of that system needs fewer FGMRES
+iterations with it; training and trial time are reported, not timed).  ``value`` is the learned
+form's s/step (mixed+learned, the form the metric names); the other forms' figures and the
+lambda error of each form against plain at equal step index are in ``config``.  ``value`` excludes the per-step host<->device state copies;
 ``e2e`` includes them: every timed step starts by copying its input state (U, U_old) from
 pinned host memory and ends by reading the new state back.  The working set (K_r 441 MB,
 Krylov bases ~1 GB) exceeds the 126 MB L2, so no flush is needed between steps.
 
-  python bench.py [--gpus N] [--steps K] [--warmup W] [--form both|plain|mixed] [--impl reference]
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--form all|both|plain|mixed|learned]
+                  [--impl reference]
 
 Multi-GPU: replicas only (each rank runs the same continuation; no collective on the path).
 """
@@ -45,6 +50,9 @@ UNIT = "s/step"
 WORKLOAD = ("3D homogeneous slope SSR, mesh_P2_3D(N_h=1, 15,10,15,10,10, z=40): 156,000 P2 tets, "
             "220,401 nodes, 631,380 free DOFs, 1,716,000 integration points")
 COUNTS_FILE = os.path.join(ROOT, "profiles", "ssr3d_z40_step_counts.json")
+# learned form: trained before the init phase's 4th linear solve on 12 residual vectors of
+# that Newton system, 60 full-batch Adam steps
+LEARNED_OPTS = dict(train_at=3, n_vectors=12, steps=60, lr=3e-3, seed=0)
 N_INSTR = 8
 
 
@@ -54,7 +62,7 @@ def parse():
     ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    ap.add_argument("--form", default="both", choices=["both", "plain", "mixed"])
+    ap.add_argument("--form", default="all", choices=["all", "both", "plain", "mixed", "learned"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--workload", default="ssr", choices=["ssr", "box"],
                     help="ssr: the SSR continuation step (headline); box: the return-map microbenchmark")
@@ -128,9 +136,11 @@ def run_form(args, form, P, rank, world):
 
     from slope_stability_octave_b200 import _lib, problems
     from slope_stability_octave_b200.continuation import SSRIndirectStepper
+    from slope_stability_octave_b200.linear_solvers import set_linear_solver
 
     t0 = time.perf_counter()
-    solver = P.solver("DFGMRES_B200_MIXED" if form == "mixed" else "DFGMRES_B200", tol=1e-1, maxit=100)
+    solver = set_linear_solver("DFGMRES_B200" if form == "plain" else "DFGMRES_B200_MIXED", 1e-1, 100, 1e-3, 0,
+                               P.dmesh, P.mesh.coord, learned=LEARNED_OPTS if form == "learned" else None, cons=P.cons)
     f = P.f_device()
     run = SSRIndirectStepper(problems.SSR_3D_EXTRUDED, P.dmesh.mask, f, P.cons, solver).init()
     t_init = time.perf_counter() - t0
@@ -183,6 +193,12 @@ def run_form(args, form, P, rank, world):
     res = dict(t_dev=t_dev, t_e2e=t_e2e, steps=steps, basis=basis, launches=launches, instr=(ms, nt, nl),
                clocks=clk, t_init=t_init, lam=[s["lam"] for s in steps], amg=solver.preconditioner.info(),
                lam_init=list(run.lambda_hist[: 2 + args.warmup]))
+    if solver.learned is not None:
+        lc = solver.learned
+        res["learned"] = dict(train_s=round(lc.train_seconds, 3), trained_at_solve=lc.train_at,
+                              loss_first=float(lc.loss_hist[0]), loss_last=float(lc.loss_hist[-1]),
+                              fallbacks=lc.fallbacks, solves=lc.solves, params=lc.info()["nparam"],
+                              acceptance_trial=lc.gate, applied=bool(lc.enabled))
     del run, solver
     torch.cuda.empty_cache()
     return res
@@ -401,13 +417,14 @@ def main():
         return
     from slope_stability_octave_b200 import problems
     P = problems.slope_3d(1).to_device()
-    forms = ["plain", "mixed"] if args.form == "both" else [args.form]
+    forms = {"all": ["plain", "mixed", "learned"], "both": ["plain", "mixed"]}.get(args.form, [args.form])
     out = {form: run_form(args, form, P, rank, world) for form in forms}
     if world > 1:
         torch.distributed.destroy_process_group()
     if rank != 0:
         return
-    head = out["mixed"] if "mixed" in out else out["plain"]
+    head_form = "learned" if "learned" in out else ("mixed" if "mixed" in out else "plain")
+    head = out[head_form]
     K = args.steps
     value_step = head["t_dev"] / K
     e2e_step = head["t_e2e"] / K
@@ -441,15 +458,19 @@ def main():
             linear_iterations=[s["linear_iterations"] for s in r["steps"]],
             attempts=[s["attempts"] for s in r["steps"]], deflation_basis=r["basis"], init_s=round(r["t_init"], 2),
             gpu_launches=r["launches"], amg_levels=[(l["rows"], l["block"]) for l in r["amg"]["levels"]])
-    if "plain" in out and "mixed" in out:
-        lp, lm = out["plain"]["lam"], out["mixed"]["lam"]
-        forms_cfg["lambda_rel_err_mixed_vs_plain"] = max(abs(a - b) / abs(a) for a, b in zip(lp, lm))
-        forms_cfg["speedup_mixed_vs_plain"] = out["plain"]["t_dev"] / out["mixed"]["t_dev"]
+        if "learned" in r:
+            forms_cfg[form]["network"] = r["learned"]
+    for other in ("mixed", "learned"):
+        if "plain" in out and other in out:
+            lp, lm = out["plain"]["lam"], out[other]["lam"]
+            forms_cfg[f"lambda_rel_err_{other}_vs_plain"] = max(abs(a - b) / abs(a) for a, b in zip(lp, lm))
+            forms_cfg[f"speedup_{other}_vs_plain"] = out["plain"]["t_dev"] / out[other]["t_dev"]
     line = dict(
         metric=METRIC, value=value_step, unit=UNIT, n_gpus=args.gpus, steps=K, warmup=args.warmup,
         ms_per_step=value_step * 1e3, higher_is_better=False, scaling="weak", vs_baseline=None,
-        dtype="f64" if "mixed" not in out else "f64 (f32 V-cycle)", data="synthetic (seeded mesh and material)",
-        config=dict(workload=WORKLOAD, form="mixed" if "mixed" in out else "plain",
+        dtype={"plain": "f64", "mixed": "f64 (f32 V-cycle)", "learned": "f64 (f32 V-cycle, bf16 network)"}[head_form],
+        data="synthetic (seeded mesh and material)",
+        config=dict(workload=WORKLOAD, form=head_form,
                     parallelism=f"replicas x{args.gpus}", solver="DFGMRES tol 1e-1 + AMG V-cycle, Newton tol 1e-4",
                     l2="working set > L2 (no flush needed)", forms=forms_cfg),
         e2e=dict(value=e2e_step, unit=UNIT, h2d_bytes_per_step=h2d, d2h_bytes_per_step=d2h),

@@ -229,9 +229,10 @@ int sg_a_orthogonalize(sg_krylov *ws, const sg_bsr *A, const double *A_vals, dou
  * G_i = MLP(phi_i), a per-node network 16 -> 64 -> 64 -> 9 (ReLU) run on the tensor cores
  * (BF16 operands, FP32 accumulation) over node features phi from the matrix, the Newton
  * residual and the constitutive state; D_i the node's diagonal block, M_i its free-DOF mask.
- * Training minimises the mean of |rz - A M G D^{-1} rz|^2 / |rz|^2 over residual vectors
- * rz = v - A V(v) of the plain preconditioner, collected from the Newton system; the last
- * layer starts at zero, so the untrained correction is the plain V-cycle.
+ * Training minimises the residual norm |rz - A M G D^{-1} rz|^2 (or, as an option, the
+ * energy norm of the error the corrected cycle leaves) over residual vectors rz = v - A V(v)
+ * of the plain preconditioner, collected from the Newton system; the last layer starts at
+ * zero, so the untrained correction is the plain V-cycle.
  * ---------------------------------------------------------------------------- */
 #define SG_LEARNED_NPARAM 6288 /* W1[16][64] b1[64] W2[64][64] b2[64] W3[64][16] b3[16] (FP32) */
 /* z += C (r - A z) after every V-cycle; C: device n_rows x 9 (row-major 3 x 3), copied;
@@ -264,7 +265,11 @@ int sg_learned_correction(sg_learned *h, sg_amg *amg, double *C_out, void *strea
  * 1 (held out), replacing (append = 0) or appending; switches amg's correction off */
 int sg_learned_collect(sg_learned *h, sg_amg *amg, const sg_bsr *A, const double *A_vals, const double *b,
                        int32_t count, int32_t slot, int32_t append, void *stream);
-/* mean relative corrected residual |rz - A d|^2/|rz|^2 over a slot's vectors */
+/* training objective: 0 (default) the mean relative corrected residual |rz - A d|^2/|rz|^2;
+ * 1 the mean change of the error's energy norm, (|e - d|_A^2 - |e|_A^2) / (rz' D^{-1} rz) with
+ * A e = rz (0 for the plain cycle, negative when the correction helps) */
+int sg_learned_set_loss(sg_learned *h, int32_t kind);
+/* the training objective over a slot's vectors */
 int sg_learned_loss(sg_learned *h, const sg_bsr *A, const double *A_vals, int32_t slot, double *loss,
                     void *stream);
 /* gradient of that loss with respect to the parameters (host, NPARAM floats) */

@@ -11,7 +11,8 @@ tensor-core kernels can be checked against it:
                                FP64 accumulation; ``exact=True`` drops the rounding (for
                                finite-difference checks of the gradient formulas)
   features                     the 16 node features
-  correction_loss              L = (1/S) sum_s |rz_s - A M G D^-1 rz_s|^2 / |rz_s|^2 and dL/dG
+  correction_loss              the training objective (energy norm of the corrected error, or
+                               the residual norm) and dL/dG
 
 Parity is pinned by the finite-difference checks of the FP64 path in the tests (there is no
 reference implementation to pin against).
@@ -146,8 +147,12 @@ def block_inv(Kdiag):
     return out
 
 
-def correction_loss(G, Dinv, mask, A, rz_list):
-    """L and dL/dG (n x 16, columns 9.. zero) for the correction d = M (G9 Dinv rz)."""
+def correction_loss(G, Dinv, mask, A, rz_list, kind="energy"):
+    """L and dL/dG (n x 16, columns 9.. zero) for the correction d = M (G9 Dinv rz).
+
+    kind "residual": L = (1/S) sum |rz - A d|^2 / |rz|^2;
+    kind "energy":   L = (1/S) sum (d'A d - 2 d'rz) / (rz' Dinv rz), the change of the
+                     error's energy norm |e - d|_A^2 - |e|_A^2 for A e = rz."""
     n = Dinv.shape[0]
     G9 = np.asarray(G, np.float64)[:, :9].reshape(n, 3, 3)
     S = len(rz_list)
@@ -155,11 +160,17 @@ def correction_loss(G, Dinv, mask, A, rz_list):
     dG = np.zeros((n, NO))
     for rz in rz_list:
         rz = np.asarray(rz, np.float64)
-        w = 1.0 / (S * float(rz @ rz))
         y = np.einsum("nij,nj->ni", Dinv, rz.reshape(n, 3))
         d = (np.einsum("nij,nj->ni", G9, y) * mask).ravel()
-        e = rz - A @ d
-        L += w * float(e @ e)
-        g = (A @ e).reshape(n, 3) * mask
+        q = A @ d
+        e = rz - q
+        if kind == "energy":
+            w = 1.0 / (S * float(rz @ y.ravel()))
+            L += w * float(d @ (q - 2.0 * rz))
+            g = e.reshape(n, 3) * mask
+        else:
+            w = 1.0 / (S * float(rz @ rz))
+            L += w * float(e @ e)
+            g = (A @ e).reshape(n, 3) * mask
         dG[:, :9] += (-2.0 * w * np.einsum("na,nb->nab", g, y)).reshape(n, 9)
     return L, dG

@@ -70,6 +70,7 @@ SIGNATURES = {
     "sg_learned_features": [vp, vp, vp, vp, vp, vp],
     "sg_learned_correction": [vp, vp, vp, vp],
     "sg_learned_collect": [vp, vp, vp, vp, vp, i32, i32, i32, vp],
+    "sg_learned_set_loss": [vp, i32],
     "sg_learned_loss": [vp, vp, vp, i32, vp, vp],
     "sg_learned_gradient": [vp, vp, vp, i32, vp, vp, vp],
     "sg_learned_train": [vp, vp, vp, i32, f64, vp, vp],

@@ -14,14 +14,18 @@
 // preconditioner is a fixed linear operator for each matrix; the network only chooses the
 // node-wise weights.  With the last layer at zero it is exactly the plain V-cycle.
 //
-// Training minimises the true FP64 residual of the corrected preconditioner on vectors that
-// the plain solver itself produced (residual sequences of the Newton system):
+// Training runs on vectors that the plain solver itself produced (residual sequences of the
+// Newton system), rz_s = v_s - A V(v_s), d_s = M G (D^{-1} rz_s), e_s = rz_s - A d_s.  The
+// default objective is the FP64 residual, L = (1/S) sum_s |e_s|^2 / |rz_s|^2 with
+// dL/dG_i = (1/S) sum_s (-2/|rz_s|^2) (M A e_s)_i (D^{-1} rz_s)_i^T.  The alternative is the
+// energy norm of the error the corrected cycle leaves: with
+// A err_s = rz_s,  |err_s - d_s|_A^2 - |err_s|_A^2 = d_s' A d_s - 2 d_s' rz_s, so
 //
-//     L = (1/S) sum_s || rz_s - A d_s ||^2 / || rz_s ||^2,   d_s = M G (D^{-1} rz_s),
-//     rz_s = v_s - A V(v_s),
+//     L = (1/S) sum_s (d_s' A d_s - 2 d_s' rz_s) / (rz_s' D^{-1} rz_s),
+//     dL/dG_i = (1/S) sum_s (-2 / rz_s' D^{-1} rz_s) (M e_s)_i (D^{-1} rz_s)_i^T
 //
-// so dL/dG_i = (1/S) sum_s (-2/||rz_s||^2) (M A e_s)_i (D^{-1} rz_s)_i^T with e_s the
-// corrected residual.  The network runs on the tensor cores: BF16 operands staged in shared
+// (measured: it over-corrects the smooth error components and raises the FGMRES iteration
+// counts several-fold, so it is kept as an option only).  The network runs on the tensor cores: BF16 operands staged in shared
 // memory in the canonical no-swizzle K-major layout, tcgen05.mma with FP32 accumulators in
 // tensor memory, one elected thread issuing, completion through an mbarrier; the backward
 // pass recomputes the forward for each 128-node tile and accumulates the weight gradients
@@ -590,6 +594,26 @@ __global__ void k_residual(int64_t n, const double *__restrict__ rz, const doubl
     if (threadIdx.x == 0) part[blockIdx.x] = red[0];
 }
 
+// e = rz - q; per-block partial sums of d . (q - 2 rz) into part[blockIdx.x] (the change of the
+// energy norm of the error, |e_z - d|_A^2 - |e_z|_A^2, for rz = A e_z and q = A d)
+__global__ void k_energy(int64_t n, const double *__restrict__ d, const double *__restrict__ rz,
+                         const double *__restrict__ q, double *__restrict__ e, double *__restrict__ part) {
+    __shared__ double red[256];
+    double s = 0.0;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        const double qi = q[i], ri = rz[i];
+        e[i] = ri - qi;
+        s += d[i] * (qi - 2.0 * ri);
+    }
+    red[threadIdx.x] = s;
+    __syncthreads();
+    for (int o = 128; o > 0; o >>= 1) {
+        if ((int)threadIdx.x < o) red[threadIdx.x] += red[threadIdx.x + o];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) part[blockIdx.x] = red[0];
+}
+
 // loss[slot] += w * sum(part)   (one thread)
 __global__ void k_loss_acc(const double *__restrict__ part, int nparts, double w, double *__restrict__ loss, int first) {
     if (threadIdx.x != 0 || blockIdx.x != 0) return;
@@ -795,6 +819,8 @@ struct sg_learned {
     double *Dinv = nullptr, *C = nullptr, *stats = nullptr, *spart = nullptr;
     double *rz[2] = {nullptr, nullptr}, *y[2] = {nullptr, nullptr};   // [slot][vec * nd]
     double *nrm[2] = {nullptr, nullptr};                               // host copies of |rz|^2
+    double *nrmE[2] = {nullptr, nullptr};                              // host copies of rz' Dinv rz
+    int loss_kind = 0;                                                 // 0 residual, 1 energy
     double *v = nullptr, *z = nullptr, *d = nullptr, *q = nullptr, *e = nullptr, *g = nullptr;
     double *loss = nullptr, *lpart = nullptr;
     int *err = nullptr;
@@ -810,6 +836,8 @@ static int lfree(sg_learned *h) {
         if (p) cudaFree(p);
     delete[] h->nrm[0];
     delete[] h->nrm[1];
+    delete[] h->nrmE[0];
+    delete[] h->nrmE[1];
     delete h;
     return SG_OK;
 }
@@ -850,6 +878,8 @@ extern "C" int sg_learned_create(const sg_mesh *mesh, const double *coord, int32
     h->max_vec = max_vectors;
     h->nrm[0] = new double[max_vectors]();
     h->nrm[1] = new double[max_vectors]();
+    h->nrmE[0] = new double[max_vectors]();
+    h->nrmE[1] = new double[max_vectors]();
     int rc = SG_OK;
     const int gparts = mlp_grid(h->nn);
 #define LA(p, n) if (!rc) rc = zalloc(&(p), (size_t)(n))
@@ -993,6 +1023,9 @@ extern "C" int sg_learned_collect(sg_learned *h, sg_amg *amg, const sg_bsr *A, c
         if ((rc = sg_dot_dev(nd, h->q, h->q, &qq, stream))) return rc;
         if ((rc = sg_dot_dev(nd, rzk, rzk, &rr, stream))) return rc;
         h->nrm[slot][base + k] = rr;
+        double ry = 0.0;
+        if ((rc = sg_dot_dev(nd, rzk, yk, &ry, stream))) return rc;
+        h->nrmE[slot][base + k] = ry;
         // next v = v - a q, a = (v.q)/(q.q): the residual of one minimal-residual step
         k_axpy_scale<<<grid_for(nd, 256), 256, 0, st>>>(nd, h->v, h->q, qq > 0 ? -vq / qq : 0.0, 1.0);
         SG_CUDA(cudaGetLastError());
@@ -1002,8 +1035,8 @@ extern "C" int sg_learned_collect(sg_learned *h, sg_amg *amg, const sg_bsr *A, c
     return SG_OK;
 }
 
-// mean relative corrected residual over slot's vectors: loss = (1/S) sum |rz - A d|^2/|rz|^2,
-// with the current network; when grad != 0 also dG (dL/dG), left in the handle.
+// training objective over slot's vectors with the current network (sg_learned_set_loss);
+// when want_grad also dG (dL/dG), left in the handle.
 static int loss_pass(sg_learned *h, const sg_bsr *A, const double *A_vals, int slot, bool want_grad, cudaStream_t st) {
     const int S = h->n_vec[slot];
     if (S <= 0) return set_error(SG_ERR_STATE, "no vectors collected in this slot");
@@ -1013,18 +1046,36 @@ static int loss_pass(sg_learned *h, const sg_bsr *A, const double *A_vals, int s
     const unsigned gr = grid_for(nd, 256);
     for (int s = 0; s < S; ++s) {
         const double *rzs = h->rz[slot] + (int64_t)s * nd, *ys = h->y[slot] + (int64_t)s * nd;
-        const double w = 1.0 / (S * (h->nrm[slot][s] > 0 ? h->nrm[slot][s] : 1.0));
+        const bool energy = h->loss_kind == 1;
+        const double nr = energy ? h->nrmE[slot][s] : h->nrm[slot][s];
+        const double w = 1.0 / (S * (nr > 0 ? nr : 1.0));
         k_apply_G<<<grid_for(nn, 256), 256, 0, st>>>(nn, h->G, h->mesh->d_mask, ys, h->d);
         if ((rc = sg_bsr_spmv_dev(A, A_vals, h->d, h->q, st))) return rc;
-        k_residual<<<gr, 256, 0, st>>>(nd, rzs, h->q, h->e, h->lpart);
+        if (energy)
+            k_energy<<<gr, 256, 0, st>>>(nd, h->d, rzs, h->q, h->e, h->lpart);
+        else
+            k_residual<<<gr, 256, 0, st>>>(nd, rzs, h->q, h->e, h->lpart);
         count_launch();
         k_loss_acc<<<1, 32, 0, st>>>(h->lpart, (int)gr, w, h->loss, s == 0);
         if (want_grad) {
-            if ((rc = sg_bsr_spmv_dev(A, A_vals, h->e, h->g, st))) return rc;
-            k_grad_G<<<grid_for(nn, 256), 256, 0, st>>>(nn, -2.0 * w, h->mesh->d_mask, h->g, ys, h->dG, s == 0);
+            // residual loss: dL/dd = -2 w A e;  energy loss: dL/dd = 2 w (A d - rz) = -2 w e
+            const double *g = h->e;
+            if (!energy) {
+                if ((rc = sg_bsr_spmv_dev(A, A_vals, h->e, h->g, st))) return rc;
+                g = h->g;
+            }
+            k_grad_G<<<grid_for(nn, 256), 256, 0, st>>>(nn, -2.0 * w, h->mesh->d_mask, g, ys, h->dG, s == 0);
         }
         SG_CUDA(cudaGetLastError());
     }
+    return SG_OK;
+}
+
+// training objective: 0 (default) the mean relative residual |rz - A d|^2 / |rz|^2, 1 the
+// mean change of the error's energy norm (|e_z - d|_A^2 - |e_z|_A^2) / (rz' D^{-1} rz)
+extern "C" int sg_learned_set_loss(sg_learned *h, int32_t kind) {
+    SG_CHECK_ARG(h && (kind == 0 || kind == 1), "bad argument");
+    h->loss_kind = kind;
     return SG_OK;
 }
 

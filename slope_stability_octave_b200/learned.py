@@ -10,8 +10,9 @@ G_i = MLP(phi_i) from a per-node network (16 -> 64 -> 64 -> 9, ReLU; BF16 tensor
 kernels with FP32 accumulation, written for sm_100a) over node features of the current
 Newton system.  The network is trained on the GPU by the library's own forward and
 backward kernels, on residual vectors that the plain preconditioner produces for the
-Newton system it is solving, by minimising the true FP64 residual of the corrected
-preconditioner.  The last layer starts at zero, so the untrained correction is exactly
+Newton system it is solving, by minimising the true FP64 residual that the corrected
+cycle leaves (optionally the energy norm of its error: A e = rz gives
+|e - d|_A^2 - |e|_A^2 = d'A d - 2 d'rz, so no solve is needed).  The last layer starts at zero, so the untrained correction is exactly
 the plain V-cycle, and ``DFGMRES.solve`` falls back to the plain V-cycle when a corrected
 solve does not reach its tolerance.
 """
@@ -32,14 +33,16 @@ class LearnedCorrection:
     """Owner of the network, its training vectors and the correction handed to an AMG.
 
     train_at       index of the DFGMRES solve (0-based, counted over the solver's life)
-                   whose Newton system provides the training vectors; training happens
-                   just before that solve, which then runs corrected
+                   whose Newton system provides the training vectors; training and the
+                   acceptance trial happen just before that solve
     n_vectors      residual vectors collected for training
     steps, lr      full-batch Adam steps and learning rate
+    loss           training objective: "residual" (the FP64 residual the corrected cycle
+                   leaves) or "energy" (the energy norm of its error)
     """
 
     def __init__(self, dmesh: DeviceMesh, cons=None, train_at=0, n_vectors=12, steps=60, lr=3e-3, seed=0,
-                 max_vectors=None):
+                 max_vectors=None, loss="residual"):
         if dmesh.dim != 3:
             raise ValueError("the learned correction is defined for 3D meshes")
         self.dmesh = dmesh
@@ -54,7 +57,11 @@ class LearnedCorrection:
         _lib.call("sg_learned_create", dmesh.handle, hptr(self._coord), int(max_vectors or max(self.n_vectors, 8)),
                   int(seed), C.byref(h))
         self.handle = h
+        _lib.call("sg_learned_set_loss", h, {"residual": 0, "energy": 1}[loss])
+        self.loss_kind = loss
         self.trained = False
+        self.enabled = False
+        self.gate = None
         self.solves = 0
         self.fallbacks = 0
         self.loss_hist = None
@@ -147,24 +154,36 @@ class LearnedCorrection:
                     adam_steps=int(buf[4]))
 
     # ------------------------------------------------------------------ DFGMRES hook
-    def before_solve(self, amg, K, b):
-        """Called by DFGMRES.solve: train on this system when its turn comes, then set the
-        correction for K on the AMG instance (off until trained)."""
+    def wants_training(self):
+        return not self.trained and self.solves >= self.train_at
+
+    def train_on(self, amg, K, b):
+        """Collect this system's residual vectors and train (called by DFGMRES.solve)."""
         import time
-        idx = self.solves
+        t0 = time.perf_counter()
+        self.features(K, b)
+        self.collect(amg, K, b, self.n_vectors, slot=0)
+        self.train(K)
+        torch.cuda.synchronize()
+        self.train_seconds += time.perf_counter() - t0
+        self.trained = True
+
+    def decide(self, it_plain, it_corrected, seconds=0.0):
+        """Acceptance gate: keep the correction only if the trial solve of the training
+        system needed fewer DFGMRES iterations with it than without."""
+        self.gate = dict(plain_iterations=int(it_plain), corrected_iterations=int(it_corrected),
+                         accepted=bool(it_corrected < it_plain))
+        self.enabled = self.gate["accepted"]
+        self.train_seconds += seconds
+
+    def before_solve(self, amg, K, b):
+        """Set the correction for the system K x = b on the AMG instance when the network is
+        trained and accepted; otherwise switch it off.  True when the solve runs corrected."""
         self.solves += 1
         if amg is None:
             return False
-        if not self.trained and idx >= self.train_at:
-            t0 = time.perf_counter()
-            self.features(K, b)
-            self.collect(amg, K, b, self.n_vectors, slot=0)
-            self.train(K)
-            torch.cuda.synchronize()
-            self.train_seconds += time.perf_counter() - t0
-            self.trained = True
-        if not self.trained:
-            _lib.call("sg_amg_set_correction", amg.handle, None, cur_stream())
+        if not (self.trained and self.enabled):
+            self.off(amg)
             return False
         self.features(K, b)
         self.correction(amg)

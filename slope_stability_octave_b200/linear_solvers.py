@@ -186,7 +186,19 @@ class DFGMRES:
         """x, nit = solve(K, b) on device vectors (dfgmres_solver.m)."""
         t0 = time.perf_counter()
         amg = self.preconditioner
-        corrected = self.learned.before_solve(amg, K, b) if self.learned is not None else False
+        lc = self.learned
+        if lc is not None and amg is not None and lc.wants_training():
+            # train on this system, then the acceptance trial: plain vs corrected solve
+            lc.train_on(amg, K, b)
+            t1 = time.perf_counter()
+            lc.off(amg)
+            _, it_plain, _ = self._solve_core(K, b)
+            lc.features(K, b)
+            lc.correction(amg)
+            _, it_corr, rr_corr = self._solve_core(K, b)
+            lc.decide(it_plain, it_corr if rr_corr <= self.tolerance else self.max_iterations + 1,
+                      time.perf_counter() - t1)
+        corrected = lc.before_solve(amg, K, b) if lc is not None else False
         x, nit, rr = self._solve_core(K, b)
         if corrected and not (rr <= self.tolerance):
             # the corrected preconditioner did not reach the tolerance: plain V-cycle

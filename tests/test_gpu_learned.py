@@ -10,13 +10,15 @@
     oracle's; the diagonal-block inverses within 1e-12;
   * the training loss and its parameter gradient through the whole chain (network, 3x3
     correction, FP64 SpMVs, backward) against the oracle on the vectors the GPU collected:
-    loss within 1e-6, gradient within 3e-2 relative per group;
+    loss within 1e-6, gradient within 3e-2 relative per group, for both objectives;
   * the gain: after training on residual vectors of the Newton system's own right-hand side,
     the corrected V-cycle leaves a smaller residual on held-out vectors of another right-hand
-    side than the plain V-cycle (loss < 0.9, the plain cycle's is exactly 1), and DFGMRES at
-    the continuation's linear tolerance (1e-1) needs no more iterations with it than without
-    (at 1e-6 at most 4 more: the local correction is not symmetric);
-  * the DFGMRES hook trains at its first solve and returns a solution at the tolerance.
+    side than the plain V-cycle (objective < 0.9, the plain cycle's is exactly 1), and DFGMRES
+    at the continuation's linear tolerance (1e-1) needs no more iterations with it than
+    without (at 1e-6 at most 4 more: the local correction is not symmetric);
+  * the DFGMRES hook trains at its first solve, runs the acceptance trial (plain vs
+    corrected solve of the training system; the correction is kept only if it needs fewer
+    iterations) and returns a solution at the tolerance.
 """
 import numpy as np
 import pytest
@@ -164,19 +166,21 @@ def test_training_gradient_matches_oracle(system):
     p = LR.init_params(11, zero_last=False)
     p[LR.OFF_W3:LR.OFF_B3] *= 0.05
     lc.set_params(p)
-    g, loss = lc.gradient(s["K"], slot=0)
     X = lc.export("features")
     Dinv = lc.export("Dinv")
     rz = [lc.export("rz0", i) for i in range(6)]
     _, mask = oracle_inputs(s)
     Y, _ = LR.mlp_forward(p, X)
-    loss_ref, dG = LR.correction_loss(Y[:nn], Dinv, mask, s["A"], rz)
-    assert abs(loss - loss_ref) <= 1e-6 * abs(loss_ref)
-    dGp = np.zeros((X.shape[0], 16))
-    dGp[:nn] = dG
-    ref = LR.mlp_backward(p, X, dGp.astype(np.float32))
-    errs = group_errors(g.astype(np.float64), ref)
-    assert max(errs.values()) <= 3e-2, errs
+    for kind, code in (("energy", 1), ("residual", 0)):
+        _lib.call("sg_learned_set_loss", lc.handle, code)
+        g, loss = lc.gradient(s["K"], slot=0)
+        loss_ref, dG = LR.correction_loss(Y[:nn], Dinv, mask, s["A"], rz, kind)
+        assert abs(loss - loss_ref) <= 1e-6 * abs(loss_ref), kind
+        dGp = np.zeros((X.shape[0], 16))
+        dGp[:nn] = dG
+        ref = LR.mlp_backward(p, X, dGp.astype(np.float32))
+        errs = group_errors(g.astype(np.float64), ref)
+        assert max(errs.values()) <= 3e-2, (kind, errs)
 
 
 def test_trained_correction_gains_over_plain_vcycle(system):
@@ -189,7 +193,7 @@ def test_trained_correction_gains_over_plain_vcycle(system):
     assert lc.loss(K, slot=1) == pytest.approx(1.0, abs=1e-12)     # untrained: the plain cycle
     hist = lc.train(K)
     held = lc.loss(K, slot=1)
-    print(f"train loss {hist[0]:.4f} -> {hist[-1]:.4f}; held-out {held:.4f}")
+    print(f"residual objective: train {hist[0]:.4f} -> {hist[-1]:.4f}; held-out {held:.4f}")
     assert hist[-1] < hist[0]
     assert held < 0.9
     # DFGMRES iterations on the Newton system, plain vs corrected, at the continuation's
@@ -219,6 +223,10 @@ def test_dfgmres_hook_trains_and_solves(system):
                                learned=dict(train_at=0, n_vectors=8, steps=30), cons=P.cons)
     solver.setup_preconditioner(K)
     x, it = solver.solve(K, s["b"])
-    assert solver.learned.trained and solver.learned.info()["adam_steps"] == 30
+    lc = solver.learned
+    assert lc.trained and lc.info()["adam_steps"] == 30
+    g = lc.gate
+    print(f"acceptance trial: {g}")
+    assert g["accepted"] == (g["corrected_iterations"] < g["plain_iterations"]) and lc.enabled == g["accepted"]
     r = (s["A"] @ x.cpu().numpy()) - s["b"].cpu().numpy()
     assert np.linalg.norm(r) <= 1.1e-6 * np.linalg.norm(s["b"].cpu().numpy())

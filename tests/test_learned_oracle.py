@@ -52,13 +52,23 @@ def test_correction_loss_gradient_matches_finite_differences():
     mask[0] = 0.0
     rz = [rng.normal(size=3 * n) for _ in range(3)]
     G = rng.normal(size=(n, L.NO)) * 0.3
-    loss, dG = L.correction_loss(G, Dinv, mask, A, rz)
-    h = 1e-6
-    for _ in range(40):
-        i, k = rng.integers(n), rng.integers(9)
-        Gp, Gm = G.copy(), G.copy()
-        Gp[i, k] += h
-        Gm[i, k] -= h
-        fd = (L.correction_loss(Gp, Dinv, mask, A, rz)[0] - L.correction_loss(Gm, Dinv, mask, A, rz)[0]) / (2 * h)
-        assert abs(fd - dG[i, k]) <= 1e-6 * max(1.0, abs(fd))
-    assert np.all(dG[:, 9:] == 0) and np.all(dG[0] == 0)
+    for kind in ("energy", "residual"):
+        loss, dG = L.correction_loss(G, Dinv, mask, A, rz, kind)
+        h = 1e-6
+        for _ in range(40):
+            i, k = rng.integers(n), rng.integers(9)
+            Gp, Gm = G.copy(), G.copy()
+            Gp[i, k] += h
+            Gm[i, k] -= h
+            fd = (L.correction_loss(Gp, Dinv, mask, A, rz, kind)[0]
+                  - L.correction_loss(Gm, Dinv, mask, A, rz, kind)[0]) / (2 * h)
+            assert abs(fd - dG[i, k]) <= 1e-6 * max(1.0, abs(fd))
+        assert np.all(dG[:, 9:] == 0) and np.all(dG[0] == 0)
+    # the energy objective is the exact change of the error's energy norm
+    d = np.zeros(3 * n)
+    y = np.einsum("nij,nj->ni", Dinv, rz[0].reshape(n, 3))
+    d[:] = (np.einsum("nij,nj->ni", G[:, :9].reshape(n, 3, 3), y) * mask).ravel()
+    e = np.linalg.solve(A.toarray(), rz[0])
+    change = (e - d) @ (A @ (e - d)) - e @ (A @ e)
+    assert abs(L.correction_loss(G, Dinv, mask, A, rz[:1], "energy")[0] * float(rz[0] @ y.ravel()) - change) \
+        <= 1e-9 * abs(change)
