@@ -49,7 +49,19 @@ METRIC = "s per SSR continuation step, 3D P2 (mixed+learned vs plain FP64 GPU) a
 UNIT = "s/step"
 WORKLOAD = ("3D homogeneous slope SSR, mesh_P2_3D(N_h=1, 15,10,15,10,10, z=40): 156,000 P2 tets, "
             "220,401 nodes, 631,380 free DOFs, 1,716,000 integration points")
-COUNTS_FILE = os.path.join(ROOT, "profiles", "ssr3d_z40_step_counts.json")
+HETERO_WORKLOAD = ("3D heterogeneous slope SSR, four horizontal layers 5/5/10/20 m from the crest down, clipped at "
+                   "the base (c, phi, E, nu, gamma = 15,30,50MPa,0.3,19 / 10,35,40MPa,0.3,20 / 18,25,60MPa,0.3,21 / "
+                   "6,45,40MPa,0.3,20), mesh_P2_3D(N_h=5/3 i.e. h=0.6 m, 15,10,15,10,10, z=40): 728,022 P2 tets, "
+                   "1,005,075 nodes, 2,932,430 free DOFs, 8,008,242 integration points")
+# workload name -> (description, problem factory, CPU-sample factory (a slice of the same
+# mesh, about 1/10 to 1/17 of its points), per-step counts file of the reference arm)
+WORKLOADS = {
+    "ssr": (WORKLOAD, lambda pb: pb.slope_3d(1), lambda pb: pb.slope_3d(1, dims=(15, 10, 15, 10, 10, 4)),
+            os.path.join(ROOT, "profiles", "ssr3d_z40_step_counts.json"), "z=4 m slice (1/10)"),
+    "hetero": (HETERO_WORKLOAD, lambda pb: pb.slope_3d_layered(5 / 3),
+               lambda pb: pb.slope_3d_layered(5 / 3, dims=(15, 10, 15, 10, 10, 2.4)),
+               os.path.join(ROOT, "profiles", "ssr3d_layered_h06_step_counts.json"), "z=2.4 m slice (4 of 67 cells)"),
+}
 # learned form: trained before the init phase's 4th linear solve on 12 residual vectors of
 # that Newton system, 60 full-batch Adam steps
 LEARNED_OPTS = dict(train_at=3, n_vectors=12, steps=60, lr=3e-3, seed=0)
@@ -64,8 +76,10 @@ def parse():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--form", default="all", choices=["all", "both", "plain", "mixed", "learned"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", default="ssr", choices=["ssr", "box"],
-                    help="ssr: the SSR continuation step (headline); box: the return-map microbenchmark")
+    ap.add_argument("--workload", default="ssr", choices=["ssr", "hetero", "ll", "box"],
+                    help="ssr: the SSR continuation step on the homogeneous 40 m slope (headline); hetero: the "
+                         "same on the layered slope at h = 0.6 m; ll: limit-load continuation on the random-field "
+                         "slope at h = 0.45 m; box: the return-map microbenchmark")
     return ap.parse_args()
 
 
@@ -120,12 +134,14 @@ def peaks():
         return 6650.0, "fallback"
 
 
-def traffic_per_spmv():
-    """DRAM bytes per fine-level SpMV launch from the committed ncu summary (null if absent)."""
+def traffic_per_spmv(n_blocks):
+    """DRAM bytes per fine-level SpMV launch from the committed ncu summary, scaled from the
+    captured matrix to ``n_blocks`` blocks (null if absent)."""
     try:
         with open(os.path.join(ROOT, "profiles", "roofline_traffic.json")) as fh:
-            return json.load(fh).get("spmv3_f64_dram_bytes_per_launch")
-    except (OSError, ValueError):
+            d = json.load(fh)
+        return d["spmv3_f64_dram_bytes_per_launch"] * n_blocks / d["spmv3_f64_blocks"]
+    except (OSError, ValueError, KeyError):
         return None
 
 
@@ -215,14 +231,14 @@ def step_counts(res):
                 branch_mix=(0.8, 0.1, 0.04, 0.04, 0.02))
 
 
-def cpu_sample(log=lambda *a: None):
-    """The CPU path's unit costs are timed on a z = 4 m slice of the workload (1/10 of its
-    points, elements and DOFs) and scaled by the size ratio."""
+def cpu_sample(workload="ssr", log=lambda *a: None):
+    """The CPU path's unit costs are timed on a slice of the workload (the same mesh spacing
+    and material, a few cells deep in z) and scaled by the size ratio."""
     from oracle.cpu_baseline import CPUSample
     from slope_stability_octave_b200 import problems, workloads
     from slope_stability_octave_b200.linear_solvers import near_null_space_elasticity
 
-    S = problems.slope_3d(1, dims=(15, 10, 15, 10, 10, 4))
+    S = WORKLOADS[workload][2](problems)
     pts = workloads.constitutive_points(S.weight.size, seed=7, fractions=(0.8, 0.1, 0.04, 0.04, 0.02))
     smp = CPUSample(S.mesh, S.dphi, S.weight, S.n_q, S.mat, pts, log=log)
     Z = near_null_space_elasticity(S.mesh.coord, S.mesh.Q)
@@ -240,12 +256,13 @@ def cpu_step_seconds(S, smp, counts, n_int_full, n_dof_full):
     return step_seconds(cs, counts), c
 
 
-CPU_SAMPLE_TEXT = ("one modelled continuation step: unit costs of every Newton-iteration operation timed on a "
-                   "z=4 m slice of the workload (1/10 of its points/elements/DOFs) and scaled by size, weighted by "
-                   "the timed GPU steps' Newton/Krylov/deflation counts; return mapping and tangent assembly are "
-                   "the reference's own C (MEX sources compiled with -O2 -fopenmp, all host threads), B*U, B'S, "
-                   "SpMV, Gram-Schmidt, deflation and the AMG set-up/V-cycle are the NumPy/SciPy port (the "
-                   "reference's Octave/sparsersb/HYPRE layer is not installable)")
+def cpu_sample_text(workload="ssr"):
+    return ("one modelled continuation step: unit costs of every Newton-iteration operation timed on a "
+            f"{WORKLOADS[workload][4]} of the workload and scaled by size, weighted by "
+            "the timed GPU steps' Newton/Krylov/deflation counts; return mapping and tangent assembly are "
+            "the reference's own C (MEX sources compiled with -O2 -fopenmp, all host threads), B*U, B'S, "
+            "SpMV, Gram-Schmidt, deflation and the AMG set-up/V-cycle are the NumPy/SciPy port (the "
+            "reference's Octave/sparsersb/HYPRE layer is not installable)")
 
 
 def reference_arm(args, rank, world):
@@ -254,9 +271,10 @@ def reference_arm(args, rank, world):
     import numpy as np
     threads = os.cpu_count() or 1
     os.environ.setdefault("OMP_NUM_THREADS", str(threads))
-    with open(COUNTS_FILE) as fh:
+    desc, _, _, counts_file, _ = WORKLOADS[args.workload]
+    with open(counts_file) as fh:
         counts = json.load(fh)
-    S, smp = cpu_sample()
+    S, smp = cpu_sample(args.workload)
     vals = []
     for i in range(args.warmup + args.steps):
         v, _ = cpu_step_seconds(S, smp, counts, counts["n_int"], counts["n_dof"])
@@ -266,13 +284,85 @@ def reference_arm(args, rank, world):
     line = dict(metric=METRIC, value=value, unit=UNIT, n_gpus=args.gpus, steps=args.steps, warmup=args.warmup,
                 ms_per_step=value * 1e3, higher_is_better=False, scaling="weak", vs_baseline=None, dtype="f64",
                 data="synthetic", impl="reference",
-                config=dict(workload=WORKLOAD, form="reference CPU path (plain FP64)", parallelism="replicas",
+                config=dict(workload=desc, form="reference CPU path (plain FP64)", parallelism="replicas",
                             counts=counts),
                 cpu_baseline=dict(value=value, unit=UNIT, cores=int(os.environ["OMP_NUM_THREADS"]), kind="port",
-                                  sample=CPU_SAMPLE_TEXT),
+                                  sample=cpu_sample_text(args.workload)),
                 e2e=dict(value=value, unit=UNIT, h2d_bytes_per_step=0, d2h_bytes_per_step=0))
     print(json.dumps(line))
     return line
+
+
+LL_METRIC = "s per LL continuation step, 3D P2 random-field slope (mixed vs plain FP64 GPU) at equal step"
+LL_WORKLOAD = ("3D limit-load (LL) indirect continuation on the extruded slope with lognormal random-field strength "
+               "(c mean 10 kPa CoV 0.3, phi mean 35 deg CoV 0.1, independent, exponential correlation 5 m, circulant "
+               "embedding on a 0.5 m grid, seed 20261203; E = 40 MPa, nu = 0.3, gamma = 20), mesh_P2_3D(N_h=20/9 "
+               "i.e. h=0.45 m, 15,10,15,10,10, z=40)")
+
+
+def run_ll_form(args, form, P):
+    """Elastic start, then W + K accepted steps of LL_indirect_continuation; the last K are
+    timed (sum of attempt wall times with the device synchronised around each attempt)."""
+    import torch
+
+    from slope_stability_octave_b200 import continuation, problems
+    from slope_stability_octave_b200.linear_solvers import set_linear_solver
+
+    p = problems.LL_3D_EXTRUDED
+    t0 = time.perf_counter()
+    solver = set_linear_solver("DFGMRES_B200" if form == "plain" else "DFGMRES_B200_MIXED", 1e-1, 100, 1e-3, 0,
+                               P.dmesh, P.mesh.coord, learned=LEARNED_OPTS if form == "learned" else None, cons=P.cons)
+    f = P.f_device()
+    Q = P.dmesh.mask
+    U0, d_omega = continuation.LL_elastic_start(Q, f, P.cons, solver)
+    torch.cuda.synchronize()
+    t_init = time.perf_counter() - t0
+    _, th, oh, _, st = continuation.LL_indirect_continuation(
+        d_omega, p["d_t_min"], p["step_max"], p["omega_max"], p["it_newt_max"], p["it_damp_max"], p["tol"],
+        p["r_min"], None, U0, Q, f, P.cons, solver.copy(), max_steps=args.warmup + args.steps)
+    n = len(st["step_wall_time"])
+    if n < args.warmup + args.steps:
+        raise RuntimeError(f"LL continuation stopped after {n} steps ({st['stop_reason']})")
+    timed = st["step_wall_time"][args.warmup:]
+    res = dict(t=list(th[1:]), omega=list(oh[1:]), newton=st["step_newton_iterations"],
+               linear=st["step_linear_iterations"], attempts=st["attempts"], wall=st["step_wall_time"],
+               s_per_step=sum(timed) / len(timed), init_s=round(t_init, 2))
+    del solver
+    torch.cuda.empty_cache()
+    return res
+
+
+def run_ll(args, rank, world):
+    import torch
+
+    from slope_stability_octave_b200 import problems
+    t0 = time.perf_counter()
+    P = problems.slope_3d_random_field(20 / 9).to_device()
+    t_setup = time.perf_counter() - t0
+    forms = {"all": ["plain", "mixed", "learned"], "both": ["plain", "mixed"]}.get(args.form, [args.form])
+    clocks = ClockSampler(torch.cuda.current_device()).start()
+    out = {form: run_ll_form(args, form, P) for form in forms}
+    clk = clocks.stop()
+    if rank != 0:
+        return
+    head_form = "mixed" if "mixed" in out else forms[0]
+    m = P.mesh
+    cfg = dict(workload=LL_WORKLOAD, mesh=dict(tets=m.n_e, nodes=m.n_n, free_dofs=int(m.Q.sum()),
+                                               points=int(P.weight.size)),
+               random_field=m.info.get("random_field"), setup_s=round(t_setup, 1), form=head_form,
+               timing="sum of attempt wall times per accepted step, device synchronised around each attempt",
+               forms=out)
+    for other in ("mixed", "learned"):
+        if "plain" in out and other in out:
+            tp, tm = out["plain"]["t"], out[other]["t"]
+            cfg[f"t_rel_err_{other}_vs_plain"] = max(abs(a - b) / abs(a) for a, b in zip(tp, tm))
+            cfg[f"speedup_{other}_vs_plain"] = out["plain"]["s_per_step"] / out[other]["s_per_step"]
+    v = out[head_form]["s_per_step"]
+    line = dict(metric=LL_METRIC, value=v, unit=UNIT, n_gpus=args.gpus, steps=args.steps, warmup=args.warmup,
+                ms_per_step=v * 1e3, higher_is_better=False, scaling="weak", vs_baseline=None,
+                dtype="f64 (f32 V-cycle)" if head_form != "plain" else "f64", data="synthetic (seeded random field)",
+                config=cfg, clocks=clk)
+    print(json.dumps(line))
 
 
 BOX_METRIC = "ms per return-map pass (S and DS), structured box 80x40x40 m, 8,448,000 points"
@@ -410,13 +500,17 @@ def main():
     if world > 1:
         torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
                                              device_id=torch.device("cuda", torch.cuda.current_device()))
-    if args.workload == "box":
-        run_box(args, rank)
+    if args.workload in ("box", "ll"):
+        if args.workload == "box":
+            run_box(args, rank)
+        else:
+            run_ll(args, rank, world)
         if world > 1:
             torch.distributed.destroy_process_group()
         return
     from slope_stability_octave_b200 import problems
-    P = problems.slope_3d(1).to_device()
+    desc = WORKLOADS[args.workload][0]
+    P = WORKLOADS[args.workload][1](problems).to_device()
     forms = {"all": ["plain", "mixed", "learned"], "both": ["plain", "mixed"]}.get(args.form, [args.form])
     out = {form: run_form(args, form, P, rank, world) for form in forms}
     if world > 1:
@@ -442,10 +536,10 @@ def main():
     cpu = None
     if not args.no_cpu_baseline and args.gpus == 1:
         try:
-            S, smp = cpu_sample()
+            S, smp = cpu_sample(args.workload)
             v, _ = cpu_step_seconds(S, smp, counts, P.dmesh.n_int, n_dof)
             cpu = dict(value=v, unit=UNIT, cores=int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1)),
-                       kind="port", sample=CPU_SAMPLE_TEXT)
+                       kind="port", sample=cpu_sample_text(args.workload))
         except Exception as exc:  # the CPU leg must not hide the GPU result
             cpu = dict(value=None, unit=UNIT, cores=None, kind="port", sample=f"failed: {exc}")
     h2d = 2 * 8 * n_dof
@@ -470,7 +564,7 @@ def main():
         ms_per_step=value_step * 1e3, higher_is_better=False, scaling="weak", vs_baseline=None,
         dtype={"plain": "f64", "mixed": "f64 (f32 V-cycle)", "learned": "f64 (f32 V-cycle, bf16 network)"}[head_form],
         data="synthetic (seeded mesh and material)",
-        config=dict(workload=WORKLOAD, form=head_form,
+        config=dict(workload=desc, form=head_form,
                     parallelism=f"replicas x{args.gpus}", solver="DFGMRES tol 1e-1 + AMG V-cycle, Newton tol 1e-4",
                     l2="working set > L2 (no flush needed)", forms=forms_cfg),
         e2e=dict(value=e2e_step, unit=UNIT, h2d_bytes_per_step=h2d, d2h_bytes_per_step=d2h),
@@ -479,11 +573,12 @@ def main():
         roofline=dict(kernel="k_spmv_blk 3x3 FP64, fine level (Arnoldi, projection, smoother, residual)",
                       bound="hbm", achieved=achieved, peak=peak, unit="GB/s",
                       frac=(achieved / peak if achieved else None), peak_kind=peak_kind,
-                      traffic=traffic_per_spmv(), algorithmic_bytes_per_launch=spmv_bytes,
+                      traffic=traffic_per_spmv(n_blocks), algorithmic_bytes_per_launch=spmv_bytes,
                       launches=int(nl[0]), timed_launches=int(nt[0]), avg_ms=spmv_ms,
                       other_kernels={name: dict(launches=int(nl[i]), avg_ms=(ms[i] / nt[i] if nt[i] else None))
                                      for i, name in enumerate(["spmv3_f64", "spmv3_f32", "constitutive_S_DS",
-                                                               "constitutive_S", "assembly"]) if nl[i]}),
+                                                               "constitutive_S", "assembly", "amg_update",
+                                                               "amg_vcycle"]) if nl[i]}),
         cpu_baseline=cpu,
         counts=counts,
     )

@@ -370,3 +370,87 @@ def davis_reduction(c0, phi, psi, lam, davis="B"):
     else:
         raise ValueError("Davis type must be 'A', 'B' or 'C'")
     return 2 * c_l * np.cos(phi_l), np.sin(phi_l)
+
+
+# ----------------------------------------------------------------- random fields
+
+
+def _embedding_eigenvalues(shape, spacing, corr_len):
+    """Eigenvalues of the block-circulant embedding of the exponential covariance
+    exp(-r / corr_len) on a periodic grid of ``shape`` points with ``spacing`` (the
+    covariance evaluated at the periodic lag min(k, m - k) * spacing per axis)."""
+    lags = [np.minimum(np.arange(m), m - np.arange(m)) * d for m, d in zip(shape, spacing)]
+    r2 = np.zeros(shape)
+    for ax, lag in enumerate(lags):
+        sh = [1] * len(shape)
+        sh[ax] = -1
+        r2 = r2 + (lag ** 2).reshape(sh)
+    cov = np.exp(-np.sqrt(r2) / corr_len)
+    return np.fft.fftn(cov).real
+
+
+def gaussian_fields_circulant(lower, upper, spacing, corr_len, seed, n_fields=2, max_pad=64):
+    """Independent standard Gaussian random fields with the isotropic exponential covariance
+    exp(-|x - y| / corr_len), sampled on the regular grid lower + spacing * k covering the box
+    [lower, upper], by circulant embedding (Dietrich & Newsam 1997, SIAM J. Sci. Comput.
+    18(4):1088-1107; Wood & Chan 1994): the covariance on a periodic grid of at least twice the
+    box is diagonalised by the FFT, white noise is coloured by the square roots of its
+    eigenvalues, and one complex FFT gives two independent fields (real and imaginary parts).
+    The periodic grid is padded until every eigenvalue is non-negative (up to ``max_pad``
+    points per axis); any negative remainder is set to zero and its share reported.
+
+    Returns (fields (n_fields, *grid_shape), grid axes, info)."""
+    lower = np.asarray(lower, np.float64)
+    upper = np.asarray(upper, np.float64)
+    n = np.maximum(np.ceil((upper - lower) / spacing).astype(int) + 1, 2)
+    axes = [lower[i] + spacing * np.arange(n[i]) for i in range(n.size)]
+    pad = 0
+    while True:
+        m = tuple(int(2 * (k - 1) + 2 * pad) for k in n)
+        lam = _embedding_eigenvalues(m, [spacing] * n.size, corr_len)
+        if lam.min() >= -1e-12 * lam.max() or pad >= max_pad:
+            break
+        pad = max(2 * pad, 4)
+    neg = float(-lam[lam < 0].sum() / lam.sum()) if (lam < 0).any() else 0.0
+    sq = np.sqrt(np.maximum(lam, 0.0) / lam.size)
+    rng = np.random.default_rng(seed)
+    out = []
+    for _ in range((n_fields + 1) // 2):
+        xi = rng.standard_normal(m) + 1j * rng.standard_normal(m)
+        y = np.fft.fftn(sq * xi)
+        sl = tuple(slice(0, k) for k in n)
+        out += [y.real[sl], y.imag[sl]]
+    info = dict(grid=tuple(int(k) for k in n), embedding=m, pad=pad, negative_eigen_share=neg,
+                method="circulant embedding, exponential covariance")
+    return np.stack(out[:n_fields]), axes, info
+
+
+def trilinear(field, axes, pts):
+    """Trilinear interpolation of a grid ``field`` (nx, ny, nz) on ``axes`` at ``pts`` (3, n)."""
+    idx, frac = [], []
+    for a, p in zip(axes, pts):
+        h = a[1] - a[0]
+        t = np.clip((p - a[0]) / h, 0.0, a.size - 1 - 1e-12)
+        i = np.floor(t).astype(np.int64)
+        idx.append(i)
+        frac.append(t - i)
+    (i, j, k), (u, v, w) = idx, frac
+    out = np.zeros(pts.shape[1])
+    for di, wi in ((0, 1 - u), (1, u)):
+        for dj, wj in ((0, 1 - v), (1, v)):
+            for dk, wk in ((0, 1 - w), (1, w)):
+                out += wi * wj * wk * field[i + di, j + dj, k + dk]
+    return out
+
+
+def lognormal_from_gaussian(g, mean, cov):
+    """Lognormal values of the given mean and coefficient of variation from standard normal g."""
+    s2 = np.log1p(cov ** 2)
+    return np.exp(np.log(mean) - s2 / 2 + np.sqrt(s2) * g)
+
+
+def integration_points(mesh: Mesh, hat):
+    """Physical coordinates (dim, n_e * n_q) of the integration points, element-major
+    (the point order of the per-point fields)."""
+    X = mesh.coord[:, mesh.elem]                      # (dim, n_p, n_e)
+    return np.einsum("dpe,pq->deq", X, hat).reshape(mesh.dim, -1)

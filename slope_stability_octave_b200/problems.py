@@ -33,6 +33,10 @@ SSR_3D_EXTRUDED = dict(SSR_3D, omega_max_stop=7e7)
 # limit-load continuation parameters of slope_stability_3D_homo_LL.m:82-96 and
 # slope_stability_2D_homo_LL.m:154-163
 LL_3D = dict(d_t_min=1e-3, step_max=100, omega_max=5100.0, it_newt_max=200, it_damp_max=10, tol=1e-4, r_min=1e-4)
+# the 40 m deep extruded slope carries ~40x the work f'U of the reference's 1 m-thick LL
+# mesh scale, so its omega bound is lifted as for SSR; runs stop on the t increment or a
+# step budget
+LL_3D_EXTRUDED = dict(LL_3D, omega_max=7e7)
 LL_2D = dict(d_t_min=1e-3, step_max=100, omega_max=2000.0, it_newt_max=100, it_damp_max=10, tol=1e-4, r_min=1e-4)
 
 
@@ -119,3 +123,41 @@ def slope_3d_layered(N_h=1, dims=(15, 10, 15, 10, 10, 40)):
     mesh = fem.mesh_p2_3d(N_h, *dims)
     ids = layered_material_ids(mesh, top=dims[3] + dims[4])
     return _assemble_problem(mesh, ids, LAYERS_CFG3)
+
+
+# strength random field of the limit-load workload: lognormal c and phi, independent,
+# isotropic exponential correlation; E = 40 MPa, nu = 0.3, gamma = 20 kN/m^3 everywhere
+RANDOM_FIELD_CFG4 = dict(c_mean=10.0, c_cov=0.3, phi_mean=35.0, phi_cov=0.1, corr_len=5.0, young=40000.0, nu=0.3,
+                         gamma=20.0, spacing=0.5)
+
+
+def random_field_materials(mesh, hat, seed, rf=RANDOM_FIELD_CFG4):
+    """Per-integration-point material of a slope whose cohesion and friction angle are
+    independent lognormal random fields (means and coefficients of variation in ``rf``) with
+    the exponential correlation exp(-r / corr_len).  The two standard Gaussian fields come
+    from one circulant-embedding draw on a grid of ``spacing`` over the mesh's bounding box
+    (fem.gaussian_fields_circulant) and are interpolated trilinearly to the integration
+    points.  The reference scripts have no random fields; this generator is this library's."""
+    lo, hi = mesh.coord.min(axis=1), mesh.coord.max(axis=1)
+    G, axes, info = fem.gaussian_fields_circulant(lo, hi, rf["spacing"], rf["corr_len"], seed, n_fields=2)
+    X = fem.integration_points(mesh, hat)
+    g_c = fem.trilinear(G[0], axes, X)
+    g_phi = fem.trilinear(G[1], axes, X)
+    c0 = fem.lognormal_from_gaussian(g_c, rf["c_mean"], rf["c_cov"])
+    phi = fem.lognormal_from_gaussian(g_phi, rf["phi_mean"], rf["phi_cov"])
+    mat = fem.elastic_fields_from_point_draws(c0, phi, rf["young"], rf["nu"])
+    mat["gamma"] = np.full(c0.size, rf["gamma"])
+    return mat, info
+
+
+def slope_3d_random_field(N_h=1, dims=(15, 10, 15, 10, 10, 40), seed=20261203, rf=RANDOM_FIELD_CFG4):
+    """The extruded 3D slope with lognormal random-field strength (limit-load workload)."""
+    mesh = fem.mesh_p2_3d(N_h, *dims)
+    xi, wf = fem.quadrature_p2_tet()
+    hat, d1, d2, d3 = fem.local_basis_p2_tet(xi)
+    D1, D2, D3, W = fem.geometry_3d(mesh, d1, d2, d3, wf)
+    mat, info = random_field_materials(mesh, hat, seed, rf)
+    f = fem.gravity_load(mesh, hat, W, mat["gamma"])
+    P = Problem(mesh, (D1, D2, D3), W, hat, wf.size, mat, f, "B")
+    mesh.info["random_field"] = info
+    return P

@@ -3,10 +3,12 @@
   * SSR indirect continuation on the GPU (DFGMRES + AMG at a linear tolerance of 1e-10, so
     lambda carries no Krylov error) against the oracle's histories computed with a sparse
     direct solver (tests/golden/ssr_oracle.npz, made by make_continuation_golden.py):
-    lambda and omega within 1e-6 relative, Newton iteration counts equal;
+    lambda and omega within 1e-6 relative, Newton iteration counts equal; homogeneous 2D and
+    3D slopes and the four-layer heterogeneous 3D slope;
   * limit-load (LL) indirect continuation from the scripts' elastic start, seven accepted
     steps, against the oracle's (tests/golden/ll_oracle.npz): load factor t and omega within
-    1e-6 relative, Newton iteration counts equal;
+    1e-6 relative, Newton iteration counts equal; homogeneous 2D and 3D slopes and the 3D
+    slope with lognormal random-field cohesion and friction angle;
   * SSR direct continuation (lambda controlled, omega from the integrated potential by a
     backward difference) against the oracle's (tests/golden/ssr_direct_oracle.npz): lambda
     and omega within 1e-6 relative over four steps after the init phase; the device
@@ -35,6 +37,8 @@ GOLDEN_DIRECT = os.path.join(os.path.dirname(__file__), "golden", "ssr_direct_or
 CASES = {
     "cfg0": (lambda: problems.slope_2d(0.5), problems.SSR_2D),
     "small3d": (lambda: problems.slope_3d(1, dims=(15, 10, 15, 10, 10, 1)), problems.SSR_3D),
+    # the four-layer heterogeneous slope (per-element materials) on the same small mesh
+    "layered3d": (lambda: problems.slope_3d_layered(1, dims=(15, 10, 15, 10, 10, 1)), problems.SSR_3D),
 }
 
 
@@ -64,6 +68,9 @@ def test_ssr_continuation_matches_oracle(cuda_device, case):
 LL_CASES = {
     "cfg0": (lambda: problems.slope_2d(0.5), problems.LL_2D),
     "small3d": (lambda: problems.slope_3d(1, dims=(15, 10, 15, 10, 10, 1)), problems.LL_3D),
+    # per-point lognormal random-field strength (the limit-load workload's material) on the same mesh
+    "rf3d": (lambda: problems.slope_3d_random_field(1, dims=(15, 10, 15, 10, 10, 1), seed=20261203),
+             problems.LL_3D),
 }
 
 
@@ -102,10 +109,13 @@ def run_direct(P, p, tol, steps=None):
     return lh, oh
 
 
-@pytest.mark.parametrize("case", sorted(CASES))
+DIRECT_CASES = {k: CASES[k] for k in ("cfg0", "small3d")}
+
+
+@pytest.mark.parametrize("case", sorted(DIRECT_CASES))
 def test_ssr_direct_continuation_matches_oracle(cuda_device, case):
     g = np.load(GOLDEN_DIRECT)
-    make, p = CASES[case]
+    make, p = DIRECT_CASES[case]
     lam_ref, om_ref = g[f"{case}_lambda"], g[f"{case}_omega"]
     lh, oh = run_direct(make(), p, 1e-10, steps=len(lam_ref) - 2)
     assert lh.shape == lam_ref.shape
