@@ -1,12 +1,23 @@
 #!/usr/bin/env python
 """Benchmark: seconds per SSR continuation step, 3D P2 (indirect continuation).
 
-Workload (``config.workload``): the 3D homogeneous slope of the reference's SSR drivers,
-extruded 40 m -- mesh_P2_3D(N_h = 1, 15, 10, 15, 10, 10, z = 40): 156,000 P2 tets, 220,401
-nodes, 631,380 free DOFs, 1,716,000 integration points; Mohr-Coulomb (c = 6 kPa, phi = 45 deg,
-psi = 0, E = 40 MPa, nu = 0.3, gamma = 20), Davis B, DFGMRES tol 1e-1 with the AMG V-cycle,
-Newton tol 1e-4 (the reference scripts' settings).  Synthetic, seeded, no dataset.
+Workloads (``--workload``, named in ``config.workload``; synthetic, seeded, no dataset):
 
+  hetero (default, the headline)  the 3D heterogeneous slope: the reference's extruded slope
+      mesh_P2_3D(N_h = 5/3, i.e. h = 0.6 m, 15, 10, 15, 10, 10, z = 40) -- 728,022 P2 tets,
+      1,005,075 nodes, 2,932,430 free DOFs, 8,008,242 integration points -- with four
+      horizontal material layers 5/5/10/20 m thick counted from the crest down and clipped
+      at the base (c, phi, E, nu, gamma per layer: 15 kPa, 30 deg, 50 MPa, 0.3, 19 / 10, 35,
+      40, 0.3, 20 / 18, 25, 60, 0.3, 21 / 6, 45, 40, 0.3, 20);
+  ssr  the 3D homogeneous slope, mesh_P2_3D(N_h = 1, 15, 10, 15, 10, 10, z = 40): 156,000 P2
+      tets, 220,401 nodes, 631,380 free DOFs, 1,716,000 points; c = 6 kPa, phi = 45 deg,
+      psi = 0, E = 40 MPa, nu = 0.3, gamma = 20;
+  ll   limit-load continuation on the slope with lognormal random-field strength at
+      h = 0.45 m (see LL_WORKLOAD);
+  box  the return-map microbenchmark (see BOX_WORKLOAD).
+
+SSR workloads: Davis B, DFGMRES tol 1e-1 with the AMG V-cycle, Newton tol 1e-4 (the
+reference scripts' settings).
 A step is one accepted step of SSR_indirect_continuation (the sum of its attempts, as
 stats.step_wall_time).  The init phase is untimed, W warm-up steps run untimed, then exactly
 K steps are timed with CUDA events (barrier + synchronize on both sides; max over ranks).
@@ -20,11 +31,12 @@ iterations with it; training and trial time are reported, not timed).  ``value``
 form's s/step (mixed+learned, the form the metric names); the other forms' figures and the
 lambda error of each form against plain at equal step index are in ``config``.  ``value`` excludes the per-step host<->device state copies;
 ``e2e`` includes them: every timed step starts by copying its input state (U, U_old) from
-pinned host memory and ends by reading the new state back.  The working set (K_r 441 MB,
-Krylov bases ~1 GB) exceeds the 126 MB L2, so no flush is needed between steps.
+pinned host memory and ends by reading the new state back.  The working set (K_r 2.0 GB on
+the layered slope, 441 MB on the homogeneous one; Krylov bases several GB) exceeds the 126 MB
+L2, so no flush is needed between steps.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--form all|both|plain|mixed|learned]
-                  [--impl reference]
+                  [--workload hetero|ssr|ll|box] [--impl reference]
 
 Multi-GPU: replicas only (each rank runs the same continuation; no collective on the path).
 """
@@ -32,6 +44,7 @@ from __future__ import annotations
 
 import argparse
 import ctypes as C
+import gc
 import json
 import os
 import statistics
@@ -76,10 +89,10 @@ def parse():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--form", default="all", choices=["all", "both", "plain", "mixed", "learned"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", default="ssr", choices=["ssr", "hetero", "ll", "box"],
-                    help="ssr: the SSR continuation step on the homogeneous 40 m slope (headline); hetero: the "
-                         "same on the layered slope at h = 0.6 m; ll: limit-load continuation on the random-field "
-                         "slope at h = 0.45 m; box: the return-map microbenchmark")
+    ap.add_argument("--workload", default="hetero", choices=["hetero", "ssr", "ll", "box"],
+                    help="hetero: the SSR continuation step on the layered slope at h = 0.6 m (headline); ssr: the "
+                         "same on the homogeneous 40 m slope at h = 1 m; ll: limit-load continuation on the "
+                         "random-field slope at h = 0.45 m; box: the return-map microbenchmark")
     return ap.parse_args()
 
 
@@ -172,6 +185,10 @@ def run_form(args, form, P, rank, world):
     steps, basis = [], []
     clocks = ClockSampler(torch.cuda.current_device()).start()
     _lib.call("sg_instr_enable", 1, 4)
+    # no Python garbage collection inside the timed region (a collection pass stalls the
+    # launching thread while the device drains its queue)
+    gc.collect()
+    gc.disable()
     torch.cuda.synchronize()
     barrier(world)
     torch.cuda.synchronize()
@@ -194,6 +211,7 @@ def run_form(args, form, P, rank, world):
         basis.append(solver.k)
     torch.cuda.synchronize()
     torch.cuda.nvtx.range_pop()
+    gc.enable()
     barrier(world)
     launches = int(_lib.lib().sg_launch_count(1))
     ms = np.zeros(N_INSTR)
@@ -206,7 +224,8 @@ def run_form(args, form, P, rank, world):
     t_dev = sum(ev[k][1].elapsed_time(ev[k][2]) for k in range(args.steps)) / 1e3
     t_e2e = sum(ev[k][0].elapsed_time(ev[k][3]) for k in range(args.steps)) / 1e3
     t_dev, t_e2e = max_over_ranks([t_dev, t_e2e], world, device="cuda")
-    res = dict(t_dev=t_dev, t_e2e=t_e2e, steps=steps, basis=basis, launches=launches, instr=(ms, nt, nl),
+    step_s = [ev[k][1].elapsed_time(ev[k][2]) / 1e3 for k in range(args.steps)]
+    res = dict(t_dev=t_dev, t_e2e=t_e2e, steps=steps, step_s=step_s, basis=basis, launches=launches, instr=(ms, nt, nl),
                clocks=clk, t_init=t_init, lam=[s["lam"] for s in steps], amg=solver.preconditioner.info(),
                lam_init=list(run.lambda_hist[: 2 + args.warmup]))
     if solver.learned is not None:
@@ -547,7 +566,8 @@ def main():
     forms_cfg = {}
     for form, r in out.items():
         forms_cfg[form] = dict(
-            s_per_step=r["t_dev"] / K, e2e_s_per_step=r["t_e2e"] / K, lambdas=r["lam"],
+            s_per_step=r["t_dev"] / K, e2e_s_per_step=r["t_e2e"] / K, step_s=[round(t, 4) for t in r["step_s"]],
+            lambdas=r["lam"],
             newton_iterations=[s["newton_iterations_total"] for s in r["steps"]],
             linear_iterations=[s["linear_iterations"] for s in r["steps"]],
             attempts=[s["attempts"] for s in r["steps"]], deflation_basis=r["basis"], init_s=round(r["t_init"], 2),

@@ -183,8 +183,11 @@ int sg_axpby_dev(int64_t n, double a, const double *x, double b, double *y, void
  *              block graph); the numeric set-up runs during creation when given
  *   nullspace  (n_rows*b) x nns column-major host array; fixed: per-DOF 1 = Dirichlet (host)
  *   opts       [max_levels, coarse_size, cheb_degree, cheb_ratio, power_its, mixed(0/1),
- *               omega_scale, theta]; entries <= 0 keep the defaults (10, 1200, 2, 30, 10, 0,
- *               4/3, 0.05) except theta, where 0 selects the whole block graph
+ *               omega_scale, theta, fine_half(0/1)]; entries <= 0 keep the defaults (10, 1200,
+ *               3, 10, 10, 0, 4/3, 0.02, 0) except theta, where 0 selects the whole block graph.
+ *               fine_half (mixed cycle, 3x3 blocks, theta > 0): the cycle's level-0 SpMVs read
+ *               an FP16 copy of A scaled by a power of two (FP32 accumulation); the numeric
+ *               set-up stays FP32
  * ---------------------------------------------------------------------------- */
 typedef struct sg_amg sg_amg;
 int sg_amg_create(const sg_bsr *A, const double *A_vals, const double *nullspace, int32_t nns,

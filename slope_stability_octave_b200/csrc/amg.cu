@@ -23,6 +23,7 @@
 //
 // Every product is a gather over a precomputed list, so the numeric set-up uses no atomics
 // and is deterministic.
+#include <cuda_fp16.h>
 #include <cuda_runtime.h>
 #include <omp.h>
 
@@ -34,6 +35,7 @@
 #include <type_traits>
 #include <vector>
 
+#include "instr.cuh"
 #include "linalg.cuh"
 #include "mesh.h"
 #include "sg_common.cuh"
@@ -63,6 +65,8 @@ struct Level {
     const double *Avals = nullptr;  // level 0: caller's values (set at update)
     double *Aown_vals = nullptr;    // coarse levels
     float *A32 = nullptr;
+    uint2 *A16 = nullptr;          // level 0 with fine_half: FP16 rows of A / a16_scale, 3 words per block
+    float a16_scale = 1.0f;        // power of two putting the set-up matrix's largest entry near 4096
     int32_t *d_diag_own = nullptr;
     double *Dinv = nullptr;
     float *Dinv32 = nullptr;
@@ -96,6 +100,7 @@ struct AmgOptions {
     int mixed = 0;            // 1: FP32 V-cycle
     double omega_scale = 4.0 / 3.0;
     double theta = 0.02;      // strength threshold (0: whole block graph)
+    int fine_half = 0;        // mixed form, 3x3 level 0: the cycle's level-0 SpMVs read an FP16 copy
 };
 
 }  // namespace sg
@@ -490,7 +495,30 @@ __device__ __forceinline__ void load_block(const float *__restrict__ src, double
     }
 }
 
-// AP block = sum over plan pairs A_a (B x B) * P_b (B x BC)
+// Block of N values in their storage type into registers (16-byte loads when the block size
+// allows it; blocks of such arrays then start on 16-byte boundaries).
+template <int N, typename V>
+__device__ __forceinline__ void load_raw(const V *__restrict__ src, V *dst) {
+    constexpr int W = 16 / (int)sizeof(V);
+    if constexpr (N % W == 0) {
+        using Vec = typename std::conditional<sizeof(V) == 8, double2, float4>::type;
+        const Vec *s = reinterpret_cast<const Vec *>(src);
+#pragma unroll
+        for (int t = 0; t < N / W; ++t) *reinterpret_cast<Vec *>(dst + t * W) = __ldg(s + t);
+    } else if constexpr (sizeof(V) == 4 && N % 2 == 0) {
+        const float2 *s = reinterpret_cast<const float2 *>(src);
+#pragma unroll
+        for (int t = 0; t < N / 2; ++t) *reinterpret_cast<float2 *>(dst + 2 * t) = __ldg(s + t);
+    } else {
+#pragma unroll
+        for (int t = 0; t < N; ++t) dst[t] = __ldg(src + t);
+    }
+}
+
+// AP block = sum over plan pairs A_a (B x B) * P_b (B x BC), one thread per AP block.  For the
+// small block shapes two pairs are in flight per iteration (their index and block loads
+// issued before either product), which doubles the loads a thread keeps outstanding; the
+// products are added in pair order, as with one pair per iteration.
 template <int B, int BC, typename V = double>
 __global__ void k_gather_AP(int64_t nblk, const int64_t *__restrict__ lptr, const int32_t *__restrict__ la,
                             const int32_t *__restrict__ lb, const V *__restrict__ A, const V *__restrict__ P,
@@ -499,18 +527,35 @@ __global__ void k_gather_AP(int64_t nblk, const int64_t *__restrict__ lptr, cons
         double acc[B * BC];
 #pragma unroll
         for (int t = 0; t < B * BC; ++t) acc[t] = 0.0;
-        for (int64_t l = lptr[q]; l < lptr[q + 1]; ++l) {
-            const V *a = A + (int64_t)la[l] * B * B;
-            double pv[B * BC];
-            load_block<B * BC>(P + (int64_t)lb[l] * B * BC, pv);
+        const int64_t l1 = lptr[q + 1];
+        int64_t l = lptr[q];
+        auto product = [&](const V *a, const V *pv) {
 #pragma unroll
             for (int r = 0; r < B; ++r)
 #pragma unroll
                 for (int m = 0; m < B; ++m) {
                     const double av = (double)a[r * B + m];
 #pragma unroll
-                    for (int c = 0; c < BC; ++c) acc[r * BC + c] += av * pv[m * BC + c];
+                    for (int c = 0; c < BC; ++c) acc[r * BC + c] += av * (double)pv[m * BC + c];
                 }
+        };
+        if constexpr (B * B + B * BC <= 27) {   // two pairs in flight (fine level and 2D shapes)
+            for (; l + 1 < l1; l += 2) {
+                const int64_t ia0 = la[l], ib0 = lb[l], ia1 = la[l + 1], ib1 = lb[l + 1];
+                V a0[B * B], p0[B * BC], a1[B * B], p1[B * BC];
+                load_raw<B * B>(A + ia0 * B * B, a0);
+                load_raw<B * BC>(P + ib0 * B * BC, p0);
+                load_raw<B * B>(A + ia1 * B * B, a1);
+                load_raw<B * BC>(P + ib1 * B * BC, p1);
+                product(a0, p0);
+                product(a1, p1);
+            }
+        }
+        for (; l < l1; ++l) {
+            V a0[B * B], p0[B * BC];
+            load_raw<B * B>(A + (int64_t)la[l] * B * B, a0);
+            load_raw<B * BC>(P + (int64_t)lb[l] * B * BC, p0);
+            product(a0, p0);
         }
 #pragma unroll
         for (int t = 0; t < B * BC; ++t) AP[q * B * BC + t] = (V)acc[t];
@@ -557,69 +602,81 @@ __global__ void k_gather_Ac(int64_t nblk, const int32_t *__restrict__ row, const
     }
 }
 
-// Warp-per-output-block variants of the two gathers for the small coarse levels, where a few
-// hundred output blocks each sum thousands of pairs and one thread per block leaves the GPU
-// idle: the lanes split the block's pairs and the partial sums are combined by a fixed
-// shuffle tree (deterministic).
-template <int B, int BC, typename V = double>
+// Lane-group variants of the two gathers for output blocks that each sum many pairs (the
+// coarse levels, and P'(AP) on the fine level): G lanes (8, 16 or 32) share one output block,
+// split its pairs and combine their partial sums by a fixed shuffle tree (deterministic).
+// Fewer lanes per block mean more pairs per lane between the log2(G) shuffle steps, whose
+// cost per output entry is fixed.
+template <int B, int BC, typename V = double, int G = 32>
 __global__ void k_gather_AP_warp(int64_t nblk, const int64_t *__restrict__ lptr, const int32_t *__restrict__ la,
                                  const int32_t *__restrict__ lb, const V *__restrict__ A,
                                  const V *__restrict__ P, V *__restrict__ AP) {
-    const int lane = threadIdx.x & 31;
-    const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
-    for (int64_t q = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5; q < nblk; q += nw) {
+    const int lane = threadIdx.x & 31, gl = lane % G;
+    const int64_t ng = ((int64_t)gridDim.x * blockDim.x) / G;
+    const int64_t q0 = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) / G;
+    // every lane of a warp runs the same number of outer iterations (the shuffles need them)
+    const int64_t span = ((nblk + ng - 1) / ng) * ng;
+    for (int64_t q = q0; q < span; q += ng) {
+        const bool live = q < nblk;
         double acc[B * BC];
 #pragma unroll
         for (int t = 0; t < B * BC; ++t) acc[t] = 0.0;
-        for (int64_t l = lptr[q] + lane; l < lptr[q + 1]; l += 32) {
-            double a[B * B], p[B * BC];
-            load_block<B * B>(A + (int64_t)la[l] * B * B, a);
-            load_block<B * BC>(P + (int64_t)lb[l] * B * BC, p);
+        if (live) {
+            for (int64_t l = lptr[q] + gl; l < lptr[q + 1]; l += G) {
+                double a[B * B], p[B * BC];
+                load_block<B * B>(A + (int64_t)la[l] * B * B, a);
+                load_block<B * BC>(P + (int64_t)lb[l] * B * BC, p);
 #pragma unroll
-            for (int r = 0; r < B; ++r)
+                for (int r = 0; r < B; ++r)
 #pragma unroll
-                for (int m = 0; m < B; ++m)
+                    for (int m = 0; m < B; ++m)
 #pragma unroll
-                    for (int c = 0; c < BC; ++c) acc[r * BC + c] += a[r * B + m] * p[m * BC + c];
+                        for (int c = 0; c < BC; ++c) acc[r * BC + c] += a[r * B + m] * p[m * BC + c];
+            }
         }
 #pragma unroll
         for (int t = 0; t < B * BC; ++t)
 #pragma unroll
-            for (int off = 16; off > 0; off >>= 1) acc[t] += __shfl_xor_sync(0xffffffffu, acc[t], off);
-        if (lane == 0)
+            for (int off = G / 2; off > 0; off >>= 1) acc[t] += __shfl_xor_sync(0xffffffffu, acc[t], off);
+        if (live && gl == 0)
 #pragma unroll
             for (int t = 0; t < B * BC; ++t) AP[q * B * BC + t] = (V)acc[t];
     }
 }
 
-template <int B, int BC, typename V = double>
+template <int B, int BC, typename V = double, int G = 32>
 __global__ void k_gather_Ac_warp(int64_t nblk, const int32_t *__restrict__ row, const int32_t *__restrict__ col,
                                  const int64_t *__restrict__ lptr, const int32_t *__restrict__ la,
                                  const int32_t *__restrict__ lb, const V *__restrict__ P,
                                  const V *__restrict__ AP, const uint8_t *__restrict__ dead,
                                  V *__restrict__ Ac) {
-    const int lane = threadIdx.x & 31;
-    const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
-    for (int64_t q = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5; q < nblk; q += nw) {
+    const int lane = threadIdx.x & 31, gl = lane % G;
+    const int64_t ng = ((int64_t)gridDim.x * blockDim.x) / G;
+    const int64_t q0 = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) / G;
+    const int64_t span = ((nblk + ng - 1) / ng) * ng;
+    for (int64_t q = q0; q < span; q += ng) {
+        const bool live = q < nblk;
         double acc[BC * BC];
 #pragma unroll
         for (int t = 0; t < BC * BC; ++t) acc[t] = 0.0;
-        for (int64_t l = lptr[q] + lane; l < lptr[q + 1]; l += 32) {
-            double p[B * BC], ap[B * BC];
-            load_block<B * BC>(P + (int64_t)la[l] * B * BC, p);
-            load_block<B * BC>(AP + (int64_t)lb[l] * B * BC, ap);
+        if (live) {
+            for (int64_t l = lptr[q] + gl; l < lptr[q + 1]; l += G) {
+                double p[B * BC], ap[B * BC];
+                load_block<B * BC>(P + (int64_t)la[l] * B * BC, p);
+                load_block<B * BC>(AP + (int64_t)lb[l] * B * BC, ap);
 #pragma unroll
-            for (int m = 0; m < B; ++m)
+                for (int m = 0; m < B; ++m)
 #pragma unroll
-                for (int r = 0; r < BC; ++r)
+                    for (int r = 0; r < BC; ++r)
 #pragma unroll
-                    for (int c = 0; c < BC; ++c) acc[r * BC + c] += p[m * BC + r] * ap[m * BC + c];
+                        for (int c = 0; c < BC; ++c) acc[r * BC + c] += p[m * BC + r] * ap[m * BC + c];
+            }
         }
 #pragma unroll
         for (int t = 0; t < BC * BC; ++t)
 #pragma unroll
-            for (int off = 16; off > 0; off >>= 1) acc[t] += __shfl_xor_sync(0xffffffffu, acc[t], off);
-        if (lane == 0) {
+            for (int off = G / 2; off > 0; off >>= 1) acc[t] += __shfl_xor_sync(0xffffffffu, acc[t], off);
+        if (live && gl == 0) {
             const int64_t I = row[q], J = col[q];
 #pragma unroll
             for (int r = 0; r < BC; ++r)
@@ -630,6 +687,33 @@ __global__ void k_gather_Ac_warp(int64_t nblk, const int32_t *__restrict__ row, 
                     Ac[(int64_t)q * BC * BC + r * BC + c] = (V)v;
                 }
         }
+    }
+}
+
+// lanes per output block for the lane-group gathers: about 8 or more pairs per lane
+inline int gather_lanes(int64_t nblk, int64_t pairs) {
+    const double avg = nblk > 0 ? (double)pairs / (double)nblk : 0.0;
+    return avg >= 256.0 ? 32 : (avg >= 128.0 ? 16 : 8);
+}
+
+template <int B, int BC, typename V>
+static void gather_AP_groups(int64_t nblk, int64_t pairs, const int64_t *ptr, const int32_t *la, const int32_t *lb,
+                             const V *A, const V *P, V *AP, cudaStream_t st) {
+    switch (gather_lanes(nblk, pairs)) {
+        case 32: k_gather_AP_warp<B, BC, V, 32><<<grid_for(nblk * 32, 128), 128, 0, st>>>(nblk, ptr, la, lb, A, P, AP); break;
+        case 16: k_gather_AP_warp<B, BC, V, 16><<<grid_for(nblk * 16, 128), 128, 0, st>>>(nblk, ptr, la, lb, A, P, AP); break;
+        default: k_gather_AP_warp<B, BC, V, 8><<<grid_for(nblk * 8, 128), 128, 0, st>>>(nblk, ptr, la, lb, A, P, AP); break;
+    }
+}
+
+template <int B, int BC, typename V>
+static void gather_Ac_groups(int64_t nblk, int64_t pairs, const int32_t *row, const int32_t *col, const int64_t *ptr,
+                             const int32_t *la, const int32_t *lb, const V *P, const V *AP, const uint8_t *dead,
+                             V *Ac, cudaStream_t st) {
+    switch (gather_lanes(nblk, pairs)) {
+        case 32: k_gather_Ac_warp<B, BC, V, 32><<<grid_for(nblk * 32, 128), 128, 0, st>>>(nblk, row, col, ptr, la, lb, P, AP, dead, Ac); break;
+        case 16: k_gather_Ac_warp<B, BC, V, 16><<<grid_for(nblk * 16, 128), 128, 0, st>>>(nblk, row, col, ptr, la, lb, P, AP, dead, Ac); break;
+        default: k_gather_Ac_warp<B, BC, V, 8><<<grid_for(nblk * 8, 128), 128, 0, st>>>(nblk, row, col, ptr, la, lb, P, AP, dead, Ac); break;
     }
 }
 
@@ -813,7 +897,7 @@ __global__ void k_dense_gemv(int64_t N, const T *__restrict__ M, const T *__rest
 
 static int free_level(Level &l) {
     auto F = [](void *p) { if (p) cudaFree(p); };
-    F(l.Aown.d_rp); F(l.Aown.d_col); F(l.d_diag_own); F(l.Aown_vals); F(l.A32); F(l.Dinv); F(l.Dinv32);
+    F(l.Aown.d_rp); F(l.Aown.d_col); F(l.d_diag_own); F(l.Aown_vals); F(l.A32); F(l.A16); F(l.Dinv); F(l.Dinv32);
     F(l.lmax); F(l.d_dead); F(l.d_agg); F(l.T); F(l.P.d_rp); F(l.P.d_col); F(l.R.d_rp); F(l.R.d_col);
     F(l.AP.d_rp); F(l.AP.d_col); F(l.d_R_from_P);
     F(l.Aown.d_row); F(l.P.d_row); F(l.R.d_row); F(l.AP.d_row);
@@ -1005,17 +1089,16 @@ static int numeric_transfer(sg_amg *h, int l, cudaStream_t st) {
                                                                           L.ap_plan.d_a, L.ap_plan.d_b, A, L.Pv,
                                                                           L.APv);
         else
-            k_gather_AP_warp<BB, BC><<<grid_for(L.AP.nblk * 32, 128), 128, 0, st>>>(
-                L.AP.nblk, L.ap_plan.d_ptr, L.ap_plan.d_a, L.ap_plan.d_b, A, L.Pv, L.APv);
+            gather_AP_groups<BB, BC, double>(L.AP.nblk, L.ap_pairs, L.ap_plan.d_ptr, L.ap_plan.d_a, L.ap_plan.d_b, A,
+                                             L.Pv, L.APv, st);
         if (!per_warp(C.Anblk, L.ac_pairs))
             k_gather_Ac<BB, BC><<<grid_for(C.Anblk, 128), 128, 0, st>>>(C.Anblk, C.Aown.d_row, C.d_Acol,
                                                                         L.ac_plan.d_ptr, L.ac_plan.d_a,
                                                                         L.ac_plan.d_b, L.Pv, L.APv, C.d_dead,
                                                                         C.Aown_vals);
         else
-            k_gather_Ac_warp<BB, BC><<<grid_for(C.Anblk * 32, 128), 128, 0, st>>>(
-                C.Anblk, C.Aown.d_row, C.d_Acol, L.ac_plan.d_ptr, L.ac_plan.d_a, L.ac_plan.d_b, L.Pv, L.APv,
-                C.d_dead, C.Aown_vals);
+            gather_Ac_groups<BB, BC, double>(C.Anblk, L.ac_pairs, C.Aown.d_row, C.d_Acol, L.ac_plan.d_ptr,
+                                             L.ac_plan.d_a, L.ac_plan.d_b, L.Pv, L.APv, C.d_dead, C.Aown_vals, st);
     }));
     SG_CUDA(cudaGetLastError());
     if (h->opt.mixed) {
@@ -1066,7 +1149,12 @@ static int numeric_update32(sg_amg *h, cudaStream_t st) {
         Level &L = h->L[l];
         if (l == 0) {
             const int64_t nv = L.Anblk * L.b * L.b;
-            k_to_float<<<grid_for(nv, 256), 256, 0, st>>>(nv, L.Avals, L.A32);
+            if (L.A16) {
+                const int rc0 = to_float_half3(L.Anblk, L.Avals, L.A32, L.A16, L.a16_scale, st);
+                if (rc0) return rc0;
+            } else {
+                k_to_float<<<grid_for(nv, 256), 256, 0, st>>>(nv, L.Avals, L.A32);
+            }
         }
         SG_B_DISPATCH(L.b, (k_block_diag_inv<BB, float><<<grid_for(L.n, 128), 128, 0, st>>>(L.n, L.d_Adiag, L.A32,
                                                                                             L.Dinv, L.Dinv32)));
@@ -1102,16 +1190,15 @@ static int numeric_update32(sg_amg *h, cudaStream_t st) {
                 k_gather_AP<BB, BC, float><<<grid_for(L.AP.nblk, 128), 128, 0, st>>>(
                     L.AP.nblk, L.ap_plan.d_ptr, L.ap_plan.d_a, L.ap_plan.d_b, L.A32, L.P32, L.APv32);
             else
-                k_gather_AP_warp<BB, BC, float><<<grid_for(L.AP.nblk * 32, 128), 128, 0, st>>>(
-                    L.AP.nblk, L.ap_plan.d_ptr, L.ap_plan.d_a, L.ap_plan.d_b, L.A32, L.P32, L.APv32);
+                gather_AP_groups<BB, BC, float>(L.AP.nblk, L.ap_pairs, L.ap_plan.d_ptr, L.ap_plan.d_a, L.ap_plan.d_b,
+                                                L.A32, L.P32, L.APv32, st);
             if (!per_warp(C.Anblk, L.ac_pairs))
                 k_gather_Ac<BB, BC, float><<<grid_for(C.Anblk, 128), 128, 0, st>>>(
                     C.Anblk, C.Aown.d_row, C.d_Acol, L.ac_plan.d_ptr, L.ac_plan.d_a, L.ac_plan.d_b, L.P32, L.APv32,
                     C.d_dead, C.A32);
             else
-                k_gather_Ac_warp<BB, BC, float><<<grid_for(C.Anblk * 32, 128), 128, 0, st>>>(
-                    C.Anblk, C.Aown.d_row, C.d_Acol, L.ac_plan.d_ptr, L.ac_plan.d_a, L.ac_plan.d_b, L.P32, L.APv32,
-                    C.d_dead, C.A32);
+                gather_Ac_groups<BB, BC, float>(C.Anblk, L.ac_pairs, C.Aown.d_row, C.d_Acol, L.ac_plan.d_ptr,
+                                                L.ac_plan.d_a, L.ac_plan.d_b, L.P32, L.APv32, C.d_dead, C.A32, st);
         }));
         SG_CUDA(cudaGetLastError());
     }
@@ -1217,6 +1304,18 @@ static int build_hierarchy(sg_amg *h, const sg_bsr *A0, const double *A0vals, co
                 SG_CUDA(cudaMemcpyAsync(vals.data(), level_values(L), sizeof(double) * vals.size(),
                                         cudaMemcpyDeviceToHost, st));
                 SG_CUDA(cudaStreamSynchronize(st));
+                if (lev == 0 && o.mixed && o.fine_half && b == 3) {
+                    // FP16 copy of level 0: a power-of-two scale maps the largest entry of the
+                    // set-up matrix to (2048, 4096], leaving 16x headroom below the FP16 maximum
+                    // for later value updates (larger magnitudes are clamped)
+                    double mx = 0.0;
+                    for (double v : vals) mx = std::max(mx, std::fabs(v));
+                    if (mx > 0.0 && std::isfinite(mx)) {
+                        L.a16_scale = (float)std::ldexp(1.0, (int)std::ceil(std::log2(mx / 4096.0)));
+                        rc = dalloc(&L.A16, (size_t)L.Anblk * 3);
+                        if (rc) return rc;
+                    }
+                }
                 std::vector<int32_t> srp, scol;
                 strength_graph(n, b, rp, col, vals, o.theta, srp, scol);
                 na = aggregate(n, srp, scol, active, L.agg);
@@ -1291,6 +1390,15 @@ LevelView<float> view<float>(Level &L) {
     return {L.A32, L.Dinv32, L.P32, L.R32, L.x32, L.rhs32, L.r32, L.d32};
 }
 
+// r = rhs - A x on a level; level 0 of the FP32 cycle reads the FP16 copy when there is one
+template <typename T>
+static int level_residual(Level &L, LevelView<T> &v, cudaStream_t st) {
+    if constexpr (std::is_same<T, float>::value) {
+        if (L.A16) return h3_spmv(L.n, L.Anblk, L.d_Arp, L.d_Acol, L.A16, L.a16_scale, v.x, v.r, v.rhs, 1, st);
+    }
+    return rect_spmv<T, T>(L.b, L.b, L.n, L.d_Arp, L.d_Acol, v.A, v.x, v.r, 1.0, 0.0, v.rhs, 1, st, L.Anblk);
+}
+
 template <typename T>
 static int smooth(sg_amg *h, Level &L, LevelView<T> &v, bool x_zero, cudaStream_t st) {
     const int deg = h->opt.cheb_degree;
@@ -1298,7 +1406,7 @@ static int smooth(sg_amg *h, Level &L, LevelView<T> &v, bool x_zero, cudaStream_
     for (int k = 0; k < deg && !rc; ++k) {
         const T *r = v.rhs;
         if (!(x_zero && k == 0)) {
-            rc = rect_spmv<T, T>(L.b, L.b, L.n, L.d_Arp, L.d_Acol, v.A, v.x, v.r, 1.0, 0.0, v.rhs, 1, st, L.Anblk);
+            rc = level_residual<T>(L, v, st);
             if (rc) return rc;
             r = v.r;
         }
@@ -1322,7 +1430,7 @@ static int vcycle(sg_amg *h, int l, cudaStream_t st) {
     Level &C = h->L[l + 1];
     LevelView<T> c = view<T>(C);
     int rc = smooth<T>(h, L, v, true, st);
-    if (!rc) rc = rect_spmv<T, T>(L.b, L.b, L.n, L.d_Arp, L.d_Acol, v.A, v.x, v.r, 1.0, 0.0, v.rhs, 1, st, L.Anblk);
+    if (!rc) rc = level_residual<T>(L, v, st);
     if (!rc) rc = rect_spmv<T, T>(L.bc, L.b, C.n, L.R.d_rp, L.R.d_col, v.R, v.r, c.rhs, 1.0, 0.0, nullptr, 0, st, L.R.nblk);
     if (!rc) rc = vcycle<T>(h, l + 1, st);
     if (!rc) rc = rect_spmv<T, T>(L.b, L.bc, L.n, L.P.d_rp, L.P.d_col, v.P, c.x, v.x, 1.0, 1.0, nullptr, 0, st, L.P.nblk);
@@ -1346,7 +1454,8 @@ extern "C" int sg_amg_create(const sg_bsr *A, const double *A_vals, const double
     sg_amg *h = new (std::nothrow) sg_amg();
     if (!h) return set_error(SG_ERR_NOMEM, "host allocation");
     cudaGetDevice(&h->device);
-    // opts: [max_levels, coarse_size, cheb_degree, cheb_ratio, power_its, mixed, omega_scale]
+    // opts: [max_levels, coarse_size, cheb_degree, cheb_ratio, power_its, mixed, omega_scale, theta,
+    //        fine_half]
     if (opts) {
         if (n_opts > 0 && opts[0] > 0) h->opt.max_levels = (int)opts[0];
         if (n_opts > 1 && opts[1] > 0) h->opt.coarse_size = (int)opts[1];
@@ -1356,6 +1465,7 @@ extern "C" int sg_amg_create(const sg_bsr *A, const double *A_vals, const double
         if (n_opts > 5) h->opt.mixed = opts[5] != 0.0;
         if (n_opts > 6 && opts[6] > 0) h->opt.omega_scale = opts[6];
         if (n_opts > 7 && opts[7] >= 0) h->opt.theta = opts[7];
+        if (n_opts > 8) h->opt.fine_half = opts[8] != 0.0;
     }
     int rc = dalloc(&h->dots, DOT_BLOCKS + 64);
     if (!rc) rc = build_hierarchy(h, A, A_vals, nullspace, nns, fixed, as_stream(stream));
@@ -1394,7 +1504,9 @@ extern "C" int sg_amg_destroy(sg_amg *h) {
 extern "C" int sg_amg_update(sg_amg *h, const double *Avals, void *stream) {
     SG_CHECK_ARG(h && Avals, "null argument");
     h->L[0].Avals = Avals;
+    const InstrToken tk = instr_begin(IK_AMG_UPDATE, as_stream(stream));
     int rc = h->opt.mixed ? numeric_update32(h, as_stream(stream)) : numeric_update(h, as_stream(stream));
+    instr_end(tk, as_stream(stream));
     if (!rc) h->updated = 1;
     return rc;
 }
@@ -1407,6 +1519,12 @@ extern "C" int sg_amg_apply(sg_amg *h, const double *r, double *z, void *stream)
     Level &L = h->L[0];
     const int64_t nd = L.n * L.b;
     int rc;
+    const InstrToken tk = instr_begin(IK_AMG_APPLY, st);
+    struct End {
+        const InstrToken &t;
+        cudaStream_t s;
+        ~End() { instr_end(t, s); }
+    } end{tk, st};
     if (h->opt.mixed) {
         k_to_float<<<grid_for(nd, 256), 256, 0, st>>>(nd, r, L.rhs32);
         rc = vcycle<float>(h, 0, st);

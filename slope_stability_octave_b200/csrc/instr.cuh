@@ -12,6 +12,9 @@ enum InstrKind {
     IK_CONST_SDS = 2,    // return mapping with tangent
     IK_CONST_S = 3,      // return mapping, stress only
     IK_ASSEMBLY = 4,     // tangent assembly into the block pattern
+    IK_AMG_UPDATE = 5,   // AMG numeric set-up for new level-0 values (all levels)
+    IK_AMG_APPLY = 6,    // one AMG V-cycle (with conversions and the optional correction)
+    IK_SPMV3_F16 = 7,    // level-0 SpMV of the FP32 V-cycle on the FP16 copy of the matrix
     IK_COUNT = 8
 };
 

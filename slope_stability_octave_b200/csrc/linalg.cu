@@ -5,6 +5,7 @@
 // warp-uniform slots so the shuffles never diverge.
 // Dot products use a fixed two-stage tree (per-block partials, then one ordered pass), so
 // results are bitwise reproducible from run to run.
+#include <cuda_fp16.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -134,6 +135,55 @@ __global__ void __launch_bounds__(256) k_spmv_row(int64_t nrows, const int32_t *
     }
 }
 
+// k_spmv_cta: a CTA of 32 * W threads per block row, for coarse levels whose few rows each
+// hold hundreds of blocks (there a warp per row occupies a fraction of the SMs and each warp
+// walks its row serially).  Each warp uses k_spmv_row's (slot, a) lane mapping over its share
+// of the row (warp w starts at slot w * SLOTS and steps by W * SLOTS); the warps' partial sums
+// meet in shared memory and are added in warp order (reproducible bitwise).
+template <int BR, int BC, int W, typename VT, typename XT>
+__global__ void __launch_bounds__(32 * W) k_spmv_cta(int64_t nrows, const int32_t *__restrict__ rp,
+                                                     const int32_t *__restrict__ col, const VT *__restrict__ vals,
+                                                     const XT *__restrict__ x, XT *__restrict__ y, double alpha,
+                                                     double beta, const XT *__restrict__ bvec, int mode) {
+    using A = typename Acc<XT>::type;
+    constexpr int BB = BR * BC, SLOTS = 32 / BR;
+    __shared__ A part[W][BR];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const int slot = lane / BR, a = lane - slot * BR;
+    const bool active = slot < SLOTS;
+    for (int64_t row = blockIdx.x; row < nrows; row += gridDim.x) {
+        A acc = 0;
+        if (active) {
+            const int32_t p1 = rp[row + 1];
+            for (int32_t p = rp[row] + w * SLOTS + slot; p < p1; p += W * SLOTS) {
+                const int64_t c = col[p];
+                const VT *v = vals + (int64_t)p * BB + a * BC;
+                const XT *xc = x + c * BC;
+#pragma unroll
+                for (int b = 0; b < BC; ++b) acc += (A)__ldg(v + b) * (A)__ldg(xc + b);
+            }
+        }
+        A tot = 0;
+#pragma unroll
+        for (int sl = 0; sl < SLOTS; ++sl) tot += __shfl_sync(0xffffffffu, acc, sl * BR + (active ? a : 0));
+        if (lane < BR) part[w][lane] = tot;
+        __syncthreads();
+        if (w == 0 && lane < BR) {
+            A sum = 0;
+#pragma unroll
+            for (int q = 0; q < W; ++q) sum += part[q][lane];
+            const int64_t k = row * BR + lane;
+            if (mode == 1) y[k] = (XT)((A)bvec[k] - sum);
+            else if (beta == 0.0) y[k] = (XT)(alpha * sum);
+            else y[k] = (XT)(alpha * sum + beta * (A)y[k]);
+        }
+        __syncthreads();
+    }
+}
+
+// rows below which a coarse 6x6 level with long rows takes a CTA per row (k_spmv_cta)
+constexpr int64_t CTA_ROW_LIMIT = 1184;
+
 template <int BR, int BC, typename VT, typename XT>
 static void spmv_launch(int64_t nrows, int64_t nblk, const int32_t *rp, const int32_t *col, const VT *vals,
                         const XT *x, XT *y, double alpha, double beta, const XT *bvec, int mode, cudaStream_t st) {
@@ -144,6 +194,14 @@ static void spmv_launch(int64_t nrows, int64_t nblk, const int32_t *rp, const in
     if (fine) tk = instr_begin(sizeof(VT) == 8 ? IK_SPMV3_F64 : IK_SPMV3_F32, st);
     constexpr bool wide = BR == 6 && BC == 6;
     constexpr bool tall_f64 = BR == 6 && BC == 3 && sizeof(VT) == 8;
+    if constexpr (wide) {
+        if (nrows < CTA_ROW_LIMIT && avg >= 48.0) {
+            count_launch();
+            k_spmv_cta<BR, BC, 8, VT, XT><<<(unsigned)nrows, 256, 0, st>>>(nrows, rp, col, vals, x, y, alpha, beta,
+                                                                           bvec, mode);
+            return;
+        }
+    }
     if (wide || tall_f64) {
         const int lpr = avg >= 48.0 ? 32 : 16;
         const unsigned grid = grid_for(nrows * lpr, 256, 16);
@@ -196,6 +254,95 @@ template int bsr_spmv<double, double>(const sg_bsr &, const double *, const doub
 template int bsr_spmv<float, float>(const sg_bsr &, const float *, const float *, float *, double, double, cudaStream_t);
 template int bsr_residual<double, double>(const sg_bsr &, const double *, const double *, const double *, double *, cudaStream_t);
 template int bsr_residual<float, float>(const sg_bsr &, const float *, const float *, const float *, float *, cudaStream_t);
+
+// ------------------------------------------------------------------ FP16 level-0 SpMV
+
+// Lane mapping of k_spmv_blk (G lanes per block row, one block per lane per step); a lane reads
+// its block as three 8-byte words (one padded block row each) and accumulates in FP32.
+template <int G>
+__global__ void __launch_bounds__(256) k_spmv_h3(int64_t nrows, const int32_t *__restrict__ rp,
+                                                 const int32_t *__restrict__ col, const uint2 *__restrict__ vals,
+                                                 float scale, const float *__restrict__ x, float *__restrict__ y,
+                                                 const float *__restrict__ bvec, int mode) {
+    constexpr int GPW = 32 / G;
+    const int lane = threadIdx.x & 31, g = lane / G, gl = lane - g * G;
+    const int64_t warp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+    const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    for (int64_t base = warp * GPW; base < nrows; base += nwarps * GPW) {
+        const int64_t row = base + g;
+        float acc[3] = {0.f, 0.f, 0.f};
+        if (row < nrows) {
+            const int32_t p1 = rp[row + 1];
+            for (int32_t p = rp[row] + gl; p < p1; p += G) {
+                const int64_t j = col[p];
+                const float x0 = x[j * 3], x1 = x[j * 3 + 1], x2 = x[j * 3 + 2];
+                const uint2 *v = vals + (int64_t)p * 3;
+#pragma unroll
+                for (int a = 0; a < 3; ++a) {
+                    const uint2 w = __ldg(v + a);
+                    const float2 lo = __half22float2(*reinterpret_cast<const __half2 *>(&w.x));
+                    const float2 hi = __half22float2(*reinterpret_cast<const __half2 *>(&w.y));
+                    acc[a] += lo.x * x0 + lo.y * x1 + hi.x * x2;
+                }
+            }
+        }
+#pragma unroll
+        for (int off = G / 2; off > 0; off >>= 1)
+#pragma unroll
+            for (int a = 0; a < 3; ++a) acc[a] += __shfl_xor_sync(0xffffffffu, acc[a], off);
+        if (row < nrows && gl == 0) {
+#pragma unroll
+            for (int a = 0; a < 3; ++a) {
+                const int64_t k = row * 3 + a;
+                y[k] = mode == 1 ? bvec[k] - scale * acc[a] : scale * acc[a];
+            }
+        }
+    }
+}
+
+int h3_spmv(int64_t nrows, int64_t nblk, const int32_t *rp, const int32_t *col, const uint2 *vals, float scale,
+            const float *x, float *y, const float *bvec, int mode, cudaStream_t st) {
+    const double avg = nblk > 0 && nrows > 0 ? (double)nblk / (double)nrows : 8.0;
+    const InstrToken tk = instr_begin(IK_SPMV3_F16, st);
+    const int G = avg >= 16.0 ? 32 : (avg >= 8.0 ? 16 : 8);
+    const unsigned grid = grid_for(nrows * G, 256, 16);
+    switch (G) {
+        case 32: k_spmv_h3<32><<<grid, 256, 0, st>>>(nrows, rp, col, vals, scale, x, y, bvec, mode); break;
+        case 16: k_spmv_h3<16><<<grid, 256, 0, st>>>(nrows, rp, col, vals, scale, x, y, bvec, mode); break;
+        default: k_spmv_h3<8><<<grid, 256, 0, st>>>(nrows, rp, col, vals, scale, x, y, bvec, mode); break;
+    }
+    instr_end(tk, st);
+    SG_CUDA(cudaGetLastError());
+    return SG_OK;
+}
+
+__global__ void k_to_float_half3(int64_t nrows3, const double *__restrict__ A, float *__restrict__ A32,
+                                 uint2 *__restrict__ A16, float inv_scale) {
+    for (int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; r < nrows3; r += (int64_t)gridDim.x * blockDim.x) {
+        float f[3];
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+            f[c] = (float)A[r * 3 + c];
+            A32[r * 3 + c] = f[c];
+        }
+        __half h[4];
+#pragma unroll
+        for (int c = 0; c < 3; ++c) h[c] = __float2half_rn(fminf(fmaxf(f[c] * inv_scale, -65504.f), 65504.f));
+        h[3] = __float2half_rn(0.f);
+        const __half2 lo = __halves2half2(h[0], h[1]), hi = __halves2half2(h[2], h[3]);
+        uint2 w;
+        w.x = *reinterpret_cast<const unsigned *>(&lo);
+        w.y = *reinterpret_cast<const unsigned *>(&hi);
+        A16[r] = w;
+    }
+}
+
+int to_float_half3(int64_t nblk, const double *A, float *A32, uint2 *A16, float scale, cudaStream_t st) {
+    const int64_t n = nblk * 3;
+    k_to_float_half3<<<grid_for(n, 256), 256, 0, st>>>(n, A, A32, A16, 1.0f / scale);
+    SG_CUDA(cudaGetLastError());
+    return SG_OK;
+}
 
 // ------------------------------------------------------------------ dots and GEMV
 

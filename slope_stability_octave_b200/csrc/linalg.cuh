@@ -33,6 +33,16 @@ int multidot(int64_t n, int m, const double *V, int64_t ldv, const double *w, do
 int gemv_sub(int64_t n, int m, const double *V, int64_t ldv, const double *h, double *w, cudaStream_t st);
 // x += V(:, 0:m) y      (y on the device)
 int gemv_add(int64_t n, int m, const double *V, int64_t ldv, const double *y, double *x, cudaStream_t st);
+// Level-0 SpMV of the FP32 V-cycle on an FP16 copy of a 3x3-block matrix: each block is
+// stored as three rows of four halves (the fourth zero), i.e. three uint2 words per block,
+// holding the values divided by ``scale`` (a power of two).  mode 1: y = b - scale * (A x);
+// mode 0: y = scale * (A x).
+int h3_spmv(int64_t nrows, int64_t nblk, const int32_t *rp, const int32_t *col, const uint2 *vals, float scale,
+            const float *x, float *y, const float *bvec, int mode, cudaStream_t st);
+// A32 = (float) A and A16 = the FP16 3x4-padded rows of A / scale (block rows of 3 doubles;
+// magnitudes beyond the FP16 range are clamped)
+int to_float_half3(int64_t nblk, const double *A, float *A32, uint2 *A16, float scale, cudaStream_t st);
+
 // y = a x + b y
 int axpby(int64_t n, double a, const double *x, double b, double *y, cudaStream_t st);
 // y = x * s where s = *num / *den on the device (den may be null -> s = *num)

@@ -39,10 +39,14 @@ class LearnedCorrection:
     steps, lr      full-batch Adam steps and learning rate
     loss           training objective: "residual" (the FP64 residual the corrected cycle
                    leaves) or "energy" (the energy norm of its error)
+    trial_tolerance, trial_margin
+                   the acceptance trial solves the training system plain and corrected to
+                   min(solver tolerance, trial_tolerance) and keeps the correction only if it
+                   needs fewer iterations and at most (1 - trial_margin) of the plain time
     """
 
     def __init__(self, dmesh: DeviceMesh, cons=None, train_at=0, n_vectors=12, steps=60, lr=3e-3, seed=0,
-                 max_vectors=None, loss="residual"):
+                 max_vectors=None, loss="residual", trial_tolerance=1e-6, trial_margin=0.05):
         if dmesh.dim != 3:
             raise ValueError("the learned correction is defined for 3D meshes")
         self.dmesh = dmesh
@@ -51,6 +55,8 @@ class LearnedCorrection:
         self.n_vectors = int(n_vectors)
         self.steps = int(steps)
         self.lr = float(lr)
+        self.trial_tolerance = float(trial_tolerance)
+        self.trial_margin = float(trial_margin)
         coord = np.ascontiguousarray(dmesh.mesh.coord, dtype=np.float64)   # 3 x n_n
         self._coord = np.ascontiguousarray(coord.T)                         # column-major 3 x n_n
         h = C.c_void_p()
@@ -168,11 +174,18 @@ class LearnedCorrection:
         self.train_seconds += time.perf_counter() - t0
         self.trained = True
 
-    def decide(self, it_plain, it_corrected, seconds=0.0):
-        """Acceptance gate: keep the correction only if the trial solve of the training
-        system needed fewer DFGMRES iterations with it than without."""
+    def decide(self, it_plain, it_corrected, seconds=0.0, t_plain=None, t_corrected=None):
+        """Acceptance gate: keep the correction only if the trial solve of the training system
+        (to the trial tolerance) needed fewer DFGMRES iterations with it than without and, when
+        the trial was timed, took at most (1 - trial_margin) of the plain solve's time: the
+        correction costs an extra fine-level SpMV per iteration, so fewer iterations alone do
+        not make it faster."""
+        faster = t_plain is None or t_corrected is None or t_corrected <= (1.0 - self.trial_margin) * t_plain
         self.gate = dict(plain_iterations=int(it_plain), corrected_iterations=int(it_corrected),
-                         accepted=bool(it_corrected < it_plain))
+                         accepted=bool(it_corrected < it_plain and faster))
+        if t_plain is not None:
+            self.gate.update(plain_s=round(float(t_plain), 4), corrected_s=round(float(t_corrected), 4),
+                             tolerance=self.trial_tolerance)
         self.enabled = self.gate["accepted"]
         self.train_seconds += seconds
 

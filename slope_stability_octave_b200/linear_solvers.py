@@ -59,7 +59,7 @@ class AMG:
     numeric set-up on the device (the pattern is fixed per mesh)."""
 
     def __init__(self, dmesh: DeviceMesh, coord=None, mixed=False, max_levels=10, coarse_size=1200,
-                 cheb_degree=3, cheb_ratio=10.0, power_its=10, theta=0.02):
+                 cheb_degree=3, cheb_ratio=10.0, power_its=10, theta=0.02, fine_half=False):
         self.dmesh = dmesh
         coord = dmesh.mesh.coord if coord is None else coord
         Z = near_null_space_elasticity(coord, dmesh.mesh.Q)
@@ -67,7 +67,7 @@ class AMG:
         self._Z = np.ascontiguousarray(Z.T)                  # column-major n_dof x nns
         self._fixed = np.ascontiguousarray((~dmesh.mesh.Q.T.ravel()).astype(np.uint8))
         self._opts = np.array([max_levels, coarse_size, cheb_degree, cheb_ratio, power_its, 1.0 if mixed else 0.0,
-                               0.0, theta], dtype=np.float64)
+                               0.0, theta, 1.0 if (mixed and fine_half) else 0.0], dtype=np.float64)
         self.handle = None
         self.setup_time = 0.0
         self.mixed = mixed
@@ -188,16 +188,19 @@ class DFGMRES:
         amg = self.preconditioner
         lc = self.learned
         if lc is not None and amg is not None and lc.wants_training():
-            # train on this system, then the acceptance trial: plain vs corrected solve
+            # train on this system, then the acceptance trial: plain vs corrected solve of the
+            # same system to the trial tolerance, timed on the device
             lc.train_on(amg, K, b)
             t1 = time.perf_counter()
+            trial_tol = min(self.tolerance, lc.trial_tolerance)
             lc.off(amg)
-            _, it_plain, _ = self._solve_core(K, b)
+            _, it_plain, _, t_plain = self._timed_solve(K, b, trial_tol)
             lc.features(K, b)
             lc.correction(amg)
-            _, it_corr, rr_corr = self._solve_core(K, b)
-            lc.decide(it_plain, it_corr if rr_corr <= self.tolerance else self.max_iterations + 1,
-                      time.perf_counter() - t1)
+            _, it_corr, rr_corr, t_corr = self._timed_solve(K, b, trial_tol)
+            if not rr_corr <= trial_tol:
+                it_corr, t_corr = self.max_iterations + 1, float("inf")
+            lc.decide(it_plain, it_corr, time.perf_counter() - t1, t_plain=t_plain, t_corrected=t_corr)
         corrected = lc.before_solve(amg, K, b) if lc is not None else False
         x, nit, rr = self._solve_core(K, b)
         if corrected and not (rr <= self.tolerance):
@@ -211,7 +214,15 @@ class DFGMRES:
         self._time("DFGMRES.solve", t0)
         return x, nit
 
-    def _solve_core(self, K, b):
+    def _timed_solve(self, K, b, tol):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        x, it, rr = self._solve_core(K, b, tol)
+        torch.cuda.synchronize()
+        return x, it, rr, time.perf_counter() - t0
+
+    def _solve_core(self, K, b, tol=None):
+        tol = self.tolerance if tol is None else tol
         x = torch.empty_like(b)
         it = C.c_int32()
         rr = C.c_double()
@@ -219,7 +230,7 @@ class DFGMRES:
         M = self.preconditioner.handle if self.preconditioner is not None else None
         aw_ok = self.k > 0 and self.AW is not None and self._aw_key == (K.data_ptr(), matrix_generation())
         _lib.call("sg_dfgmres_solve", self._ws.handle, self.dmesh.bsr, ptr(K), M, ptr(B) if self.k else None,
-                  ptr(self.AW) if aw_ok else None, self.k, ptr(b), ptr(x), self.tolerance, self.max_iterations,
+                  ptr(self.AW) if aw_ok else None, self.k, ptr(b), ptr(x), tol, self.max_iterations,
                   C.byref(it), C.byref(rr), None, cur_stream())
         return x, it.value, rr.value
 
@@ -244,7 +255,8 @@ class DFGMRES:
 def set_linear_solver(solver_type, linear_solver_tolerance, linear_solver_maxit, deflation_basis_tolerance,
                       linear_solver_printing, dmesh: DeviceMesh, coord=None, amg_opts=None, learned=None, cons=None):
     """Solver factory (set_linear_solver.m).  Tokens: 'DFGMRES_B200' (FP64 AMG V-cycle),
-    'DFGMRES_B200_MIXED' (FP32 V-cycle inside the FP64 FGMRES), 'DFGMRES_NONE' (no
+    'DFGMRES_B200_MIXED' (FP32 V-cycle inside the FP64 FGMRES; its level-0 SpMVs read an
+    FP16 copy of the matrix unless ``amg_opts`` sets fine_half=False), 'DFGMRES_NONE' (no
     preconditioner).  ``learned`` (a dict of LearnedCorrection options, or True) adds the
     learned node-wise correction of the V-cycle; ``cons`` supplies its constitutive
     features (branch ids, reduced cohesion)."""
@@ -253,6 +265,7 @@ def set_linear_solver(solver_type, linear_solver_tolerance, linear_solver_maxit,
     if tok in ("DFGMRES_B200", "DFGMRES_HYPRE_BOOMERAMG", "DFGMRES_BOOMERAMG", "BOOMERAMG", "HYPRE_BOOMERAMG"):
         amg = AMG(dmesh, coord, mixed=False, **opts)
     elif tok == "DFGMRES_B200_MIXED":
+        opts.setdefault("fine_half", True)
         amg = AMG(dmesh, coord, mixed=True, **opts)
     elif tok == "DFGMRES_NONE":
         amg = None

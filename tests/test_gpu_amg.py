@@ -105,7 +105,7 @@ def test_amg_hierarchy_and_vcycle_match_restatement(cuda_device, theta):
 def test_amg_mixed_precision_cycle(cuda_device):
     P, K = elastic_problem()
     a64 = AMG(P.dmesh)
-    a32 = AMG(P.dmesh, mixed=True)
+    a32 = AMG(P.dmesh, mixed=True, fine_half=False)
     a64.update(K)
     a32.update(K)
     rng = np.random.default_rng(1)
@@ -116,6 +116,35 @@ def test_amg_mixed_precision_cycle(cuda_device):
     torch.cuda.synchronize()
     err = torch.linalg.norm(z64 - z32) / torch.linalg.norm(z64)
     assert err.item() < 1e-4
+
+
+def test_amg_mixed_cycle_with_fp16_level0(cuda_device):
+    # the FP32 cycle whose level-0 SpMVs read the FP16 copy of A (11-bit significand, values
+    # scaled by a power of two): the cycle agrees with the FP64 one to FP16 accuracy (1e-2),
+    # and DFGMRES preconditioned by it reaches the same FP64 residual tolerance
+    from slope_stability_octave_b200.linear_solvers import DFGMRES
+    P, K = elastic_problem()
+    a64 = AMG(P.dmesh)
+    a16 = AMG(P.dmesh, mixed=True, fine_half=True)
+    a64.update(K)
+    a16.update(K)
+    rng = np.random.default_rng(1)
+    r = torch.from_numpy(rng.normal(size=P.dmesh.n_dof) * P.mesh.Q.T.ravel()).to(cuda_device)
+    z64, z16 = torch.zeros_like(r), torch.zeros_like(r)
+    a64.apply(r, z64)
+    a16.apply(r, z16)
+    torch.cuda.synchronize()
+    err = torch.linalg.norm(z64 - z16) / torch.linalg.norm(z64)
+    assert 0 < err.item() < 1e-2
+    its = []
+    for amg in (a64, a16):
+        s = DFGMRES(P.dmesh, 1e-8, 200, 1e-3, amg=amg)
+        x, it = s.solve(K, r)
+        res = torch.zeros_like(r)
+        P.dmesh.spmv(K, x, res)
+        assert torch.linalg.norm((r - res) * P.dmesh.mask).item() <= 1e-7 * torch.linalg.norm(r).item()
+        its.append(it)
+    assert its[1] <= its[0] + 2
 
 
 def test_amg_apply_before_update_is_an_error(cuda_device):

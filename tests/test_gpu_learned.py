@@ -227,6 +227,8 @@ def test_dfgmres_hook_trains_and_solves(system):
     assert lc.trained and lc.info()["adam_steps"] == 30
     g = lc.gate
     print(f"acceptance trial: {g}")
-    assert g["accepted"] == (g["corrected_iterations"] < g["plain_iterations"]) and lc.enabled == g["accepted"]
+    faster = g["corrected_s"] <= (1.0 - lc.trial_margin) * g["plain_s"]
+    assert g["accepted"] == (g["corrected_iterations"] < g["plain_iterations"] and faster)
+    assert lc.enabled == g["accepted"] and g["tolerance"] == lc.trial_tolerance
     r = (s["A"] @ x.cpu().numpy()) - s["b"].cpu().numpy()
     assert np.linalg.norm(r) <= 1.1e-6 * np.linalg.norm(s["b"].cpu().numpy())
