@@ -72,6 +72,7 @@ class AMG:
         self.setup_time = 0.0
         self.mixed = mixed
         self._A = None
+        self._ready = None     # event after an update issued on a side stream
 
     def _create(self, K):
         h = C.c_void_p()
@@ -90,13 +91,36 @@ class AMG:
                 pass
             self.handle = None
 
-    def update(self, K):
+    def update(self, K, stream=None):
+        """Numeric set-up for the values K.  With ``stream`` (a side torch stream) the update is
+        issued there after the work that produced K on the current stream, and the current
+        stream waits for it only at the next ``wait`` (called by every consumer of the
+        hierarchy), so the caller's independent work in between overlaps with it."""
+        self.wait()
         self._A = K     # keep the values alive: the hierarchy references them
-        if self.handle is None:
-            self._create(K)
-        _lib.call("sg_amg_update", self.handle, ptr(K), cur_stream())
+        if stream is None:
+            if self.handle is None:
+                self._create(K)
+            _lib.call("sg_amg_update", self.handle, ptr(K), cur_stream())
+            return
+        produced = torch.cuda.Event()
+        produced.record()
+        stream.wait_event(produced)
+        with torch.cuda.stream(stream):
+            if self.handle is None:
+                self._create(K)
+            _lib.call("sg_amg_update", self.handle, ptr(K), cur_stream())
+            self._ready = torch.cuda.Event()
+            self._ready.record(stream)
+
+    def wait(self):
+        """Make the current stream wait for an update issued on a side stream."""
+        if self._ready is not None:
+            torch.cuda.current_stream().wait_event(self._ready)
+            self._ready = None
 
     def apply(self, r, z):
+        self.wait()
         _lib.call("sg_amg_apply", self.handle, ptr(r), ptr(z), cur_stream())
 
     def info(self):
@@ -147,6 +171,7 @@ class DFGMRES:
         self.last_relres = 0.0
         # optional learned node-wise correction of the V-cycle (learned.LearnedCorrection)
         self.learned = None
+        self.overlap_update = True
 
     @property
     def k(self):
@@ -158,9 +183,19 @@ class DFGMRES:
             self.profiler.add_time(name, time.perf_counter() - t0)
 
     def setup_preconditioner(self, K):
+        """AMG numeric set-up for K.  When ``overlap_update`` is set (the default) it runs on
+        the AMG's side stream: the Newton step's work up to the next solve (the residual at
+        lambda + eps, the A-orthogonalisation of the deflation basis) overlaps with it, and
+        the solve waits for it."""
         t0 = time.perf_counter()
-        if self.preconditioner is not None:
-            self.preconditioner.update(K)
+        amg = self.preconditioner
+        if amg is not None:
+            if self.overlap_update and torch.cuda.is_available():
+                if getattr(amg, "_side", None) is None:
+                    amg._side = torch.cuda.Stream()
+                amg.update(K, stream=amg._side)
+            else:
+                amg.update(K)
         self._time("DFGMRES.update_preconditioner", t0)
 
     # the reference's IJV hooks map onto the same update on the device pattern
@@ -186,6 +221,8 @@ class DFGMRES:
         """x, nit = solve(K, b) on device vectors (dfgmres_solver.m)."""
         t0 = time.perf_counter()
         amg = self.preconditioner
+        if amg is not None:
+            amg.wait()
         lc = self.learned
         if lc is not None and amg is not None and lc.wants_training():
             # train on this system, then the acceptance trial: plain vs corrected solve of the
@@ -227,6 +264,8 @@ class DFGMRES:
         it = C.c_int32()
         rr = C.c_double()
         B = self.basis
+        if self.preconditioner is not None:
+            self.preconditioner.wait()
         M = self.preconditioner.handle if self.preconditioner is not None else None
         aw_ok = self.k > 0 and self.AW is not None and self._aw_key == (K.data_ptr(), matrix_generation())
         _lib.call("sg_dfgmres_solve", self._ws.handle, self.dmesh.bsr, ptr(K), M, ptr(B) if self.k else None,
@@ -249,6 +288,7 @@ class DFGMRES:
             new.AW, new._aw_key = self.AW.clone(), self._aw_key
         new.profiler = self.profiler
         new.learned = self.learned
+        new.overlap_update = self.overlap_update
         return new
 
 
