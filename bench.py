@@ -78,7 +78,7 @@ WORKLOADS = {
 # learned form: trained before the init phase's 4th linear solve on 12 residual vectors of
 # that Newton system, 60 full-batch Adam steps
 LEARNED_OPTS = dict(train_at=3, n_vectors=12, steps=60, lr=3e-3, seed=0)
-N_INSTR = 8
+N_INSTR = 10
 
 
 def parse():
@@ -598,7 +598,9 @@ def main():
                       other_kernels={name: dict(launches=int(nl[i]), avg_ms=(ms[i] / nt[i] if nt[i] else None))
                                      for i, name in enumerate(["spmv3_f64", "spmv3_f32", "constitutive_S_DS",
                                                                "constitutive_S", "assembly", "amg_update",
-                                                               "amg_vcycle"]) if nl[i]}),
+                                                               "amg_vcycle", "spmv3_f16", "spmv3_f64_aorth",
+                                                               "residual"])
+                                     if nl[i]}),
         cpu_baseline=cpu,
         counts=counts,
     )

@@ -147,6 +147,14 @@ int sg_mesh_free_dofs(const sg_mesh *mesh, int64_t *q_flat);
 int sg_strain_dev(const sg_mesh *mesh, const double *U, double *E, void *stream);
 /* (a6) F = B' (w .* S(1:n_strain,:)): S has s_rows rows per point; F dim x n_n (CONSTITUTIVE.m:281) */
 int sg_force_dev(const sg_mesh *mesh, const double *S, int32_t s_rows, double *F, void *stream);
+/* (a5 + a1/a2 + a6 fused) stress-only residual of P2 tetrahedra: F = B'(w .* S(B U)) with
+ * the reduced strength (c_bar, sin_phi) and the stress-only return mapping in between: the
+ * chain sg_strain_dev -> sg_constitutive3d_dev(DS = NULL) -> sg_force_dev of
+ * CONSTITUTIVE.build_F_reduced / build_F_all (CONSTITUTIVE.m:218-233, 268-285) in one kernel,
+ * E and S never stored.  branch (n_int, optional) receives the branch ids; F (3 x n_n) is
+ * zeroed and written.  3D, n_p = 10 only (SG_ERR_ARG otherwise). */
+int sg_residual_dev(const sg_mesh *mesh, const double *U, const double *c_bar, const double *sin_phi,
+                    const double *shear, const double *lame, uint8_t *branch, double *F, void *stream);
 /* (b3) K_t = sum_e B'(w DS)B into the block pattern (values zeroed first) */
 int sg_assemble_bsr_dev(const sg_mesh *mesh, const double *DS, double *K, void *stream);
 /* DS_elast of CONSTITUTIVE.m:413-422 per point (n_strain^2 x n_int) */
@@ -291,10 +299,12 @@ int sg_learned_info(const sg_learned *h, int64_t *info);
 
 /* ------------------------------------------------------------------------------
  * Live kernel timing (no reference counterpart: profiling support in the spirit of the
- * reference's PROFILING.Profiler).  When enabled, every `sample`-th launch of the fine-level
- * SpMV, the return mapping and the assembly is bracketed by CUDA events on its stream.
- * Kinds: 0 SpMV FP64, 1 SpMV FP32, 2 return mapping + tangent, 3 return mapping (stress),
- * 4 assembly.  sg_instr_read synchronises the device and resets the counters.
+ * reference's PROFILING.Profiler).  When enabled, every `sample`-th launch of each kind is
+ * bracketed by CUDA events on its stream.  Kinds (capacity 10): 0 fine SpMV FP64 (FGMRES,
+ * residuals), 1 fine SpMV FP32, 2 return mapping + tangent, 3 return mapping (stress),
+ * 4 assembly, 5 AMG value update, 6 AMG V-cycle, 7 fine SpMV on the FP16 copy, 8 fine SpMV
+ * FP64 inside sg_a_orthogonalize, 9 fused residual (sg_residual_dev).  sg_instr_read synchronises the device and resets the
+ * counters.
  * ---------------------------------------------------------------------------- */
 int sg_instr_enable(int on, int sample);
 int sg_instr_read(double *ms, int64_t *timed, int64_t *launches, int32_t cap);

@@ -41,6 +41,7 @@ SIGNATURES = {
     "sg_mesh_free_dofs": [vp, vp],
     "sg_strain_dev": [vp, vp, vp, vp],
     "sg_force_dev": [vp, vp, i32, vp, vp],
+    "sg_residual_dev": [vp] * 9,
     "sg_assemble_bsr_dev": [vp, vp, vp, vp],
     "sg_elastic_ds_dev": [vp, vp, vp, vp, vp],
     "sg_symmetrize_bsr_dev": [vp, vp, vp, vp],

@@ -133,14 +133,23 @@ class CONSTITUTIVE:
             self.m.force(self.S, self.s_rows, F)
         return F.clone() if out is None else F
 
+    def _residual(self, U):
+        """F(U) at the current reduction: one fused kernel (strain, stress-only return mapping,
+        internal force) on P2 tetrahedra, the three steps otherwise.  The fused path leaves
+        E and S unset."""
+        if not self.m.fused_residual:
+            self.constitutive_problem_stress(U)
+            return self.build_F()
+        with _Timer(self.profiler, "CONSTITUTIVE.residual"):
+            self.m.residual(U, self.c_bar, self.sin_phi, self.shear, self.lame, self.branch, self.F)
+        return self.F.clone()
+
     def build_F_all(self, lam, U):
         self.reduction(lam)
-        self.constitutive_problem_stress(U)
-        return self.build_F()
+        return self._residual(U)
 
     def build_F_reduced(self, U):
-        self.constitutive_problem_stress(U)
-        return self.build_F()
+        return self._residual(U)
 
     def build_F_and_DS_all(self, lam, U):
         self.reduction(lam)

@@ -12,9 +12,12 @@
 // Strain rows: 3D (e11, e22, e33, g12, g23, g13); 2D (e11, e22, g12).
 #include <cuda_runtime.h>
 
+#include <algorithm>
+
 #include <vector>
 
 #include "instr.cuh"
+#include "mc_point.cuh"
 #include "mesh.h"
 #include "sg_common.cuh"
 
@@ -86,6 +89,83 @@ __global__ void k_force(const int32_t *__restrict__ elem, const double *__restri
         const int64_t v = elem[e * np + i];
 #pragma unroll
         for (int c = 0; c < DIM; ++c) atomicAdd(&F[v * DIM + c], f[c]);
+    }
+}
+
+// Fused stress-only residual of 3D P2 tetrahedra: F = B'(w S(B U)) with the return mapping
+// in between (CONSTITUTIVE.build_F_all / build_F_reduced after the reduction: strain
+// CONSTITUTIVE.m:218, stress constitutive_3D_kernel.h:101-410 without the tangent, force
+// CONSTITUTIVE.m:268-285).  A CTA takes RES_ELEMS elements.  Phase 1, a thread per point:
+// E = B U in registers (k_strain's summation order), S from the stress-only return mapping,
+// kept in shared memory; phase 2, a thread per (element, node): the node's force over the
+// element's points from the shared stresses (k_force's order), added with atomics.  E and S
+// never reach global memory, and each point's gradients are read from DRAM once.  F must be
+// zeroed first.
+constexpr int RES_ELEMS = 16;
+constexpr int RES_MAXQ = 16;
+constexpr int RES_THREADS = 192;
+
+__global__ void __launch_bounds__(RES_THREADS) k_residual3d(const int32_t *__restrict__ elem,
+                                                            const double *__restrict__ dphi,
+                                                            const double *__restrict__ w, int nq, int64_t n_e,
+                                                            const double *__restrict__ U,
+                                                            const double *__restrict__ c_bar,
+                                                            const double *__restrict__ sin_phi,
+                                                            const double *__restrict__ shear,
+                                                            const double *__restrict__ lame,
+                                                            uint8_t *__restrict__ branch, double *__restrict__ F) {
+    constexpr int NP = 10;
+    __shared__ double sS[RES_ELEMS * RES_MAXQ * 7];
+    const int t = threadIdx.x;
+    for (int64_t e0 = (int64_t)blockIdx.x * RES_ELEMS; e0 < n_e; e0 += (int64_t)gridDim.x * RES_ELEMS) {
+        {
+            const int le = t / nq, q = t - le * nq;
+            const int64_t e = e0 + le;
+            if (le < RES_ELEMS && e < n_e) {
+                const int64_t g = e * nq + q;
+                const double *d = dphi + g * 3 * NP;
+                double E[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+                for (int i = 0; i < NP; ++i) {
+                    const int64_t v = elem[e * NP + i];
+                    const double d1 = d[i], d2 = d[NP + i], d3 = d[2 * NP + i];
+                    const double ux = U[3 * v], uy = U[3 * v + 1], uz = U[3 * v + 2];
+                    E[0] += d1 * ux;
+                    E[1] += d2 * uy;
+                    E[2] += d3 * uz;
+                    E[3] += d2 * ux + d1 * uy;
+                    E[4] += d3 * uy + d2 * uz;
+                    E[5] += d3 * ux + d1 * uz;
+                }
+                double st[6];
+                const int b = mc3d_point<false>(E, c_bar[g], sin_phi[g], shear[g], lame[g], st, nullptr);
+                if (branch) branch[g] = (uint8_t)b;
+#pragma unroll
+                for (int c = 0; c < 6; ++c) sS[(le * nq + q) * 7 + c] = st[c];
+            }
+        }
+        __syncthreads();
+        {
+            const int le = t / NP, i = t - le * NP;
+            const int64_t e = e0 + le;
+            if (le < RES_ELEMS && e < n_e) {
+                double f0 = 0.0, f1 = 0.0, f2 = 0.0;
+                for (int q = 0; q < nq; ++q) {
+                    const int64_t g = e * nq + q;
+                    const double *d = dphi + g * 3 * NP;
+                    const double *s = sS + (le * nq + q) * 7;
+                    const double wq = w[g];
+                    const double d1 = d[i], d2 = d[NP + i], d3 = d[2 * NP + i];
+                    f0 += wq * (d1 * s[0] + d2 * s[3] + d3 * s[5]);
+                    f1 += wq * (d2 * s[1] + d1 * s[3] + d3 * s[4]);
+                    f2 += wq * (d3 * s[2] + d2 * s[4] + d1 * s[5]);
+                }
+                const int64_t v = elem[e * NP + i];
+                atomicAdd(&F[3 * v], f0);
+                atomicAdd(&F[3 * v + 1], f1);
+                atomicAdd(&F[3 * v + 2], f2);
+            }
+        }
+        __syncthreads();
     }
 }
 
@@ -249,6 +329,25 @@ extern "C" int sg_force_dev(const sg_mesh *m, const double *S, int32_t s_rows, d
     const int64_t work = m->n_e * m->np;
     if (m->dim == 3) k_force<3><<<grid_for(work, 256), 256, 0, st>>>(m->d_elem, m->d_dphi, m->d_w, m->np, m->nq, m->n_e, S, s_rows, F);
     else k_force<2><<<grid_for(work, 256), 256, 0, st>>>(m->d_elem, m->d_dphi, m->d_w, m->np, m->nq, m->n_e, S, s_rows, F);
+    SG_CUDA(cudaGetLastError());
+    return SG_OK;
+}
+
+extern "C" int sg_residual_dev(const sg_mesh *m, const double *U, const double *c_bar, const double *sin_phi,
+                               const double *shear, const double *lame, uint8_t *branch, double *F, void *stream) {
+    SG_CHECK_ARG(m && U && c_bar && sin_phi && shear && lame && F, "null argument");
+    SG_CHECK_ARG(m->dim == 3 && m->np == 10, "the fused residual is for P2 tetrahedra");
+    SG_CHECK_ARG(m->nq >= 1 && m->nq <= RES_MAXQ, "too many integration points per element");
+    const cudaStream_t st = as_stream(stream);
+    SG_CUDA(cudaMemsetAsync(F, 0, sizeof(double) * m->n_n * 3, st));
+    if (m->n_e == 0) return SG_OK;
+    const InstrToken tk = instr_begin(IK_RESIDUAL, st);
+    count_launch();
+    const int64_t ctas = (m->n_e + RES_ELEMS - 1) / RES_ELEMS;
+    const unsigned grid = (unsigned)std::min<int64_t>(ctas, (int64_t)sm_count() * 8);
+    k_residual3d<<<grid, RES_THREADS, 0, st>>>(m->d_elem, m->d_dphi, m->d_w, m->nq, m->n_e, U, c_bar, sin_phi,
+                                               shear, lame, branch, F);
+    instr_end(tk, st);
     SG_CUDA(cudaGetLastError());
     return SG_OK;
 }

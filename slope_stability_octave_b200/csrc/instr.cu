@@ -36,10 +36,22 @@ static cudaEvent_t take_event(InstrState &s) {
     return e;
 }
 
+static thread_local int t_redirect_from = -1, t_redirect_to = -1;
+
+InstrRedirect::InstrRedirect(int from, int to) : saved_from(t_redirect_from), saved_to(t_redirect_to) {
+    t_redirect_from = from;
+    t_redirect_to = to;
+}
+InstrRedirect::~InstrRedirect() {
+    t_redirect_from = saved_from;
+    t_redirect_to = saved_to;
+}
+
 InstrToken instr_begin(int kind, cudaStream_t st) {
     InstrState &s = state();
     InstrToken t;
     if (!s.on) return t;
+    if (kind == t_redirect_from) kind = t_redirect_to;
     std::lock_guard<std::mutex> g(s.mu);
     const int64_t c = s.launches[kind]++;
     if (c % s.sample != 0) return t;

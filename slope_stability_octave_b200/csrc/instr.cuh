@@ -15,7 +15,18 @@ enum InstrKind {
     IK_AMG_UPDATE = 5,   // AMG numeric set-up for new level-0 values (all levels)
     IK_AMG_APPLY = 6,    // one AMG V-cycle (with conversions and the optional correction)
     IK_SPMV3_F16 = 7,    // level-0 SpMV of the FP32 V-cycle on the FP16 copy of the matrix
-    IK_COUNT = 8
+    IK_SPMV3_F64_AORTH = 8,  // FP64 node-block SpMVs of the deflation-basis A-orthogonalisation
+                             // (these may run beside an AMG update on another stream)
+    IK_RESIDUAL = 9,     // fused stress-only residual F = B'(w S(B U))
+    IK_COUNT = 10
+};
+
+// While an InstrRedirect lives on a thread, launches of kind `from` on that thread are
+// counted and timed as kind `to`.
+struct InstrRedirect {
+    int saved_from, saved_to;
+    InstrRedirect(int from, int to);
+    ~InstrRedirect();
 };
 
 struct InstrToken {

@@ -20,6 +20,7 @@
 #include <new>
 #include <vector>
 
+#include "instr.cuh"
 #include "linalg.cuh"
 #include "mesh.h"
 #include "sg_common.cuh"
@@ -265,6 +266,7 @@ extern "C" int sg_a_orthogonalize(sg_krylov *ws, const sg_bsr *A, const double *
     const int64_t n = ws->n;
     const cudaStream_t st = as_stream(stream);
     if (k == 0) { *k_out = 0; return SG_OK; }
+    const InstrRedirect redirect(IK_SPMV3_F64, IK_SPMV3_F64_AORTH);
     int rc = ensure_kcap(ws, k);
     if (rc) return rc;
     // Wo, AWo: the A-orthonormalised columns and A times them, in processing order; nt[i] is

@@ -129,6 +129,15 @@ class DeviceMesh:
     def force(self, S, s_rows, F):
         _lib.call("sg_force_dev", self.handle, ptr(S), int(s_rows), ptr(F), cur_stream())
 
+    @property
+    def fused_residual(self):
+        """The fused stress-only residual kernel covers P2 tetrahedra."""
+        return self.dim == 3 and self.mesh.elem.shape[0] == 10
+
+    def residual(self, U, c_bar, sin_phi, shear, lame, branch, F):
+        _lib.call("sg_residual_dev", self.handle, ptr(U), ptr(c_bar), ptr(sin_phi), ptr(shear), ptr(lame),
+                  ptr(branch) if branch is not None else None, ptr(F), cur_stream())
+
     def assemble(self, DS, K):
         _bump()
         _lib.call("sg_assemble_bsr_dev", self.handle, ptr(DS), ptr(K), cur_stream())

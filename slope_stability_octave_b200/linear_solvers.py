@@ -295,8 +295,8 @@ class DFGMRES:
 def set_linear_solver(solver_type, linear_solver_tolerance, linear_solver_maxit, deflation_basis_tolerance,
                       linear_solver_printing, dmesh: DeviceMesh, coord=None, amg_opts=None, learned=None, cons=None):
     """Solver factory (set_linear_solver.m).  Tokens: 'DFGMRES_B200' (FP64 AMG V-cycle),
-    'DFGMRES_B200_MIXED' (FP32 V-cycle inside the FP64 FGMRES; its level-0 SpMVs read an
-    FP16 copy of the matrix unless ``amg_opts`` sets fine_half=False), 'DFGMRES_NONE' (no
+    'DFGMRES_B200_MIXED' (FP32 V-cycle inside the FP64 FGMRES; ``amg_opts`` fine_half=True
+    makes its level-0 SpMVs read an FP16 copy of the matrix), 'DFGMRES_NONE' (no
     preconditioner).  ``learned`` (a dict of LearnedCorrection options, or True) adds the
     learned node-wise correction of the V-cycle; ``cons`` supplies its constitutive
     features (branch ids, reduced cohesion)."""
@@ -305,7 +305,6 @@ def set_linear_solver(solver_type, linear_solver_tolerance, linear_solver_maxit,
     if tok in ("DFGMRES_B200", "DFGMRES_HYPRE_BOOMERAMG", "DFGMRES_BOOMERAMG", "BOOMERAMG", "HYPRE_BOOMERAMG"):
         amg = AMG(dmesh, coord, mixed=False, **opts)
     elif tok == "DFGMRES_B200_MIXED":
-        opts.setdefault("fine_half", True)
         amg = AMG(dmesh, coord, mixed=True, **opts)
     elif tok == "DFGMRES_NONE":
         amg = None

@@ -169,13 +169,16 @@ def newton_ind_SSR(U_ini, omega, lambda_ini, it_newt_max, it_damp_max, tol, r_mi
                 break
         hist["r"].append(r)
         K = cons.build_K_r_QQ_vals(r)
-        F_eps = cons.build_F_all(lambda_it + eps, U_it)
-        G = (F_eps - F) / eps
+        # the preconditioner update is issued before the residual at lambda + eps (the
+        # reference computes F_eps first; neither depends on the other), so that the two,
+        # and the A-orthogonalisation, overlap when the update runs on a side stream
         if not ijv_init:
             solver.setup_preconditioner_ijv(K)
             ijv_init = True
         else:
             solver.update_preconditioner_values(K)
+        F_eps = cons.build_F_all(lambda_it + eps, U_it)
+        G = (F_eps - F) / eps
         solver.A_orthogonalize(K)
         W, lin_w = solver.solve(K, -G * Q)
         V, lin_v = solver.solve(K, fQ - F * Q)

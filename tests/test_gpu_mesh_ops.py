@@ -105,3 +105,32 @@ def test_strain_force_assembly_kr(cuda_device, kind):
     fd = torch.from_numpy(f).to(cuda_device)
     ref = np.linalg.norm((x - f)[q])
     assert abs(masked_diff_norm(xd, fd, dm.mask) - ref) <= 1e-12 * ref
+
+
+def test_fused_residual_matches_three_kernel_chain(cuda_device):
+    """sg_residual_dev (strain, stress-only return mapping and internal force in one kernel)
+    against the chain sg_strain_dev -> sg_constitutive3d_dev -> sg_force_dev (F within 1e-12,
+    branch ids equal) and against the oracle's F = B'(w S(B U)) (1e-11, as above), on a
+    displacement that puts points on several plastic branches."""
+    import torch
+    mesh, dphi, w, nq, mat = build_case("slope3d")
+    dm = DeviceMesh(mesh, dphi, w, nq)
+    assert dm.fused_residual
+    pat = OctavePattern(3, mesh.elem, mesh.n_n, dphi, w, mesh.Q, mat["shear"], mat["bulk"])
+    cons = CONSTITUTIVE(dm, mat["c0"], mat["phi"], mat["psi"], "B", mat["shear"], mat["bulk"], mat["lame"])
+    rng = np.random.default_rng(5)
+    U = rng.normal(size=(3, mesh.n_n)) * 4e-3 * mesh.Q
+    Ud = torch.from_numpy(np.ascontiguousarray(U.T).ravel()).to(cuda_device)
+    lam = 1.4
+    F_fused = cons.build_F_all(lam, Ud)
+    br_fused = cons.branch.clone()
+    cons.constitutive_problem_stress(Ud)
+    F_chain = cons.build_F()
+    assert torch.equal(br_fused, cons.branch)
+    close(F_fused.cpu().numpy(), F_chain.cpu().numpy())
+    E = pat.strain(U)
+    cb, spn = native.reduction(mat["c0"], mat["phi"], mat["psi"], lam, "B")
+    S, _, br = native.constitutive(3, E, cb, spn, mat["shear"], mat["bulk"], mat["lame"], want_ds=False)
+    assert np.mean(br_fused.cpu().numpy() == br) > 0.999
+    assert len(np.unique(br)) >= 3
+    close(F_fused.cpu().numpy().reshape(mesh.n_n, 3).T, pat.force(S), 1e-11)
