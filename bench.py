@@ -182,7 +182,7 @@ def run_form(args, form, P, rank, world):
     U_h.copy_(run.U)
     Uo_h.copy_(run.U_old)
     ev = [[torch.cuda.Event(enable_timing=True) for _ in range(4)] for _ in range(args.steps)]
-    steps, basis = [], []
+    steps, basis, host = [], [], []
     clocks = ClockSampler(torch.cuda.current_device()).start()
     _lib.call("sg_instr_enable", 1, 4)
     # no Python garbage collection inside the timed region (a collection pass stalls the
@@ -192,6 +192,7 @@ def run_form(args, form, P, rank, world):
     torch.cuda.synchronize()
     barrier(world)
     torch.cuda.synchronize()
+    mem0 = torch.cuda.memory_stats()
     _lib.lib().sg_launch_count(1)
     torch.cuda.nvtx.range_push("timed_step")
     for k in range(args.steps):
@@ -200,7 +201,9 @@ def run_form(args, form, P, rank, world):
         run.U_old.copy_(Uo_h, non_blocking=True)
         run.U.copy_(U_h, non_blocking=True)
         e1.record()
+        w0, c0 = time.perf_counter(), time.process_time()
         acc = run.step()
+        host.append((time.perf_counter() - w0, time.process_time() - c0))
         e2.record()
         U_h.copy_(run.U, non_blocking=True)
         Uo_h.copy_(run.U_old, non_blocking=True)
@@ -211,6 +214,7 @@ def run_form(args, form, P, rank, world):
         basis.append(solver.k)
     torch.cuda.synchronize()
     torch.cuda.nvtx.range_pop()
+    mem1 = torch.cuda.memory_stats()
     gc.enable()
     barrier(world)
     launches = int(_lib.lib().sg_launch_count(1))
@@ -225,7 +229,10 @@ def run_form(args, form, P, rank, world):
     t_e2e = sum(ev[k][0].elapsed_time(ev[k][3]) for k in range(args.steps)) / 1e3
     t_dev, t_e2e = max_over_ranks([t_dev, t_e2e], world, device="cuda")
     step_s = [ev[k][1].elapsed_time(ev[k][2]) / 1e3 for k in range(args.steps)]
-    res = dict(t_dev=t_dev, t_e2e=t_e2e, steps=steps, step_s=step_s, basis=basis, launches=launches, instr=(ms, nt, nl),
+    # device allocations made by the caching allocator inside the timed steps
+    alloc = {k: int(mem1.get(k, 0) - mem0.get(k, 0)) for k in ("num_device_alloc", "num_device_free",
+                                                              "num_alloc_retries")}
+    res = dict(t_dev=t_dev, t_e2e=t_e2e, steps=steps, step_s=step_s, alloc=alloc, host=host, basis=basis, launches=launches, instr=(ms, nt, nl),
                clocks=clk, t_init=t_init, lam=[s["lam"] for s in steps], amg=solver.preconditioner.info(),
                lam_init=list(run.lambda_hist[: 2 + args.warmup]))
     if solver.learned is not None:
@@ -567,6 +574,8 @@ def main():
     for form, r in out.items():
         forms_cfg[form] = dict(
             s_per_step=r["t_dev"] / K, e2e_s_per_step=r["t_e2e"] / K, step_s=[round(t, 4) for t in r["step_s"]],
+            device_allocs_in_timed_steps=r["alloc"],
+            host_wall_and_cpu_s=[[round(a, 4), round(b, 4)] for a, b in r["host"]],
             lambdas=r["lam"],
             newton_iterations=[s["newton_iterations_total"] for s in r["steps"]],
             linear_iterations=[s["linear_iterations"] for s in r["steps"]],
