@@ -72,3 +72,20 @@ def test_correction_loss_gradient_matches_finite_differences():
     change = (e - d) @ (A @ (e - d)) - e @ (A @ e)
     assert abs(L.correction_loss(G, Dinv, mask, A, rz[:1], "energy")[0] * float(rz[0] @ y.ravel()) - change) \
         <= 1e-9 * abs(change)
+
+
+def test_acceptance_trial_rule():
+    """The correction is kept only with fewer iterations AND at most (1 - margin) of the plain
+    trial time (host logic of LearnedCorrection.decide; no device state involved)."""
+    from slope_stability_octave_b200.learned import LearnedCorrection
+    lc = LearnedCorrection.__new__(LearnedCorrection)
+    lc.trial_margin, lc.trial_tolerance, lc.train_seconds = 0.05, 1e-6, 0.0
+    cases = [((30, 25, 1.0, 0.90), True),     # fewer iterations and 10 % faster
+             ((30, 25, 1.0, 0.97), False),    # fewer iterations but within the margin
+             ((25, 25, 1.0, 0.50), False),    # not fewer iterations
+             ((25, 30, 1.0, 0.80), False),
+             ((30, 25, None, None), True)]    # untimed trial: iterations alone
+    for (ip, ic, tp, tc), want in cases:
+        lc.decide(ip, ic, 0.1, t_plain=tp, t_corrected=tc)
+        assert lc.gate["accepted"] is want and lc.enabled is want, (ip, ic, tp, tc)
+    assert abs(lc.train_seconds - 0.5) < 1e-12
