@@ -201,6 +201,13 @@ typedef struct sg_amg sg_amg;
 int sg_amg_create(const sg_bsr *A, const double *A_vals, const double *nullspace, int32_t nns,
                   const uint8_t *fixed, const double *opts, int32_t n_opts, sg_amg **out, void *stream);
 int sg_amg_destroy(sg_amg *amg);
+/* A second set of V-cycle vectors over the hierarchy of `amg` (no counterpart in the
+ * reference): the clone shares every matrix, transfer operator and inverse and follows the
+ * parent's updates, so sg_amg_apply on the parent and on the clone may run at the same time
+ * on different streams (the two independent Krylov solves of a Newton step).  Only the parent
+ * is updated (sg_amg_update on a clone is SG_ERR_ARG); destroy the clone before the parent;
+ * no learned correction on a clone. */
+int sg_amg_clone(const sg_amg *amg, sg_amg **clone);
 /* numeric set-up from device values of A (kept by reference until the next update) */
 int sg_amg_update(sg_amg *amg, const double *A_vals, void *stream);
 /* z = V-cycle(r), device vectors of n_rows*b entries */

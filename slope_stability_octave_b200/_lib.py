@@ -57,6 +57,7 @@ SIGNATURES = {
     "sg_amg_create": [vp, vp, vp, i32, vp, vp, i32, vp, vp],
     "sg_amg_destroy": [vp],
     "sg_amg_update": [vp, vp, vp],
+    "sg_amg_clone": [vp, vp],
     "sg_amg_apply": [vp, vp, vp, vp],
     "sg_amg_info": [vp, vp, i32],
     "sg_amg_export": [vp, i32, vp, vp, vp, vp, vp, vp],

@@ -120,6 +120,9 @@ struct sg_amg {
     int corr_on = 0;
     int device = 0;
     int updated = 0;
+    // a clone (sg_amg_clone) shares every matrix, transfer operator and inverse of its parent
+    // and owns only its cycle vectors
+    const sg_amg *parent = nullptr;
 };
 
 namespace sg {
@@ -1485,6 +1488,15 @@ extern "C" int sg_amg_destroy(sg_amg *h) {
     int cur = 0;
     cudaGetDevice(&cur);
     cudaSetDevice(h->device);
+    if (h->parent) {
+        for (auto &L : h->L) {
+            cudaFree(L.x); cudaFree(L.rhs); cudaFree(L.r); cudaFree(L.d);
+            cudaFree(L.x32); cudaFree(L.rhs32); cudaFree(L.r32); cudaFree(L.d32);
+        }
+        cudaSetDevice(cur);
+        delete h;
+        return SG_OK;
+    }
     for (auto &L : h->L) free_level(L);
     cudaFree(h->Ainv);
     cudaFree(h->Ainv32);
@@ -1499,10 +1511,52 @@ extern "C" int sg_amg_destroy(sg_amg *h) {
     return SG_OK;
 }
 
+// A second set of cycle vectors over the same hierarchy (no counterpart in the reference),
+// so that two V-cycles can run at the same time on different streams (the two independent
+// Krylov solves of a Newton step).  The clone reads the parent's matrices, transfer operators
+// and inverses as the parent's updates leave them; only the parent is updated, the parent
+// must outlive the clone, and the learned correction is not available on a clone.
+extern "C" int sg_amg_clone(const sg_amg *h, sg_amg **out) {
+    SG_CHECK_ARG(h && out, "null argument");
+    SG_CHECK_ARG(!h->parent, "clone of a clone");
+    *out = nullptr;
+    sg_amg *c = new (std::nothrow) sg_amg(*h);
+    if (!c) return set_error(SG_ERR_NOMEM, "host allocation");
+    c->parent = h;
+    c->corrC = nullptr;
+    c->corrC32 = nullptr;
+    c->corr_on = 0;
+    int rc = SG_OK;
+    for (auto &L : c->L) {
+        L.x = L.rhs = L.r = L.d = nullptr;
+        L.x32 = L.rhs32 = L.r32 = L.d32 = nullptr;
+    }
+    for (auto &L : c->L) {
+        const size_t nb = (size_t)L.n * L.b;
+        if (!rc) rc = dalloc(&L.x, nb);
+        if (!rc) rc = dalloc(&L.rhs, nb);
+        if (!rc) rc = dalloc(&L.r, nb);
+        if (!rc) rc = dalloc(&L.d, nb);
+        if (!rc && h->opt.mixed) {
+            rc = dalloc(&L.x32, nb);
+            if (!rc) rc = dalloc(&L.rhs32, nb);
+            if (!rc) rc = dalloc(&L.r32, nb);
+            if (!rc) rc = dalloc(&L.d32, nb);
+        }
+    }
+    if (rc) {
+        sg_amg_destroy(c);
+        return rc;
+    }
+    *out = c;
+    return SG_OK;
+}
+
 // Numeric set-up for new values of the level-0 matrix (device pointer, kept by reference
 // until the next update: the caller must not free or overwrite it while applying).
 extern "C" int sg_amg_update(sg_amg *h, const double *Avals, void *stream) {
     SG_CHECK_ARG(h && Avals, "null argument");
+    SG_CHECK_ARG(!h->parent, "a clone is updated through its parent");
     h->L[0].Avals = Avals;
     const InstrToken tk = instr_begin(IK_AMG_UPDATE, as_stream(stream));
     int rc = h->opt.mixed ? numeric_update32(h, as_stream(stream)) : numeric_update(h, as_stream(stream));
@@ -1514,6 +1568,10 @@ extern "C" int sg_amg_update(sg_amg *h, const double *Avals, void *stream) {
 // z = one V-cycle applied to r (device pointers, FP64 in and out).
 extern "C" int sg_amg_apply(sg_amg *h, const double *r, double *z, void *stream) {
     SG_CHECK_ARG(h && r && z, "null argument");
+    if (h->parent) {   // the parent's latest update: level-0 values and state
+        h->L[0].Avals = h->parent->L[0].Avals;
+        h->updated = h->parent->updated;
+    }
     if (!h->updated) return set_error(SG_ERR_STATE, "sg_amg_update must be called before sg_amg_apply");
     const cudaStream_t st = as_stream(stream);
     Level &L = h->L[0];
@@ -1555,6 +1613,7 @@ extern "C" int sg_amg_apply(sg_amg *h, const double *r, double *z, void *stream)
 // switches it off.
 extern "C" int sg_amg_set_correction(sg_amg *h, const double *Cb, void *stream) {
     SG_CHECK_ARG(h, "null argument");
+    SG_CHECK_ARG(!h->parent || !Cb, "the learned correction is not available on a clone");
     if (!Cb) {
         h->corr_on = 0;
         return SG_OK;

@@ -180,8 +180,8 @@ def newton_ind_SSR(U_ini, omega, lambda_ini, it_newt_max, it_damp_max, tol, r_mi
         F_eps = cons.build_F_all(lambda_it + eps, U_it)
         G = (F_eps - F) / eps
         solver.A_orthogonalize(K)
-        W, lin_w = solver.solve(K, -G * Q)
-        V, lin_v = solver.solve(K, fQ - F * Q)
+        # the two systems are independent: solved side by side when the solver can
+        (W, lin_w), (V, lin_v) = solver.solve_pair(K, -G * Q, fQ - F * Q)
         hist["linear_iters_W"].append(lin_w)
         hist["linear_iters_V"].append(lin_v)
         d_l = -dot(fQ, V) / dot(fQ, W)
@@ -261,8 +261,7 @@ def newton_ind_LL(U_ini, t_ini, omega, it_newt_max, it_damp_max, tol, r_min, K_e
         else:
             solver.update_preconditioner_values(K)
         solver.A_orthogonalize(K)
-        W, lin_w = solver.solve(K, fQ)
-        V, lin_v = solver.solve(K, t_it * fQ - F * Q)
+        (W, lin_w), (V, lin_v) = solver.solve_pair(K, fQ, t_it * fQ - F * Q)
         hist["linear_iters_W"].append(lin_w)
         hist["linear_iters_V"].append(lin_v)
         d_t = -dot(fQ, V) / dot(fQ, W)
