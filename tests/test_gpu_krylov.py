@@ -129,3 +129,33 @@ def test_cached_projection_matches_spmv_projection(cuda_device):
     assert sol._aw_key == (K.data_ptr(), matrix_generation())
     P.cons.build_K_r_QQ_vals(1e-4)
     assert sol._aw_key != (K.data_ptr(), matrix_generation())
+
+
+@pytest.mark.parametrize("mixed", [False, True])
+def test_concurrent_solve_pair_equals_sequential(cuda_device, mixed):
+    """DFGMRES.solve_pair with the second solve on its own stream, Krylov workspace and AMG
+    clone (sg_amg_clone) from a second host thread returns bitwise the same solutions and
+    iteration counts as the two solves in sequence, with a deflation basis present; the clone
+    follows the parent's next value update."""
+    P, K, KQ, q = elastic_system()
+    amg = AMG(P.dmesh, mixed=mixed)
+    s = DFGMRES(P.dmesh, 1e-6, 100, 1e-3, amg=amg)
+    s.setup_preconditioner(K)
+    rng = np.random.default_rng(4)
+    mask = P.dmesh.mask
+    for _ in range(2):
+        s.expand_deflation_basis(torch.from_numpy(rng.normal(size=P.dmesh.n_dof)).to(cuda_device) * mask)
+    s.A_orthogonalize(K)
+    b1 = torch.from_numpy(rng.normal(size=P.dmesh.n_dof)).to(cuda_device) * mask
+    b2 = torch.from_numpy(rng.normal(size=P.dmesh.n_dof)).to(cuda_device) * mask
+    for K_now in (K, P.cons.build_K_r_QQ_vals(0.3)):
+        if K_now is not K:
+            s.setup_preconditioner(K_now)
+            s.A_orthogonalize(K_now)
+        s.concurrent_pair = False
+        (x1, i1), (x2, i2) = s.solve_pair(K_now, b1, b2)
+        s.concurrent_pair = True
+        (y1, j1), (y2, j2) = s.solve_pair(K_now, b1, b2)
+        torch.cuda.synchronize()
+        assert (i1, i2) == (j1, j2)
+        assert torch.equal(x1, y1) and torch.equal(x2, y2)
