@@ -26,10 +26,13 @@ throughout), ``mixed`` (FP32 V-cycle inside the FP64 FGMRES; return mapping, New
 residual, Arnoldi and the lambda update in FP64) and ``learned`` (mixed plus the learned
 node-wise correction of the V-cycle: a per-node BF16 network trained on the GPU during the
 init phase, on the residual vectors of the plain V-cycle for the init phase's fourth
-Newton system, then kept only if a trial solve of that system needs fewer FGMRES
-iterations with it; training and trial time are reported, not timed).  ``value`` is the learned
-form's s/step (mixed+learned, the form the metric names); the other forms' figures and the
-lambda error of each form against plain at equal step index are in ``config``.  ``value`` excludes the per-step host<->device state copies;
+Newton system, then kept only if a trial solve of that system to 1e-6 needs fewer FGMRES
+iterations and at most 95 % of the time with it; training and trial time are reported, not
+timed).  ``value`` is the learned form's s/step (mixed+learned, the form the metric names);
+the other forms' figures, the lambda error of each form against plain at equal step index,
+and per timed step the device time, the driver thread's host wall and CPU time and the
+caching allocator's device allocations are in ``config.forms``.  Python's garbage collector
+is paused inside the timed region.  ``value`` excludes the per-step host<->device state copies;
 ``e2e`` includes them: every timed step starts by copying its input state (U, U_old) from
 pinned host memory and ends by reading the new state back.  The working set (K_r 2.0 GB on
 the layered slope, 441 MB on the homogeneous one; Krylov bases several GB) exceeds the 126 MB
