@@ -92,6 +92,9 @@ def parse():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--form", default="all", choices=["all", "both", "plain", "mixed", "learned"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--concurrent-solves", action="store_true",
+                    help="run the two Krylov solves of each Newton step side by side (DFGMRES.solve_pair); "
+                         "per-kernel timings then include the sharing of the GPU")
     ap.add_argument("--workload", default="hetero", choices=["hetero", "ssr", "ll", "box"],
                     help="hetero: the SSR continuation step on the layered slope at h = 0.6 m (headline); ssr: the "
                          "same on the homogeneous 40 m slope at h = 1 m; ll: limit-load continuation on the "
@@ -173,6 +176,7 @@ def run_form(args, form, P, rank, world):
     t0 = time.perf_counter()
     solver = set_linear_solver("DFGMRES_B200" if form == "plain" else "DFGMRES_B200_MIXED", 1e-1, 100, 1e-3, 0,
                                P.dmesh, P.mesh.coord, learned=LEARNED_OPTS if form == "learned" else None, cons=P.cons)
+    solver.concurrent_pair = bool(args.concurrent_solves)
     f = P.f_device()
     run = SSRIndirectStepper(problems.SSR_3D_EXTRUDED, P.dmesh.mask, f, P.cons, solver).init()
     t_init = time.perf_counter() - t0
@@ -341,6 +345,7 @@ def run_ll_form(args, form, P):
     t0 = time.perf_counter()
     solver = set_linear_solver("DFGMRES_B200" if form == "plain" else "DFGMRES_B200_MIXED", 1e-1, 100, 1e-3, 0,
                                P.dmesh, P.mesh.coord, learned=LEARNED_OPTS if form == "learned" else None, cons=P.cons)
+    solver.concurrent_pair = bool(args.concurrent_solves)
     f = P.f_device()
     Q = P.dmesh.mask
     U0, d_omega = continuation.LL_elastic_start(Q, f, P.cons, solver)
