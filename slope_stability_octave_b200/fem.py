@@ -325,7 +325,7 @@ def materials(mat_id_per_elem, n_q, mat_table, saturation=None):
 
 
 def elastic_fields_from_point_draws(c0, phi_deg, young, nu):
-    """Per-point c0 / phi / psi=0 / moduli for point-wise material draws (config 1)."""
+    """Per-point c0 / phi / psi=0 / moduli for point-wise material draws (the box microbenchmark)."""
     shear = young / (2 * (1 + nu))
     bulk = young / (3 * (1 - 2 * nu))
     lame = bulk - 2 * shear / 3

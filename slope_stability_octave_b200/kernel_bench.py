@@ -57,7 +57,7 @@ def timed(fn, reps, warmup=3):
 
 def build(workload):
     if workload == "box":
-        mesh = workloads.box_mesh_config1()
+        mesh = workloads.box_mesh_80x40x40()
         xi, wf = fem.quadrature_p2_tet()
         _, d1, d2, d3 = fem.local_basis_p2_tet(xi)
         D1, D2, D3, W = fem.geometry_3d(mesh, d1, d2, d3, wf)

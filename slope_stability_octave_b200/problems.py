@@ -1,9 +1,11 @@
-"""Problem set-up for the benchmark configurations (host inputs + device objects).
+"""Problem set-up for the benchmark workloads (host inputs + device objects).
 
-Config 0   2D homogeneous slope, P2 triangles, h = 0.5 (slope_stability_2D_homo_SSR.m:30-48)
-Config 2   3D homogeneous slope, P2 tets: the 2D profile extruded 40 m, mesh_P2_3D(N_h = 1,
-           15, 10, 15, 10, 10, 40) (slope_stability_3D_homo_SSR.m parameters)
-Config 3   3D slope with horizontal material layers (heterogeneous), see ``layered_material_ids``
+slope_2d                2D homogeneous slope, P2 triangles, h = 0.5 (slope_stability_2D_homo_SSR.m:30-48)
+slope_3d                3D homogeneous slope, P2 tets: the 2D profile extruded 40 m, mesh_P2_3D(N_h = 1,
+                        15, 10, 15, 10, 10, 40) (slope_stability_3D_homo_SSR.m parameters)
+slope_3d_layered        3D slope with horizontal material layers (heterogeneous), see
+                        ``layered_material_ids``
+slope_3d_random_field   3D slope with lognormal random-field strength (limit-load workload)``
 
 Material rows are (c0 [kPa], phi [deg], psi [deg], E [kPa], nu, gamma_sat, gamma_unsat).
 """
@@ -104,14 +106,14 @@ def slope_3d(N_h=1, dims=(15, 10, 15, 10, 10, 40), mat=HOMO):
 # downward and clipped at the base (y = 0): the body is 20 m high, so the two lower layers
 # of the listed four fall below the base and only the first three (plus the clipped 10 m one)
 # carry material.  Rows: (c0, phi, psi, E, nu, gamma, gamma).
-LAYERS_CFG3 = [[15.0, 30.0, 0.0, 50000.0, 0.30, 19.0, 19.0],
+SLOPE_LAYERS = [[15.0, 30.0, 0.0, 50000.0, 0.30, 19.0, 19.0],
                [10.0, 35.0, 0.0, 40000.0, 0.30, 20.0, 20.0],
                [18.0, 25.0, 0.0, 60000.0, 0.30, 21.0, 21.0],
                [6.0, 45.0, 0.0, 40000.0, 0.30, 20.0, 20.0]]
-LAYER_THICKNESS_CFG3 = (5.0, 5.0, 10.0, 20.0)
+SLOPE_LAYER_THICKNESS = (5.0, 5.0, 10.0, 20.0)
 
 
-def layered_material_ids(mesh, top=20.0, thickness=LAYER_THICKNESS_CFG3):
+def layered_material_ids(mesh, top=20.0, thickness=SLOPE_LAYER_THICKNESS):
     """Layer index of every element by the depth of its centroid below ``top``."""
     yc = mesh.coord[1, mesh.elem[:4]].mean(axis=0)
     depth = top - yc
@@ -122,16 +124,16 @@ def layered_material_ids(mesh, top=20.0, thickness=LAYER_THICKNESS_CFG3):
 def slope_3d_layered(N_h=1, dims=(15, 10, 15, 10, 10, 40)):
     mesh = fem.mesh_p2_3d(N_h, *dims)
     ids = layered_material_ids(mesh, top=dims[3] + dims[4])
-    return _assemble_problem(mesh, ids, LAYERS_CFG3)
+    return _assemble_problem(mesh, ids, SLOPE_LAYERS)
 
 
 # strength random field of the limit-load workload: lognormal c and phi, independent,
 # isotropic exponential correlation; E = 40 MPa, nu = 0.3, gamma = 20 kN/m^3 everywhere
-RANDOM_FIELD_CFG4 = dict(c_mean=10.0, c_cov=0.3, phi_mean=35.0, phi_cov=0.1, corr_len=5.0, young=40000.0, nu=0.3,
+RANDOM_FIELD_STRENGTH = dict(c_mean=10.0, c_cov=0.3, phi_mean=35.0, phi_cov=0.1, corr_len=5.0, young=40000.0, nu=0.3,
                          gamma=20.0, spacing=0.5)
 
 
-def random_field_materials(mesh, hat, seed, rf=RANDOM_FIELD_CFG4):
+def random_field_materials(mesh, hat, seed, rf=RANDOM_FIELD_STRENGTH):
     """Per-integration-point material of a slope whose cohesion and friction angle are
     independent lognormal random fields (means and coefficients of variation in ``rf``) with
     the exponential correlation exp(-r / corr_len).  The two standard Gaussian fields come
@@ -150,7 +152,7 @@ def random_field_materials(mesh, hat, seed, rf=RANDOM_FIELD_CFG4):
     return mat, info
 
 
-def slope_3d_random_field(N_h=1, dims=(15, 10, 15, 10, 10, 40), seed=20261203, rf=RANDOM_FIELD_CFG4):
+def slope_3d_random_field(N_h=1, dims=(15, 10, 15, 10, 10, 40), seed=20261203, rf=RANDOM_FIELD_STRENGTH):
     """The extruded 3D slope with lognormal random-field strength (limit-load workload)."""
     mesh = fem.mesh_p2_3d(N_h, *dims)
     xi, wf = fem.quadrature_p2_tet()

@@ -1,4 +1,4 @@
-"""Seeded synthetic workloads with the shapes and value ranges of the benchmark configs.
+"""Seeded synthetic workloads with the shapes and value ranges of the benchmark workloads.
 
 The reference publishes no input data for these sizes; the inputs here are generated:
 
@@ -10,7 +10,7 @@ The reference publishes no input data for these sizes; the inputs here are gener
   random rotation, and kept only if the branch decision has a relative margin of at least
   ``margin`` on every criterion, and the principal strains are separated, so that 1-ulp
   differences between CPU and GPU libm cannot change the branch.
-* ``box_mesh_config1``: the 80 x 40 x 40 m box split into 6 P2 tets per unit cell.
+* ``box_mesh_80x40x40``: the 80 x 40 x 40 m box split into 6 P2 tets per unit cell.
 """
 from __future__ import annotations
 
@@ -104,7 +104,7 @@ _PROPOSALS = {0: (-1.0, 0.3, 0.0, 1.0), 1: (-2.0, 2.0, 0.0, 4.0), 2: (-2.0, 2.0,
 
 def constitutive_points(n, seed=20261203, fractions=(0.2, 0.2, 0.2, 0.2, 0.2), margin=1e-8,
                         young=40000.0, poisson=0.3, sort_by_branch=False, separation=1e-4):
-    """Seeded per-point inputs for the constitutive kernels (config 1 draws).
+    """Seeded per-point inputs for the constitutive kernels (the box microbenchmark's draws).
 
     ``separation``: minimum relative gap of the principal strains entering the branch's
     tangent (``separation3d``); nearly coincident principal strains make the reference's
@@ -160,6 +160,7 @@ def constitutive_points(n, seed=20261203, fractions=(0.2, 0.2, 0.2, 0.2, 0.2), m
     return dict(E=np.ascontiguousarray(E), c_bar=c_bar, sin_phi=sin_phi, target=target, **mat)
 
 
-def box_mesh_config1(nx=80, ny=40, nz=40):
-    """Config-1 mesh: 80 x 40 x 40 unit cells -> 768,000 P2 tets, 1,056,321 nodes."""
+def box_mesh_80x40x40(nx=80, ny=40, nz=40):
+    """Box mesh of the return-map microbenchmark: 80 x 40 x 40 unit cells -> 768,000 P2 tets,
+    1,056,321 nodes."""
     return fem.mesh_p2_box(nx, ny, nz, 1.0)

@@ -8,7 +8,7 @@ newton_ind_SSR.m, newton.m and damping_ALG5.m driving the reference's own compil
 mapping and assembly) runs with a sparse direct solver, so lambda and omega carry no Krylov or
 AMG error.  Cases (three accepted steps after the two-step init phase):
 
-  cfg0    the 2D homogeneous slope at h = 0.5 (mesh_P2_2D(0.5, 15, 10, 15, 10, 10)),
+  slope2d the 2D homogeneous slope at h = 0.5 (mesh_P2_2D(0.5, 15, 10, 15, 10, 10)),
           parameters of slope_stability_2D_homo_SSR.m
   small3d the 3D homogeneous slope mesh_P2_3D(N_h = 1, 15, 10, 15, 10, 10, z = 1),
           parameters of slope_stability_3D_homo_SSR.m
@@ -42,7 +42,7 @@ STEPS = 3
 
 def cases():
     return {
-        "cfg0": (lambda: problems.slope_2d(0.5), problems.SSR_2D),
+        "slope2d": (lambda: problems.slope_2d(0.5), problems.SSR_2D),
         "small3d": (lambda: problems.slope_3d(1, dims=(15, 10, 15, 10, 10, 1)), problems.SSR_3D),
     }
 
@@ -64,7 +64,7 @@ LL_STEPS = 7
 
 def ll_cases():
     return {
-        "cfg0": (lambda: problems.slope_2d(0.5), problems.LL_2D),
+        "slope2d": (lambda: problems.slope_2d(0.5), problems.LL_2D),
         "small3d": (lambda: problems.slope_3d(1, dims=(15, 10, 15, 10, 10, 1)), problems.LL_3D),
         # lognormal random-field strength (per-point c and phi) on the same small mesh
         "rf3d": (lambda: problems.slope_3d_random_field(1, dims=(15, 10, 15, 10, 10, 1), seed=20261203),

@@ -35,7 +35,7 @@ GOLDEN_LL = os.path.join(os.path.dirname(__file__), "golden", "ll_oracle.npz")
 GOLDEN_DIRECT = os.path.join(os.path.dirname(__file__), "golden", "ssr_direct_oracle.npz")
 
 CASES = {
-    "cfg0": (lambda: problems.slope_2d(0.5), problems.SSR_2D),
+    "slope2d": (lambda: problems.slope_2d(0.5), problems.SSR_2D),
     "small3d": (lambda: problems.slope_3d(1, dims=(15, 10, 15, 10, 10, 1)), problems.SSR_3D),
     # the four-layer heterogeneous slope (per-element materials) on the same small mesh
     "layered3d": (lambda: problems.slope_3d_layered(1, dims=(15, 10, 15, 10, 10, 1)), problems.SSR_3D),
@@ -66,7 +66,7 @@ def test_ssr_continuation_matches_oracle(cuda_device, case):
 
 
 LL_CASES = {
-    "cfg0": (lambda: problems.slope_2d(0.5), problems.LL_2D),
+    "slope2d": (lambda: problems.slope_2d(0.5), problems.LL_2D),
     "small3d": (lambda: problems.slope_3d(1, dims=(15, 10, 15, 10, 10, 1)), problems.LL_3D),
     # per-point lognormal random-field strength (the limit-load workload's material) on the same mesh
     "rf3d": (lambda: problems.slope_3d_random_field(1, dims=(15, 10, 15, 10, 10, 1), seed=20261203),
@@ -109,7 +109,7 @@ def run_direct(P, p, tol, steps=None):
     return lh, oh
 
 
-DIRECT_CASES = {k: CASES[k] for k in ("cfg0", "small3d")}
+DIRECT_CASES = {k: CASES[k] for k in ("slope2d", "small3d")}
 
 
 @pytest.mark.parametrize("case", sorted(DIRECT_CASES))

@@ -140,8 +140,8 @@ def test_oracle_continuation_reproduces_fixture():
     sys.path.insert(0, os.path.join(os.path.dirname(__file__), "golden"))
     from make_continuation_golden import cases, run_case
     g = np.load(os.path.join(os.path.dirname(__file__), "golden", "ssr_oracle.npz"))
-    make, params = cases()["cfg0"]
+    make, params = cases()["slope2d"]
     lh, oh, its = run_case(make, params)
-    np.testing.assert_allclose(lh, g["cfg0_lambda"], rtol=1e-10)
-    np.testing.assert_allclose(oh, g["cfg0_omega"], rtol=1e-10)
-    assert list(its) == list(g["cfg0_newton"])
+    np.testing.assert_allclose(lh, g["slope2d_lambda"], rtol=1e-10)
+    np.testing.assert_allclose(oh, g["slope2d_omega"], rtol=1e-10)
+    assert list(its) == list(g["slope2d_newton"])
