@@ -518,6 +518,11 @@ __device__ __forceinline__ void load_raw(const V *__restrict__ src, V *dst) {
     }
 }
 
+// Accumulator type of the Galerkin gathers: FP64 for the FP64 set-up, FP32 for the FP32 one
+// (the mixed form's coarse operators are stored in FP32 anyway).
+template <typename V> struct GAcc { using type = double; };
+template <> struct GAcc<float> { using type = float; };
+
 // AP block = sum over plan pairs A_a (B x B) * P_b (B x BC), one thread per AP block.  For the
 // small block shapes two pairs are in flight per iteration (their index and block loads
 // issued before either product), which doubles the loads a thread keeps outstanding; the
@@ -526,10 +531,11 @@ template <int B, int BC, typename V = double>
 __global__ void k_gather_AP(int64_t nblk, const int64_t *__restrict__ lptr, const int32_t *__restrict__ la,
                             const int32_t *__restrict__ lb, const V *__restrict__ A, const V *__restrict__ P,
                             V *__restrict__ AP) {
+    using T = typename GAcc<V>::type;
     for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q < nblk; q += (int64_t)gridDim.x * blockDim.x) {
-        double acc[B * BC];
+        T acc[B * BC];
 #pragma unroll
-        for (int t = 0; t < B * BC; ++t) acc[t] = 0.0;
+        for (int t = 0; t < B * BC; ++t) acc[t] = 0;
         const int64_t l1 = lptr[q + 1];
         int64_t l = lptr[q];
         auto product = [&](const V *a, const V *pv) {
@@ -537,9 +543,9 @@ __global__ void k_gather_AP(int64_t nblk, const int64_t *__restrict__ lptr, cons
             for (int r = 0; r < B; ++r)
 #pragma unroll
                 for (int m = 0; m < B; ++m) {
-                    const double av = (double)a[r * B + m];
+                    const T av = (T)a[r * B + m];
 #pragma unroll
-                    for (int c = 0; c < BC; ++c) acc[r * BC + c] += av * (double)pv[m * BC + c];
+                    for (int c = 0; c < BC; ++c) acc[r * BC + c] += av * (T)pv[m * BC + c];
                 }
         };
         if constexpr (B * B + B * BC <= 27) {   // two pairs in flight (fine level and 2D shapes)
@@ -621,14 +627,14 @@ __global__ void k_gather_AP_warp(int64_t nblk, const int64_t *__restrict__ lptr,
     const int64_t span = ((nblk + ng - 1) / ng) * ng;
     for (int64_t q = q0; q < span; q += ng) {
         const bool live = q < nblk;
-        double acc[B * BC];
+        typename GAcc<V>::type acc[B * BC];
 #pragma unroll
-        for (int t = 0; t < B * BC; ++t) acc[t] = 0.0;
+        for (int t = 0; t < B * BC; ++t) acc[t] = 0;
         if (live) {
             for (int64_t l = lptr[q] + gl; l < lptr[q + 1]; l += G) {
-                double a[B * B], p[B * BC];
-                load_block<B * B>(A + (int64_t)la[l] * B * B, a);
-                load_block<B * BC>(P + (int64_t)lb[l] * B * BC, p);
+                V a[B * B], p[B * BC];
+                load_raw<B * B>(A + (int64_t)la[l] * B * B, a);
+                load_raw<B * BC>(P + (int64_t)lb[l] * B * BC, p);
 #pragma unroll
                 for (int r = 0; r < B; ++r)
 #pragma unroll
@@ -659,14 +665,14 @@ __global__ void k_gather_Ac_warp(int64_t nblk, const int32_t *__restrict__ row, 
     const int64_t span = ((nblk + ng - 1) / ng) * ng;
     for (int64_t q = q0; q < span; q += ng) {
         const bool live = q < nblk;
-        double acc[BC * BC];
+        typename GAcc<V>::type acc[BC * BC];
 #pragma unroll
-        for (int t = 0; t < BC * BC; ++t) acc[t] = 0.0;
+        for (int t = 0; t < BC * BC; ++t) acc[t] = 0;
         if (live) {
             for (int64_t l = lptr[q] + gl; l < lptr[q + 1]; l += G) {
-                double p[B * BC], ap[B * BC];
-                load_block<B * BC>(P + (int64_t)la[l] * B * BC, p);
-                load_block<B * BC>(AP + (int64_t)lb[l] * B * BC, ap);
+                V p[B * BC], ap[B * BC];
+                load_raw<B * BC>(P + (int64_t)la[l] * B * BC, p);
+                load_raw<B * BC>(AP + (int64_t)lb[l] * B * BC, ap);
 #pragma unroll
                 for (int m = 0; m < B; ++m)
 #pragma unroll
@@ -1142,8 +1148,9 @@ static int numeric_update(sg_amg *h, cudaStream_t st) {
 }
 
 // Mixed form: the numeric update in FP32 for the FP32 V-cycle.  The level matrices, P, R and
-// A P are formed directly in FP32 (products accumulated in FP64 registers), the block
-// inverses and lambda_max in FP64 from the FP32 values; the coarsest dense inverse in FP64.
+// A P are formed directly in FP32 (the Galerkin gathers accumulate in FP32, the prolongator
+// smoothing in FP64 registers), the block inverses and lambda_max in FP64 from the FP32
+// values; the coarsest dense inverse in FP64.
 // The set-up inside sg_amg_create keeps the FP64 path, so the mixed form has the same
 // hierarchy structure as the plain one.
 static int numeric_update32(sg_amg *h, cudaStream_t st) {
