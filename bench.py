@@ -523,6 +523,11 @@ def main():
     if args.impl == "reference":
         if args.workload == "box":
             box_reference_arm(args, rank)
+        elif args.workload == "ll":
+            if rank == 0:
+                print(json.dumps(dict(impl="reference", metric=LL_METRIC,
+                                      unavailable="no CPU model of the limit-load step: the reference CPU path is "
+                                                  "modelled for the SSR step workloads (hetero, ssr) and the box")))
         else:
             reference_arm(args, rank, world)
         return
