@@ -145,3 +145,25 @@ def test_oracle_continuation_reproduces_fixture():
     np.testing.assert_allclose(lh, g["slope2d_lambda"], rtol=1e-10)
     np.testing.assert_allclose(oh, g["slope2d_omega"], rtol=1e-10)
     assert list(its) == list(g["slope2d_newton"])
+
+
+def test_oracle_layered_and_random_field_fixtures_reproduce():
+    """The heterogeneous-material fixtures regenerate exactly from their script: the layered
+    slope's SSR history (per-element materials) and the random-field slope's LL history
+    (per-point lognormal c and phi from the seeded circulant-embedding field)."""
+    import sys
+    sys.path.insert(0, os.path.join(os.path.dirname(__file__), "golden"))
+    from make_continuation_golden import layered_cases, ll_cases, run_case, run_ll_case
+    gdir = os.path.join(os.path.dirname(__file__), "golden")
+    g = np.load(os.path.join(gdir, "ssr_oracle.npz"))
+    make, params = layered_cases()["layered3d"]
+    lh, oh, its = run_case(make, params)
+    np.testing.assert_allclose(lh, g["layered3d_lambda"], rtol=1e-10)
+    np.testing.assert_allclose(oh, g["layered3d_omega"], rtol=1e-10)
+    assert list(its) == list(g["layered3d_newton"])
+    g = np.load(os.path.join(gdir, "ll_oracle.npz"))
+    make, p = ll_cases()["rf3d"]
+    th, oh, its = run_ll_case(make, p)
+    np.testing.assert_allclose(th, g["rf3d_t"], rtol=1e-10)
+    np.testing.assert_allclose(oh, g["rf3d_omega"], rtol=1e-10)
+    assert list(its) == list(g["rf3d_newton"])
