@@ -18,7 +18,7 @@ import torch
 
 from . import fem
 from .constitutive import CONSTITUTIVE
-from .device import DeviceMesh, F64
+from .device import DeviceMesh
 from .linear_solvers import set_linear_solver
 
 HOMO = [6.0, 45.0, 0.0, 40000.0, 0.3, 20.0, 20.0]
