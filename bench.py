@@ -249,7 +249,10 @@ def run_form(args, form, P, rank, world):
                               fallbacks=lc.fallbacks, solves=lc.solves, params=lc.info()["nparam"],
                               acceptance_trial=lc.gate, applied=bool(lc.enabled))
     del run, solver
-    torch.cuda.empty_cache()
+    # the caching allocator keeps its blocks for the next form, whose timed steps then run on
+    # a warm allocator as a long-running solver's would (the first form warms it during its
+    # own set-up); only cyclic garbage is collected here
+    gc.collect()
     return res
 
 
@@ -362,7 +365,7 @@ def run_ll_form(args, form, P):
                linear=st["step_linear_iterations"], attempts=st["attempts"], wall=st["step_wall_time"],
                s_per_step=sum(timed) / len(timed), init_s=round(t_init, 2))
     del solver
-    torch.cuda.empty_cache()
+    gc.collect()
     return res
 
 
