@@ -45,3 +45,15 @@ def test_argument_errors_need_no_device():
     assert rc == -1 and b"Davis" in L.sg_last_error()
     rc = L.sg_constitutive3d(None, None, None, None, None, None, ctypes.c_int64(-1), None, None, None)
     assert rc == -1
+
+
+def test_new_entry_points_reject_bad_arguments_without_device():
+    """The fused residual and the AMG clone check their arguments before any device work."""
+    L = _lib.lib()
+    rc = L.sg_residual_dev(None, None, None, None, None, None, None, None, None)
+    assert rc == -1 and b"null" in L.sg_last_error()
+    out = ctypes.c_void_p()
+    rc = L.sg_amg_clone(None, ctypes.byref(out))
+    assert rc == -1 and out.value is None
+    rc = L.sg_amg_update(None, None, None)
+    assert rc == -1
