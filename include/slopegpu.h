@@ -212,8 +212,43 @@ int sg_amg_clone(const sg_amg *amg, sg_amg **clone);
 int sg_amg_update(sg_amg *amg, const double *A_vals, void *stream);
 /* z = V-cycle(r), device vectors of n_rows*b entries */
 int sg_amg_apply(sg_amg *amg, const double *r, double *z, void *stream);
-/* info[0] levels, info[1] coarsest dense size, then (block size, block rows, blocks) per level */
+/* info[0] levels, info[1] coarsest dense size, then (block size, block rows, blocks) per level
+ * (at most 10 levels); with cap > 32, info[32 + l] = blocks of level l's prolongator */
 int sg_amg_info(const sg_amg *amg, int64_t *info, int32_t cap);
+/* ------------------------------------------------------------------------------
+ * (d1, d2) Preconditioner instances keyed by id over host COO triplets.  Replaces the
+ * command set of hypre_boomeramg_mex (+LINEAR_SOLVERS/mex/hypre_boomeramg_mex.cpp:
+ * 'setup_ijv' :1013-1146, 'update_values' :1151-1213, 'apply' :751-796, 'clear' :798-835,
+ * 'info' :837-860), as called by DFGMRES.setup_preconditioner_ijv /
+ * update_preconditioner_values (+LINEAR_SOLVERS/DFGMRES.m:172-202) through the closures of
+ * set_linear_solver.m:216-240.
+ *   id        instance name (the reference's instance_id string)
+ *   I, J, V   nnz triplets of the full n x n matrix, I and J 1-based, stored as doubles
+ *             (Octave numeric arrays); duplicate (I, J) entries are summed
+ *   Z         n x nns near-null space, column-major (nns 0: the translations)
+ *   dof_func  length n, component index of every unknown in [0, num_functions) (NULL:
+ *             (q - 1) mod num_functions, as set_linear_solver.m builds it); consecutive
+ *             unknowns with increasing component form one node block
+ *   opts      numeric AMG options as for sg_amg_create (may be NULL)
+ *   force_rebuild  0: an existing id with the same nnz keeps its pattern and takes the new
+ *             values only (the reference's fast path); 1: rebuild
+ *   setup_seconds  out (optional): wall time of the call, as the reference's
+ *             setup_time_seconds
+ * The instance lives on the device that is current at its creation and is used from any
+ * thread (calls are serialised by the library).  apply takes and returns host vectors of
+ * length n and returns when done.  Unknown ids give SG_ERR_STATE, bad sizes SG_ERR_ARG.
+ * ---------------------------------------------------------------------------- */
+int sg_amg_setup_ijv(const char *id, const double *I, const double *J, const double *V, int64_t nnz,
+                     int64_t n, const double *Z, int32_t nns, const double *dof_func,
+                     int32_t num_functions, const double *opts, int32_t n_opts, int32_t force_rebuild,
+                     double *setup_seconds);
+int sg_amg_update_values(const char *id, const double *V, int64_t nnz, double *setup_seconds);
+int sg_amg_apply_host(const char *id, const double *r, double *y, int64_t n);
+/* id NULL clears every instance */
+int sg_amg_clear(const char *id);
+/* id NULL: info[0] = number of instances; else info = [n, nnz, num_functions, nns, nodes,
+ * blocks, full builds, value updates] (up to cap entries) */
+int sg_amg_ijv_info(const char *id, int64_t *info, int32_t cap);
 /* host copies of level l's A pattern/values and P pattern/values (any pointer may be NULL);
  * values are those of the FP64 numeric set-up: for a mixed-precision hierarchy (opts[5] != 0),
  * whose value updates run in FP32, they are the values of its set-up in sg_amg_create */
@@ -307,16 +342,22 @@ int sg_learned_info(const sg_learned *h, int64_t *info);
 /* ------------------------------------------------------------------------------
  * Live kernel timing (no reference counterpart: profiling support in the spirit of the
  * reference's PROFILING.Profiler).  When enabled, every `sample`-th launch of each kind is
- * bracketed by CUDA events on its stream.  Kinds (capacity 10): 0 fine SpMV FP64 (FGMRES,
+ * bracketed by CUDA events on its stream.  Kinds (capacity 11): 0 fine SpMV FP64 (FGMRES,
  * residuals), 1 fine SpMV FP32, 2 return mapping + tangent, 3 return mapping (stress),
  * 4 assembly, 5 AMG value update, 6 AMG V-cycle, 7 fine SpMV on the FP16 copy, 8 fine SpMV
- * FP64 inside sg_a_orthogonalize, 9 fused residual (sg_residual_dev).  sg_instr_read synchronises the device and resets the
+ * FP64 inside sg_a_orthogonalize, 9 fused residual (sg_residual_dev), 10 fine SpMM FP64 of
+ * sg_a_orthogonalize (several vectors per launch).  sg_instr_read synchronises the device and resets the
  * counters.
  * ---------------------------------------------------------------------------- */
 int sg_instr_enable(int on, int sample);
 int sg_instr_read(double *ms, int64_t *timed, int64_t *launches, int32_t cap);
+/* work units per kind since the last sg_instr_read (kind 10: vectors multiplied) */
+int sg_instr_units(int64_t *units, int32_t cap);
 /* number of kernels the library launched since the last reset (reset != 0 clears it) */
 int64_t sg_launch_count(int reset);
+/* number of device allocations (cudaMalloc) the library made since the last reset (reset != 0
+ * clears it); lets a caller check that a timed region allocated no device memory */
+int64_t sg_device_alloc_count(int reset);
 
 #ifdef __cplusplus
 }

@@ -58,6 +58,11 @@ SIGNATURES = {
     "sg_amg_destroy": [vp],
     "sg_amg_update": [vp, vp, vp],
     "sg_amg_clone": [vp, vp],
+    "sg_amg_setup_ijv": [C.c_char_p, vp, vp, vp, i64, i64, vp, i32, vp, i32, vp, i32, i32, vp],
+    "sg_amg_update_values": [C.c_char_p, vp, i64, vp],
+    "sg_amg_apply_host": [C.c_char_p, vp, vp, i64],
+    "sg_amg_clear": [C.c_char_p],
+    "sg_amg_ijv_info": [C.c_char_p, vp, i32],
     "sg_amg_apply": [vp, vp, vp, vp],
     "sg_amg_info": [vp, vp, i32],
     "sg_amg_export": [vp, i32, vp, vp, vp, vp, vp, vp],
@@ -87,8 +92,10 @@ SIGNATURES = {
     "sg_instr_enable": [cint, cint],
     "sg_instr_read": [vp, vp, vp, i32],
     "sg_launch_count": [cint],
+    "sg_instr_units": [vp, i32],
+    "sg_device_alloc_count": [cint],
 }
-_RESTYPES = {"sg_last_error": C.c_char_p, "sg_launch_count": C.c_int64, "sg_mlp_part_size": C.c_int64}
+_RESTYPES = {"sg_last_error": C.c_char_p, "sg_launch_count": C.c_int64, "sg_device_alloc_count": C.c_int64, "sg_mlp_part_size": C.c_int64}
 
 
 class SlopeGPUError(RuntimeError):

@@ -111,6 +111,30 @@ class SSRIndirectStepper:
         self.n_omega = 0
         return self
 
+    # step-control state besides U, U_old and the deflation basis
+    _STATE = ("omega", "omega_old", "lam", "d_omega", "step_no", "n_omega", "finished", "stop_reason")
+
+    def snapshot(self):
+        """The continuation's state after its last accepted step: U and U_old (device copies),
+        the step-control scalars, the lambda/omega/Umax histories and the solver's deflation
+        basis.  ``restore(snapshot)`` puts the run back there (checkpoint/resume; a benchmark
+        replays the continuation from a fixed point)."""
+        return dict(U=self.U.clone(), U_old=self.U_old.clone(), basis=self.solver.basis.clone(),
+                    state={k: getattr(self, k) for k in self._STATE},
+                    hist=(list(self.lambda_hist), list(self.omega_hist), list(self.Umax_hist)))
+
+    def restore(self, snap):
+        """Continue from a ``snapshot()``: the next step() repeats the step that followed it.
+        The statistics keep accumulating."""
+        self.U = snap["U"].clone()
+        self.U_old = snap["U_old"].clone()
+        for k, v in snap["state"].items():
+            setattr(self, k, v)
+        self.lambda_hist, self.omega_hist, self.Umax_hist = (list(h) for h in snap["hist"])
+        self.solver.basis = snap["basis"].clone()
+        self.solver.AW, self.solver._aw_key = None, None
+        return self
+
     def step(self):
         """Attempts until one is accepted (or the run stops).  Returns the accepted step's
         statistics, or None if the continuation stopped without accepting a step."""

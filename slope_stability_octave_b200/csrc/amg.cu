@@ -131,7 +131,7 @@ template <typename T>
 static int dalloc(T **p, size_t n) {
     *p = nullptr;
     if (n == 0) n = 1;
-    SG_CUDA(cudaMalloc((void **)p, n * sizeof(T)));
+    SG_CUDA(sg::device_alloc((void **)p, n * sizeof(T)));
     return SG_OK;
 }
 template <typename T>
@@ -1629,10 +1629,10 @@ extern "C" int sg_amg_set_correction(sg_amg *h, const double *Cb, void *stream) 
     SG_CHECK_ARG(L.b == 3, "the node-wise correction needs 3 x 3 node blocks");
     const cudaStream_t st = as_stream(stream);
     const int64_t nv = L.n * 9;
-    if (!h->corrC) SG_CUDA(cudaMalloc(&h->corrC, sizeof(double) * nv));
+    if (!h->corrC) SG_CUDA(sg::device_alloc(&h->corrC, sizeof(double) * nv));
     SG_CUDA(cudaMemcpyAsync(h->corrC, Cb, sizeof(double) * nv, cudaMemcpyDeviceToDevice, st));
     if (h->opt.mixed) {
-        if (!h->corrC32) SG_CUDA(cudaMalloc(&h->corrC32, sizeof(float) * nv));
+        if (!h->corrC32) SG_CUDA(sg::device_alloc(&h->corrC32, sizeof(float) * nv));
         k_to_float<<<grid_for(nv, 256), 256, 0, st>>>(nv, h->corrC, h->corrC32);
         SG_CUDA(cudaGetLastError());
     }
@@ -1640,18 +1640,20 @@ extern "C" int sg_amg_set_correction(sg_amg *h, const double *Cb, void *stream) 
     return SG_OK;
 }
 
-// info: [levels, dense size, then per level: block size, block rows, blocks] (capacity 3 + 3*10)
+// info: [levels, dense size, then per level: block size, block rows, blocks] in the first
+// 2 + 3*10 entries; from entry 32 on, per level: blocks of its prolongator P (0 on the coarsest)
 extern "C" int sg_amg_info(const sg_amg *h, int64_t *info, int32_t cap) {
     SG_CHECK_ARG(h && info && cap >= 2, "bad argument");
     info[0] = (int64_t)h->L.size();
     info[1] = h->nc_dense;
     int k = 2;
     for (const auto &L : h->L) {
-        if (k + 3 > cap) break;
+        if (k + 3 > 32 || k + 3 > cap) break;
         info[k++] = L.b;
         info[k++] = L.n;
         info[k++] = L.Anblk;
     }
+    for (size_t l = 0; l < h->L.size() && 32 + (int)l < cap; ++l) info[32 + l] = h->L[l].P.nblk;
     return SG_OK;
 }
 

@@ -11,8 +11,14 @@ namespace sg {
 
 static thread_local std::string g_last_error;
 static std::atomic<int64_t> g_launches{0};
+static std::atomic<int64_t> g_device_allocs{0};
 
 void count_launch(int n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
+
+cudaError_t device_alloc_raw(void **p, size_t bytes) {
+    g_device_allocs.fetch_add(1, std::memory_order_relaxed);
+    return cudaMalloc(p, bytes);
+}
 
 int set_error(int code, const std::string &msg) {
     g_last_error = msg;
@@ -51,7 +57,7 @@ int Scratch::reserve(size_t want) {
         ptr = nullptr;
         bytes = 0;
     }
-    cudaError_t e = cudaMalloc(&ptr, want);
+    cudaError_t e = device_alloc(&ptr, want);
     if (e != cudaSuccess) {
         ptr = nullptr;
         return cuda_error(e, "scratch allocation");
@@ -74,6 +80,12 @@ extern "C" int sg_abi_version(void) { return 1; }
 extern "C" int64_t sg_launch_count(int reset) {
     const int64_t v = sg::g_launches.load();
     if (reset) sg::g_launches.store(0);
+    return v;
+}
+
+extern "C" int64_t sg_device_alloc_count(int reset) {
+    const int64_t v = sg::g_device_allocs.load();
+    if (reset) sg::g_device_allocs.store(0);
     return v;
 }
 

@@ -434,7 +434,7 @@ extern "C" int sg_bsr_to_ref_dev(sg_mesh *m, const double *K, double *V_ref, voi
                     }
                 }
             }
-        SG_CUDA(cudaMalloc(&m->d_ref2bsr, sizeof(int64_t) * (idx.size() ? idx.size() : 1)));
+        SG_CUDA(sg::device_alloc(&m->d_ref2bsr, sizeof(int64_t) * (idx.size() ? idx.size() : 1)));
         SG_CUDA(cudaMemcpy(m->d_ref2bsr, idx.data(), sizeof(int64_t) * idx.size(), cudaMemcpyHostToDevice));
     }
     k_gather<<<grid_for(m->nnz_ref, 256), 256, 0, st>>>(m->nnz_ref, m->d_ref2bsr, K, V_ref);

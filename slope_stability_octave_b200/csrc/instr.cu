@@ -16,6 +16,7 @@ struct InstrState {
     bool on = false;
     int sample = 1;
     int64_t launches[IK_COUNT] = {0};
+    int64_t units[IK_COUNT] = {0};
     std::vector<std::pair<cudaEvent_t, cudaEvent_t>> timed[IK_COUNT];
     std::vector<cudaEvent_t> pool;
 };
@@ -62,6 +63,13 @@ InstrToken instr_begin(int kind, cudaStream_t st) {
     return t;
 }
 
+void instr_units(int kind, int64_t units) {
+    InstrState &s = state();
+    if (!s.on || kind < 0 || kind >= IK_COUNT) return;
+    std::lock_guard<std::mutex> g(s.mu);
+    s.units[kind] += units;
+}
+
 void instr_end(const InstrToken &t, cudaStream_t st) {
     if (t.kind < 0 || !t.a || !t.b) return;
     InstrState &s = state();
@@ -79,6 +87,15 @@ extern "C" int sg_instr_enable(int on, int sample) {
     std::lock_guard<std::mutex> g(s.mu);
     s.on = on != 0;
     s.sample = sample > 0 ? sample : 1;
+    return SG_OK;
+}
+
+// units[k] = the work units recorded for kind k since the last sg_instr_read (not reset here).
+extern "C" int sg_instr_units(int64_t *units, int32_t cap) {
+    InstrState &s = state();
+    SG_CHECK_ARG(units && cap >= 0, "bad argument");
+    std::lock_guard<std::mutex> g(s.mu);
+    for (int k = 0; k < IK_COUNT && k < cap; ++k) units[k] = s.units[k];
     return SG_OK;
 }
 
@@ -103,6 +120,7 @@ extern "C" int sg_instr_read(double *ms, int64_t *timed, int64_t *launches, int3
         }
         s.timed[k].clear();
         s.launches[k] = 0;
+        s.units[k] = 0;
     }
     return SG_OK;
 }

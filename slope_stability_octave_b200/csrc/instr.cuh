@@ -18,8 +18,13 @@ enum InstrKind {
     IK_SPMV3_F64_AORTH = 8,  // FP64 node-block SpMVs of the deflation-basis A-orthogonalisation
                              // (these may run beside an AMG update on another stream)
     IK_RESIDUAL = 9,     // fused stress-only residual F = B'(w S(B U))
-    IK_COUNT = 10
+    IK_SPMM_AORTH = 10,  // FP64 node-block SpMM (several vectors per pass) of the A-orthogonalisation
+    IK_COUNT = 11
 };
+
+// Units of work done by launches of a kind (e.g. vectors multiplied by one SpMM launch), added
+// while timing is enabled and read by sg_instr_units.
+void instr_units(int kind, int64_t units);
 
 // While an InstrRedirect lives on a thread, launches of kind `from` on that thread are
 // counted and timed as kind `to`.

@@ -50,12 +50,12 @@ static int ensure_kcap(sg_krylov *ws, int64_t k) {
     const int64_t cap = std::max<int64_t>(k, ws->kcap * 2 + 16);
     double *part = nullptr, *hd = nullptr, *Wo = nullptr, *AWo = nullptr, *nt = nullptr, *sig = nullptr;
     const int64_t rows = std::max<int64_t>(cap, ws->maxit + 2);
-    SG_CUDA(cudaMalloc(&part, sizeof(double) * DOT_BLOCKS * rows));
-    SG_CUDA(cudaMalloc(&hd, sizeof(double) * (cap + 8)));
-    SG_CUDA(cudaMalloc(&Wo, sizeof(double) * ws->n * cap));
-    SG_CUDA(cudaMalloc(&AWo, sizeof(double) * ws->n * cap));
-    SG_CUDA(cudaMalloc(&nt, sizeof(double) * (cap + 8)));
-    SG_CUDA(cudaMalloc(&sig, sizeof(double) * (cap + 8)));
+    SG_CUDA(sg::device_alloc(&part, sizeof(double) * DOT_BLOCKS * rows));
+    SG_CUDA(sg::device_alloc(&hd, sizeof(double) * (cap + 8)));
+    SG_CUDA(sg::device_alloc(&Wo, sizeof(double) * ws->n * cap));
+    SG_CUDA(sg::device_alloc(&AWo, sizeof(double) * ws->n * cap));
+    SG_CUDA(sg::device_alloc(&nt, sizeof(double) * (cap + 8)));
+    SG_CUDA(sg::device_alloc(&sig, sizeof(double) * (cap + 8)));
     cudaFree(ws->part);
     cudaFree(ws->hd);
     cudaFree(ws->Worth);
@@ -108,11 +108,11 @@ extern "C" int sg_krylov_create(int64_t n, int32_t maxit, sg_krylov **out) {
     ws->n = n;
     ws->maxit = maxit;
     cudaGetDevice(&ws->device);
-    cudaError_t e = cudaMalloc(&ws->V, sizeof(double) * n * (maxit + 1));
-    if (!e) e = cudaMalloc(&ws->Z, sizeof(double) * n * maxit);
-    if (!e) e = cudaMalloc(&ws->w, sizeof(double) * n);
-    if (!e) e = cudaMalloc(&ws->t, sizeof(double) * n);
-    if (!e) e = cudaMalloc(&ws->hdev, sizeof(double) * (2 * (maxit + 2) + 8));
+    cudaError_t e = sg::device_alloc(&ws->V, sizeof(double) * n * (maxit + 1));
+    if (!e) e = sg::device_alloc(&ws->Z, sizeof(double) * n * maxit);
+    if (!e) e = sg::device_alloc(&ws->w, sizeof(double) * n);
+    if (!e) e = sg::device_alloc(&ws->t, sizeof(double) * n);
+    if (!e) e = sg::device_alloc(&ws->hdev, sizeof(double) * (2 * (maxit + 2) + 8));
     if (!e) e = cudaMallocHost(&ws->hpin, sizeof(double) * (2 * (maxit + 2) + 8));
     int rc = e ? cuda_error(e, "Krylov workspace") : ensure_kcap(ws, 16);
     if (rc) {
@@ -275,12 +275,21 @@ extern "C" int sg_a_orthogonalize(sg_krylov *ws, const sg_bsr *A, const double *
     double *Wo = ws->Worth, *AWo = ws->AWorth, *At = ws->t, *tmp = ws->w, *part = ws->part, *c = ws->hd;
     double *nt = ws->nt, *sig = ws->sig;
     const unsigned gb = grid_for(n, 256, 8);
+    // A times every input column up front (processing order i takes column k - 1 - i): the
+    // products do not depend on the orthogonalisation, and one SpMM reads A once per eight
+    // columns where a SpMV per column reads it k times
+    if (A->b == 3) {
+        rc = bsr_spmm(*A, Avals, W + (int64_t)(k - 1) * n, -n, AWo, n, k, st);
+    } else {
+        for (int i = 0; i < k && !rc; ++i)
+            rc = bsr_spmv<double, double>(*A, Avals, W + (int64_t)(k - 1 - i) * n, AWo + (int64_t)i * n, 1.0, 0.0, st);
+    }
+    if (rc) return rc;
     for (int i = 0; i < k && !rc; ++i) {
         const double *src = W + (int64_t)(k - 1 - i) * n;
         double *col_i = Wo + (int64_t)i * n, *acol_i = AWo + (int64_t)i * n;
-        if ((rc = bsr_spmv<double, double>(*A, Avals, src, At, 1.0, 0.0, st))) break;
+        SG_CUDA(cudaMemcpyAsync(At, acol_i, sizeof(double) * n, cudaMemcpyDeviceToDevice, st));
         SG_CUDA(cudaMemcpyAsync(tmp, src, sizeof(double) * n, cudaMemcpyDeviceToDevice, st));
-        SG_CUDA(cudaMemcpyAsync(acol_i, At, sizeof(double) * n, cudaMemcpyDeviceToDevice, st));
         if (i > 0) {
             // c_j = sig_j (A src)' u_j ;  tmp -= sum c_j u_j ;  A tmp = A src - sum c_j A u_j
             if ((rc = multidot(n, i, Wo, n, At, part, c, st))) break;

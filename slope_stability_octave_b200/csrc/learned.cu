@@ -845,7 +845,7 @@ static int lfree(sg_learned *h) {
 template <typename T>
 static int zalloc(T **p, size_t n) {
     *p = nullptr;
-    SG_CUDA(cudaMalloc((void **)p, (n ? n : 1) * sizeof(T)));
+    SG_CUDA(sg::device_alloc((void **)p, (n ? n : 1) * sizeof(T)));
     SG_CUDA(cudaMemset(*p, 0, (n ? n : 1) * sizeof(T)));
     return SG_OK;
 }
@@ -1115,7 +1115,7 @@ extern "C" int sg_learned_train(sg_learned *h, const sg_bsr *A, const double *A_
     if (!h->have_features) return set_error(SG_ERR_STATE, "sg_learned_features must be called first");
     const cudaStream_t st = as_stream(stream);
     double *dl = nullptr;
-    if (loss_hist && steps > 0) SG_CUDA(cudaMalloc(&dl, sizeof(double) * steps));
+    if (loss_hist && steps > 0) SG_CUDA(sg::device_alloc(&dl, sizeof(double) * steps));
     int rc = SG_OK;
     const float b1 = 0.9f, b2 = 0.999f;
     for (int k = 0; k < steps && !rc; ++k) {

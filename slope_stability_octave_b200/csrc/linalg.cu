@@ -255,6 +255,92 @@ template int bsr_spmv<float, float>(const sg_bsr &, const float *, const float *
 template int bsr_residual<double, double>(const sg_bsr &, const double *, const double *, const double *, double *, cudaStream_t);
 template int bsr_residual<float, float>(const sg_bsr &, const float *, const float *, const float *, float *, cudaStream_t);
 
+// ------------------------------------------------------------------ multi-vector SpMM
+
+// Y(:, c) = A X(:, c) for c < kc (FP64 3x3 blocks; X, Y column-major with leading dimensions
+// ldx, ldy, which may be negative to walk the columns backwards).  k_spmv_blk's lane mapping
+// (G lanes per block row, one block per lane per step) with KC columns per pass: each block's
+// values are read once per pass and multiplied into every column, where KC SpMVs would read
+// the matrix KC times.  Partial sums are combined by the same fixed shuffle tree, so every
+// column equals the single-vector SpMV of that column bitwise.
+template <int G, int KC>
+__global__ void __launch_bounds__(256) k_spmm3(int64_t nrows, const int32_t *__restrict__ rp,
+                                               const int32_t *__restrict__ col, const double *__restrict__ vals,
+                                               const double *__restrict__ X, int64_t ldx, double *__restrict__ Y,
+                                               int64_t ldy, int kc) {
+    constexpr int GPW = 32 / G;
+    const int lane = threadIdx.x & 31, g = lane / G, gl = lane - g * G;
+    const int64_t warp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+    const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    for (int64_t base = warp * GPW; base < nrows; base += nwarps * GPW) {
+        const int64_t row = base + g;
+        double acc[KC][3];
+#pragma unroll
+        for (int c = 0; c < KC; ++c) acc[c][0] = acc[c][1] = acc[c][2] = 0.0;
+        if (row < nrows) {
+            const int32_t p1 = rp[row + 1];
+            for (int32_t p = rp[row] + gl; p < p1; p += G) {
+                const int64_t j = col[p];
+                double v[9];
+#pragma unroll
+                for (int t = 0; t < 9; ++t) v[t] = __ldg(vals + (int64_t)p * 9 + t);
+#pragma unroll
+                for (int c = 0; c < KC; ++c) {
+                    if (c < kc) {
+                        const double *xc = X + c * ldx + j * 3;
+                        const double x0 = __ldg(xc), x1 = __ldg(xc + 1), x2 = __ldg(xc + 2);
+#pragma unroll
+                        for (int a = 0; a < 3; ++a) {
+                            acc[c][a] += v[a * 3] * x0;
+                            acc[c][a] += v[a * 3 + 1] * x1;
+                            acc[c][a] += v[a * 3 + 2] * x2;
+                        }
+                    }
+                }
+            }
+        }
+#pragma unroll
+        for (int off = G / 2; off > 0; off >>= 1)
+#pragma unroll
+            for (int c = 0; c < KC; ++c)
+                if (c < kc)
+#pragma unroll
+                    for (int a = 0; a < 3; ++a) acc[c][a] += __shfl_xor_sync(0xffffffffu, acc[c][a], off);
+        if (row < nrows && gl == 0) {
+#pragma unroll
+            for (int c = 0; c < KC; ++c)
+                if (c < kc)
+#pragma unroll
+                    for (int a = 0; a < 3; ++a) Y[c * ldy + row * 3 + a] = acc[c][a];
+        }
+    }
+}
+
+int bsr_spmm(const sg_bsr &A, const double *vals, const double *X, int64_t ldx, double *Y, int64_t ldy, int k,
+             cudaStream_t st) {
+    if (A.b != 3) return set_error(SG_ERR_ARG, "bsr_spmm: 3x3 blocks only");
+    const double avg = A.n_rows > 0 ? (double)A.n_blocks / (double)A.n_rows : 8.0;
+    // the same lanes per row as the single-vector SpMV (bitwise-equal columns)
+    const int G = avg >= 16.0 ? 32 : (avg >= 8.0 ? 16 : 8);
+    constexpr int KC = 8;
+    for (int c0 = 0; c0 < k; c0 += KC) {
+        const int kc = std::min(KC, k - c0);
+        const InstrToken tk = instr_begin(IK_SPMM_AORTH, st);
+        instr_units(IK_SPMM_AORTH, kc);
+        const unsigned grid = grid_for(A.n_rows * G, 256, 16);
+        const double *Xc = X + c0 * ldx;
+        double *Yc = Y + c0 * ldy;
+        switch (G) {
+            case 32: k_spmm3<32, KC><<<grid, 256, 0, st>>>(A.n_rows, A.d_row_ptr, A.d_col, vals, Xc, ldx, Yc, ldy, kc); break;
+            case 16: k_spmm3<16, KC><<<grid, 256, 0, st>>>(A.n_rows, A.d_row_ptr, A.d_col, vals, Xc, ldx, Yc, ldy, kc); break;
+            default: k_spmm3<8, KC><<<grid, 256, 0, st>>>(A.n_rows, A.d_row_ptr, A.d_col, vals, Xc, ldx, Yc, ldy, kc); break;
+        }
+        instr_end(tk, st);
+        SG_CUDA(cudaGetLastError());
+    }
+    return SG_OK;
+}
+
 // ------------------------------------------------------------------ FP16 level-0 SpMV
 
 // Lane mapping of k_spmv_blk (G lanes per block row, one block per lane per step); a lane reads

@@ -22,6 +22,11 @@ template <typename VT, typename XT>
 int rect_spmv(int br, int bc, int64_t nrows, const int32_t *rp, const int32_t *col, const VT *vals, const XT *x,
               XT *y, double alpha, double beta, const XT *bvec, int mode, cudaStream_t st, int64_t nblk = -1);
 
+// Y(:, c) = A X(:, c) for c < k, FP64 3x3 blocks; X, Y column-major (leading dimensions may
+// be negative).  Reads the matrix once per 8 columns; each column equals bsr_spmv's bitwise.
+int bsr_spmm(const sg_bsr &A, const double *vals, const double *X, int64_t ldx, double *Y, int64_t ldy, int k,
+             cudaStream_t st);
+
 // Reduction workspace for dot products: partial sums of `nblk` blocks per column.
 constexpr int DOT_BLOCKS = 296;  // 2 x 148 SMs
 constexpr int DOT_THREADS = 256;

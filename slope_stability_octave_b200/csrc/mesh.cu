@@ -29,7 +29,7 @@ namespace sg {
 template <typename T>
 static int upload(T **dst, const T *src, size_t n) {
     if (n == 0) { *dst = nullptr; return SG_OK; }
-    SG_CUDA(cudaMalloc((void **)dst, n * sizeof(T)));
+    SG_CUDA(sg::device_alloc((void **)dst, n * sizeof(T)));
     SG_CUDA(cudaMemcpy(*dst, src, n * sizeof(T), cudaMemcpyHostToDevice));
     return SG_OK;
 }

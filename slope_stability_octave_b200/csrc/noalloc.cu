@@ -22,6 +22,7 @@
 
 #include <cstdint>
 #include <mutex>
+#include <string>
 
 #include "sg_common.cuh"
 
@@ -33,7 +34,9 @@ int launch_constitutive(int dim, bool fused, const double *E, const double *m0, 
 
 namespace {
 
-constexpr int64_t kMaxPoints = 16384;          // SG_NOALLOC_MAX_POINTS in slopegpu.h
+// the capacity is the one the public header states; the array below is sized from it
+constexpr int64_t kMaxPoints = SG_NOALLOC_MAX_POINTS;
+static_assert(kMaxPoints > 0, "SG_NOALLOC_MAX_POINTS must be positive");
 constexpr size_t kAlign = 256;
 // per point: E 6 + c_bar, sin_phi, shear, lame 4 + S 6 + DS 36 doubles + 1 branch byte;
 // each of the 8 carved arrays is rounded up to kAlign
@@ -71,7 +74,8 @@ extern "C" int sg_constitutive3d_noalloc(const double *E, const double *c_bar, c
     (void)bulk;  // unused by the return mapping, as in the reference kernel
     SG_CHECK_ARG(n_int >= 0, "n_int must be >= 0");
     if (n_int > kMaxPoints)
-        return set_error(SG_ERR_ARG, "n_int exceeds the no-allocation scratch (16384 points per call)");
+        return set_error(SG_ERR_ARG, "n_int exceeds the no-allocation scratch (" + std::to_string(kMaxPoints) +
+                                         " points per call)");
     if (n_int == 0) return SG_OK;
     SG_CHECK_ARG(E && c_bar && sin_phi && shear && lame && S, "null input/output pointer");
     unsigned char *base = nullptr;

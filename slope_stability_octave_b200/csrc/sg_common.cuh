@@ -29,6 +29,14 @@ int cuda_error(cudaError_t e, const char *what);
 // grid_for or calls count_launch), read by sg_launch_count for benchmark reporting.
 void count_launch(int n = 1);
 
+// Every device allocation of the library goes through device_alloc (counted, read by
+// sg_device_alloc_count), so a caller can check that a timed region allocated nothing.
+cudaError_t device_alloc_raw(void **p, size_t bytes);
+template <typename T>
+inline cudaError_t device_alloc(T **p, size_t bytes) {
+    return device_alloc_raw(reinterpret_cast<void **>(p), bytes);
+}
+
 // Launch shape: grid sized in multiples of the SM count (148 on B200) for
 // grid-stride kernels, capped by the work.
 int sm_count();

@@ -140,11 +140,13 @@ class AMG:
         return self._clone
 
     def info(self):
-        buf = np.zeros(32, np.int64)
-        _lib.call("sg_amg_info", self.handle, hptr(buf), 32)
+        buf = np.zeros(48, np.int64)
+        _lib.call("sg_amg_info", self.handle, hptr(buf), 48)
         nl = int(buf[0])
-        levels = [dict(block=int(buf[2 + 3 * i]), rows=int(buf[3 + 3 * i]), blocks=int(buf[4 + 3 * i])) for i in range(nl)]
-        return dict(levels=levels, coarse_dense=int(buf[1]))
+        levels = [dict(block=int(buf[2 + 3 * i]), rows=int(buf[3 + 3 * i]), blocks=int(buf[4 + 3 * i]),
+                       p_blocks=int(buf[32 + i])) for i in range(nl)]
+        return dict(levels=levels, coarse_dense=int(buf[1]), mixed=bool(self.mixed),
+                    cheb_degree=int(self._opts[2]))
 
 
 class _Workspace:

@@ -1,7 +1,7 @@
 """Generate ssr_oracle.npz, ssr_direct_oracle.npz and ll_oracle.npz: the oracle's SSR
 (indirect and direct) and limit-load (LL) continuation histories.
 
-    python tests/golden/make_continuation_golden.py [ssr] [ll] [direct]   (default: all three)
+    python tests/golden/make_continuation_golden.py [ssr] [ll] [direct] [full]   (default: all four)
 
 The oracle (oracle/drivers.py, a NumPy restatement of SSR_indirect_continuation.m,
 newton_ind_SSR.m, newton.m and damping_ALG5.m driving the reference's own compiled return
@@ -21,6 +21,10 @@ LL_indirect_continuation.m / newton_ind_LL.m (seven accepted steps from the scri
 elastic start), the same two meshes with the parameters of slope_stability_{2D,3D}_homo_LL.m,
 and (rf3d) the small 3D mesh with lognormal random-field strength
 (problems.slope_3d_random_field, seed 20261203) and the 3D LL parameters.
+``full`` (ssr_full_oracle.npz): the SSR indirect continuation of slope2d (the 2D homogeneous
+slope at h = 0.5, slope_stability_2D_homo_SSR.m's parameters) and of small3d run to the
+reference's own stop tests (SSR_indirect_continuation.m:203-211), so the last lambda is the
+factor of safety.
 """
 from __future__ import annotations
 
@@ -94,7 +98,11 @@ def run_direct_case(make, params, steps=DIRECT_STEPS):
     return SSR_direct_continuation(params, cons.Q, f, cons, DirectSolver(), max_steps_after_init=steps)
 
 
-def main(sections=("ssr", "ll", "direct")):
+def full_cases():
+    return cases()
+
+
+def main(sections=("ssr", "ll", "direct", "full")):
     out = {}
     for name, (make, params) in ({**cases(), **layered_cases()}.items() if "ssr" in sections else ()):
         t0 = time.perf_counter()
@@ -119,7 +127,15 @@ def main(sections=("ssr", "ll", "direct")):
         print("direct", name, f"{time.perf_counter() - t0:.1f}s", "lambda", lh, "omega", oh)
     if out:
         np.savez(os.path.join(HERE, "ssr_direct_oracle.npz"), **out)
+    out = {}
+    for name, (make, params) in (full_cases().items() if "full" in sections else ()):
+        t0 = time.perf_counter()
+        lh, oh, its = run_case(make, params, steps=None)
+        out[f"{name}_lambda"], out[f"{name}_omega"], out[f"{name}_newton"] = lh, oh, its
+        print("full", name, f"{time.perf_counter() - t0:.1f}s", "steps", its.size, "FoS", lh[-1], "newton", its)
+    if out:
+        np.savez(os.path.join(HERE, "ssr_full_oracle.npz"), **out)
 
 
 if __name__ == "__main__":
-    main(tuple(sys.argv[1:]) or ("ssr", "ll", "direct"))
+    main(tuple(sys.argv[1:]) or ("ssr", "ll", "direct", "full"))

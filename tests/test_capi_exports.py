@@ -57,3 +57,34 @@ def test_new_entry_points_reject_bad_arguments_without_device():
     assert rc == -1 and out.value is None
     rc = L.sg_amg_update(None, None, None)
     assert rc == -1
+
+
+def test_noalloc_capacity_matches_header():
+    """The allocation-free entry point's capacity is the header's SG_NOALLOC_MAX_POINTS; its
+    GPU test uses the same figure."""
+    text = open(os.path.join(ROOT, "include", "slopegpu.h")).read()
+    m = re.search(r"#define\s+SG_NOALLOC_MAX_POINTS\s+(\d+)", text)
+    assert m
+    import tests.test_zz_no_alloc as t
+    assert t.MAX_POINTS == int(m.group(1))
+    L = _lib.lib()
+    rc = L.sg_constitutive3d_noalloc(None, None, None, None, None, None, ctypes.c_int64(int(m.group(1)) + 1),
+                                     None, None, None)
+    assert rc == -1 and m.group(1).encode() in L.sg_last_error()
+
+
+def test_ijv_instances_reject_bad_arguments_without_device():
+    """The id-keyed preconditioner entry points check ids and sizes before any device work."""
+    L = _lib.lib()
+    buf = (ctypes.c_int64 * 8)()
+    assert L.sg_amg_ijv_info(b"no_such_id", buf, 8) == -4
+    assert L.sg_amg_update_values(b"no_such_id", None, 0, None) == -4
+    assert L.sg_amg_apply_host(b"no_such_id", buf, buf, 1) == -4
+    rc = L.sg_amg_setup_ijv(b"x", None, None, None, 0, 0, None, 0, None, 3, None, 0, 0, None)
+    assert rc == -1 and b"n must be positive" in L.sg_last_error()
+    rc = L.sg_amg_setup_ijv(b"x", buf, buf, buf, 1, 4, None, 0, None, 1, None, 0, 0, None)
+    assert rc == -1 and b"num_functions" in L.sg_last_error()
+    rc = L.sg_amg_setup_ijv(b"", buf, buf, buf, 1, 4, None, 0, None, 3, None, 0, 0, None)
+    assert rc == -1
+    assert L.sg_amg_clear(b"no_such_id") == 0
+    assert L.sg_amg_ijv_info(None, buf, 8) == 0 and buf[0] == 0

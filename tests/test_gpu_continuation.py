@@ -145,3 +145,51 @@ def test_potential_matches_restatement(cuda_device):
 def test_ssr_direct_2d_reproduces_reference_notebook_run(cuda_device):
     lh, oh = run_direct(problems.slope_2d(0.25), problems.SSR_2D, 1e-1)
     assert abs(lh[-1] - 1.1640625) / 1.1640625 <= 1e-4
+
+
+GOLDEN_FULL = os.path.join(os.path.dirname(__file__), "golden", "ssr_full_oracle.npz")
+
+
+@pytest.mark.parametrize("case", ["slope2d", "small3d"])
+def test_ssr_continuation_to_factor_of_safety(cuda_device, case):
+    """The whole SSR indirect continuation, run to the reference's own stop tests
+    (SSR_indirect_continuation.m:203-211), against the oracle's direct-solver run
+    (tests/golden/ssr_full_oracle.npz): the same number of accepted steps, every lambda and
+    omega within 1e-6 relative, hence the factor of safety (the last lambda) too, and equal
+    Newton iteration counts.  slope2d is the 2D homogeneous slope at h = 0.5 with the
+    parameters of slope_stability_2D_homo_SSR.m (the CPU-runnable configuration); DFGMRES
+    runs at 1e-10 so lambda carries no Krylov error."""
+    g = np.load(GOLDEN_FULL)
+    if f"{case}_lambda" not in g:
+        pytest.skip(f"no full-run fixture for {case}")
+    make, params = CASES[case]
+    lam_ref, om_ref, its_ref = g[f"{case}_lambda"], g[f"{case}_omega"], g[f"{case}_newton"]
+    lh, oh, st = run_gpu(make(), params, 1e-10)
+    assert st["stop_reason"] in ("minimal increase of lambda", "maximal omega", "maximal number of steps")
+    assert lh.shape == lam_ref.shape, (lh.shape, lam_ref.shape, st["stop_reason"])
+    assert abs(lh[-1] - lam_ref[-1]) / lam_ref[-1] <= 1e-6
+    assert np.max(np.abs(lh - lam_ref) / np.abs(lam_ref)) <= 1e-6
+    assert np.max(np.abs(oh - om_ref) / np.abs(om_ref)) <= 1e-6
+    assert list(st["step_newton_iterations"]) == list(its_ref)
+
+
+MIXED_STEPS = 5
+
+
+@pytest.mark.parametrize("case", ["small3d", "layered3d"])
+def test_mixed_form_continuation_matches_plain(cuda_device, case):
+    """The mixed-precision form (FP32 V-cycle and AMG value updates inside the FP64 FGMRES) at
+    the benchmark's solver settings (DFGMRES tolerance 1e-1, Newton 1e-4) against the plain
+    FP64 form: lambda within 1e-4 relative at every accepted step (the bound the mixed form is
+    held to), and, at DFGMRES 1e-10, the oracle's direct-solver lambda within 1e-6."""
+    make, params = CASES[case]
+    lp, op, sp = run_gpu(make(), params, 1e-1, steps=MIXED_STEPS)
+    lm, om, sm = run_gpu(make(), params, 1e-1, steps=MIXED_STEPS, solver_type="DFGMRES_B200_MIXED")
+    assert lp.shape == lm.shape
+    assert np.max(np.abs(lm - lp) / np.abs(lp)) <= 1e-4
+    assert np.max(np.abs(om - op) / np.abs(op)) <= 1e-4
+    g = np.load(GOLDEN)
+    lam_ref, its_ref = g[f"{case}_lambda"], g[f"{case}_newton"]
+    lx, ox, sx = run_gpu(make(), params, 1e-10, steps=len(its_ref), solver_type="DFGMRES_B200_MIXED")
+    assert np.max(np.abs(lx - lam_ref) / np.abs(lam_ref)) <= 1e-6
+    assert list(sx["step_newton_iterations"]) == list(its_ref)

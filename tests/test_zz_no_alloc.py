@@ -16,7 +16,7 @@ from slope_stability_octave_b200 import _lib, workloads
 
 pytestmark = pytest.mark.gpu
 
-MAX_POINTS = 16384  # SG_NOALLOC_MAX_POINTS
+MAX_POINTS = 16384  # SG_NOALLOC_MAX_POINTS in include/slopegpu.h
 RTOL = 1e-12
 
 
@@ -24,10 +24,10 @@ def ptr(a):
     return None if a is None else a.ctypes.data_as(C.c_void_p)
 
 
-def run(name, d, n):
+def run(name, d, n, want_ds=True, want_branch=True):
     S = np.zeros((n, 6))
-    DS = np.zeros((n, 36))
-    br = np.zeros(n, np.uint8)
+    DS = np.zeros((n, 36)) if want_ds else None
+    br = np.zeros(n, np.uint8) if want_branch else None
     args = [ptr(np.ascontiguousarray(d[k][:n])) for k in ("E", "c_bar", "sin_phi", "shear", "bulk", "lame")]
     rc = getattr(_lib.lib(), name)(*args, n, ptr(S), ptr(DS), ptr(br))
     return rc, S, DS, br
@@ -48,6 +48,24 @@ def test_noalloc_matches_allocating_entry_point(cuda_device):
             assert rc == 0, _lib.lib().sg_last_error()
             assert np.array_equal(b, b0)
             assert close(S, S0) and close(DS, DS0)
+
+
+@pytest.mark.parametrize("want_ds,want_branch", [(False, False), (True, False), (False, True)])
+def test_noalloc_optional_outputs(cuda_device, want_ds, want_branch):
+    """Stress only and/or no branch ids: the scratch is carved without the DS and branch
+    regions, so S (and whichever optional output is asked for) sits at other offsets."""
+    d = workloads.constitutive_points(MAX_POINTS, seed=20261204)
+    n = MAX_POINTS
+    rc, S0, DS0, b0 = run("sg_constitutive3d", d, n)
+    assert rc == 0
+    for _ in range(2):
+        rc, S, DS, b = run("sg_constitutive3d_noalloc", d, n, want_ds, want_branch)
+        assert rc == 0, _lib.lib().sg_last_error()
+        assert close(S, S0)
+        if want_ds:
+            assert close(DS, DS0)
+        if want_branch:
+            assert np.array_equal(b, b0)
 
 
 def test_noalloc_rejects_oversize(cuda_device):
