@@ -6,6 +6,9 @@ slope_3d                3D homogeneous slope, P2 tets: the 2D profile extruded 4
 slope_3d_layered        3D slope with horizontal material layers (heterogeneous), see
                         ``layered_material_ids``
 slope_3d_random_field   3D slope with lognormal random-field strength (limit-load workload)``
+slope_3d_from_mesh      a P2 tetrahedral mesh given as arrays (e.g. one of the reference's HDF5
+                        meshes read by h5mesh.load_mesh_P2), homogeneous or with per-element
+                        material ids (slope_stability_3D_{homo,hetero}_SSR.m)
 
 Material rows are (c0 [kPa], phi [deg], psi [deg], E [kPa], nu, gamma_sat, gamma_unsat).
 """
@@ -24,6 +27,13 @@ from .linear_solvers import set_linear_solver
 HOMO = [6.0, 45.0, 0.0, 40000.0, 0.3, 20.0, 20.0]
 
 # continuation parameters of the reference drivers
+# the stored runs of slope_stability_3D_hetero_SSR.m (mesh SSR_hetero_ada_L1.h5): material
+# rows by the mesh's material id 0..3 (cover layer, general foundation, relatively weak
+# foundation, general slope mass) and the script's continuation parameters
+HETERO_SSR_MATERIALS = [[15.0, 30.0, 0.0, 10000.0, 0.33, 19.0, 19.0],
+                        [15.0, 38.0, 0.0, 50000.0, 0.30, 22.0, 22.0],
+                        [10.0, 35.0, 0.0, 50000.0, 0.30, 21.0, 21.0],
+                        [18.0, 32.0, 0.0, 20000.0, 0.33, 20.0, 20.0]]
 SSR_3D = dict(lambda_init=0.9, d_lambda_init=0.1, d_lambda_min=1e-3, d_lambda_diff_scaled_min=1e-3,
               step_max=100, omega_max_stop=3000.0, it_newt_max=100, it_damp_max=10, tol=1e-4, r_min=1e-4)
 SSR_2D = dict(lambda_init=0.9, d_lambda_init=0.05, d_lambda_min=1e-5, d_lambda_diff_scaled_min=1e-3,
@@ -32,6 +42,7 @@ SSR_2D = dict(lambda_init=0.9, d_lambda_init=0.05, d_lambda_min=1e-5, d_lambda_d
 # reference 3D driver's omega_max_stop = 3000 (chosen for its own smaller mesh) would stop at
 # once, so the bound is lifted to the 2D script's 7e7 and the lambda-increment test stops.
 SSR_3D_EXTRUDED = dict(SSR_3D, omega_max_stop=7e7)
+SSR_3D_HETERO = dict(SSR_3D, lambda_init=1.0, omega_max_stop=1.2e7, it_newt_max=200)
 # limit-load continuation parameters of slope_stability_3D_homo_LL.m:82-96 and
 # slope_stability_2D_homo_LL.m:154-163
 LL_3D = dict(d_t_min=1e-3, step_max=100, omega_max=5100.0, it_newt_max=200, it_damp_max=10, tol=1e-4, r_min=1e-4)
@@ -100,6 +111,15 @@ def slope_2d(h=0.5, mat=HOMO):
 def slope_3d(N_h=1, dims=(15, 10, 15, 10, 10, 40), mat=HOMO):
     mesh = fem.mesh_p2_3d(N_h, *dims)
     return _assemble_problem(mesh, np.zeros(mesh.n_e, int), mat)
+
+
+def slope_3d_from_mesh(coord, elem, Q, material=None, table=HOMO):
+    """Problem on a given P2 tetrahedral mesh: coord (3, n_n), elem (10, n_e) 0-based, Q (3, n_n)
+    free-DOF mask; ``material`` = per-element row index into ``table`` (None: all row 0)."""
+    mesh = fem.Mesh(np.ascontiguousarray(coord, np.float64), np.ascontiguousarray(elem, np.int64),
+                    np.ascontiguousarray(Q, bool))
+    ids = np.zeros(mesh.n_e, int) if material is None else np.asarray(material, int)
+    return _assemble_problem(mesh, ids, table)
 
 
 # four horizontal layers, thicknesses 5/5/10/20 m measured from the crest (y = 20 m)
