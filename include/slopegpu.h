@@ -163,6 +163,13 @@ int sg_elastic_ds_dev(const sg_mesh *mesh, const double *shear, const double *bu
 int sg_symmetrize_bsr_dev(const sg_mesh *mesh, const double *K, double *Ks, void *stream);
 /* (b4) K_r = sym(r K_el + (1-r) K_t) with Dirichlet identity (CONSTITUTIVE.m:515-532) */
 int sg_kr_blend_dev(const sg_mesh *mesh, double r, const double *K_el, const double *K_t, double *K_r, void *stream);
+/* (b3 + b4) K_r = r K_el + (1 - r) K_t with K_t assembled from DS in the same call (the
+ * sequence build_K_tangent_QQ_vals + build_K_r_QQ_vals, CONSTITUTIVE.m:515-532 and
+ * assemble_K_tangent_vals.c:77-171).  On P2 tetrahedra the assembly is deterministic (fixed
+ * summation order, bitwise reproducible) and exactly symmetric, and K_t itself is not stored
+ * (K_t_scratch may be NULL); other elements assemble into K_t_scratch, then blend. */
+int sg_assemble_kr_dev(sg_mesh *mesh, const double *DS, double r, const double *K_el, double *K_t_scratch,
+                       double *K_r, void *stream);
 /* block-pattern values -> V in the reference's find() order (nnz of K(Q,Q)) */
 int sg_bsr_to_ref_dev(sg_mesh *mesh, const double *K, double *V_ref, void *stream);
 

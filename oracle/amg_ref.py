@@ -233,6 +233,32 @@ class Hierarchy:
             B = Bc
             active = ~dead.reshape(na, nns).all(axis=1)
 
+    def update(self, A, power_its=10, omega_scale=4.0 / 3.0):
+        """Numeric set-up for new values of the level-0 matrix on the kept aggregates and
+        tentative prolongators (what the device's sg_amg_update redoes per value update):
+        block inverses, lambda_max, P = T - omega D^-1 A T, A_c = P' A P with identity on dead
+        coarse DOFs, the coarsest inverse."""
+        A = sp.csr_matrix(A)
+        for l, lev in enumerate(self.levels):
+            lev["A"] = A
+            lev["Dinv"] = _block_dinv(A, lev["b"])
+            if "T" not in lev:
+                lev["Ainv"] = np.linalg.inv(A.toarray())
+                break
+            v = _init_vec(A.shape[0])
+            lmax = 1.0
+            for _ in range(power_its):
+                w = self.dinv(lev, A @ v)
+                lmax = np.linalg.norm(w) or 1.0
+                v = w / lmax
+            lev["lmax"] = lmax
+            P = (lev["T"] - (omega_scale / lmax) * self._dinv_mat(lev, A @ lev["T"])).tocsr()
+            lev["P"] = P
+            dead = lev["dead_next"]
+            keep = sp.diags((~dead).astype(float))
+            A = (keep @ (P.T @ A @ P) @ keep + sp.diags(dead.astype(float))).tocsr()
+        return self
+
     @classmethod
     def from_levels(cls, mats, prolongators, blocks, cheb_degree=3, cheb_ratio=10.0, power_its=10):
         """V-cycle on a given hierarchy: mats[l] (level matrices), prolongators[l] (l < L-1);

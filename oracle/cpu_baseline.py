@@ -3,9 +3,12 @@
 Used only by bench.py (the ``cpu_baseline`` leg and ``--impl reference``).  A full SSR
 continuation step of the benchmark workload takes the CPU path minutes to hours, so the
 baseline is a bounded sample: every operation of a Newton iteration of
-+NEWTON/newton_ind_SSR.m:68-175 is timed once on the full-size workload, and the step time is
-the sum of those unit costs weighted by the operation counts of one continuation step of the
-same workload.
++NEWTON/newton_ind_SSR.m:68-175 is timed once on a slice of the workload's mesh (a few cells
+deep, the same spacing and materials), the unit costs are scaled to the full size, and the
+step time is their sum weighted by the operation counts of the GPU's timed continuation steps
+(``step_seconds``).  The model is calibrated against a measurement: ``measured_steps`` runs
+genuine continuation steps of the CPU path (the oracle's drivers with ``HostAMGDFGMRES``) on a
+one-cell slice, and bench.py scales the model by the measured / modelled time of that step.
 
   reference's own compiled C (oracle/_ref, OpenMP on all host threads):
       return mapping S+DS and S        constitutive_problem_3D_{SDS,S}_mex.c
@@ -183,3 +186,84 @@ def step_seconds(c, counts):
     amg_setup = c.get("amg_setup", 0.0)
     return nn * (stress_tangent + linearise + stress_only + a_orth + amg_setup) + n_damp * stress_only \
         + lin * per_krylov
+
+
+class HostAMGDFGMRES:
+    """The reference's linear solver on the host cores, for timing genuine CPU continuation
+    steps: DFGMRES (dfgmres_solver.m restated as oracle.drivers.dfgmres, MGS Arnoldi) with
+    deflation by the A-orthogonalised basis of earlier solutions (DFGMRES.m, A_orthogonalize.m)
+    and one V-cycle of the oracle's AMG restatement as preconditioner, set up on the first
+    matrix and numerically updated for every later one (the reference re-runs BoomerAMG's set-up
+    per value update).  Matrices are K(Q,Q) (SciPy); the AMG works on its embedding into all
+    DOFs with identity rows on the Dirichlet DOFs.  ``copy()`` shares the AMG and keeps its own
+    basis, like the reference's copies."""
+
+    def __init__(self, q, n_full, Z_full, dim, tol=1e-1, maxit=100, defl_tol=1e-3, shared=None):
+        self.q, self.n_full, self.dim = q, n_full, dim
+        self.tol, self.maxit, self.defl_tol = tol, maxit, defl_tol
+        self.shared = shared if shared is not None else dict(Z=Z_full)
+        self.W = np.zeros((q.size, 0))
+        self.Wa = self.W
+        nQ = q.size
+        self.E = sp.csr_matrix((np.ones(nQ), (q, np.arange(nQ))), shape=(n_full, nQ))
+        fixed = np.ones(n_full, bool)
+        fixed[q] = False
+        self.fixed = fixed
+
+    def setup_preconditioner(self, K):
+        A = (self.E @ K @ self.E.T + sp.diags(self.fixed.astype(float))).tocsr()
+        H = self.shared.get("H")
+        if H is None:
+            self.shared["H"] = Hierarchy(A, self.shared["Z"], self.dim, fixed=self.fixed, theta=0.02)
+        else:
+            H.update(A)
+
+    setup_preconditioner_ijv = setup_preconditioner
+    update_preconditioner_values = setup_preconditioner
+
+    def A_orthogonalize(self, K):
+        from .drivers import a_orthogonalize
+        self.Wa = a_orthogonalize(self.W, K, self.defl_tol)[0] if self.W.shape[1] else self.W
+
+    def _M(self, r):
+        x = np.zeros(self.n_full)
+        x[self.q] = r
+        return self.shared["H"].vcycle(x)[self.q]
+
+    def solve(self, K, b):
+        from .drivers import dfgmres
+        x, it, _ = dfgmres(K, b, self._M, self.Wa, self.maxit, self.tol)
+        return x, it
+
+    def expand_deflation_basis(self, v):
+        self.W = np.column_stack([self.W, v])
+
+    def copy(self):
+        new = HostAMGDFGMRES(self.q, self.n_full, None, self.dim, self.tol, self.maxit, self.defl_tol, self.shared)
+        new.W = self.W.copy()
+        new.Wa = self.Wa
+        return new
+
+
+def measured_steps(S, params, n_steps=1, log=print):
+    """Wall time of genuine SSR continuation steps of the CPU path on the problem ``S``: the
+    oracle's drivers (newton_ind_SSR.m, SSR_indirect_continuation.m) on the reference's
+    return mapping restated in C (liboracle, OpenMP) and HostAMGDFGMRES, ``n_steps`` accepted
+    steps after the init phase (the init phase is not timed).  Returns dict(step_wall_time,
+    step_newton_iterations, step_linear_iterations, deflation)."""
+    from slope_stability_octave_b200.linear_solvers import near_null_space_elasticity
+
+    from .drivers import OracleConstitutive, SSR_indirect_continuation
+    mesh = S.mesh
+    cons = OracleConstitutive(mesh, S.dphi, S.weight, S.n_q, S.mat)
+    f = np.ascontiguousarray(S.f.T).ravel()
+    q = np.nonzero(cons.Q)[0]
+    Z = near_null_space_elasticity(mesh.coord, mesh.Q)
+    solver = HostAMGDFGMRES(q, f.size, Z, mesh.dim)
+    stats = {}
+    t0 = time.perf_counter()
+    SSR_indirect_continuation(params, cons.Q, f, cons, solver, max_steps_after_init=n_steps, stats=stats)
+    log(f"cpu continuation: init + {n_steps} steps in {time.perf_counter() - t0:.1f}s, "
+        f"steps {stats['step_wall_time']}")
+    stats["deflation"] = solver.W.shape[1]
+    return stats

@@ -334,8 +334,14 @@ def newton_ind_SSR(U_ini, omega, lambda_ini, it_newt_max, it_damp_max, tol, r_mi
     return U, lam, flag, it, hist
 
 
-def SSR_indirect_continuation(p, Q, f, cons, solver, max_steps_after_init=None):
-    """p: dict of the continuation parameters (SSR_indirect_continuation.m arguments)."""
+def SSR_indirect_continuation(p, Q, f, cons, solver, max_steps_after_init=None, stats=None):
+    """p: dict of the continuation parameters (SSR_indirect_continuation.m arguments).
+    ``stats`` (optional dict) receives per accepted step its wall time (the sum of its
+    attempts, SSR_indirect_continuation.m:186), Newton iterations and linear iterations."""
+    import time
+    if stats is not None:
+        stats.update(step_wall_time=[], step_newton_iterations=[], step_linear_iterations=[])
+    wall_acc = lin_acc = it_acc = 0
     fQ = f[Q]
     cons.reduction(p["lambda_init"])
     U1, flag, _ = newton(np.zeros_like(f), p["tol"], p["it_newt_max"], p["it_damp_max"], p["r_min"], Q, f, cons,
@@ -344,6 +350,7 @@ def SSR_indirect_continuation(p, Q, f, cons, solver, max_steps_after_init=None):
         raise RuntimeError("Initial choice of lambda seems to be too large.")
     omega1 = fQ @ U1[Q]
     d_lambda, lambda1 = p["d_lambda_init"], p["lambda_init"]
+    solver.expand_deflation_basis(U1[Q])        # init_phase_SSR_indirect_continuation.m:97
     while True:
         lam_it = lambda1 + d_lambda
         cons.reduction(lam_it)
@@ -362,6 +369,7 @@ def SSR_indirect_continuation(p, Q, f, cons, solver, max_steps_after_init=None):
         if lambda1 > 10:
             raise RuntimeError("It seems that the FoS is greater than 10.")
     U_old, U, omega_old, omega, lam = U1, U2, omega1, omega2, lambda2
+    solver.expand_deflation_basis(U_old[Q])     # SSR_indirect_continuation.m:85
     lambda_hist, omega_hist = [lambda1, lambda2], [omega1, omega2]
     newton_its = []
     d_omega = omega - omega_old
@@ -370,14 +378,19 @@ def SSR_indirect_continuation(p, Q, f, cons, solver, max_steps_after_init=None):
         omega_it = min(omega + d_omega, p["omega_max_stop"])
         d_omega = omega_it - omega
         U_ini = d_omega * (U - U_old) / (omega - omega_old) + U
-        U_it, lam_it, flag, it, _ = newton_ind_SSR(U_ini, omega_it, lam, p["it_newt_max"], p["it_damp_max"], p["tol"],
-                                                   p["r_min"], Q, f, cons, solver.copy())
+        t0 = time.perf_counter()
+        U_it, lam_it, flag, it, hist = newton_ind_SSR(U_ini, omega_it, lam, p["it_newt_max"], p["it_damp_max"],
+                                                      p["tol"], p["r_min"], Q, f, cons, solver.copy())
+        wall_acc += time.perf_counter() - t0
+        it_acc += it
+        lin_acc += sum(hist["lin_W"]) + sum(hist["lin_V"])
         if flag:
             d_omega /= 2
             n_omega += 1
         else:
             step += 1
             U_old, U = U, U_it
+            solver.expand_deflation_basis(U[Q])     # SSR_indirect_continuation.m:173
             omega_old, omega = omega, omega_it
             d_lambda = lam_it - lam
             lam = lam_it
@@ -386,6 +399,11 @@ def SSR_indirect_continuation(p, Q, f, cons, solver, max_steps_after_init=None):
             lambda_hist.append(lam)
             newton_its.append(it)
             accepted += 1
+            if stats is not None:
+                stats["step_wall_time"].append(wall_acc)
+                stats["step_newton_iterations"].append(it_acc)
+                stats["step_linear_iterations"].append(lin_acc)
+            wall_acc = lin_acc = it_acc = 0
             if (d_lambda / d_omega) * (omega_hist[step - 1] - omega_hist[0]) < p["d_lambda_diff_scaled_min"]:
                 break
             if omega >= p["omega_max_stop"]:

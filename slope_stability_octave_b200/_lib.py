@@ -46,6 +46,7 @@ SIGNATURES = {
     "sg_elastic_ds_dev": [vp, vp, vp, vp, vp],
     "sg_symmetrize_bsr_dev": [vp, vp, vp, vp],
     "sg_kr_blend_dev": [vp, f64, vp, vp, vp, vp],
+    "sg_assemble_kr_dev": [vp, vp, f64, vp, vp, vp, vp],
     "sg_bsr_to_ref_dev": [vp, vp, vp, vp],
     # sparse and vector operations
     "sg_bsr_info": [vp, vp],

@@ -195,11 +195,13 @@ class CONSTITUTIVE:
         return self.K_t
 
     def build_K_r_QQ_vals(self, r):
-        """K_r = sym(r K_el + (1-r) K_t) on the device pattern (Dirichlet rows identity)."""
+        """K_r = sym(r K_el + (1-r) K_t) on the device pattern (Dirichlet rows identity): the
+        tangent assembly and the blend in one call (``sg_assemble_kr_dev``); on P2 tetrahedra
+        K_t is not stored on the way (``build_K_tangent_QQ_vals`` assembles it on request)."""
         if not self.pattern_initialized:
             raise _lib.SlopeGPUError("init_K_r_pattern must be called first")
-        self.build_K_tangent_QQ_vals()
-        self.m.kr_blend(r, self.K_el, self.K_t, self.K_r)
+        with _Timer(self.profiler, "CONSTITUTIVE.build_K_tangent_QQ_vals"):
+            self.m.assemble_kr(self.DS, r, self.K_el, self.K_t, self.K_r)
         return self.K_r
 
     def build_K_r_QQ_vals_ref(self, r):

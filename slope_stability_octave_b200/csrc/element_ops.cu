@@ -242,6 +242,170 @@ __global__ void __launch_bounds__(128) k_assemble_bsr(const int32_t *__restrict_
     }
 }
 
+// ------------------------------------------------------------------ deterministic P2-tet assembly
+//
+// Two passes instead of one pass of atomics (same arithmetic as k_assemble_bsr up to rounding,
+// but every block sums its terms in a fixed order, so K is bitwise reproducible; and exactly
+// symmetric):
+//   k_element_blocks_p2tet  per element, its 55 upper node blocks (i <= j) of
+//       sum_q w_q B_q' sym(D_q) B_q, with the element's D, gradients and weights staged in
+//       shared memory once; D B is formed once per (point, column) and shared by the blocks;
+//       diagonal blocks are computed on and above their diagonal and mirrored;
+//   k_gather_blocks3        per BSR block, the sum of its element contributions in element
+//       order (the transpose of an upper block for the lower ones), written as K_t, or
+//       blended into K_r = r K_el + (1 - r) K_t with identity on Dirichlet rows/columns
+//       (the k_kr_blend epilogue; K_el and K_t being exactly symmetric, its averaging with the
+//       transposed block is the identity).
+// sym(D) = (D + D')/2 is what the reference's symmetrisation of K_r applies to its unsymmetric
+// sums (CONSTITUTIVE.m:515-532): B' sym(D) B = sym(B' D B).
+constexpr int KE_EPB = 2, KE_TPE = 64;   // elements per CTA, threads per element
+
+__device__ __forceinline__ void ke_slot_ij(int s, int &i, int &j) {
+    int lo = 0, start = 0;
+    while (s >= start + (10 - lo)) { start += 10 - lo; ++lo; }
+    i = lo;
+    j = lo + (s - start);
+}
+
+__global__ void __launch_bounds__(KE_EPB * KE_TPE) k_element_blocks_p2tet(int64_t n_e, int nq,
+                                                                          const double *__restrict__ dphi,
+                                                                          const double *__restrict__ w,
+                                                                          const double *__restrict__ DS,
+                                                                          double *__restrict__ Ke) {
+    extern __shared__ double ke_smem[];
+    const int le = threadIdx.x / KE_TPE, lt = threadIdx.x - le * KE_TPE;
+    const int per = nq * (36 + 30 + 1 + 180);
+    double *sD = ke_smem + le * per;     // [q][36] column-major 6x6
+    double *sPhi = sD + nq * 36;         // [q][d][i]
+    double *sW = sPhi + nq * 30;         // [q]
+    double *sDB = sW + nq;               // [q][col = 3 j + c][a]: w_q sym(D_q) B_q(:, col)
+    for (int64_t e0 = (int64_t)blockIdx.x * KE_EPB; e0 < n_e; e0 += (int64_t)gridDim.x * KE_EPB) {
+        const int64_t e = e0 + le;
+        const bool live = e < n_e;
+        if (live) {
+            const int64_t g0 = e * nq;
+            for (int t = lt; t < nq * 36; t += KE_TPE) sD[t] = DS[g0 * 36 + t];
+            for (int t = lt; t < nq * 30; t += KE_TPE) sPhi[t] = dphi[g0 * 30 + t];
+            for (int t = lt; t < nq; t += KE_TPE) sW[t] = w[g0 + t];
+        }
+        __syncthreads();
+        if (live) {
+            for (int t = lt; t < nq * 30; t += KE_TPE) {
+                const int q = t / 30, col = t - q * 30, j = col / 3, c = col - j * 3;
+                const double *D = sD + q * 36;
+                int r[3];
+                double v[3];
+                bcol<3>(sPhi + q * 30, 10, j, c, r, v);
+                const double wq = sW[q];
+#pragma unroll
+                for (int a = 0; a < 6; ++a) {
+                    double x = 0.0;
+#pragma unroll
+                    for (int u = 0; u < 3; ++u) x += 0.5 * (D[a + 6 * r[u]] + D[r[u] + 6 * a]) * v[u];
+                    sDB[t * 6 + a] = wq * x;
+                }
+            }
+        }
+        __syncthreads();
+        if (live && lt < 55) {
+            int i, j;
+            ke_slot_ij(lt, i, j);
+            double acc[9];
+#pragma unroll
+            for (int k = 0; k < 9; ++k) acc[k] = 0.0;
+            for (int q = 0; q < nq; ++q) {
+                const double *d = sPhi + q * 30;
+                const double *db = sDB + (q * 30 + 3 * j) * 6;
+#pragma unroll
+                for (int ci = 0; ci < 3; ++ci) {
+                    int r[3];
+                    double v[3];
+                    bcol<3>(d, 10, i, ci, r, v);
+#pragma unroll
+                    for (int cj = 0; cj < 3; ++cj) {
+                        if (i == j && cj < ci) continue;
+                        const double *x = db + cj * 6;
+                        acc[ci * 3 + cj] += v[0] * x[r[0]] + v[1] * x[r[1]] + v[2] * x[r[2]];
+                    }
+                }
+            }
+            if (i == j) {
+                acc[3] = acc[1];
+                acc[6] = acc[2];
+                acc[7] = acc[5];
+            }
+            double *out = Ke + (e * 55 + lt) * 9;
+#pragma unroll
+            for (int k = 0; k < 9; ++k) out[k] = acc[k];
+        }
+        __syncthreads();
+    }
+}
+
+template <bool BLEND>
+__global__ void k_gather_blocks3(int64_t n_blocks, const int32_t *__restrict__ cptr,
+                                 const uint32_t *__restrict__ contrib, const double *__restrict__ Ke,
+                                 const int32_t *__restrict__ row_of, const int32_t *__restrict__ col,
+                                 const double *__restrict__ mask, double r, const double *__restrict__ Kel,
+                                 double *__restrict__ Kout) {
+    for (int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; p < n_blocks;
+         p += (int64_t)gridDim.x * blockDim.x) {
+        double acc[9];
+#pragma unroll
+        for (int k = 0; k < 9; ++k) acc[k] = 0.0;
+        for (int32_t l = cptr[p]; l < cptr[p + 1]; ++l) {
+            const uint32_t src = contrib[l];
+            const double *v = Ke + (int64_t)(src & 0x7fffffffu) * 9;
+            double x[9];
+#pragma unroll
+            for (int k = 0; k < 9; ++k) x[k] = __ldg(v + k);
+            if (src >> 31) {
+#pragma unroll
+                for (int a = 0; a < 3; ++a)
+#pragma unroll
+                    for (int b = 0; b < 3; ++b) acc[a * 3 + b] += x[b * 3 + a];
+            } else {
+#pragma unroll
+                for (int k = 0; k < 9; ++k) acc[k] += x[k];
+            }
+        }
+        if (BLEND) {
+            const int64_t I = row_of[p], J = col[p];
+#pragma unroll
+            for (int a = 0; a < 3; ++a)
+#pragma unroll
+                for (int b = 0; b < 3; ++b) {
+                    const bool free = mask[I * 3 + a] != 0.0 && mask[J * 3 + b] != 0.0;
+                    const double el = Kel ? Kel[p * 9 + a * 3 + b] : 0.0;
+                    Kout[p * 9 + a * 3 + b] = free ? r * el + (1.0 - r) * acc[a * 3 + b]
+                                                   : ((I == J && a == b) ? 1.0 : 0.0);
+                }
+        } else {
+#pragma unroll
+            for (int k = 0; k < 9; ++k) Kout[p * 9 + k] = acc[k];
+        }
+    }
+}
+
+// Element blocks of the deterministic path into m->d_ke (allocated on first use).
+static int element_blocks(sg_mesh *m, const double *DS, cudaStream_t st) {
+    if (!m->d_ke) SG_CUDA(device_alloc(&m->d_ke, sizeof(double) * (size_t)m->n_e * 55 * 9));
+    const size_t smem = sizeof(double) * (size_t)KE_EPB * m->nq * (36 + 30 + 1 + 180);
+    static thread_local size_t configured = 0;
+    if (smem > configured) {
+        SG_CUDA(cudaFuncSetAttribute(k_element_blocks_p2tet, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        configured = smem;
+    }
+    count_launch();
+    const int64_t ctas = (m->n_e + KE_EPB - 1) / KE_EPB;
+    const unsigned grid = (unsigned)std::max<int64_t>(1, std::min<int64_t>(ctas, (int64_t)sm_count() * 16));
+    k_element_blocks_p2tet<<<grid, KE_EPB * KE_TPE, smem, st>>>(m->n_e, m->nq, m->d_dphi, m->d_w, DS, m->d_ke);
+    SG_CUDA(cudaGetLastError());
+    return SG_OK;
+}
+
+static bool deterministic_path(const sg_mesh *m) { return m->d_contrib && m->dim == 3 && m->np == 10; }
+
 // DS_elast = 2 * shear * DEV + bulk * VOL with IOTA = [1;1;1; zeros(ns-3,1)] (CONSTITUTIVE.m:413-422).
 // For ns == 3 (2D) the reference's IOTA has three ones, so VOL is the all-ones 3x3 matrix;
 // that arithmetic is reproduced as is.
@@ -352,9 +516,21 @@ extern "C" int sg_residual_dev(const sg_mesh *m, const double *U, const double *
     return SG_OK;
 }
 
-extern "C" int sg_assemble_bsr_dev(const sg_mesh *m, const double *DS, double *K, void *stream) {
-    SG_CHECK_ARG(m && DS && K, "null argument");
+extern "C" int sg_assemble_bsr_dev(const sg_mesh *m_, const double *DS, double *K, void *stream) {
+    SG_CHECK_ARG(m_ && DS && K, "null argument");
+    sg_mesh *m = const_cast<sg_mesh *>(m_);   // the element-block scratch is the mesh's own
     const cudaStream_t st = as_stream(stream);
+    if (deterministic_path(m)) {
+        const InstrToken tk = instr_begin(IK_ASSEMBLY, st);
+        int rc = element_blocks(m, DS, st);
+        if (!rc) {
+            k_gather_blocks3<false><<<grid_for(m->bsr.n_blocks, 256), 256, 0, st>>>(
+                m->bsr.n_blocks, m->d_contrib_ptr, m->d_contrib, m->d_ke, nullptr, nullptr, nullptr, 0.0, nullptr, K);
+            if (cudaGetLastError() != cudaSuccess) rc = set_error(SG_ERR_CUDA, "k_gather_blocks3 launch");
+        }
+        instr_end(tk, st);
+        return rc;
+    }
     SG_CUDA(cudaMemsetAsync(K, 0, sizeof(double) * m->bsr.n_blocks * m->dim * m->dim, st));
     const int64_t work = m->n_e * m->dim * m->np;
     const InstrToken tk = instr_begin(IK_ASSEMBLY, st);
@@ -409,6 +585,31 @@ extern "C" int sg_kr_blend_dev(const sg_mesh *m, double r, const double *Kel, co
         k_kr_blend<2><<<grid_for(work, 256), 256, 0, st>>>(m->bsr.n_blocks, row_of, m->bsr.d_col, m->bsr.d_transpose, m->d_mask, r, Kel, Kt, Kr);
     SG_CUDA(cudaGetLastError());
     return SG_OK;
+}
+
+// K_r = r K_el + (1 - r) K_t from the tangent DS in one assembly (P2 tetrahedra: the
+// deterministic two-pass assembly with the blend as its epilogue; other elements: assembly into
+// Kt_scratch, then k_kr_blend).  Kt_scratch may be null on the P2-tetrahedron path.
+extern "C" int sg_assemble_kr_dev(sg_mesh *m, const double *DS, double r, const double *Kel, double *Kt_scratch,
+                                  double *Kr, void *stream) {
+    SG_CHECK_ARG(m && DS && Kr && Kr != Kel, "null or aliased argument");
+    const cudaStream_t st = as_stream(stream);
+    if (deterministic_path(m)) {
+        const InstrToken tk = instr_begin(IK_ASSEMBLY, st);
+        int rc = element_blocks(m, DS, st);
+        if (!rc) {
+            k_gather_blocks3<true><<<grid_for(m->bsr.n_blocks, 256), 256, 0, st>>>(
+                m->bsr.n_blocks, m->d_contrib_ptr, m->d_contrib, m->d_ke, m->bsr.d_row_of, m->bsr.d_col, m->d_mask, r,
+                Kel, Kr);
+            if (cudaGetLastError() != cudaSuccess) rc = set_error(SG_ERR_CUDA, "k_gather_blocks3 launch");
+        }
+        instr_end(tk, st);
+        return rc;
+    }
+    SG_CHECK_ARG(Kt_scratch && Kt_scratch != Kr, "this element type needs a separate K_t buffer");
+    int rc = sg_assemble_bsr_dev(m, DS, Kt_scratch, stream);
+    if (!rc) rc = sg_kr_blend_dev(m, r, Kel, Kt_scratch, Kr, stream);
+    return rc;
 }
 
 extern "C" int sg_bsr_to_ref_dev(sg_mesh *m, const double *K, double *V_ref, void *stream) {

@@ -163,7 +163,30 @@ static int mesh_build(sg_mesh *m, const int32_t *elem, const double *D1, const d
     std::vector<double> mask(n_n * dim);
     for (int64_t d = 0; d < n_n * dim; ++d) mask[d] = m->Q[d] ? 1.0 : 0.0;
 
+    // contribution lists of the deterministic P2-tetrahedron assembly: block (node_i, node_j)
+    // of element e takes its upper slot s(min(i,j), max(i,j)), transposed when i > j; the lists
+    // are filled in element order, so every block sums its contributions in a fixed order
+    std::vector<int32_t> cptr;
+    std::vector<uint32_t> contrib;
+    if (dim == 3 && np == 10 && n_e * 55 < ((int64_t)1 << 31)) {
+        cptr.assign(B.n_blocks + 1, 0);
+        for (size_t t = 0; t < pair.size(); ++t) cptr[pair[t] + 1]++;
+        for (int64_t p = 0; p < B.n_blocks; ++p) cptr[p + 1] += cptr[p];
+        std::vector<int32_t> fill(cptr.begin(), cptr.end() - 1);
+        contrib.resize(pair.size());
+        for (int64_t e = 0; e < n_e; ++e)
+            for (int i = 0; i < np; ++i)
+                for (int j = 0; j < np; ++j) {
+                    const int lo = std::min(i, j), hi = std::max(i, j);
+                    const uint32_t slot = (uint32_t)(lo * np - lo * (lo - 1) / 2 + (hi - lo));
+                    contrib[fill[pair[(e * np + i) * np + j]]++] =
+                        (uint32_t)(e * 55 + slot) | (i > j ? 0x80000000u : 0u);
+                }
+    }
+
     int rc = bsr_upload(B);
+    if (!rc && !contrib.empty()) rc = upload(&m->d_contrib_ptr, cptr.data(), cptr.size());
+    if (!rc && !contrib.empty()) rc = upload(&m->d_contrib, contrib.data(), contrib.size());
     if (!rc) rc = upload(&m->d_elem, m->elem.data(), (size_t)n_e * np);
     if (!rc) rc = upload(&m->d_dphi, dphi.data(), dphi.size());
     if (!rc) rc = upload(&m->d_w, W, (size_t)n_int);
@@ -243,6 +266,9 @@ extern "C" int sg_mesh_destroy(sg_mesh *m) {
     cudaFree(m->d_w);
     cudaFree(m->d_mask);
     cudaFree(m->d_pair_blk);
+    cudaFree(m->d_contrib_ptr);
+    cudaFree(m->d_contrib);
+    cudaFree(m->d_ke);
     cudaFree(m->d_ref2bsr);
     cudaSetDevice(cur);
     delete m;

@@ -35,6 +35,11 @@ struct sg_mesh {
     double *d_mask = nullptr;         // dim * n_n, 1 free / 0 Dirichlet
     int32_t *d_pair_blk = nullptr;    // n_e * np * np: block index of (node_i, node_j)
     int64_t *d_ref2bsr = nullptr;     // nnz_ref: value index of K(ref_I, ref_J) inside BSR values
+    // deterministic assembly of P2 tetrahedra: every BSR block's contributions (element e,
+    // upper node-block slot s of that element, transposed flag in bit 31) in element order
+    int32_t *d_contrib_ptr = nullptr; // n_blocks + 1
+    uint32_t *d_contrib = nullptr;    // n_e * np * np entries: e * 55 + s | transposed << 31
+    double *d_ke = nullptr;           // n_e * 55 * 9: element upper node blocks (allocated on first use)
     int device = 0;
 };
 

@@ -154,6 +154,18 @@ class DeviceMesh:
         _bump()
         _lib.call("sg_kr_blend_dev", self.handle, float(r), ptr(Kel), ptr(Kt), ptr(Kr), cur_stream())
 
+    def assemble_kr(self, DS, r, Kel, Kt_scratch, Kr):
+        """K_r = r K_el + (1 - r) K_t with K_t assembled from DS in the same call; on P2
+        tetrahedra deterministic and without writing K_t (Kt_scratch is left untouched)."""
+        _bump()
+        _lib.call("sg_assemble_kr_dev", self.handle, ptr(DS), float(r), ptr(Kel), ptr(Kt_scratch), ptr(Kr),
+                  cur_stream())
+
+    @property
+    def tangent_fused(self):
+        """The fused assembly + blend leaves K_t unwritten on P2 tetrahedra."""
+        return self.dim == 3 and self.mesh.elem.shape[0] == 10
+
     def spmv(self, K, x, y):
         _lib.call("sg_bsr_spmv_dev", self.bsr, ptr(K), ptr(x), ptr(y), cur_stream())
 

@@ -88,8 +88,9 @@ def test_strain_force_assembly_kr(cuda_device, kind):
     I, J, V = cons.build_K_r_QQ_vals_ref(r)
     smap = pat.scatter_map()
     Vt = native.assemble(dim, dphi[0], dphi[1], dphi[2] if dim == 3 else None, DS, w, smap, nq, pat.nnz)
-    close(dm.to_ref(cons.K_t).cpu().numpy(), Vt)
     close(V, pat.K_r_values(Vt, r))
+    # K_t on its own (the fused K_r call does not store it on P2 tetrahedra)
+    close(dm.to_ref(cons.build_K_tangent_QQ_vals()).cpu().numpy(), Vt)
     # SpMV on the free DOFs equals K(Q,Q) x; Dirichlet rows are identity
     Kq = sp.csr_matrix((V, (I - 1, J - 1)), shape=(pat.n_Q, pat.n_Q))
     x = rng.normal(size=dm.n_dof) * dm.mask.cpu().numpy()
@@ -134,3 +135,48 @@ def test_fused_residual_matches_three_kernel_chain(cuda_device):
     assert np.mean(br_fused.cpu().numpy() == br) > 0.999
     assert len(np.unique(br)) >= 3
     close(F_fused.cpu().numpy().reshape(mesh.n_n, 3).T, pat.force(S), 1e-11)
+
+
+@pytest.mark.parametrize("kind", ["slope3d", "slope2d"])
+def test_assembly_run_twice_and_symmetry(cuda_device, kind):
+    """The tangent assembly and K_r are deterministic: two assemblies of the same DS give
+    bitwise equal K_t and K_r (P2 tetrahedra: fixed summation order per block; the 2D path
+    adds with FP64 atomics, whose order may vary, so there the bound is a few ulps of the
+    block's magnitude), and K_r is exactly symmetric on P2 tetrahedra."""
+    import torch
+    mesh, dphi, w, nq, mat = build_case(kind)
+    dm = DeviceMesh(mesh, dphi, w, nq)
+    cons = CONSTITUTIVE(dm, mat["c0"], mat["phi"], mat["psi"], "B", mat["shear"], mat["bulk"], mat["lame"])
+    cons.init_K_r_pattern(mesh.Q)
+    rng = np.random.default_rng(11)
+    U = rng.normal(size=(mesh.dim, mesh.n_n)) * 3e-3 * mesh.Q
+    Ud = torch.from_numpy(np.ascontiguousarray(U.T).ravel()).to(cuda_device)
+    cons.build_F_and_DS_all(1.2, Ud)
+    Kr1 = cons.build_K_r_QQ_vals(0.3).clone()
+    Kr2 = cons.build_K_r_QQ_vals(0.3).clone()
+    Kt1 = cons.build_K_tangent_QQ_vals().clone()
+    Kt2 = cons.build_K_tangent_QQ_vals().clone()
+    if kind == "slope3d":
+        assert torch.equal(Kr1, Kr2) and torch.equal(Kt1, Kt2)
+        b = 3
+        tr = torch.from_numpy(transpose_blocks(mesh)).to(cuda_device)
+        blocks = Kr1.reshape(-1, b, b)
+        assert torch.equal(blocks, blocks[tr].transpose(1, 2))
+    else:
+        scale = Kt1.abs().max()
+        assert (Kt1 - Kt2).abs().max() <= 8 * 2.2e-16 * scale
+        assert (Kr1 - Kr2).abs().max() <= 8 * 2.2e-16 * scale
+
+
+def transpose_blocks(mesh):
+    """Index of block (j, i) for every block (i, j) of the device pattern (the node adjacency
+    with sorted rows, rebuilt on the host)."""
+    from oracle.cpu_baseline import node_adjacency_csr
+    A = node_adjacency_csr(mesh.elem, mesh.n_n)
+    rp, col = A.indptr, A.indices
+    n = rp.size - 1
+    row = np.repeat(np.arange(n), np.diff(rp))
+    key = row.astype(np.int64) * n + col
+    tkey = col.astype(np.int64) * n + row
+    order = np.argsort(key)
+    return order[np.searchsorted(key[order], tkey)]
