@@ -225,8 +225,8 @@ int sg_amg_info(const sg_amg *amg, int64_t *info, int32_t cap);
 /* ------------------------------------------------------------------------------
  * (d1, d2) Preconditioner instances keyed by id over host COO triplets.  Replaces the
  * command set of hypre_boomeramg_mex (+LINEAR_SOLVERS/mex/hypre_boomeramg_mex.cpp:
- * 'setup_ijv' :1013-1146, 'update_values' :1151-1213, 'apply' :751-796, 'clear' :798-835,
- * 'info' :837-860), as called by DFGMRES.setup_preconditioner_ijv /
+ * 'setup_ijv' :1013-1146, 'update_values' :1151-1213, 'apply' :751-796, 'clear' :798-829,
+ * 'info' :830-853), as called by DFGMRES.setup_preconditioner_ijv /
  * update_preconditioner_values (+LINEAR_SOLVERS/DFGMRES.m:172-202) through the closures of
  * set_linear_solver.m:216-240.
  *   id        instance name (the reference's instance_id string)
@@ -277,6 +277,11 @@ int sg_krylov_destroy(sg_krylov *ws);
 int sg_dfgmres_solve(sg_krylov *ws, const sg_bsr *A, const double *A_vals, sg_amg *M, const double *W,
                      const double *AW, int32_t k, const double *b, double *x, double tol, int32_t maxit,
                      int32_t *iters, double *relres, double *res_hist, void *stream);
+/* Solves run as one replayed CUDA graph per (matrix, preconditioner): start, the iteration
+ * loop (a conditional WHILE node) and the least-squares solution stay on the device, with one
+ * host synchronisation per solve (on = 1, the default); on = 0 selects the host-driven loop
+ * (one synchronisation per iteration).  Both give the same iterates. */
+int sg_krylov_set_graph(sg_krylov *ws, int32_t on);
 /* AW (optional, may be NULL): receives A times the kept columns of W, in W's output order. */
 int sg_a_orthogonalize(sg_krylov *ws, const sg_bsr *A, const double *A_vals, double *W, double *AW,
                        int32_t k, double eps_add, int32_t *k_out, void *stream);

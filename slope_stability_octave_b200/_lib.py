@@ -59,6 +59,7 @@ SIGNATURES = {
     "sg_amg_destroy": [vp],
     "sg_amg_update": [vp, vp, vp],
     "sg_amg_clone": [vp, vp],
+    "sg_krylov_set_graph": [vp, i32],
     "sg_amg_setup_ijv": [C.c_char_p, vp, vp, vp, i64, i64, vp, i32, vp, i32, vp, i32, i32, vp],
     "sg_amg_update_values": [C.c_char_p, vp, i64, vp],
     "sg_amg_apply_host": [C.c_char_p, vp, vp, i64],

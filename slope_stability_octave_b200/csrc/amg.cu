@@ -1882,6 +1882,17 @@ extern "C" int sg_amg_clone(const sg_amg *h, sg_amg **out) {
     return SG_OK;
 }
 
+namespace sg {
+// Everything a captured V-cycle (sg_amg_apply inside a CUDA graph) depends on beyond the
+// hierarchy's own buffers: the level-0 values pointer (the caller's, in the FP64 cycle; the
+// parent's for a clone) and whether the learned correction is on.  A graph that captured the
+// cycle is valid while this key is unchanged.
+uint64_t amg_capture_key(const sg_amg *h) {
+    const double *a0 = h->parent ? h->parent->L[0].Avals : h->L[0].Avals;
+    return (uint64_t)(uintptr_t)a0 * 31u + (uint64_t)(h->corr_on ? 1 : 0) + (uint64_t)(uintptr_t)h;
+}
+}  // namespace sg
+
 // Numeric set-up for new values of the level-0 matrix (device pointer, kept by reference
 // until the next update: the caller must not free or overwrite it while applying).
 extern "C" int sg_amg_update(sg_amg *h, const double *Avals, void *stream) {

@@ -4,8 +4,8 @@
 //   sg_amg_setup_ijv      'setup_ijv', I, J, V, n, Z, opts, id   (:1013-1146)
 //   sg_amg_update_values  'update_values', V, id                 (:1151-1213)
 //   sg_amg_apply_host     'apply', r, id                         (:751-796)
-//   sg_amg_clear          'clear' [, id]                         (:798-835)
-//   sg_amg_ijv_info       'info'                                 (:837-860)
+//   sg_amg_clear          'clear' [, id]                         (:798-829)
+//   sg_amg_ijv_info       'info'                                 (:830-853)
 //
 // Semantics kept from the reference: I and J are 1-based indices stored as doubles (Octave's
 // numeric arrays), the triplets give the full (both-triangle) matrix, an id names a

@@ -35,10 +35,18 @@ __global__ void __launch_bounds__(MC_BLOCK) k_mc3d(const double *__restrict__ E,
     for (int64_t base = ((int64_t)blockIdx.x * MC_WARPS + warp) * 32; base < n; base += stride) {
         const int64_t p = base + lane;
         const int cnt = (int)(n - base < 32 ? n - base : 32);
-        if (p < n) {
-            double e[6];
+        // the warp's strains (6 consecutive doubles per point) arrive as one contiguous run,
+        // staged through the S buffer instead of six loads with a 48-byte lane stride
+        for (int idx = lane; idx < cnt * 6; idx += 32) {
+            const int q = idx / 6, c = idx - q * 6;
+            ss[q * S3_PITCH + c] = __ldcs(E + 6 * base + idx);
+        }
+        __syncwarp();
+        double e[6];
 #pragma unroll
-            for (int c = 0; c < 6; ++c) e[c] = E[6 * p + c];
+        for (int c = 0; c < 6; ++c) e[c] = ss[lane * S3_PITCH + c];
+        __syncwarp();
+        if (p < n) {
             double cb, sp;
             if (FUSED_REDUCTION) {
                 davis_reduce(m0[p], m1[p], psi[p], lambda, davis, cb, sp);

@@ -48,10 +48,14 @@ InstrRedirect::~InstrRedirect() {
     t_redirect_to = saved_to;
 }
 
+static thread_local bool t_suspended = false;
+InstrSuspend::InstrSuspend() : saved(t_suspended) { t_suspended = true; }
+InstrSuspend::~InstrSuspend() { t_suspended = saved; }
+
 InstrToken instr_begin(int kind, cudaStream_t st) {
     InstrState &s = state();
     InstrToken t;
-    if (!s.on) return t;
+    if (!s.on || t_suspended) return t;
     if (kind == t_redirect_from) kind = t_redirect_to;
     std::lock_guard<std::mutex> g(s.mu);
     const int64_t c = s.launches[kind]++;
@@ -65,7 +69,7 @@ InstrToken instr_begin(int kind, cudaStream_t st) {
 
 void instr_units(int kind, int64_t units) {
     InstrState &s = state();
-    if (!s.on || kind < 0 || kind >= IK_COUNT) return;
+    if (!s.on || t_suspended || kind < 0 || kind >= IK_COUNT) return;
     std::lock_guard<std::mutex> g(s.mu);
     s.units[kind] += units;
 }

@@ -39,6 +39,14 @@ struct InstrToken {
     cudaEvent_t a = nullptr, b = nullptr;
 };
 
+// While an InstrSuspend lives on a thread, nothing is timed or counted (stream capture into a
+// CUDA graph, whose loop bodies cannot hold event records).
+struct InstrSuspend {
+    bool saved;
+    InstrSuspend();
+    ~InstrSuspend();
+};
+
 InstrToken instr_begin(int kind, cudaStream_t st);
 void instr_end(const InstrToken &t, cudaStream_t st);
 

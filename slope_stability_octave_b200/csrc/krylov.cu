@@ -41,6 +41,21 @@ struct sg_krylov {
     int64_t kcap = 0;
     double *hpin = nullptr;     // pinned host mirror of hdev
     int device = 0;
+    // graph-replayed solve (dfgmres_graph): one CUDA graph holds the start, the iteration loop
+    // (a conditional WHILE node whose body is one FGMRES iteration) and the small
+    // least-squares solve; it is captured once per (matrix, preconditioner) and replayed
+    double *u = nullptr;        // n: A z during its orthogonalisation
+    int32_t *dstate = nullptr;  // [0] iterations done (j), [1] deflation columns k, [2] maxit
+    double *dscal = nullptr;    // [0] |b|, [1] relative residual, [2] tol, [3] scale of the new basis vector,
+                                // [4] b'b, [5] r0'r0
+    double *dH = nullptr, *dcs = nullptr, *dsn = nullptr, *dg = nullptr, *dy = nullptr, *dhist = nullptr;
+    const double **dptr = nullptr;  // [0] W, [1] A W of the current solve
+    cudaStream_t cap = nullptr, cap2 = nullptr;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t gexec = nullptr;
+    uint64_t gkey = 0;
+    int64_t launches_start = 0, launches_body = 0, launches_end = 0;
+    int use_graph = 1;
 };
 
 namespace sg {
@@ -96,6 +111,278 @@ __global__ void k_anorm_scale(int64_t n, const double *__restrict__ ntp, double 
     }
 }
 
+// ------------------------------------------------------------------ graph-replayed solve
+
+// the basis column j (j read from the device) into w, and back
+__global__ void k_col_get(int64_t n, const double *__restrict__ V, const int32_t *__restrict__ j,
+                          double *__restrict__ w) {
+    const double *c = V + (int64_t)j[0] * n;
+    for (int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; r < n; r += (int64_t)gridDim.x * blockDim.x)
+        w[r] = c[r];
+}
+__global__ void k_col_put(int64_t n, const double *__restrict__ w, double *__restrict__ V,
+                          const int32_t *__restrict__ j, const double *__restrict__ scale) {
+    double *c = V + (int64_t)j[0] * n;
+    const double s = scale ? scale[0] : 1.0;
+    for (int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; r < n; r += (int64_t)gridDim.x * blockDim.x)
+        c[r] = scale ? w[r] * s : w[r];
+}
+
+__global__ void k_fg_params(int32_t *st, double *sc, const double **ptrs, double tol, int maxit, int k,
+                            const double *W, const double *AW) {
+    st[0] = 0;
+    st[1] = k;
+    st[2] = maxit;
+    sc[2] = tol;
+    ptrs[0] = W;
+    ptrs[1] = AW;
+}
+
+// start of the loop: |b|, |r0|, the first residual estimate, g = (|r0|, 0, ...), and whether
+// to iterate at all (dfgmres_solver.m: no iteration when |r0| / |b| < tol)
+__global__ void k_fg_start(cudaGraphConditionalHandle h, int mcap, int32_t *st, double *sc, double *g,
+                           double *hist) {
+    if (threadIdx.x != 0) return;
+    double b_norm = sqrt(sc[4]);
+    if (b_norm == 0.0) b_norm = 1.0;
+    const double res = sqrt(sc[5]);
+    const double rel = res / b_norm;
+    sc[0] = b_norm;
+    sc[1] = rel;
+    hist[0] = rel;
+    g[0] = res;
+    for (int i = 1; i <= mcap; ++i) g[i] = 0.0;
+    st[0] = 0;
+    const bool go = (rel >= sc[2]) && st[2] > 0;
+    sc[3] = go ? 1.0 / res : 0.0;
+    cudaGraphSetConditional(h, go ? 1u : 0u);
+}
+
+// End of iteration j: the new Hessenberg column (the two CGS passes' coefficients), the
+// previous Givens rotations and a new one, the residual estimate |g_{j+1}| / |b|, the scale of
+// the next basis vector and the loop condition -- the host loop's arithmetic, on the device.
+__global__ void k_fg_arnoldi(cudaGraphConditionalHandle h, int mcap, int32_t *st, double *sc,
+                             const double *__restrict__ h1, const double *__restrict__ h2,
+                             const double *__restrict__ hn, double *H, double *cs, double *sn, double *g,
+                             double *hist) {
+    if (threadIdx.x != 0) return;
+    const int j = st[0];
+    for (int i = 0; i <= j; ++i) H[(size_t)i * mcap + j] = h1[i] + h2[i];
+    const double hjj = sqrt(hn[0]);
+    H[(size_t)(j + 1) * mcap + j] = hjj;
+    for (int i = 0; i < j; ++i) {
+        const double a = H[(size_t)i * mcap + j], bb = H[(size_t)(i + 1) * mcap + j];
+        H[(size_t)i * mcap + j] = cs[i] * a + sn[i] * bb;
+        H[(size_t)(i + 1) * mcap + j] = -sn[i] * a + cs[i] * bb;
+    }
+    const double a = H[(size_t)j * mcap + j], bb = H[(size_t)(j + 1) * mcap + j];
+    const double den = hypot(a, bb);
+    cs[j] = den > 0 ? a / den : 1.0;
+    sn[j] = den > 0 ? bb / den : 0.0;
+    H[(size_t)j * mcap + j] = den;
+    H[(size_t)(j + 1) * mcap + j] = 0.0;
+    g[j + 1] = -sn[j] * g[j];
+    g[j] = cs[j] * g[j];
+    const double rr = fabs(g[j + 1]) / sc[0];
+    hist[j + 1] = rr;
+    sc[1] = rr;
+    const bool broke = hjj < 1e-14;   // happy breakdown (dfgmres_solver.m: H(j+1,j) < 1e-14)
+    sc[3] = broke ? 0.0 : 1.0 / hjj;
+    st[0] = j + 1;
+    const bool go = !broke && !(rr < sc[2]) && (j + 1) < st[2];
+    cudaGraphSetConditional(h, go ? 1u : 0u);
+}
+
+// y = R \ g over the iterations done
+__global__ void k_fg_solve_y(int mcap, const int32_t *st, const double *H, const double *g, double *y) {
+    if (threadIdx.x != 0) return;
+    const int it = st[0];
+    for (int i = it - 1; i >= 0; --i) {
+        double s = g[i];
+        for (int c = i + 1; c < it; ++c) s -= H[(size_t)i * mcap + c] * y[c];
+        y[i] = H[(size_t)i * mcap + i] != 0.0 ? s / H[(size_t)i * mcap + i] : 0.0;
+    }
+}
+
+uint64_t amg_capture_key(const sg_amg *h);
+
+static int graph_alloc(sg_krylov *ws) {
+    if (ws->dstate) return SG_OK;
+    const int m = ws->maxit;
+    SG_CUDA(device_alloc(&ws->u, sizeof(double) * ws->n));
+    SG_CUDA(device_alloc(&ws->dstate, sizeof(int32_t) * 8));
+    SG_CUDA(device_alloc(&ws->dscal, sizeof(double) * 8));
+    SG_CUDA(device_alloc(&ws->dH, sizeof(double) * (size_t)(m + 1) * m));
+    SG_CUDA(device_alloc(&ws->dcs, sizeof(double) * m));
+    SG_CUDA(device_alloc(&ws->dsn, sizeof(double) * m));
+    SG_CUDA(device_alloc(&ws->dg, sizeof(double) * (m + 1)));
+    SG_CUDA(device_alloc(&ws->dy, sizeof(double) * m));
+    SG_CUDA(device_alloc(&ws->dhist, sizeof(double) * (m + 1)));
+    SG_CUDA(device_alloc(&ws->dptr, sizeof(double *) * 2));
+    SG_CUDA(cudaStreamCreateWithFlags(&ws->cap, cudaStreamNonBlocking));
+    SG_CUDA(cudaStreamCreateWithFlags(&ws->cap2, cudaStreamNonBlocking));
+    return SG_OK;
+}
+
+static void graph_release(sg_krylov *ws) {
+    if (ws->gexec) cudaGraphExecDestroy(ws->gexec);
+    if (ws->graph) cudaGraphDestroy(ws->graph);
+    ws->gexec = nullptr;
+    ws->graph = nullptr;
+    ws->gkey = 0;
+}
+
+// Captures start, loop and least-squares solve for (A, Avals, M) into ws->gexec.
+static int graph_capture(sg_krylov *ws, const sg_bsr *A, const double *Avals, sg_amg *M) {
+    graph_release(ws);
+    const int64_t n = ws->n;
+    const int m = ws->maxit;
+    const int kcap = (int)ws->kcap;
+    double *h1 = ws->hdev, *h2 = ws->hdev + (m + 2), *hn = ws->hdev + 2 * (m + 2);
+    InstrSuspend quiet;   // no event records inside the graph
+    int rc = SG_OK;
+    cudaStream_t cap = ws->cap, cap2 = ws->cap2;
+    SG_CUDA(cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal));
+    cudaGraph_t g = nullptr;
+    auto abort_capture = [&](int code) {
+        cudaGraph_t dead = nullptr;
+        cudaStreamEndCapture(cap, &dead);
+        if (dead) cudaGraphDestroy(dead);
+        cudaGetLastError();
+        return code;
+    };
+    cudaStreamCaptureStatus status;
+    const cudaGraphNode_t *deps = nullptr;
+    size_t ndeps = 0;
+    if (cudaStreamGetCaptureInfo(cap, &status, nullptr, &g, &deps, &ndeps) != cudaSuccess)
+        return abort_capture(set_error(SG_ERR_CUDA, "capture info"));
+    cudaGraphConditionalHandle hcond;
+    if (cudaGraphConditionalHandleCreate(&hcond, g, 0, cudaGraphCondAssignDefault) != cudaSuccess)
+        return abort_capture(set_error(SG_ERR_CUDA, "conditional handle"));
+    const int64_t l0 = sg_launch_count(0);
+    count_launch(1);
+    k_fg_start<<<1, 32, 0, cap>>>(hcond, m, ws->dstate, ws->dscal, ws->dg, ws->dhist);
+    if (scale_dev(n, ws->V, ws->dscal + 3, 0, ws->V, cap) || cudaGetLastError() != cudaSuccess)
+        return abort_capture(set_error(SG_ERR_CUDA, "capture start"));
+    const int64_t l1 = sg_launch_count(0);
+    if (cudaStreamGetCaptureInfo(cap, &status, nullptr, &g, &deps, &ndeps) != cudaSuccess)
+        return abort_capture(set_error(SG_ERR_CUDA, "capture info"));
+    cudaGraphNodeParams cp = {};
+    cp.type = cudaGraphNodeTypeConditional;
+    cp.conditional.handle = hcond;
+    cp.conditional.type = cudaGraphCondTypeWhile;
+    cp.conditional.size = 1;
+    cudaGraphNode_t cnode;
+    if (cudaGraphAddNode(&cnode, g, deps, ndeps, &cp) != cudaSuccess)
+        return abort_capture(set_error(SG_ERR_CUDA, "conditional node"));
+    cudaGraph_t body = cp.conditional.phGraph_out[0];
+    if (cudaStreamUpdateCaptureDependencies(cap, &cnode, 1, cudaStreamSetCaptureDependencies) != cudaSuccess)
+        return abort_capture(set_error(SG_ERR_CUDA, "capture dependencies"));
+    // one iteration, captured into the loop body
+    if (cudaStreamBeginCaptureToGraph(cap2, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal) != cudaSuccess)
+        return abort_capture(set_error(SG_ERR_CUDA, "body capture"));
+    {
+        k_col_get<<<grid_for(n, 256, 8), 256, 0, cap2>>>(n, ws->V, ws->dstate, ws->w);
+        if (M) rc = sg_amg_apply(M, ws->w, ws->t, cap2);
+        else if (cudaMemcpyAsync(ws->t, ws->w, sizeof(double) * n, cudaMemcpyDeviceToDevice, cap2) != cudaSuccess)
+            rc = set_error(SG_ERR_CUDA, "body copy");
+        if (!rc) rc = multidot_dc(n, ws->dstate + 1, 0, kcap, nullptr, ws->dptr + 1, n, ws->t, ws->part, ws->hd, cap2);
+        if (!rc) rc = gemv_dc(-1, n, ws->dstate + 1, 0, kcap, nullptr, ws->dptr, n, ws->hd, ws->t, cap2);
+        if (!rc) k_col_put<<<grid_for(n, 256, 8), 256, 0, cap2>>>(n, ws->t, ws->Z, ws->dstate, nullptr);
+        if (!rc) rc = bsr_spmv<double, double>(*A, Avals, ws->t, ws->u, 1.0, 0.0, cap2);
+        if (!rc) rc = multidot_dc(n, ws->dstate, 1, m, ws->V, nullptr, n, ws->u, ws->part, h1, cap2);
+        if (!rc) rc = gemv_dc(-1, n, ws->dstate, 1, m, ws->V, nullptr, n, h1, ws->u, cap2);
+        if (!rc) rc = multidot_dc(n, ws->dstate, 1, m, ws->V, nullptr, n, ws->u, ws->part, h2, cap2);
+        if (!rc) rc = gemv_dc(-1, n, ws->dstate, 1, m, ws->V, nullptr, n, h2, ws->u, cap2);
+        if (!rc) rc = multidot(n, 1, ws->u, n, ws->u, ws->part, hn, cap2);
+        if (!rc) {
+            count_launch(1);
+            k_fg_arnoldi<<<1, 32, 0, cap2>>>(hcond, m, ws->dstate, ws->dscal, h1, h2, hn, ws->dH, ws->dcs, ws->dsn,
+                                             ws->dg, ws->dhist);
+            k_col_put<<<grid_for(n, 256, 8), 256, 0, cap2>>>(n, ws->u, ws->V, ws->dstate, ws->dscal + 3);
+        }
+        cudaGraph_t body_out = nullptr;
+        const cudaError_t e = cudaStreamEndCapture(cap2, &body_out);
+        if (!rc && (e != cudaSuccess || cudaGetLastError() != cudaSuccess)) rc = set_error(SG_ERR_CUDA, "body capture");
+    }
+    if (rc) return abort_capture(rc);
+    const int64_t l2 = sg_launch_count(0);
+    count_launch(1);
+    k_fg_solve_y<<<1, 32, 0, cap>>>(m, ws->dstate, ws->dH, ws->dg, ws->dy);
+    cudaGraph_t full = nullptr;
+    if (cudaStreamEndCapture(cap, &full) != cudaSuccess || !full) {
+        if (full) cudaGraphDestroy(full);
+        cudaGetLastError();
+        return set_error(SG_ERR_CUDA, "graph capture");
+    }
+    cudaGraphExec_t ex = nullptr;
+    if (cudaGraphInstantiate(&ex, full, 0) != cudaSuccess) {
+        cudaGraphDestroy(full);
+        cudaGetLastError();
+        return set_error(SG_ERR_CUDA, "graph instantiation");
+    }
+    const int64_t l3 = sg_launch_count(0);
+    ws->graph = full;
+    ws->gexec = ex;
+    ws->launches_start = l1 - l0;
+    ws->launches_body = l2 - l1;
+    ws->launches_end = l3 - l2;
+    // the captured launches were counted at capture; executions are counted per solve instead
+    count_launch((int)-(l3 - l0));
+    return SG_OK;
+}
+
+static uint64_t graph_key(const sg_krylov *ws, const sg_bsr *A, const double *Avals, sg_amg *M) {
+    uint64_t k = (uint64_t)(uintptr_t)A * 1000003u ^ (uint64_t)(uintptr_t)Avals * 10007u;
+    k ^= (uint64_t)(uintptr_t)ws->part * 131u ^ (uint64_t)(uintptr_t)ws->hd * 137u ^ (uint64_t)ws->kcap * 7919u;
+    if (M) k ^= amg_capture_key(M) * 1315423911u;
+    return k | 1u;
+}
+
+// The graph-replayed solve: the same start, iterations, stopping test and least-squares
+// solution as the host loop of sg_dfgmres_solve, with one host synchronisation per solve
+// instead of one per iteration.
+static int dfgmres_graph(sg_krylov *ws, const sg_bsr *A, const double *Avals, sg_amg *M, const double *Wd,
+                         const double *AWd, int32_t k, const double *b, double *x, double tol, int32_t maxit,
+                         int32_t *iters, double *relres, double *res_hist, cudaStream_t st) {
+    const int64_t n = ws->n;
+    int rc = graph_alloc(ws);
+    if (rc) return rc;
+    const uint64_t key = graph_key(ws, A, Avals, M);
+    if (!ws->gexec || ws->gkey != key) {
+        rc = graph_capture(ws, A, Avals, M);
+        if (rc) return rc;
+        ws->gkey = key;
+    }
+    // x0 = Wd (Wd' b), r0 = b - A x0 = V(:, 0), b'b and r0'r0, the solve's parameters
+    SG_CUDA(cudaMemsetAsync(x, 0, sizeof(double) * n, st));
+    if (k > 0) {
+        if ((rc = multidot(n, k, Wd, n, b, ws->part, ws->hd, st))) return rc;
+        if ((rc = gemv_add(n, k, Wd, n, ws->hd, x, st))) return rc;
+    }
+    if ((rc = bsr_residual<double, double>(*A, Avals, x, b, ws->V, st))) return rc;
+    if ((rc = multidot(n, 1, b, n, b, ws->part, ws->dscal + 4, st))) return rc;
+    if ((rc = multidot(n, 1, ws->V, n, ws->V, ws->part, ws->dscal + 5, st))) return rc;
+    count_launch(1);
+    k_fg_params<<<1, 1, 0, st>>>(ws->dstate, ws->dscal, ws->dptr, tol, maxit, k, Wd, AWd);
+    SG_CUDA(cudaGetLastError());
+    SG_CUDA(cudaGraphLaunch(ws->gexec, st));
+    if ((rc = gemv_dc(1, n, ws->dstate, 0, ws->maxit, ws->Z, nullptr, n, ws->dy, x, st))) return rc;
+    double *hp = ws->hpin;
+    int32_t *ip = reinterpret_cast<int32_t *>(hp + ws->maxit + 4);
+    SG_CUDA(cudaMemcpyAsync(ip, ws->dstate, sizeof(int32_t), cudaMemcpyDeviceToHost, st));
+    SG_CUDA(cudaMemcpyAsync(hp, ws->dscal + 1, sizeof(double), cudaMemcpyDeviceToHost, st));
+    if (res_hist) SG_CUDA(cudaMemcpyAsync(hp + 1, ws->dhist, sizeof(double) * (maxit + 1), cudaMemcpyDeviceToHost, st));
+    SG_CUDA(cudaStreamSynchronize(st));
+    const int it = ip[0];
+    count_launch((int)(ws->launches_start + ws->launches_body * it + ws->launches_end));
+    *iters = it;
+    if (relres) *relres = hp[0];
+    if (res_hist)
+        for (int i = 0; i <= it; ++i) res_hist[i] = hp[1 + i];
+    return SG_OK;
+}
+
 }  // namespace sg
 
 using namespace sg;
@@ -133,9 +420,22 @@ extern "C" int sg_krylov_destroy(sg_krylov *ws) {
     cudaFree(ws->V); cudaFree(ws->Z); cudaFree(ws->w); cudaFree(ws->t); cudaFree(ws->hdev);
     cudaFree(ws->part); cudaFree(ws->hd); cudaFree(ws->Worth); cudaFree(ws->AWorth); cudaFree(ws->nt);
     cudaFree(ws->sig);
+    graph_release(ws);
+    cudaFree(ws->u); cudaFree(ws->dstate); cudaFree(ws->dscal); cudaFree(ws->dH); cudaFree(ws->dcs);
+    cudaFree(ws->dsn); cudaFree(ws->dg); cudaFree(ws->dy); cudaFree(ws->dhist); cudaFree(ws->dptr);
+    if (ws->cap) cudaStreamDestroy(ws->cap);
+    if (ws->cap2) cudaStreamDestroy(ws->cap2);
     if (ws->hpin) cudaFreeHost(ws->hpin);
     cudaSetDevice(cur);
     delete ws;
+    return SG_OK;
+}
+
+// 1: solves run as a replayed CUDA graph (default); 0: the host-driven loop, one host
+// synchronisation per iteration (same arithmetic)
+extern "C" int sg_krylov_set_graph(sg_krylov *ws, int32_t on) {
+    SG_CHECK_ARG(ws, "null workspace");
+    ws->use_graph = on != 0;
     return SG_OK;
 }
 
@@ -154,6 +454,8 @@ extern "C" int sg_dfgmres_solve(sg_krylov *ws, const sg_bsr *A, const double *Av
     const cudaStream_t st = as_stream(stream);
     int rc = ensure_kcap(ws, std::max<int64_t>(k, 1));
     if (rc) return rc;
+    if (ws->use_graph && (k == 0 || AWd))
+        return dfgmres_graph(ws, A, Avals, M, Wd, AWd, k, b, x, tol, maxit, iters, relres, res_hist, st);
     double *part = ws->part, *hdev = ws->hdev, *hp = ws->hpin;
     const unsigned gb = grid_for(n, 256, 8);
     // x0 = Wd (Wd' b) ; r0 = b - A x0

@@ -529,6 +529,98 @@ int gemv_add(int64_t n, int m, const double *V, int64_t ldv, const double *y, do
     return SG_OK;
 }
 
+// ------------------------------------------------------------------ device-count variants
+//
+// The number of columns is read from device memory (cnt[0] + add, at most mmax) and the basis
+// pointer may be too (Vp[0] when V is null), so that one captured sequence of launches serves
+// every iteration of a graph-replayed loop.  Same arithmetic and summation order as the
+// host-count kernels above.
+
+__global__ void __launch_bounds__(DOT_THREADS) k_multidot_dc(int64_t n, const int32_t *__restrict__ cnt, int add,
+                                                             int mmax, const double *V, const double *const *Vp,
+                                                             int64_t ldv, const double *__restrict__ w,
+                                                             double *__restrict__ partial) {
+    __shared__ double sh[32];
+    const int m = min(cnt[0] + add, mmax);
+    const double *__restrict__ B = V ? V : Vp[0];
+    const int64_t chunk = (n + gridDim.x - 1) / gridDim.x;
+    const int64_t r0 = blockIdx.x * chunk, r1 = min(n, r0 + chunk);
+    int i = 0;
+    for (; i + 4 <= m; i += 4) {
+        double s0 = 0, s1 = 0, s2 = 0, s3 = 0;
+        for (int64_t r = r0 + threadIdx.x; r < r1; r += blockDim.x) {
+            const double wr = w[r];
+            s0 += B[(i + 0) * ldv + r] * wr;
+            s1 += B[(i + 1) * ldv + r] * wr;
+            s2 += B[(i + 2) * ldv + r] * wr;
+            s3 += B[(i + 3) * ldv + r] * wr;
+        }
+        s0 = block_sum(s0, sh);
+        if (threadIdx.x == 0) partial[(i + 0) * gridDim.x + blockIdx.x] = s0;
+        s1 = block_sum(s1, sh);
+        if (threadIdx.x == 0) partial[(i + 1) * gridDim.x + blockIdx.x] = s1;
+        s2 = block_sum(s2, sh);
+        if (threadIdx.x == 0) partial[(i + 2) * gridDim.x + blockIdx.x] = s2;
+        s3 = block_sum(s3, sh);
+        if (threadIdx.x == 0) partial[(i + 3) * gridDim.x + blockIdx.x] = s3;
+    }
+    for (; i < m; ++i) {
+        double s = 0;
+        for (int64_t r = r0 + threadIdx.x; r < r1; r += blockDim.x) s += B[i * ldv + r] * w[r];
+        s = block_sum(s, sh);
+        if (threadIdx.x == 0) partial[i * gridDim.x + blockIdx.x] = s;
+    }
+}
+
+__global__ void k_reduce_partials_dc(const int32_t *__restrict__ cnt, int add, int mmax, int nb,
+                                     const double *__restrict__ partial, double *__restrict__ out) {
+    __shared__ double sh[32];
+    const int m = min(cnt[0] + add, mmax);
+    for (int i = blockIdx.x; i < m; i += gridDim.x) {
+        double s = 0;
+        for (int b = threadIdx.x; b < nb; b += blockDim.x) s += partial[(int64_t)i * nb + b];
+        s = block_sum(s, sh);
+        if (threadIdx.x == 0) out[i] = s;
+    }
+}
+
+template <int SIGN>
+__global__ void k_gemv_dc(int64_t n, const int32_t *__restrict__ cnt, int add, int mmax, const double *V,
+                          const double *const *Vp, int64_t ldv, const double *__restrict__ h,
+                          double *__restrict__ w) {
+    extern __shared__ double hs[];
+    const int m = min(cnt[0] + add, mmax);
+    const double *__restrict__ B = V ? V : Vp[0];
+    for (int i = threadIdx.x; i < m; i += blockDim.x) hs[i] = h[i];
+    __syncthreads();
+    if (m <= 0) return;
+    for (int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; r < n; r += (int64_t)gridDim.x * blockDim.x) {
+        double s = 0;
+        for (int i = 0; i < m; ++i) s += hs[i] * B[i * ldv + r];
+        w[r] = SIGN > 0 ? w[r] + s : w[r] - s;
+    }
+}
+
+int multidot_dc(int64_t n, const int32_t *cnt, int add, int mmax, const double *V, const double *const *Vp,
+                int64_t ldv, const double *w, double *partial, double *out, cudaStream_t st) {
+    if (mmax <= 0) return SG_OK;
+    count_launch(2);
+    k_multidot_dc<<<DOT_BLOCKS, DOT_THREADS, 0, st>>>(n, cnt, add, mmax, V, Vp, ldv, w, partial);
+    k_reduce_partials_dc<<<std::min(mmax, 1024), 256, 0, st>>>(cnt, add, mmax, DOT_BLOCKS, partial, out);
+    SG_CUDA(cudaGetLastError());
+    return SG_OK;
+}
+
+int gemv_dc(int sign, int64_t n, const int32_t *cnt, int add, int mmax, const double *V, const double *const *Vp,
+            int64_t ldv, const double *h, double *w, cudaStream_t st) {
+    if (mmax <= 0) return SG_OK;
+    const unsigned grid = grid_for(n, 256, 8);
+    if (sign > 0) k_gemv_dc<1><<<grid, 256, sizeof(double) * mmax, st>>>(n, cnt, add, mmax, V, Vp, ldv, h, w);
+    else k_gemv_dc<-1><<<grid, 256, sizeof(double) * mmax, st>>>(n, cnt, add, mmax, V, Vp, ldv, h, w);
+    SG_CUDA(cudaGetLastError());
+    return SG_OK;
+}
+
 __global__ void k_axpby(int64_t n, double a, const double *__restrict__ x, double b, double *__restrict__ y) {
     for (int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; r < n; r += (int64_t)gridDim.x * blockDim.x)
         y[r] = (b == 0.0) ? a * x[r] : a * x[r] + b * y[r];

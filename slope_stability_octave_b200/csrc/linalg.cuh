@@ -48,6 +48,14 @@ int h3_spmv(int64_t nrows, int64_t nblk, const int32_t *rp, const int32_t *col, 
 // magnitudes beyond the FP16 range are clamped)
 int to_float_half3(int64_t nblk, const double *A, float *A32, uint2 *A16, float scale, cudaStream_t st);
 
+// Device-count variants for graph-replayed loops: m = min(cnt[0] + add, mmax) columns, basis
+// V, or *Vp when V is null (both on the device)
+int multidot_dc(int64_t n, const int32_t *cnt, int add, int mmax, const double *V, const double *const *Vp,
+                int64_t ldv, const double *w, double *partial, double *out, cudaStream_t st);
+// w += sign * V(:, 0:m) h
+int gemv_dc(int sign, int64_t n, const int32_t *cnt, int add, int mmax, const double *V, const double *const *Vp,
+            int64_t ldv, const double *h, double *w, cudaStream_t st);
+
 // y = a x + b y
 int axpby(int64_t n, double a, const double *x, double b, double *y, cudaStream_t st);
 // y = x * s where s = *num / *den on the device (den may be null -> s = *num)
