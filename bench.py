@@ -91,7 +91,7 @@ MEASURED_SLICES = {
 # learned form: trained before the init phase's 4th linear solve on 12 residual vectors of
 # that Newton system, 60 full-batch Adam steps
 LEARNED_OPTS = dict(train_at=3, n_vectors=12, steps=60, lr=3e-3, seed=0)
-N_INSTR = 11
+N_INSTR = 12
 
 
 def parse():
@@ -706,7 +706,7 @@ def box_reference_arm(args, rank):
 
 
 KINDS = ["spmv3_f64", "spmv3_f32", "constitutive_S_DS", "constitutive_S", "assembly", "amg_update", "amg_vcycle",
-         "spmv3_f16", "spmv3_f64_aorth", "residual", "spmm3_f64_aorth"]
+         "spmv3_f16", "spmv3_f64_aorth", "residual", "spmm3_f64_aorth", "a_orthogonalize"]
 KIND_NAMES = {
     "spmv3_f64": "k_spmv_blk 3x3 FP64, fine level (Arnoldi, projection, residuals)",
     "spmv3_f32": "k_spmv_blk 3x3 FP32, fine level of the FP32 V-cycle",
@@ -719,6 +719,7 @@ KIND_NAMES = {
     "spmv3_f64_aorth": "k_spmv_blk 3x3 FP64 inside the A-orthogonalisation",
     "residual": "k_residual3d fused stress-only residual",
     "spmm3_f64_aorth": "k_spmm3 FP64 multi-vector SpMM of the A-orthogonalisation",
+    "a_orthogonalize": "whole A-orthogonalisation of the deflation basis (SpMM + blocked Gram-Schmidt)",
 }
 
 
@@ -754,7 +755,7 @@ def kind_bytes(P, amg, units=None, launches=None):
             "spmv3_f16": nb * (24 + 4) + (nr + 1) * 4 + 3 * 4 * nd,
             "constitutive_S_DS": ni * 416, "constitutive_S": ni * 128,
             "assembly": ne * 5896 + nb * 72, "residual": ni * 280 + ne * 30 * 8 + nd * 8,
-            "amg_update": upd, "amg_vcycle": cyc}
+            "amg_update": upd, "amg_vcycle": cyc, "a_orthogonalize": None}
 
 
 def roofline_report(head, kbytes, K, peak, peak_kind, n_blocks):
@@ -767,11 +768,16 @@ def roofline_report(head, kbytes, K, peak, peak_kind, n_blocks):
         if not nl[i] or not nt[i]:
             continue
         avg = ms[i] / nt[i]
-        ach = kbytes[name] / (avg * 1e-3) / 1e9
-        rows[name] = dict(kernel=KIND_NAMES[name], launches=int(nl[i]), timed_launches=int(nt[i]), avg_ms=avg,
-                          share_of_timed_steps=avg * nl[i] / total, algorithmic_bytes_per_launch=int(kbytes[name]),
-                          achieved=ach, frac=ach / peak)
-    top = max(rows, key=lambda k: rows[k]["share_of_timed_steps"])
+        row = dict(kernel=KIND_NAMES[name], launches=int(nl[i]), timed_launches=int(nt[i]), avg_ms=avg,
+                   share_of_timed_steps=avg * nl[i] / total)
+        if kbytes.get(name) is not None:
+            ach = kbytes[name] / (avg * 1e-3) / 1e9
+            row.update(algorithmic_bytes_per_launch=int(kbytes[name]), achieved=ach, frac=ach / peak)
+        else:
+            units = head["instr"][3][i]
+            row["mean_units_per_launch"] = float(units) / nl[i] if nl[i] else None
+        rows[name] = row
+    top = max((k for k in rows if "achieved" in rows[k]), key=lambda k: rows[k]["share_of_timed_steps"])
     r = rows[top]
     return dict(kernel=r["kernel"], kind=top, bound="hbm", achieved=r["achieved"], peak=peak, unit="GB/s",
                 frac=r["frac"], peak_kind=peak_kind, traffic=traffic_per_launch(top, n_blocks),

@@ -354,16 +354,18 @@ int sg_learned_info(const sg_learned *h, int64_t *info);
 /* ------------------------------------------------------------------------------
  * Live kernel timing (no reference counterpart: profiling support in the spirit of the
  * reference's PROFILING.Profiler).  When enabled, every `sample`-th launch of each kind is
- * bracketed by CUDA events on its stream.  Kinds (capacity 11): 0 fine SpMV FP64 (FGMRES,
+ * bracketed by CUDA events on its stream.  Kinds (capacity 12): 0 fine SpMV FP64 (FGMRES,
  * residuals), 1 fine SpMV FP32, 2 return mapping + tangent, 3 return mapping (stress),
  * 4 assembly, 5 AMG value update, 6 AMG V-cycle, 7 fine SpMV on the FP16 copy, 8 fine SpMV
  * FP64 inside sg_a_orthogonalize, 9 fused residual (sg_residual_dev), 10 fine SpMM FP64 of
- * sg_a_orthogonalize (several vectors per launch).  sg_instr_read synchronises the device and resets the
+ * sg_a_orthogonalize (several vectors per launch), 11 a whole sg_a_orthogonalize call (units:
+ * basis columns).  sg_instr_read synchronises the device and resets the
  * counters.
  * ---------------------------------------------------------------------------- */
 int sg_instr_enable(int on, int sample);
 int sg_instr_read(double *ms, int64_t *timed, int64_t *launches, int32_t cap);
-/* work units per kind since the last sg_instr_read (kind 10: vectors multiplied) */
+/* work units per kind since the last sg_instr_read (kind 10: vectors multiplied, kind 11:
+ * basis columns) */
 int sg_instr_units(int64_t *units, int32_t cap);
 /* number of kernels the library launched since the last reset (reset != 0 clears it) */
 int64_t sg_launch_count(int reset);

@@ -79,22 +79,6 @@ struct Level {
     Pattern P, R, AP;
     int32_t *d_R_from_P = nullptr;
     Plan at_plan, ap_plan, ac_plan;  // at: (A block) per P block; ap: (A, P); ac: (P, AP)
-    // Shared-memory tiles of the A P gather on 3 x 3 levels (k_gather_AP_tiled): a tile is a
-    // run of consecutive block rows; it stages the rows' A blocks (one contiguous range) and
-    // the P rows they reference, and its pairs address those copies by 16-bit local indices
-    int64_t ap_ntiles = 0;
-    int ap_maxA = 0, ap_maxP = 0;      // largest tile's A and P blocks (dynamic shared memory)
-    int32_t *d_tile_row0 = nullptr;    // ap_ntiles + 1
-    int32_t *d_tile_kptr = nullptr;    // ap_ntiles + 1: range of the tile's staged P rows
-    int32_t *d_tile_k = nullptr;       // staged P rows, in staging order
-    int32_t *d_tile_kofs = nullptr;    // local block offset of each staged P row
-    uint32_t *d_tile_pairs = nullptr;  // per plan pair: A local index | P local index << 16
-    // Chunked P'(A P) gather on the same levels (k_gather_Ac_chunked): a CTA per coarse row
-    // streams the row's fine rows in chunks of AC_CHUNK (their R blocks and A P rows staged in
-    // shared memory); pairs packed as AP local | R local << 16 | chunk << 24
-    int ac_maxAP = 0;                  // largest chunk's staged A P blocks
-    int ac_maxblk = 0;                 // most coarse blocks in one coarse row
-    uint32_t *d_ac_pairs = nullptr;
     int64_t ap_pairs = 0, ac_pairs = 0;  // plan lengths (pairs of input blocks)
     double *Pv = nullptr, *Rv = nullptr, *APv = nullptr;
     float *P32 = nullptr, *R32 = nullptr;
@@ -587,151 +571,6 @@ __global__ void k_gather_AP(int64_t nblk, const int64_t *__restrict__ lptr, cons
     }
 }
 
-// AP block = sum over plan pairs A_a (3 x 3) * P_b (3 x 6) on a 3 x 3 level, by tiles of
-// consecutive block rows (AP_TILE_THREADS AP blocks at most per tile, one thread each).  The
-// CTA first copies the tile's A blocks (a contiguous range) and every P row they reference into
-// shared memory; each thread then walks its block's pairs, packed as (A local | P local << 16),
-// entirely out of shared memory.  The pairs are summed in plan order, as in k_gather_AP.
-constexpr int AP_TILE_THREADS = 128;
-template <typename V>
-__global__ void __launch_bounds__(AP_TILE_THREADS) k_gather_AP_tiled(
-    int64_t ntiles, const int32_t *__restrict__ row0, const int32_t *__restrict__ Arp,
-    const int32_t *__restrict__ APrp, const int64_t *__restrict__ lptr, const uint32_t *__restrict__ pairs,
-    const int32_t *__restrict__ kptr, const int32_t *__restrict__ klist, const int32_t *__restrict__ kofs,
-    const int32_t *__restrict__ Prp, const V *__restrict__ A, const V *__restrict__ P, V *__restrict__ AP,
-    int maxA) {
-    using T = typename GAcc<V>::type;
-    extern __shared__ __align__(16) unsigned char ap_smem[];
-    V *sA = reinterpret_cast<V *>(ap_smem);
-    V *sP = sA + (size_t)maxA * 9;
-    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    constexpr int NW = AP_TILE_THREADS / 32;
-    for (int64_t t = blockIdx.x; t < ntiles; t += gridDim.x) {
-        const int32_t r0 = row0[t], r1 = row0[t + 1];
-        const int64_t a0 = Arp[r0], na = (int64_t)Arp[r1] - a0;
-        for (int64_t e = tid; e < na * 9; e += AP_TILE_THREADS) sA[e] = A[a0 * 9 + e];
-        for (int32_t j = kptr[t] + warp; j < kptr[t + 1]; j += NW) {
-            const int32_t k = klist[j];
-            const int64_t p0 = Prp[k], np = (int64_t)Prp[k + 1] - p0;
-            V *dst = sP + (int64_t)kofs[j] * 18;
-            for (int64_t e = lane; e < np * 18; e += 32) dst[e] = P[p0 * 18 + e];
-        }
-        __syncthreads();
-        const int64_t q1 = APrp[r1];
-        for (int64_t q = APrp[r0] + tid; q < q1; q += AP_TILE_THREADS) {
-            T acc[18];
-#pragma unroll
-            for (int c = 0; c < 18; ++c) acc[c] = 0;
-            const int64_t l1 = lptr[q + 1];
-            for (int64_t l = lptr[q]; l < l1; ++l) {
-                const uint32_t pk = pairs[l];
-                const V *a = sA + (pk & 0xffffu) * 9;
-                const V *pv = sP + (pk >> 16) * 18;
-#pragma unroll
-                for (int r = 0; r < 3; ++r)
-#pragma unroll
-                    for (int m = 0; m < 3; ++m) {
-                        const T av = (T)a[r * 3 + m];
-#pragma unroll
-                        for (int c = 0; c < 6; ++c) acc[r * 6 + c] += av * (T)pv[m * 6 + c];
-                    }
-            }
-#pragma unroll
-            for (int c = 0; c < 18; ++c) AP[q * 18 + c] = (V)acc[c];
-        }
-        __syncthreads();
-    }
-}
-
-// Ac block (I, J) = sum over plan pairs R_(I,i) (6 x 3) * AP_(i,J) (3 x 6) on a 3 x 3 level
-// with 6 coarse modes, a CTA per coarse row I.  The row's fine rows i (its R row) are streamed
-// in chunks of AC_CHUNK: the chunk's R blocks (contiguous in R) and A P rows are copied into
-// shared memory, then two threads per coarse block (rows 0-2 and 3-5 of the 6 x 6) add the
-// chunk's pairs of their block, in plan order, from shared memory.  Rows and columns of dead
-// coarse DOFs become identity, as in k_gather_Ac.
-constexpr int AC_CHUNK = 32, AC_THREADS = 256;
-template <typename V>
-__global__ void __launch_bounds__(AC_THREADS) k_gather_Ac_chunked(
-    int64_t nrows_c, const int32_t *__restrict__ Rrp, const int32_t *__restrict__ Rcol,
-    const int32_t *__restrict__ APrp, const int32_t *__restrict__ Acrp, const int32_t *__restrict__ Accol,
-    const int64_t *__restrict__ lptr, const uint32_t *__restrict__ pairs, const V *__restrict__ R,
-    const V *__restrict__ AP, const uint8_t *__restrict__ dead, V *__restrict__ Ac, int maxAP) {
-    using T = typename GAcc<V>::type;
-    extern __shared__ __align__(16) unsigned char ac_smem[];
-    V *sR = reinterpret_cast<V *>(ac_smem);
-    V *sAP = sR + AC_CHUNK * 18;
-    __shared__ int32_t s_off[AC_CHUNK + 1];
-    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    constexpr int NW = AC_THREADS / 32;
-    for (int64_t I = blockIdx.x; I < nrows_c; I += gridDim.x) {
-        const int32_t k0 = Rrp[I], k1 = Rrp[I + 1];
-        const int32_t b0 = Acrp[I], b1 = Acrp[I + 1];
-        const int nchunks = (k1 - k0 + AC_CHUNK - 1) / AC_CHUNK;
-        for (int32_t pass = b0; pass < b1; pass += AC_THREADS / 2) {
-            const int32_t q = pass + tid / 2;
-            const int h = tid & 1;
-            const bool live = q < b1;
-            T acc[18];
-#pragma unroll
-            for (int c = 0; c < 18; ++c) acc[c] = 0;
-            int64_t l = live ? lptr[q] : 0;
-            const int64_t l1 = live ? lptr[q + 1] : 0;
-            for (int ch = 0; ch < nchunks; ++ch) {
-                const int32_t c0 = k0 + ch * AC_CHUNK, c1 = min(c0 + AC_CHUNK, k1);
-                // A P row offsets of the chunk (one lane per fine row, warp-wide prefix sum)
-                if (warp == 0) {
-                    const int len = (c0 + lane < c1) ? APrp[Rcol[c0 + lane] + 1] - APrp[Rcol[c0 + lane]] : 0;
-                    int x = len;
-#pragma unroll
-                    for (int o = 1; o < 32; o <<= 1) {
-                        const int y = __shfl_up_sync(0xffffffffu, x, o);
-                        if (lane >= o) x += y;
-                    }
-                    s_off[lane + 1] = x;
-                    if (lane == 0) s_off[0] = 0;
-                }
-                for (int e = tid; e < (c1 - c0) * 18; e += AC_THREADS) sR[e] = R[(int64_t)c0 * 18 + e];
-                __syncthreads();
-                for (int j = warp; j < c1 - c0; j += NW) {
-                    const int32_t i = Rcol[c0 + j];
-                    const int64_t a0 = APrp[i];
-                    const int n = (APrp[i + 1] - (int32_t)a0) * 18;
-                    V *dst = sAP + (int64_t)s_off[j] * 18;
-                    for (int e = lane; e < n; e += 32) dst[e] = AP[a0 * 18 + e];
-                }
-                __syncthreads();
-                for (; l < l1; ++l) {
-                    const uint32_t pk = pairs[l];
-                    if ((int)(pk >> 24) != ch) break;
-                    const V *rb = sR + ((pk >> 16) & 0xffu) * 18 + h * 9;   // rows 3h..3h+2 of R (6 x 3)
-                    const V *ab = sAP + (pk & 0xffffu) * 18;
-#pragma unroll
-                    for (int r = 0; r < 3; ++r)
-#pragma unroll
-                        for (int m = 0; m < 3; ++m) {
-                            const T rv = (T)rb[r * 3 + m];
-#pragma unroll
-                            for (int c = 0; c < 6; ++c) acc[r * 6 + c] += rv * (T)ab[m * 6 + c];
-                        }
-                }
-                __syncthreads();
-            }
-            if (live) {
-                const int64_t J = Accol[q];
-#pragma unroll
-                for (int r = 0; r < 3; ++r)
-#pragma unroll
-                    for (int c = 0; c < 6; ++c) {
-                        const int rr = 3 * h + r;
-                        T v = acc[r * 6 + c];
-                        if (dead[I * 6 + rr] || dead[J * 6 + c]) v = (I == J && rr == c) ? (T)1 : (T)0;
-                        Ac[(int64_t)q * 36 + rr * 6 + c] = (V)v;
-                    }
-            }
-        }
-    }
-}
-
 // Ac block (I,J) = sum over plan pairs P_a' (BC x B) * AP_b (B x BC); dead DOFs get identity.
 // One thread per coarse block.
 template <int B, int BC, typename V = double>
@@ -1073,7 +912,6 @@ static int free_level(Level &l) {
     F(l.Aown.d_row); F(l.P.d_row); F(l.R.d_row); F(l.AP.d_row);
     for (Plan *p : {&l.at_plan, &l.ap_plan, &l.ac_plan}) { F(p->d_ptr); F(p->d_a); F(p->d_b); }
     F(l.Pv); F(l.Rv); F(l.APv); F(l.P32); F(l.R32); F(l.T32); F(l.APv32);
-    F(l.d_tile_row0); F(l.d_tile_kptr); F(l.d_tile_k); F(l.d_tile_kofs); F(l.d_tile_pairs); F(l.d_ac_pairs);
     F(l.x); F(l.rhs); F(l.r); F(l.d); F(l.t); F(l.pv); F(l.x32); F(l.rhs32); F(l.r32); F(l.d32);
     return SG_OK;
 }
@@ -1097,146 +935,6 @@ static int alloc_level_buffers(Level &L, int mixed) {
         if (!rc) rc = dalloc(&L.d32, nb);
     }
     return rc;
-}
-
-// Tiles of k_gather_AP_tiled over a level with 3 x 3 blocks and a 6-vector near-null space
-// (A pattern rp/col, P and AP patterns and the A P plan of L): consecutive block rows while the tile holds at most AP_TILE_THREADS AP
-// blocks, TILE_CAP_A A blocks and TILE_CAP_P staged P blocks.  Each plan pair becomes
-// (A index - first A block of the tile) | (local block of the P block << 16).
-constexpr int TILE_CAP_A = 640, TILE_CAP_P = 1280;
-static int build_ap_tiles(Level &L, const std::vector<int32_t> &rp, const std::vector<int32_t> &col) {
-    const int64_t n = L.n;
-    const Pattern &P = L.P, &AP = L.AP;
-    const Plan &pl = L.ap_plan;
-    std::vector<int32_t> prow(P.nblk);
-    for (int64_t i = 0; i < n; ++i)
-        for (int32_t q = P.rp[i]; q < P.rp[i + 1]; ++q) prow[q] = (int32_t)i;
-    std::vector<int32_t> row0{0}, kptr{0}, klist, kofs, mark(n, -1), loc(n, 0);
-    std::vector<uint32_t> pairs(pl.a.size());
-    int maxA = 0, maxP = 0;
-    int64_t t = 0;
-    for (int64_t r = 0; r < n; ++t) {
-        int nA = 0, nP = 0, nAP = 0;
-        int64_t r1 = r;
-        while (r1 < n) {
-            const int addA = rp[r1 + 1] - rp[r1], addAP = AP.rp[r1 + 1] - AP.rp[r1];
-            int addP = 0;
-            for (int32_t p = rp[r1]; p < rp[r1 + 1]; ++p)
-                if (mark[col[p]] != t) addP += P.rp[col[p] + 1] - P.rp[col[p]];
-            if (r1 > r && (nA + addA > TILE_CAP_A || nP + addP > TILE_CAP_P || nAP + addAP > AP_TILE_THREADS)) break;
-            if (addA > 65535 || nP + addP > 65535 || addAP > AP_TILE_THREADS)
-                return set_error(SG_ERR_NUMERIC, "AMG tile: a block row is too wide for the shared-memory tiles");
-            for (int32_t p = rp[r1]; p < rp[r1 + 1]; ++p) {
-                const int32_t k = col[p];
-                if (mark[k] == t) continue;
-                mark[k] = (int32_t)t;
-                loc[k] = nP;
-                klist.push_back(k);
-                kofs.push_back(nP);
-                nP += P.rp[k + 1] - P.rp[k];
-            }
-            nA += addA;
-            nAP += addAP;
-            ++r1;
-        }
-        for (int32_t q = AP.rp[r]; q < AP.rp[r1]; ++q)
-            for (int64_t l = pl.ptr[q]; l < pl.ptr[q + 1]; ++l) {
-                const int32_t pq = pl.b[l], k = prow[pq];
-                const uint32_t al = (uint32_t)(pl.a[l] - rp[r]);
-                const uint32_t plc = (uint32_t)(loc[k] + (pq - P.rp[k]));
-                pairs[l] = al | (plc << 16);
-            }
-        maxA = std::max(maxA, nA);
-        maxP = std::max(maxP, nP);
-        row0.push_back((int32_t)r1);
-        kptr.push_back((int32_t)klist.size());
-        r = r1;
-    }
-    L.ap_ntiles = t;
-    L.ap_maxA = maxA;
-    L.ap_maxP = maxP;
-    int rc = dup(&L.d_tile_row0, row0);
-    if (!rc) rc = dup(&L.d_tile_kptr, kptr);
-    if (!rc) rc = dup(&L.d_tile_k, klist);
-    if (!rc) rc = dup(&L.d_tile_kofs, kofs);
-    if (!rc) rc = dup(&L.d_tile_pairs, pairs);
-    return rc;
-}
-
-// Packed pairs of k_gather_Ac_chunked for the P'(A P) plan of L (coarse pattern Ac, R = P'
-// with R block k the transpose of P block from[k]).  Returns SG_OK without building anything
-// (the lane-group gather stays in use) when a coarse row has more than 255 chunks.
-static int build_ac_chunks(Level &L, const Pattern &Ac, const std::vector<int32_t> &from) {
-    const Pattern &R = L.R, &AP = L.AP;
-    const Plan &pl = L.ac_plan;
-    for (int64_t I = 0; I < R.nrows; ++I)
-        if ((R.rp[I + 1] - R.rp[I] + AC_CHUNK - 1) / AC_CHUNK > 255) return SG_OK;
-    std::vector<int32_t> rpos(L.P.nblk);
-    for (int64_t I = 0; I < R.nrows; ++I)
-        for (int32_t k = R.rp[I]; k < R.rp[I + 1]; ++k) rpos[from[k]] = k - R.rp[I];
-    std::vector<uint32_t> pairs(pl.a.size());
-    int maxAP = 0, maxblk = 0;
-    std::vector<int32_t> off;
-    for (int64_t I = 0; I < Ac.nrows; ++I) {
-        const int32_t k0 = R.rp[I], nk = R.rp[I + 1] - k0;
-        off.assign(nk, 0);
-        for (int32_t c0 = 0; c0 < nk; c0 += AC_CHUNK) {
-            int acc = 0;
-            for (int32_t j = c0; j < std::min(c0 + AC_CHUNK, nk); ++j) {
-                off[j] = acc;
-                const int32_t i = R.col[k0 + j];
-                acc += AP.rp[i + 1] - AP.rp[i];
-            }
-            maxAP = std::max(maxAP, acc);
-        }
-        maxblk = std::max(maxblk, Ac.rp[I + 1] - Ac.rp[I]);
-        for (int32_t q = Ac.rp[I]; q < Ac.rp[I + 1]; ++q)
-            for (int64_t l = pl.ptr[q]; l < pl.ptr[q + 1]; ++l) {
-                const int32_t rp_ = rpos[pl.a[l]], i = R.col[k0 + rp_];
-                const int32_t apl = off[rp_] + (pl.b[l] - AP.rp[i]);
-                if (apl > 65535) return set_error(SG_ERR_NUMERIC, "AMG chunk: too many A P blocks in one chunk");
-                pairs[l] = (uint32_t)apl | ((uint32_t)(rp_ % AC_CHUNK) << 16) | ((uint32_t)(rp_ / AC_CHUNK) << 24);
-            }
-    }
-    L.ac_maxAP = maxAP;
-    L.ac_maxblk = maxblk;
-    return dup(&L.d_ac_pairs, pairs);
-}
-
-template <typename V>
-static int gather_Ac_chunked(const Level &L, const Level &C, const V *R, const V *AP, V *Ac, cudaStream_t st) {
-    const size_t smem = ((size_t)AC_CHUNK * 18 + (size_t)L.ac_maxAP * 18) * sizeof(V);
-    static thread_local size_t configured[2] = {0, 0};
-    size_t &cfg = configured[sizeof(V) == 8];
-    if (smem > cfg) {
-        SG_CUDA(cudaFuncSetAttribute(k_gather_Ac_chunked<V>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        cfg = smem;
-    }
-    count_launch();
-    const int64_t grid = std::min<int64_t>(C.n, (int64_t)sm_count() * 8);
-    k_gather_Ac_chunked<V><<<(unsigned)std::max<int64_t>(grid, 1), AC_THREADS, smem, st>>>(
-        C.n, L.R.d_rp, L.R.d_col, L.AP.d_rp, C.Aown.d_rp, C.d_Acol, L.ac_plan.d_ptr, L.d_ac_pairs, R, AP, C.d_dead, Ac,
-        L.ac_maxAP);
-    SG_CUDA(cudaGetLastError());
-    return SG_OK;
-}
-
-template <typename V>
-static int gather_AP_tiled(const Level &L, const V *A, const V *P, V *AP, cudaStream_t st) {
-    const size_t smem = ((size_t)L.ap_maxA * 9 + (size_t)L.ap_maxP * 18) * sizeof(V);
-    static thread_local size_t configured[2] = {0, 0};
-    size_t &cfg = configured[sizeof(V) == 8];
-    if (smem > cfg) {
-        SG_CUDA(cudaFuncSetAttribute(k_gather_AP_tiled<V>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        cfg = smem;
-    }
-    count_launch();
-    const int64_t grid = std::min<int64_t>(L.ap_ntiles, (int64_t)sm_count() * 16);
-    k_gather_AP_tiled<V><<<(unsigned)std::max<int64_t>(grid, 1), AP_TILE_THREADS, smem, st>>>(
-        L.ap_ntiles, L.d_tile_row0, L.d_Arp, L.AP.d_rp, L.ap_plan.d_ptr, L.d_tile_pairs, L.d_tile_kptr, L.d_tile_k,
-        L.d_tile_kofs, L.P.d_rp, A, P, AP, L.ap_maxA);
-    SG_CUDA(cudaGetLastError());
-    return SG_OK;
 }
 
 // Structure of the transfer from level L (pattern rp/col, near-null space B) to the next
@@ -1297,17 +995,8 @@ static int setup_transfer(Level &L, const std::vector<int32_t> &rp, const std::v
     if (!rc) rc = upload_pattern(L.R);
     if (!rc) rc = upload_pattern(L.AP);
     if (!rc) rc = upload_plan(L.at_plan);
-    if (!rc && b == 3 && bc == 6) {
-        // tiled A P gather (3 x 3 A blocks, 3 x 6 P blocks): the plan's pair indices live in
-        // the packed tile form only
-        rc = build_ap_tiles(L, rp, col);
-        if (!rc) rc = dup(&L.ap_plan.d_ptr, L.ap_plan.ptr);
-    } else if (!rc) {
-        rc = upload_plan(L.ap_plan);
-    }
-    if (!rc && b == 3 && bc == 6) rc = build_ac_chunks(L, Ac, from);
-    if (!rc && L.d_ac_pairs) rc = dup(&L.ac_plan.d_ptr, L.ac_plan.ptr);
-    else if (!rc) rc = upload_plan(L.ac_plan);
+    if (!rc) rc = upload_plan(L.ap_plan);
+    if (!rc) rc = upload_plan(L.ac_plan);
     if (!rc) rc = dalloc(&L.Pv, (size_t)L.P.nblk * b * bc);
     if (!rc) rc = dalloc(&L.Rv, (size_t)L.P.nblk * b * bc);
     if (!rc) rc = dalloc(&L.APv, (size_t)L.AP.nblk * b * bc);
@@ -1404,20 +1093,14 @@ static int numeric_transfer(sg_amg *h, int l, cudaStream_t st) {
         // faster per thread; P'(A P), ~63 pairs per block, 1.3x faster per warp; the small
         // coarse levels 10-20x faster per warp)
         auto per_warp = [](int64_t nblk, int64_t pairs) { return nblk < 32768 || pairs >= 24 * nblk; };
-        if (L.d_tile_pairs) {
-            const int rc2 = gather_AP_tiled<double>(L, A, L.Pv, L.APv, st);
-            if (rc2) return rc2;
-        } else if (!per_warp(L.AP.nblk, L.ap_pairs))
+        if (!per_warp(L.AP.nblk, L.ap_pairs))
             k_gather_AP<BB, BC><<<grid_for(L.AP.nblk, 128), 128, 0, st>>>(L.AP.nblk, L.ap_plan.d_ptr,
                                                                           L.ap_plan.d_a, L.ap_plan.d_b, A, L.Pv,
                                                                           L.APv);
         else
             gather_AP_groups<BB, BC, double>(L.AP.nblk, L.ap_pairs, L.ap_plan.d_ptr, L.ap_plan.d_a, L.ap_plan.d_b, A,
                                              L.Pv, L.APv, st);
-        if (L.d_ac_pairs) {
-            const int rc3 = gather_Ac_chunked<double>(L, C, L.Rv, L.APv, C.Aown_vals, st);
-            if (rc3) return rc3;
-        } else if (!per_warp(C.Anblk, L.ac_pairs))
+        if (!per_warp(C.Anblk, L.ac_pairs))
             k_gather_Ac<BB, BC><<<grid_for(C.Anblk, 128), 128, 0, st>>>(C.Anblk, C.Aown.d_row, C.d_Acol,
                                                                         L.ac_plan.d_ptr, L.ac_plan.d_a,
                                                                         L.ac_plan.d_b, L.Pv, L.APv, C.d_dead,
@@ -1513,19 +1196,13 @@ static int numeric_update32(sg_amg *h, cudaStream_t st) {
             k_transpose_blocks<BB, BC, float><<<grid_for(L.P.nblk * BB * BC, 256), 256, 0, st>>>(
                 L.P.nblk, L.d_R_from_P, L.P32, L.R32);
             auto per_warp = [](int64_t nblk, int64_t pairs) { return nblk < 32768 || pairs >= 24 * nblk; };
-            if (L.d_tile_pairs) {
-                const int rc2 = gather_AP_tiled<float>(L, L.A32, L.P32, L.APv32, st);
-                if (rc2) return rc2;
-            } else if (!per_warp(L.AP.nblk, L.ap_pairs))
+            if (!per_warp(L.AP.nblk, L.ap_pairs))
                 k_gather_AP<BB, BC, float><<<grid_for(L.AP.nblk, 128), 128, 0, st>>>(
                     L.AP.nblk, L.ap_plan.d_ptr, L.ap_plan.d_a, L.ap_plan.d_b, L.A32, L.P32, L.APv32);
             else
                 gather_AP_groups<BB, BC, float>(L.AP.nblk, L.ap_pairs, L.ap_plan.d_ptr, L.ap_plan.d_a, L.ap_plan.d_b,
                                                 L.A32, L.P32, L.APv32, st);
-            if (L.d_ac_pairs) {
-                const int rc3 = gather_Ac_chunked<float>(L, C, L.R32, L.APv32, C.A32, st);
-                if (rc3) return rc3;
-            } else if (!per_warp(C.Anblk, L.ac_pairs))
+            if (!per_warp(C.Anblk, L.ac_pairs))
                 k_gather_Ac<BB, BC, float><<<grid_for(C.Anblk, 128), 128, 0, st>>>(
                     C.Anblk, C.Aown.d_row, C.d_Acol, L.ac_plan.d_ptr, L.ac_plan.d_a, L.ac_plan.d_b, L.P32, L.APv32,
                     C.d_dead, C.A32);

@@ -258,139 +258,168 @@ __global__ void __launch_bounds__(128) k_assemble_bsr(const int32_t *__restrict_
 //       transposed block is the identity).
 // sym(D) = (D + D')/2 is what the reference's symmetrisation of K_r applies to its unsymmetric
 // sums (CONSTITUTIVE.m:515-532): B' sym(D) B = sym(B' D B).
-constexpr int KE_EPB = 2, KE_TPE = 64;   // elements per CTA, threads per element
+constexpr int KE_EPB = 8, KE_TPE = 18;   // elements per CTA, threads per element (one per chunk)
+constexpr int KE_PITCH = 10;             // doubles per stored element block (9 + 1: 16-byte aligned)
 
-__device__ __forceinline__ void ke_slot_ij(int s, int &i, int &j) {
-    int lo = 0, start = 0;
-    while (s >= start + (10 - lo)) { start += 10 - lo; ++lo; }
-    i = lo;
-    j = lo + (s - start);
-}
+// The 18 chunks of an element's upper node blocks: node j and up to 4 row nodes i0 .. i0+3
+// (i <= j); chunk c owns blocks (i, j) for i in [i0, min(i0 + 4, j + 1)).
+__constant__ int8_t c_ke_j[KE_TPE] = {0, 1, 2, 3, 4, 4, 5, 5, 6, 6, 7, 7, 8, 8, 8, 9, 9, 9};
+__constant__ int8_t c_ke_i0[KE_TPE] = {0, 0, 0, 0, 0, 4, 0, 4, 0, 4, 0, 4, 0, 4, 8, 0, 4, 8};
 
-__global__ void __launch_bounds__(KE_EPB * KE_TPE) k_element_blocks_p2tet(int64_t n_e, int nq,
+__device__ __forceinline__ int ke_slot(int i, int j) { return i * 10 - i * (i - 1) / 2 + (j - i); }
+
+__global__ void __launch_bounds__(KE_EPB * KE_TPE, 3) k_element_blocks_p2tet(int64_t n_e, int nq,
                                                                           const double *__restrict__ dphi,
                                                                           const double *__restrict__ w,
                                                                           const double *__restrict__ DS,
                                                                           double *__restrict__ Ke) {
     extern __shared__ double ke_smem[];
-    const int le = threadIdx.x / KE_TPE, lt = threadIdx.x - le * KE_TPE;
-    const int per = nq * (36 + 30 + 1 + 180);
-    double *sD = ke_smem + le * per;     // [q][36] column-major 6x6
-    double *sPhi = sD + nq * 36;         // [q][d][i]
-    double *sW = sPhi + nq * 30;         // [q]
-    double *sDB = sW + nq;               // [q][col = 3 j + c][a]: w_q sym(D_q) B_q(:, col)
+    const int per = nq * (36 + 30 + 1);
+    const int le = threadIdx.x / KE_TPE, lc = threadIdx.x - le * KE_TPE;
+    const int j = c_ke_j[lc], i0 = c_ke_i0[lc];
     for (int64_t e0 = (int64_t)blockIdx.x * KE_EPB; e0 < n_e; e0 += (int64_t)gridDim.x * KE_EPB) {
-        const int64_t e = e0 + le;
-        const bool live = e < n_e;
-        if (live) {
-            const int64_t g0 = e * nq;
-            for (int t = lt; t < nq * 36; t += KE_TPE) sD[t] = DS[g0 * 36 + t];
-            for (int t = lt; t < nq * 30; t += KE_TPE) sPhi[t] = dphi[g0 * 30 + t];
-            for (int t = lt; t < nq; t += KE_TPE) sW[t] = w[g0 + t];
+        // stage the CTA's elements: sym(D) per point, gradients [q][d][i], weights
+        const int64_t ne_here = n_e - e0 < KE_EPB ? n_e - e0 : KE_EPB;
+        __syncthreads();
+        for (int t = threadIdx.x; t < ne_here * nq * 36; t += blockDim.x) {
+            const int64_t ge = t / 36;                         // element-local point index (el * nq + q)
+            const int k = t - (int)ge * 36, a = k % 6, b = k / 6;
+            const double *D = DS + (e0 * nq + ge) * 36;
+            const int el = (int)(ge / nq);
+            ke_smem[el * per + (ge - (int64_t)el * nq) * 36 + k] = 0.5 * (D[a + 6 * b] + D[b + 6 * a]);
+        }
+        for (int t = threadIdx.x; t < ne_here * nq * 30; t += blockDim.x) {
+            const int el = t / (nq * 30), r = t - el * nq * 30;
+            ke_smem[el * per + nq * 36 + r] = dphi[(e0 * nq) * 30 + t];
+        }
+        for (int t = threadIdx.x; t < ne_here * nq; t += blockDim.x) {
+            const int el = t / nq, q = t - el * nq;
+            ke_smem[el * per + nq * 66 + q] = w[e0 * nq + t];
         }
         __syncthreads();
-        if (live) {
-            for (int t = lt; t < nq * 30; t += KE_TPE) {
-                const int q = t / 30, col = t - q * 30, j = col / 3, c = col - j * 3;
-                const double *D = sD + q * 36;
-                int r[3];
-                double v[3];
-                bcol<3>(sPhi + q * 30, 10, j, c, r, v);
-                const double wq = sW[q];
+        if (le < ne_here) {
+            const double *sD = ke_smem + le * per, *sPhi = sD + nq * 36, *sW = sPhi + nq * 30;
+            double acc[4][9];
 #pragma unroll
-                for (int a = 0; a < 6; ++a) {
-                    double x = 0.0;
+            for (int ii = 0; ii < 4; ++ii)
 #pragma unroll
-                    for (int u = 0; u < 3; ++u) x += 0.5 * (D[a + 6 * r[u]] + D[r[u] + 6 * a]) * v[u];
-                    sDB[t * 6 + a] = wq * x;
-                }
-            }
-        }
-        __syncthreads();
-        if (live && lt < 55) {
-            int i, j;
-            ke_slot_ij(lt, i, j);
-            double acc[9];
-#pragma unroll
-            for (int k = 0; k < 9; ++k) acc[k] = 0.0;
+                for (int k = 0; k < 9; ++k) acc[ii][k] = 0.0;
             for (int q = 0; q < nq; ++q) {
-                const double *d = sPhi + q * 30;
-                const double *db = sDB + (q * 30 + 3 * j) * 6;
+                const double *D = sD + q * 36, *d = sPhi + q * 30;
+                const double wq = sW[q];
+                // w sym(D) B(:, (j, cj)) for the three components of node j
+                double db[3][6];
 #pragma unroll
-                for (int ci = 0; ci < 3; ++ci) {
+                for (int cj = 0; cj < 3; ++cj) {
                     int r[3];
                     double v[3];
-                    bcol<3>(d, 10, i, ci, r, v);
+                    bcol<3>(d, 10, j, cj, r, v);
 #pragma unroll
-                    for (int cj = 0; cj < 3; ++cj) {
-                        if (i == j && cj < ci) continue;
-                        const double *x = db + cj * 6;
-                        acc[ci * 3 + cj] += v[0] * x[r[0]] + v[1] * x[r[1]] + v[2] * x[r[2]];
+                    for (int a = 0; a < 6; ++a)
+                        db[cj][a] = wq * (D[a + 6 * r[0]] * v[0] + D[a + 6 * r[1]] * v[1] + D[a + 6 * r[2]] * v[2]);
+                }
+#pragma unroll
+                for (int ii = 0; ii < 4; ++ii) {
+                    const int i = i0 + ii;
+                    if (i > j) break;
+#pragma unroll
+                    for (int ci = 0; ci < 3; ++ci) {
+                        int r[3];
+                        double v[3];
+                        bcol<3>(d, 10, i, ci, r, v);
+#pragma unroll
+                        for (int cj = 0; cj < 3; ++cj)
+                            acc[ii][ci * 3 + cj] += v[0] * db[cj][r[0]] + v[1] * db[cj][r[1]] + v[2] * db[cj][r[2]];
                     }
                 }
             }
-            if (i == j) {
-                acc[3] = acc[1];
-                acc[6] = acc[2];
-                acc[7] = acc[5];
-            }
-            double *out = Ke + (e * 55 + lt) * 9;
+            const int64_t e = e0 + le;
 #pragma unroll
-            for (int k = 0; k < 9; ++k) out[k] = acc[k];
+            for (int ii = 0; ii < 4; ++ii) {
+                const int i = i0 + ii;
+                if (i > j) break;
+                if (i == j) {   // diagonal node block: its upper triangle, mirrored (exactly symmetric)
+                    acc[ii][3] = acc[ii][1];
+                    acc[ii][6] = acc[ii][2];
+                    acc[ii][7] = acc[ii][5];
+                }
+                double *out = Ke + (e * 55 + ke_slot(i, j)) * KE_PITCH;
+#pragma unroll
+                for (int k = 0; k < 9; ++k) out[k] = acc[ii][k];
+            }
         }
-        __syncthreads();
     }
 }
 
+// A warp sums the contributions of 32 consecutive blocks (a lane per block, its element
+// blocks read as five 16-byte words), then writes the 32 results as one contiguous run through
+// shared memory (and reads K_el for the blend the same way).
+constexpr int KG_WARPS = 8;
 template <bool BLEND>
-__global__ void k_gather_blocks3(int64_t n_blocks, const int32_t *__restrict__ cptr,
-                                 const uint32_t *__restrict__ contrib, const double *__restrict__ Ke,
-                                 const int32_t *__restrict__ row_of, const int32_t *__restrict__ col,
-                                 const double *__restrict__ mask, double r, const double *__restrict__ Kel,
-                                 double *__restrict__ Kout) {
-    for (int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; p < n_blocks;
-         p += (int64_t)gridDim.x * blockDim.x) {
+__global__ void __launch_bounds__(KG_WARPS * 32) k_gather_blocks3(int64_t n_blocks, const int32_t *__restrict__ cptr,
+                                                                  const uint32_t *__restrict__ contrib,
+                                                                  const double *__restrict__ Ke,
+                                                                  const int32_t *__restrict__ row_of,
+                                                                  const int32_t *__restrict__ col,
+                                                                  const double *__restrict__ mask, double r,
+                                                                  const double *__restrict__ Kel,
+                                                                  double *__restrict__ Kout) {
+    __shared__ double sOut[KG_WARPS][32 * 9];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    double *so = sOut[warp];
+    const int64_t stride = (int64_t)gridDim.x * KG_WARPS * 32;
+    for (int64_t base = ((int64_t)blockIdx.x * KG_WARPS + warp) * 32; base < n_blocks; base += stride) {
+        const int64_t p = base + lane;
         double acc[9];
 #pragma unroll
         for (int k = 0; k < 9; ++k) acc[k] = 0.0;
-        for (int32_t l = cptr[p]; l < cptr[p + 1]; ++l) {
-            const uint32_t src = contrib[l];
-            const double *v = Ke + (int64_t)(src & 0x7fffffffu) * 9;
-            double x[9];
+        if (p < n_blocks) {
+            for (int32_t l = cptr[p]; l < cptr[p + 1]; ++l) {
+                const uint32_t src = contrib[l];
+                const double2 *v = reinterpret_cast<const double2 *>(Ke + (int64_t)(src & 0x7fffffffu) * KE_PITCH);
+                double x[10];
 #pragma unroll
-            for (int k = 0; k < 9; ++k) x[k] = __ldg(v + k);
-            if (src >> 31) {
+                for (int h = 0; h < 5; ++h) {
+                    const double2 t = __ldg(v + h);
+                    x[2 * h] = t.x;
+                    x[2 * h + 1] = t.y;
+                }
+                if (src >> 31) {
 #pragma unroll
-                for (int a = 0; a < 3; ++a)
+                    for (int a = 0; a < 3; ++a)
 #pragma unroll
-                    for (int b = 0; b < 3; ++b) acc[a * 3 + b] += x[b * 3 + a];
-            } else {
+                        for (int b = 0; b < 3; ++b) acc[a * 3 + b] += x[b * 3 + a];
+                } else {
 #pragma unroll
-                for (int k = 0; k < 9; ++k) acc[k] += x[k];
+                    for (int k = 0; k < 9; ++k) acc[k] += x[k];
+                }
             }
         }
-        if (BLEND) {
-            const int64_t I = row_of[p], J = col[p];
 #pragma unroll
-            for (int a = 0; a < 3; ++a)
-#pragma unroll
-                for (int b = 0; b < 3; ++b) {
-                    const bool free = mask[I * 3 + a] != 0.0 && mask[J * 3 + b] != 0.0;
-                    const double el = Kel ? Kel[p * 9 + a * 3 + b] : 0.0;
-                    Kout[p * 9 + a * 3 + b] = free ? r * el + (1.0 - r) * acc[a * 3 + b]
-                                                   : ((I == J && a == b) ? 1.0 : 0.0);
-                }
-        } else {
-#pragma unroll
-            for (int k = 0; k < 9; ++k) Kout[p * 9 + k] = acc[k];
+        for (int k = 0; k < 9; ++k) so[lane * 9 + k] = acc[k];
+        __syncwarp();
+        const int cnt = (int)(n_blocks - base < 32 ? n_blocks - base : 32);
+        for (int idx = lane; idx < cnt * 9; idx += 32) {
+            const int pl = idx / 9, k = idx - pl * 9;
+            const int64_t o = base * 9 + idx;
+            double v = so[idx];
+            if (BLEND) {
+                const int64_t pb = base + pl, I = row_of[pb], J = col[pb];
+                const int a = k / 3, b = k - a * 3;
+                const bool free = mask[I * 3 + a] != 0.0 && mask[J * 3 + b] != 0.0;
+                const double el = Kel ? Kel[o] : 0.0;
+                v = free ? r * el + (1.0 - r) * v : ((I == J && a == b) ? 1.0 : 0.0);
+            }
+            Kout[o] = v;
         }
+        __syncwarp();
     }
 }
 
 // Element blocks of the deterministic path into m->d_ke (allocated on first use).
 static int element_blocks(sg_mesh *m, const double *DS, cudaStream_t st) {
-    if (!m->d_ke) SG_CUDA(device_alloc(&m->d_ke, sizeof(double) * (size_t)m->n_e * 55 * 9));
-    const size_t smem = sizeof(double) * (size_t)KE_EPB * m->nq * (36 + 30 + 1 + 180);
+    if (!m->d_ke) SG_CUDA(device_alloc(&m->d_ke, sizeof(double) * (size_t)m->n_e * 55 * KE_PITCH));
+    const size_t smem = sizeof(double) * (size_t)KE_EPB * m->nq * (36 + 30 + 1);
     static thread_local size_t configured = 0;
     if (smem > configured) {
         SG_CUDA(cudaFuncSetAttribute(k_element_blocks_p2tet, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
@@ -398,7 +427,7 @@ static int element_blocks(sg_mesh *m, const double *DS, cudaStream_t st) {
     }
     count_launch();
     const int64_t ctas = (m->n_e + KE_EPB - 1) / KE_EPB;
-    const unsigned grid = (unsigned)std::max<int64_t>(1, std::min<int64_t>(ctas, (int64_t)sm_count() * 16));
+    const unsigned grid = (unsigned)std::max<int64_t>(1, std::min<int64_t>(ctas, (int64_t)sm_count() * 8));
     k_element_blocks_p2tet<<<grid, KE_EPB * KE_TPE, smem, st>>>(m->n_e, m->nq, m->d_dphi, m->d_w, DS, m->d_ke);
     SG_CUDA(cudaGetLastError());
     return SG_OK;
@@ -524,7 +553,7 @@ extern "C" int sg_assemble_bsr_dev(const sg_mesh *m_, const double *DS, double *
         const InstrToken tk = instr_begin(IK_ASSEMBLY, st);
         int rc = element_blocks(m, DS, st);
         if (!rc) {
-            k_gather_blocks3<false><<<grid_for(m->bsr.n_blocks, 256), 256, 0, st>>>(
+            k_gather_blocks3<false><<<grid_for(m->bsr.n_blocks, KG_WARPS * 32, 8), KG_WARPS * 32, 0, st>>>(
                 m->bsr.n_blocks, m->d_contrib_ptr, m->d_contrib, m->d_ke, nullptr, nullptr, nullptr, 0.0, nullptr, K);
             if (cudaGetLastError() != cudaSuccess) rc = set_error(SG_ERR_CUDA, "k_gather_blocks3 launch");
         }
@@ -598,7 +627,7 @@ extern "C" int sg_assemble_kr_dev(sg_mesh *m, const double *DS, double r, const 
         const InstrToken tk = instr_begin(IK_ASSEMBLY, st);
         int rc = element_blocks(m, DS, st);
         if (!rc) {
-            k_gather_blocks3<true><<<grid_for(m->bsr.n_blocks, 256), 256, 0, st>>>(
+            k_gather_blocks3<true><<<grid_for(m->bsr.n_blocks, KG_WARPS * 32, 8), KG_WARPS * 32, 0, st>>>(
                 m->bsr.n_blocks, m->d_contrib_ptr, m->d_contrib, m->d_ke, m->bsr.d_row_of, m->bsr.d_col, m->d_mask, r,
                 Kel, Kr);
             if (cudaGetLastError() != cudaSuccess) rc = set_error(SG_ERR_CUDA, "k_gather_blocks3 launch");

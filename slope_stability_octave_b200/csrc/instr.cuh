@@ -19,7 +19,8 @@ enum InstrKind {
                              // (these may run beside an AMG update on another stream)
     IK_RESIDUAL = 9,     // fused stress-only residual F = B'(w S(B U))
     IK_SPMM_AORTH = 10,  // FP64 node-block SpMM (several vectors per pass) of the A-orthogonalisation
-    IK_COUNT = 11
+    IK_AORTH = 11,       // the whole A-orthogonalisation of a deflation basis (units: basis columns)
+    IK_COUNT = 12
 };
 
 // Units of work done by launches of a kind (e.g. vectors multiplied by one SpMM launch), added

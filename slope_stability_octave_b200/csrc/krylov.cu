@@ -56,6 +56,9 @@ struct sg_krylov {
     uint64_t gkey = 0;
     int64_t launches_start = 0, launches_body = 0, launches_end = 0;
     int use_graph = 1;
+    // blocked A-orthogonalisation: A times the block's input columns (n x 16), the block's
+    // coefficients against earlier columns (256 x 16) and the per-CTA partial sums
+    double *atb = nullptr, *cblk = nullptr, *tspart = nullptr;
 };
 
 namespace sg {
@@ -421,6 +424,7 @@ extern "C" int sg_krylov_destroy(sg_krylov *ws) {
     cudaFree(ws->part); cudaFree(ws->hd); cudaFree(ws->Worth); cudaFree(ws->AWorth); cudaFree(ws->nt);
     cudaFree(ws->sig);
     graph_release(ws);
+    cudaFree(ws->atb); cudaFree(ws->cblk); cudaFree(ws->tspart);
     cudaFree(ws->u); cudaFree(ws->dstate); cudaFree(ws->dscal); cudaFree(ws->dH); cudaFree(ws->dcs);
     cudaFree(ws->dsn); cudaFree(ws->dg); cudaFree(ws->dy); cudaFree(ws->dhist); cudaFree(ws->dptr);
     if (ws->cap) cudaStreamDestroy(ws->cap);
@@ -569,12 +573,19 @@ extern "C" int sg_a_orthogonalize(sg_krylov *ws, const sg_bsr *A, const double *
     const cudaStream_t st = as_stream(stream);
     if (k == 0) { *k_out = 0; return SG_OK; }
     const InstrRedirect redirect(IK_SPMV3_F64, IK_SPMV3_F64_AORTH);
+    const InstrToken tk_all = instr_begin(IK_AORTH, st);
+    instr_units(IK_AORTH, k);
+    struct EndAll {
+        const InstrToken &t;
+        cudaStream_t s;
+        ~EndAll() { instr_end(t, s); }
+    } end_all{tk_all, st};
     int rc = ensure_kcap(ws, k);
     if (rc) return rc;
     // Wo, AWo: the A-orthonormalised columns and A times them, in processing order; nt[i] is
     // column i's A-norm^2 and sig[i] its sign (kept, scaled and signed on the device, so the
     // loop needs no host round trip; dropped columns are left as zeros).
-    double *Wo = ws->Worth, *AWo = ws->AWorth, *At = ws->t, *tmp = ws->w, *part = ws->part, *c = ws->hd;
+    double *Wo = ws->Worth, *AWo = ws->AWorth, *part = ws->part, *c = ws->hd;
     double *nt = ws->nt, *sig = ws->sig;
     const unsigned gb = grid_for(n, 256, 8);
     // A times every input column up front (processing order i takes column k - 1 - i): the
@@ -587,22 +598,49 @@ extern "C" int sg_a_orthogonalize(sg_krylov *ws, const sg_bsr *A, const double *
             rc = bsr_spmv<double, double>(*A, Avals, W + (int64_t)(k - 1 - i) * n, AWo + (int64_t)i * n, 1.0, 0.0, st);
     }
     if (rc) return rc;
-    for (int i = 0; i < k && !rc; ++i) {
-        const double *src = W + (int64_t)(k - 1 - i) * n;
-        double *col_i = Wo + (int64_t)i * n, *acol_i = AWo + (int64_t)i * n;
-        SG_CUDA(cudaMemcpyAsync(At, acol_i, sizeof(double) * n, cudaMemcpyDeviceToDevice, st));
-        SG_CUDA(cudaMemcpyAsync(tmp, src, sizeof(double) * n, cudaMemcpyDeviceToDevice, st));
-        if (i > 0) {
-            // c_j = sig_j (A src)' u_j ;  tmp -= sum c_j u_j ;  A tmp = A src - sum c_j A u_j
-            if ((rc = multidot(n, i, Wo, n, At, part, c, st))) break;
-            count_launch();
-            k_mul_sign<<<1, 256, 0, st>>>(i, c, sig);
-            if ((rc = gemv_sub(n, i, Wo, n, c, tmp, st))) break;
-            if ((rc = gemv_sub(n, i, AWo, n, c, acol_i, st))) break;
+    // Blocked one-pass Gram-Schmidt: columns are processed in blocks of AORTH_BLOCK; a block's
+    // coefficients against all earlier (final) columns come from one tall-skinny product
+    // c = diag(sig) U' (A S_blk), applied to the block's columns and their A-images by two more,
+    // then the columns inside the block are treated one after another as before.  Every
+    // coefficient is sig_j (A src_i)' u_j as in the column-by-column loop, so the result is the
+    // same one-pass A-orthogonalisation summed in another order; the earlier columns are read
+    // a few times per block instead of three times per column.
+    constexpr int AORTH_BLOCK = 16;
+    if (!ws->atb) {
+        SG_CUDA(device_alloc(&ws->atb, sizeof(double) * n * AORTH_BLOCK));
+        SG_CUDA(device_alloc(&ws->cblk, sizeof(double) * 256 * AORTH_BLOCK));
+        SG_CUDA(device_alloc(&ws->tspart, sizeof(double) * TS_PART_CTAS * 256 * AORTH_BLOCK));
+    }
+    for (int i0 = 0; i0 < k && !rc; i0 += AORTH_BLOCK) {
+        const int b = std::min(AORTH_BLOCK, k - i0);
+        double *WoB = Wo + (int64_t)i0 * n, *AWoB = AWo + (int64_t)i0 * n;
+        // A src of the block's columns (kept: AWo's columns change below) and src itself
+        SG_CUDA(cudaMemcpyAsync(ws->atb, AWoB, sizeof(double) * n * b, cudaMemcpyDeviceToDevice, st));
+        for (int l = 0; l < b; ++l)
+            SG_CUDA(cudaMemcpyAsync(WoB + (int64_t)l * n, W + (int64_t)(k - 1 - i0 - l) * n, sizeof(double) * n,
+                                    cudaMemcpyDeviceToDevice, st));
+        for (int j0 = 0; j0 < i0 && !rc; j0 += 256) {
+            const int mj = std::min(256, i0 - j0);
+            rc = gemm_tn(n, mj, b, Wo + (int64_t)j0 * n, n, ws->atb, n, sig + j0, ws->cblk, mj, ws->tspart, st);
+            if (!rc) rc = gemm_nn_sub(n, mj, b, Wo + (int64_t)j0 * n, n, ws->cblk, mj, WoB, n, st);
+            if (!rc) rc = gemm_nn_sub(n, mj, b, AWo + (int64_t)j0 * n, n, ws->cblk, mj, AWoB, n, st);
         }
-        if ((rc = multidot(n, 1, tmp, n, At, part, nt + i, st))) break;
-        k_anorm_scale<<<gb, 256, 0, st>>>(n, nt + i, eps_add, tmp, col_i, acol_i, sig + i);
-        SG_CUDA(cudaGetLastError());
+        for (int l = 0; l < b && !rc; ++l) {
+            const int i = i0 + l;
+            const double *At_i = ws->atb + (int64_t)l * n;
+            double *col_i = Wo + (int64_t)i * n, *acol_i = AWo + (int64_t)i * n;
+            if (l > 0) {
+                // c_j = sig_j (A src)' u_j for the block's earlier columns
+                if ((rc = multidot(n, l, WoB, n, At_i, part, c, st))) break;
+                count_launch();
+                k_mul_sign<<<1, 256, 0, st>>>(l, c, sig + i0);
+                if ((rc = gemv_sub(n, l, WoB, n, c, col_i, st))) break;
+                if ((rc = gemv_sub(n, l, AWoB, n, c, acol_i, st))) break;
+            }
+            if ((rc = multidot(n, 1, col_i, n, At_i, part, nt + i, st))) break;
+            k_anorm_scale<<<gb, 256, 0, st>>>(n, nt + i, eps_add, col_i, col_i, acol_i, sig + i);
+            SG_CUDA(cudaGetLastError());
+        }
     }
     if (rc) return rc;
     std::vector<double> nth(k);

@@ -316,25 +316,38 @@ __global__ void __launch_bounds__(256) k_spmm3(int64_t nrows, const int32_t *__r
     }
 }
 
+template <int KC>
+static void spmm_pass(const sg_bsr &A, int G, const double *vals, const double *X, int64_t ldx, double *Y,
+                      int64_t ldy, int kc, cudaStream_t st) {
+    const unsigned grid = grid_for(A.n_rows * G, 256, 16);
+    switch (G) {
+        case 32: k_spmm3<32, KC><<<grid, 256, 0, st>>>(A.n_rows, A.d_row_ptr, A.d_col, vals, X, ldx, Y, ldy, kc); break;
+        case 16: k_spmm3<16, KC><<<grid, 256, 0, st>>>(A.n_rows, A.d_row_ptr, A.d_col, vals, X, ldx, Y, ldy, kc); break;
+        default: k_spmm3<8, KC><<<grid, 256, 0, st>>>(A.n_rows, A.d_row_ptr, A.d_col, vals, X, ldx, Y, ldy, kc); break;
+    }
+}
+
 int bsr_spmm(const sg_bsr &A, const double *vals, const double *X, int64_t ldx, double *Y, int64_t ldy, int k,
              cudaStream_t st) {
     if (A.b != 3) return set_error(SG_ERR_ARG, "bsr_spmm: 3x3 blocks only");
     const double avg = A.n_rows > 0 ? (double)A.n_blocks / (double)A.n_rows : 8.0;
     // the same lanes per row as the single-vector SpMV (bitwise-equal columns)
     const int G = avg >= 16.0 ? 32 : (avg >= 8.0 ? 16 : 8);
-    constexpr int KC = 8;
-    for (int c0 = 0; c0 < k; c0 += KC) {
-        const int kc = std::min(KC, k - c0);
+    // Columns per pass: every block row gathers x entries of its ~28 neighbours from each
+    // column, so the pass's input vectors must stay resident in L2 (126 MB) to be read from
+    // DRAM about once; keep them within ~48 MB (8 columns on meshes up to 0.6M nodes, 2 on the
+    // 3M-DOF slope) and read the matrix once per pass.
+    const double vec_bytes = 8.0 * (double)A.n_rows * 3;
+    const int kcmax = vec_bytes * 8 <= 48e6 ? 8 : (vec_bytes * 4 <= 48e6 ? 4 : (vec_bytes * 2 <= 48e6 ? 2 : 1));
+    for (int c0 = 0; c0 < k; c0 += kcmax) {
+        const int kc = std::min(kcmax, k - c0);
         const InstrToken tk = instr_begin(IK_SPMM_AORTH, st);
         instr_units(IK_SPMM_AORTH, kc);
-        const unsigned grid = grid_for(A.n_rows * G, 256, 16);
         const double *Xc = X + c0 * ldx;
         double *Yc = Y + c0 * ldy;
-        switch (G) {
-            case 32: k_spmm3<32, KC><<<grid, 256, 0, st>>>(A.n_rows, A.d_row_ptr, A.d_col, vals, Xc, ldx, Yc, ldy, kc); break;
-            case 16: k_spmm3<16, KC><<<grid, 256, 0, st>>>(A.n_rows, A.d_row_ptr, A.d_col, vals, Xc, ldx, Yc, ldy, kc); break;
-            default: k_spmm3<8, KC><<<grid, 256, 0, st>>>(A.n_rows, A.d_row_ptr, A.d_col, vals, Xc, ldx, Yc, ldy, kc); break;
-        }
+        if (kcmax == 8) spmm_pass<8>(A, G, vals, Xc, ldx, Yc, ldy, kc, st);
+        else if (kcmax == 4) spmm_pass<4>(A, G, vals, Xc, ldx, Yc, ldy, kc, st);
+        else spmm_pass<2>(A, G, vals, Xc, ldx, Yc, ldy, kc, st);
         instr_end(tk, st);
         SG_CUDA(cudaGetLastError());
     }
@@ -525,6 +538,113 @@ int gemv_sub(int64_t n, int m, const double *V, int64_t ldv, const double *h, do
 int gemv_add(int64_t n, int m, const double *V, int64_t ldv, const double *y, double *x, cudaStream_t st) {
     if (m <= 0) return SG_OK;
     k_gemv<1><<<grid_for(n, 256, 8), 256, sizeof(double) * m, st>>>(n, m, V, ldv, y, x);
+    SG_CUDA(cudaGetLastError());
+    return SG_OK;
+}
+
+// ------------------------------------------------------------------ tall-skinny block products
+//
+// For the blocked Gram-Schmidt of the A-orthogonalisation: C = U' X with U an n x m basis and
+// X an n x b block (b <= TS_B), and Y -= U C.  Each of TS_CTAS CTAs owns a contiguous row range
+// and runs over it in tiles of TS_ROWS rows: the tile's X rows and, 16 columns at a time, its
+// U rows are staged in shared memory and thread (j, l) adds U(r, j) X(r, l) over the tile's rows;
+// the CTAs' partial sums are then added in CTA order (bitwise reproducible).  U is read once
+// for the whole block instead of once per column of X.
+constexpr int TS_B = 16, TS_ROWS = 32, TS_CTAS = 296, TS_MAXM = 256;
+
+__global__ void __launch_bounds__(256) k_gemm_tn_partial(int64_t n, int m, int b, const double *__restrict__ U,
+                                                         int64_t ldu, const double *__restrict__ X, int64_t ldx,
+                                                         double *__restrict__ part) {
+    __shared__ double sX[TS_ROWS][TS_B];
+    __shared__ double sU[TS_ROWS][17];
+    const int t = threadIdx.x, jj = t >> 4, ll = t & 15;
+    const int64_t chunk = (n + gridDim.x - 1) / gridDim.x;
+    const int64_t r0 = blockIdx.x * chunk, r1 = min(n, r0 + chunk);
+    constexpr int MAXG = TS_MAXM / 16;
+    double acc[MAXG];
+#pragma unroll
+    for (int g = 0; g < MAXG; ++g) acc[g] = 0.0;
+    const int ng = (m + 15) / 16;
+    for (int64_t rt = r0; rt < r1; rt += TS_ROWS) {
+        const int nr = (int)min((int64_t)TS_ROWS, r1 - rt);
+        __syncthreads();
+        for (int e = t; e < TS_ROWS * TS_B; e += 256) {
+            const int r = e % TS_ROWS, l = e / TS_ROWS;
+            sX[r][l] = (r < nr && l < b) ? X[l * ldx + rt + r] : 0.0;
+        }
+#pragma unroll
+        for (int g = 0; g < MAXG; ++g) {
+            if (g < ng) {
+                __syncthreads();
+                for (int e = t; e < TS_ROWS * 16; e += 256) {
+                    const int r = e % TS_ROWS, j = e / TS_ROWS, jc = g * 16 + j;
+                    sU[r][j] = (r < nr && jc < m) ? U[jc * ldu + rt + r] : 0.0;
+                }
+                __syncthreads();
+                double a = acc[g];
+#pragma unroll 8
+                for (int r = 0; r < TS_ROWS; ++r) a += sU[r][jj] * sX[r][ll];
+                acc[g] = a;
+            }
+        }
+    }
+#pragma unroll
+    for (int g = 0; g < MAXG; ++g) {
+        const int j = g * 16 + jj;
+        if (g < ng && j < m && ll < b) part[((int64_t)blockIdx.x * m + j) * TS_B + ll] = acc[g];
+    }
+}
+
+// C(j, l) = sign(j) * sum over CTAs of the partials (sign may be null)
+__global__ void k_gemm_tn_reduce(int m, int b, int nparts, const double *__restrict__ part,
+                                 const double *__restrict__ sign, double *__restrict__ C, int ldc) {
+    for (int o = blockIdx.x * blockDim.x + threadIdx.x; o < m * b; o += gridDim.x * blockDim.x) {
+        const int j = o / b, l = o - j * b;
+        double s = 0.0;
+        for (int p = 0; p < nparts; ++p) s += part[((int64_t)p * m + j) * TS_B + l];
+        C[j + (int64_t)l * ldc] = sign ? s * sign[j] : s;
+    }
+}
+
+// Y(:, l) -= U(:, 0:m) C(:, l) for l < b; C is m x b column-major (ldc), staged in shared memory
+__global__ void __launch_bounds__(256) k_gemm_nn_sub(int64_t n, int m, int b, const double *__restrict__ U,
+                                                     int64_t ldu, const double *__restrict__ C, int ldc,
+                                                     double *__restrict__ Y, int64_t ldy) {
+    extern __shared__ double sC[];   // [j][l], m x TS_B
+    for (int e = threadIdx.x; e < m * TS_B; e += blockDim.x) {
+        const int j = e / TS_B, l = e - j * TS_B;
+        sC[e] = l < b ? C[j + (int64_t)l * ldc] : 0.0;
+    }
+    __syncthreads();
+    for (int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; r < n; r += (int64_t)gridDim.x * blockDim.x) {
+        double y[TS_B];
+#pragma unroll
+        for (int l = 0; l < TS_B; ++l) y[l] = 0.0;
+        for (int j = 0; j < m; ++j) {
+            const double u = U[j * ldu + r];
+#pragma unroll
+            for (int l = 0; l < TS_B; ++l) y[l] += u * sC[j * TS_B + l];
+        }
+        for (int l = 0; l < b; ++l) Y[l * ldy + r] -= y[l];
+    }
+}
+
+int gemm_tn(int64_t n, int m, int b, const double *U, int64_t ldu, const double *X, int64_t ldx,
+            const double *sign, double *C, int ldc, double *part, cudaStream_t st) {
+    if (m <= 0 || b <= 0) return SG_OK;
+    if (m > TS_MAXM || b > TS_B) return set_error(SG_ERR_ARG, "gemm_tn: block too large");
+    count_launch(2);
+    k_gemm_tn_partial<<<TS_CTAS, 256, 0, st>>>(n, m, b, U, ldu, X, ldx, part);
+    k_gemm_tn_reduce<<<(m * b + 255) / 256, 256, 0, st>>>(m, b, TS_CTAS, part, sign, C, ldc);
+    SG_CUDA(cudaGetLastError());
+    return SG_OK;
+}
+
+int gemm_nn_sub(int64_t n, int m, int b, const double *U, int64_t ldu, const double *C, int ldc, double *Y,
+                int64_t ldy, cudaStream_t st) {
+    if (m <= 0 || b <= 0) return SG_OK;
+    if (m > TS_MAXM || b > TS_B) return set_error(SG_ERR_ARG, "gemm_nn_sub: block too large");
+    k_gemm_nn_sub<<<grid_for(n, 256, 8), 256, sizeof(double) * m * TS_B, st>>>(n, m, b, U, ldu, C, ldc, Y, ldy);
     SG_CUDA(cudaGetLastError());
     return SG_OK;
 }

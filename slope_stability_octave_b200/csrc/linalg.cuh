@@ -48,6 +48,15 @@ int h3_spmv(int64_t nrows, int64_t nblk, const int32_t *rp, const int32_t *col, 
 // magnitudes beyond the FP16 range are clamped)
 int to_float_half3(int64_t nblk, const double *A, float *A32, uint2 *A16, float scale, cudaStream_t st);
 
+// Tall-skinny block products (blocked Gram-Schmidt): C = diag(sign) U' X (U n x m with m <= 256,
+// X n x b with b <= 16; C column-major m x b, ldc; part: 296 * m * 16 doubles of scratch),
+// deterministic; and Y -= U C.
+constexpr int TS_PART_CTAS = 296;
+int gemm_tn(int64_t n, int m, int b, const double *U, int64_t ldu, const double *X, int64_t ldx,
+            const double *sign, double *C, int ldc, double *part, cudaStream_t st);
+int gemm_nn_sub(int64_t n, int m, int b, const double *U, int64_t ldu, const double *C, int ldc, double *Y,
+                int64_t ldy, cudaStream_t st);
+
 // Device-count variants for graph-replayed loops: m = min(cnt[0] + add, mmax) columns, basis
 // V, or *Vp when V is null (both on the device)
 int multidot_dc(int64_t n, const int32_t *cnt, int add, int mmax, const double *V, const double *const *Vp,

@@ -39,7 +39,7 @@ struct sg_mesh {
     // upper node-block slot s of that element, transposed flag in bit 31) in element order
     int32_t *d_contrib_ptr = nullptr; // n_blocks + 1
     uint32_t *d_contrib = nullptr;    // n_e * np * np entries: e * 55 + s | transposed << 31
-    double *d_ke = nullptr;           // n_e * 55 * 9: element upper node blocks (allocated on first use)
+    double *d_ke = nullptr;           // n_e * 55 * 10: element upper node blocks, 9 values + 1 pad (allocated on first use)
     int device = 0;
 };
 

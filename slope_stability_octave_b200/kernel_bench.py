@@ -118,7 +118,8 @@ def main(argv=None):
     specs = {
         "sds": (sds, n * 416, "k_mc3d (S and DS)"),
         "s": (s_only, n * 128, "k_mc3d (S only)"),
-        "assembly": (lambda: dm.assemble(DS, K), dm.n_e * 5896 + nnz_vals * 8, "k_assemble_bsr"),
+        "assembly": (lambda: dm.assemble(DS, K), dm.n_e * 5896 + nnz_vals * 8,
+                     "k_element_blocks_p2tet + k_gather_blocks3" if dm.tangent_fused else "k_assemble_bsr"),
         "spmv": (lambda: dm.spmv(K, x, y), dm.n_blocks * 76 + (dm.n_n + 1) * 4 + 16 * dm.n_dof,
                  "k_spmv_blk 3x3"),
     }

@@ -201,6 +201,17 @@ class DFGMRES:
     def k(self):
         return self.basis.shape[0]
 
+    # the deflation basis lives in buffers whose row capacity is a multiple of 16, so that
+    # appending a vector writes one row and copies of the basis fall into few allocation size
+    # classes (the caching allocator then serves the Newton steps without new device memory)
+    ROW_STEP = 16
+
+    def _rows(self, k):
+        if k == 0:
+            return torch.empty((0, self.n), dtype=F64, device=self.dmesh.device)
+        cap = -(-k // self.ROW_STEP) * self.ROW_STEP
+        return torch.empty((cap, self.n), dtype=F64, device=self.dmesh.device)[:k]
+
     def _time(self, name, t0):
         if self.profiler is not None:
             torch.cuda.synchronize()
@@ -232,7 +243,7 @@ class DFGMRES:
         self.AW, self._aw_key = None, None
         if k > 0:
             B = self.basis.contiguous()
-            AW = torch.empty_like(B)
+            AW = self._rows(k)
             kout = C.c_int32()
             _lib.call("sg_a_orthogonalize", self._ws.handle, self.dmesh.bsr, ptr(K), ptr(B), ptr(AW), k,
                       self.tolerance_deflation_basis, C.byref(kout), cur_stream())
@@ -354,8 +365,18 @@ class DFGMRES:
 
     def expand_deflation_basis(self, v):
         t0 = time.perf_counter()
-        v = v.reshape(1, -1).to(F64)
-        self.basis = torch.cat([self.basis, v], 0)
+        v = v.reshape(-1).to(F64)
+        k = self.k
+        base = self.basis._base
+        if (base is not None and base.dim() == 2 and base.shape[0] > k and self.basis.is_contiguous()
+                and self.basis.data_ptr() == base.data_ptr()):
+            base[k].copy_(v)
+            self.basis = base[: k + 1]
+        else:
+            nb = self._rows(k + 1)
+            nb[:k].copy_(self.basis)
+            nb[k].copy_(v)
+            self.basis = nb
         self.AW, self._aw_key = None, None
         self._time("DFGMRES.expand_deflation_basis", t0)
 
@@ -363,7 +384,8 @@ class DFGMRES:
         new = DFGMRES(self.dmesh, self.tolerance, self.max_iterations, self.tolerance_deflation_basis, self.verbose,
                       amg=self.preconditioner, _ws=self._ws, _pair=self._pair)
         new.concurrent_pair = self.concurrent_pair
-        new.basis = self.basis.clone()
+        new.basis = new._rows(self.k)
+        new.basis.copy_(self.basis)
         if self.AW is not None:
             new.AW, new._aw_key = self.AW.clone(), self._aw_key
         new.profiler = self.profiler

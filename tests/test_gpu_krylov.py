@@ -191,3 +191,26 @@ def test_graph_replayed_solve_equals_host_loop(cuda_device, mixed):
         assert ig == ih and ig > 0
         assert np.abs(xg - xh).max() <= 1e-12 * np.abs(xh).max()
         assert abs(rg - rh) <= 1e-12 + 1e-10 * rh
+
+
+def test_blocked_a_orthogonalize_matches_reference(cuda_device):
+    """A 40-column basis (three blocks of the blocked Gram-Schmidt) with a dependent column and
+    a column of zero A-norm: the same kept columns, the same A-orthonormal basis within 1e-10
+    and A W within 1e-10 as the column-by-column restatement of A_orthogonalize.m."""
+    P, K, KQ, q = elastic_system()
+    n = P.dmesh.n_dof
+    k = 40
+    W = basis(n, q, k, 13)
+    W[17] = 0.5 * W[3] - 2.0 * W[30]          # dependent on columns processed before it
+    eps = 1e-3
+    Wo_ref, norms = a_orthogonalize(W[:, q].T, KQ, eps)
+    sol = DFGMRES(P.dmesh, 1e-8, 40, eps)
+    sol.basis = torch.from_numpy(W).to(cuda_device)
+    sol.A_orthogonalize(K)
+    torch.cuda.synchronize()
+    Wd = sol.basis.cpu().numpy()
+    assert Wd.shape[0] == Wo_ref.shape[1] == k - 2
+    assert np.abs(Wd[:, q].T - Wo_ref).max() <= 1e-10 * np.abs(Wo_ref).max()
+    AW = sol.AW.cpu().numpy()
+    KW = (KQ @ Wd[:, q].T).T
+    assert np.abs(AW[:, q] - KW).max() <= 1e-10 * np.abs(KW).max()
