@@ -282,6 +282,13 @@ int sg_dfgmres_solve(sg_krylov *ws, const sg_bsr *A, const double *A_vals, sg_am
  * host synchronisation per solve (on = 1, the default); on = 0 selects the host-driven loop
  * (one synchronisation per iteration).  Both give the same iterates. */
 int sg_krylov_set_graph(sg_krylov *ws, int32_t on);
+/* How sg_a_orthogonalize forms the basis (replaces nothing in the reference: both modes are
+ * A_orthogonalize.m's one-pass recurrence, +LINEAR_SOLVERS/A_orthogonalize.m:27-48).
+ * mode 1 (default): G = S'(A S) for the input columns S, the recurrence on the k x k matrix
+ * G (coefficients (T'G)(j,i), norms t'G(:,i)), then the kept columns U = S T and A U = (A S) T
+ * by two tall-skinny products; mode 0: column-blocked Gram-Schmidt on the n-long vectors.
+ * Same kept columns and the same basis up to rounding. */
+int sg_krylov_set_aorth(sg_krylov *ws, int32_t mode);
 /* AW (optional, may be NULL): receives A times the kept columns of W, in W's output order. */
 int sg_a_orthogonalize(sg_krylov *ws, const sg_bsr *A, const double *A_vals, double *W, double *AW,
                        int32_t k, double eps_add, int32_t *k_out, void *stream);
@@ -372,6 +379,11 @@ int64_t sg_launch_count(int reset);
 /* number of device allocations (cudaMalloc) the library made since the last reset (reset != 0
  * clears it); lets a caller check that a timed region allocated no device memory */
 int64_t sg_device_alloc_count(int reset);
+/* the library's device status word on the current device: bit 0 is set when the bulk-staged
+ * element-block kernel of the P2-tetrahedron assembly gave up its bounded wait for a copy
+ * (about one second; the K_t / K_r of that call is then incomplete).  Synchronises the device;
+ * reset != 0 clears the word after reading it.  Returns SG_OK or an error code. */
+int sg_device_status(int32_t reset, int32_t *status);
 
 #ifdef __cplusplus
 }

@@ -60,6 +60,7 @@ SIGNATURES = {
     "sg_amg_update": [vp, vp, vp],
     "sg_amg_clone": [vp, vp],
     "sg_krylov_set_graph": [vp, i32],
+    "sg_krylov_set_aorth": [vp, i32],
     "sg_amg_setup_ijv": [C.c_char_p, vp, vp, vp, i64, i64, vp, i32, vp, i32, vp, i32, i32, vp],
     "sg_amg_update_values": [C.c_char_p, vp, i64, vp],
     "sg_amg_apply_host": [C.c_char_p, vp, vp, i64],
@@ -96,6 +97,7 @@ SIGNATURES = {
     "sg_launch_count": [cint],
     "sg_instr_units": [vp, i32],
     "sg_device_alloc_count": [cint],
+    "sg_device_status": [C.c_int32, vp],
 }
 _RESTYPES = {"sg_last_error": C.c_char_p, "sg_launch_count": C.c_int64, "sg_device_alloc_count": C.c_int64, "sg_mlp_part_size": C.c_int64}
 

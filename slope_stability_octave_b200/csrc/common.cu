@@ -2,6 +2,7 @@
 #include <cuda_runtime.h>
 
 #include <atomic>
+#include <mutex>
 #include <cstdio>
 #include <string>
 
@@ -18,6 +19,25 @@ void count_launch(int n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
 cudaError_t device_alloc_raw(void **p, size_t bytes) {
     g_device_allocs.fetch_add(1, std::memory_order_relaxed);
     return cudaMalloc(p, bytes);
+}
+
+static int32_t *g_status[64] = {};
+
+int32_t *device_status_word() {
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return nullptr;
+    static std::mutex mu;
+    std::lock_guard<std::mutex> lock(mu);
+    if (!g_status[dev]) {
+        int32_t *p = nullptr;
+        if (device_alloc(&p, sizeof(int32_t)) != cudaSuccess) return nullptr;
+        if (cudaMemset(p, 0, sizeof(int32_t)) != cudaSuccess) {
+            cudaFree(p);
+            return nullptr;
+        }
+        g_status[dev] = p;
+    }
+    return g_status[dev];
 }
 
 int set_error(int code, const std::string &msg) {
@@ -87,6 +107,16 @@ extern "C" int64_t sg_device_alloc_count(int reset) {
     const int64_t v = sg::g_device_allocs.load();
     if (reset) sg::g_device_allocs.store(0);
     return v;
+}
+
+extern "C" int sg_device_status(int32_t reset, int32_t *status) {
+    SG_CHECK_ARG(status, "status is null");
+    int32_t *w = sg::device_status_word();
+    if (!w) return sg::set_error(SG_ERR_CUDA, "device status word unavailable");
+    SG_CUDA(cudaDeviceSynchronize());
+    SG_CUDA(cudaMemcpy(status, w, sizeof(int32_t), cudaMemcpyDeviceToHost));
+    if (reset) SG_CUDA(cudaMemset(w, 0, sizeof(int32_t)));
+    return SG_OK;
 }
 
 extern "C" const char *sg_last_error(void) { return sg::g_last_error.c_str(); }

@@ -268,6 +268,61 @@ __constant__ int8_t c_ke_i0[KE_TPE] = {0, 0, 0, 0, 0, 4, 0, 4, 0, 4, 0, 4, 0, 4,
 
 __device__ __forceinline__ int ke_slot(int i, int j) { return i * 10 - i * (i - 1) / 2 + (j - i); }
 
+// One thread's chunk of an element (node j, row nodes i0 .. min(i0 + 3, j)): its node blocks
+// summed over the element's points from sym(D) (nq x 36), the gradients (nq x [3][10]) and
+// the weights in shared memory, written to the element's slots of Ke.
+__device__ __forceinline__ void ke_chunk(const double *sD, const double *sPhi, const double *sW, int nq, int j,
+                                         int i0, double *__restrict__ Ke_e) {
+    double acc[4][9];
+#pragma unroll
+    for (int ii = 0; ii < 4; ++ii)
+#pragma unroll
+        for (int k = 0; k < 9; ++k) acc[ii][k] = 0.0;
+    for (int q = 0; q < nq; ++q) {
+        const double *D = sD + q * 36, *d = sPhi + q * 30;
+        const double wq = sW[q];
+        // w sym(D) B(:, (j, cj)) for the three components of node j
+        double db[3][6];
+#pragma unroll
+        for (int cj = 0; cj < 3; ++cj) {
+            int r[3];
+            double v[3];
+            bcol<3>(d, 10, j, cj, r, v);
+#pragma unroll
+            for (int a = 0; a < 6; ++a)
+                db[cj][a] = wq * (D[a + 6 * r[0]] * v[0] + D[a + 6 * r[1]] * v[1] + D[a + 6 * r[2]] * v[2]);
+        }
+#pragma unroll
+        for (int ii = 0; ii < 4; ++ii) {
+            const int i = i0 + ii;
+            if (i > j) break;
+#pragma unroll
+            for (int ci = 0; ci < 3; ++ci) {
+                int r[3];
+                double v[3];
+                bcol<3>(d, 10, i, ci, r, v);
+#pragma unroll
+                for (int cj = 0; cj < 3; ++cj)
+                    acc[ii][ci * 3 + cj] += v[0] * db[cj][r[0]] + v[1] * db[cj][r[1]] + v[2] * db[cj][r[2]];
+            }
+        }
+    }
+#pragma unroll
+    for (int ii = 0; ii < 4; ++ii) {
+        const int i = i0 + ii;
+        if (i > j) break;
+        if (i == j) {   // diagonal node block: its upper triangle, mirrored (exactly symmetric)
+            acc[ii][3] = acc[ii][1];
+            acc[ii][6] = acc[ii][2];
+            acc[ii][7] = acc[ii][5];
+        }
+        double *out = Ke_e + ke_slot(i, j) * KE_PITCH;
+#pragma unroll
+        for (int k = 0; k < 9; ++k) out[k] = acc[ii][k];
+    }
+}
+
+// Staging by plain loads (any alignment of DS, any nq).
 __global__ void __launch_bounds__(KE_EPB * KE_TPE, 3) k_element_blocks_p2tet(int64_t n_e, int nq,
                                                                           const double *__restrict__ dphi,
                                                                           const double *__restrict__ w,
@@ -298,56 +353,121 @@ __global__ void __launch_bounds__(KE_EPB * KE_TPE, 3) k_element_blocks_p2tet(int
         }
         __syncthreads();
         if (le < ne_here) {
-            const double *sD = ke_smem + le * per, *sPhi = sD + nq * 36, *sW = sPhi + nq * 30;
-            double acc[4][9];
-#pragma unroll
-            for (int ii = 0; ii < 4; ++ii)
-#pragma unroll
-                for (int k = 0; k < 9; ++k) acc[ii][k] = 0.0;
-            for (int q = 0; q < nq; ++q) {
-                const double *D = sD + q * 36, *d = sPhi + q * 30;
-                const double wq = sW[q];
-                // w sym(D) B(:, (j, cj)) for the three components of node j
-                double db[3][6];
-#pragma unroll
-                for (int cj = 0; cj < 3; ++cj) {
-                    int r[3];
-                    double v[3];
-                    bcol<3>(d, 10, j, cj, r, v);
-#pragma unroll
-                    for (int a = 0; a < 6; ++a)
-                        db[cj][a] = wq * (D[a + 6 * r[0]] * v[0] + D[a + 6 * r[1]] * v[1] + D[a + 6 * r[2]] * v[2]);
-                }
-#pragma unroll
-                for (int ii = 0; ii < 4; ++ii) {
-                    const int i = i0 + ii;
-                    if (i > j) break;
-#pragma unroll
-                    for (int ci = 0; ci < 3; ++ci) {
-                        int r[3];
-                        double v[3];
-                        bcol<3>(d, 10, i, ci, r, v);
-#pragma unroll
-                        for (int cj = 0; cj < 3; ++cj)
-                            acc[ii][ci * 3 + cj] += v[0] * db[cj][r[0]] + v[1] * db[cj][r[1]] + v[2] * db[cj][r[2]];
-                    }
-                }
-            }
-            const int64_t e = e0 + le;
-#pragma unroll
-            for (int ii = 0; ii < 4; ++ii) {
-                const int i = i0 + ii;
-                if (i > j) break;
-                if (i == j) {   // diagonal node block: its upper triangle, mirrored (exactly symmetric)
-                    acc[ii][3] = acc[ii][1];
-                    acc[ii][6] = acc[ii][2];
-                    acc[ii][7] = acc[ii][5];
-                }
-                double *out = Ke + (e * 55 + ke_slot(i, j)) * KE_PITCH;
-#pragma unroll
-                for (int k = 0; k < 9; ++k) out[k] = acc[ii][k];
-            }
+            const double *sD = ke_smem + le * per;
+            ke_chunk(sD, sD + nq * 36, sD + nq * 66, nq, j, i0, Ke + (e0 + le) * 55 * KE_PITCH);
         }
+    }
+}
+
+// Staging by bulk copies, two stages: a batch's DS, gradients and weights are three contiguous
+// ranges of global memory (element-major), each brought into shared memory by one
+// cp.async.bulk whose completion is counted on the stage's mbarrier; the copy of the next
+// batch runs while the current one is computed.  sym(D) is formed in place once a batch has
+// landed (each off-diagonal pair by one thread, the same rounding as the plain-load kernel),
+// so both kernels write bitwise the same blocks.  Needs DS, dphi and w 16-byte aligned.
+//   shared: [2 mbarriers | status | pad] then 2 stages of
+//           D (KE_EPB nq 36) | gradients (KE_EPB nq 30) | weights (KE_EPB nq, rounded up to even)
+constexpr long long KE_WAIT_CYCLES = 2000000000LL;   // about one second at the boost clock
+__constant__ int8_t c_sym_a[15] = {0, 0, 0, 0, 0, 1, 1, 1, 1, 2, 2, 2, 3, 3, 4};
+__constant__ int8_t c_sym_b[15] = {1, 2, 3, 4, 5, 2, 3, 4, 5, 3, 4, 5, 4, 5, 5};
+
+__device__ __forceinline__ uint32_t smem_u32(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ bool ke_wait(uint32_t bar, uint32_t parity) {
+    const long long t0 = clock64();
+    while (true) {
+        uint32_t done;
+        asm volatile(
+            "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+            "selp.u32 %0, 1, 0, p;\n\t}\n"
+            : "=r"(done)
+            : "r"(bar), "r"(parity)
+            : "memory");
+        if (done) return true;
+        if (clock64() - t0 > KE_WAIT_CYCLES) return false;
+    }
+}
+
+__device__ __forceinline__ void ke_bulk(uint32_t dst, const void *src, uint32_t bytes, uint32_t bar) {
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(dst),
+                 "l"(src), "r"(bytes), "r"(bar)
+                 : "memory");
+}
+
+// Thread 0: the copies of batch b (elements b KE_EPB ..) into the stage at shared address `stage`.
+__device__ __forceinline__ void ke_issue(int64_t b, int64_t n_e, int nq, const double *dphi, const double *w,
+                                         const double *DS, uint32_t stage, uint32_t bar) {
+    const int64_t e0 = b * KE_EPB;
+    const int64_t ne = n_e - e0 < KE_EPB ? n_e - e0 : KE_EPB;
+    const uint32_t dB = (uint32_t)(ne * nq * 36 * 8), pB = (uint32_t)(ne * nq * 30 * 8);
+    const uint32_t wB = (uint32_t)(ne * nq * 8) & ~15u;   // an odd last weight is loaded plainly
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(dB + pB + wB) : "memory");
+    ke_bulk(stage, DS + e0 * nq * 36, dB, bar);
+    ke_bulk(stage + (uint32_t)(KE_EPB * nq * 36 * 8), dphi + e0 * nq * 30, pB, bar);
+    if (wB) ke_bulk(stage + (uint32_t)(KE_EPB * nq * 66 * 8), w + e0 * nq, wB, bar);
+}
+
+__global__ void __launch_bounds__(KE_EPB * KE_TPE, 2) k_element_blocks_p2tet_bulk(int64_t n_e, int nq,
+                                                                               const double *__restrict__ dphi,
+                                                                               const double *__restrict__ w,
+                                                                               const double *__restrict__ DS,
+                                                                               double *__restrict__ Ke,
+                                                                               int32_t *__restrict__ status) {
+    extern __shared__ __align__(16) unsigned char ke_sm[];
+    uint64_t *bars = reinterpret_cast<uint64_t *>(ke_sm);
+    volatile int *s_fail = reinterpret_cast<volatile int *>(ke_sm + 16);
+    const int wpad = (KE_EPB * nq + 1) & ~1;
+    const int per_stage = KE_EPB * nq * 66 + wpad;   // doubles
+    double *stages = reinterpret_cast<double *>(ke_sm + 32);
+    const uint32_t bar0 = smem_u32(&bars[0]), bar1 = smem_u32(&bars[1]);
+    const uint32_t st0 = smem_u32(stages), st1 = st0 + (uint32_t)per_stage * 8;
+    const int tid = threadIdx.x;
+    const int le = tid / KE_TPE, lc = tid - le * KE_TPE;
+    const int j = c_ke_j[lc], i0 = c_ke_i0[lc];
+    const int64_t n_batches = (n_e + KE_EPB - 1) / KE_EPB;
+    if (tid == 0) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar0) : "memory");
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar1) : "memory");
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        *s_fail = 0;
+    }
+    __syncthreads();
+    int64_t b = blockIdx.x;
+    if (tid == 0 && b < n_batches) ke_issue(b, n_e, nq, dphi, w, DS, st0, bar0);
+    for (int it = 0; b < n_batches; ++it, b += gridDim.x) {
+        const int s = it & 1;
+        const uint32_t bar = s ? bar1 : bar0;
+        const int64_t bn = b + gridDim.x;
+        // the other stage was released by the barrier that ended the previous batch
+        if (tid == 0 && bn < n_batches) ke_issue(bn, n_e, nq, dphi, w, DS, s ? st0 : st1, s ? bar0 : bar1);
+        if (tid == 0 && !ke_wait(bar, (uint32_t)((it >> 1) & 1))) *s_fail = 1;
+        __syncthreads();
+        if (*s_fail) {
+            if (tid == 0) {
+                atomicOr(status, 1);
+                if (bn < n_batches) ke_wait(s ? bar0 : bar1, (uint32_t)(((it + 1) >> 1) & 1));   // bounded drain
+            }
+            return;
+        }
+        double *sD = stages + (int64_t)s * per_stage;
+        double *sPhi = sD + KE_EPB * nq * 36, *sW = sD + KE_EPB * nq * 66;
+        const int64_t e0 = b * KE_EPB;
+        const int ne = (int)(n_e - e0 < KE_EPB ? n_e - e0 : KE_EPB);
+        for (int t = tid; t < ne * nq * 15; t += blockDim.x) {
+            const int p = t / 15, k = t - p * 15;
+            double *D = sD + p * 36;
+            const int a = c_sym_a[k], c = c_sym_b[k];
+            const double v = 0.5 * (D[a + 6 * c] + D[c + 6 * a]);
+            D[a + 6 * c] = v;
+            D[c + 6 * a] = v;
+        }
+        if (tid == 0 && ((ne * nq) & 1)) sW[ne * nq - 1] = w[e0 * nq + ne * nq - 1];
+        // generic writes to the stage, ordered before the bulk copy that refills it
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        __syncthreads();
+        if (le < ne)
+            ke_chunk(sD + le * nq * 36, sPhi + le * nq * 30, sW + le * nq, nq, j, i0, Ke + (e0 + le) * 55 * KE_PITCH);
+        __syncthreads();
     }
 }
 
@@ -416,9 +536,31 @@ __global__ void __launch_bounds__(KG_WARPS * 32) k_gather_blocks3(int64_t n_bloc
     }
 }
 
-// Element blocks of the deterministic path into m->d_ke (allocated on first use).
+// Element blocks of the deterministic path into m->d_ke (allocated on first use): the
+// bulk-staged kernel (two CTAs per SM) when DS, the gradients and the weights are 16-byte
+// aligned and two stages fit in shared memory, else the plain-load kernel.
 static int element_blocks(sg_mesh *m, const double *DS, cudaStream_t st) {
     if (!m->d_ke) SG_CUDA(device_alloc(&m->d_ke, sizeof(double) * (size_t)m->n_e * 55 * KE_PITCH));
+    const int64_t batches = (m->n_e + KE_EPB - 1) / KE_EPB;
+    const size_t stage = sizeof(double) * ((size_t)KE_EPB * m->nq * 66 + (size_t)((KE_EPB * m->nq + 1) & ~1));
+    const size_t smem_bulk = 32 + 2 * stage;
+    const bool aligned = ((reinterpret_cast<uintptr_t>(DS) | reinterpret_cast<uintptr_t>(m->d_dphi) |
+                           reinterpret_cast<uintptr_t>(m->d_w)) & 15) == 0;
+    int32_t *status = device_status_word();
+    if (aligned && status && smem_bulk <= 113 * 1024) {
+        static thread_local size_t configured_bulk = 0;
+        if (smem_bulk > configured_bulk) {
+            SG_CUDA(cudaFuncSetAttribute(k_element_blocks_p2tet_bulk, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)smem_bulk));
+            configured_bulk = smem_bulk;
+        }
+        count_launch();
+        const unsigned grid = (unsigned)std::max<int64_t>(1, std::min<int64_t>(batches, (int64_t)sm_count() * 2));
+        k_element_blocks_p2tet_bulk<<<grid, KE_EPB * KE_TPE, smem_bulk, st>>>(m->n_e, m->nq, m->d_dphi, m->d_w, DS,
+                                                                             m->d_ke, status);
+        SG_CUDA(cudaGetLastError());
+        return SG_OK;
+    }
     const size_t smem = sizeof(double) * (size_t)KE_EPB * m->nq * (36 + 30 + 1);
     static thread_local size_t configured = 0;
     if (smem > configured) {
@@ -426,8 +568,7 @@ static int element_blocks(sg_mesh *m, const double *DS, cudaStream_t st) {
         configured = smem;
     }
     count_launch();
-    const int64_t ctas = (m->n_e + KE_EPB - 1) / KE_EPB;
-    const unsigned grid = (unsigned)std::max<int64_t>(1, std::min<int64_t>(ctas, (int64_t)sm_count() * 8));
+    const unsigned grid = (unsigned)std::max<int64_t>(1, std::min<int64_t>(batches, (int64_t)sm_count() * 8));
     k_element_blocks_p2tet<<<grid, KE_EPB * KE_TPE, smem, st>>>(m->n_e, m->nq, m->d_dphi, m->d_w, DS, m->d_ke);
     SG_CUDA(cudaGetLastError());
     return SG_OK;

@@ -59,13 +59,18 @@ struct sg_krylov {
     // blocked A-orthogonalisation: A times the block's input columns (n x 16), the block's
     // coefficients against earlier columns (256 x 16) and the per-CTA partial sums
     double *atb = nullptr, *cblk = nullptr, *tspart = nullptr;
+    // Gram-matrix A-orthogonalisation (default, aorth_mode 1): G, T and the output-ordered T
+    // (3 kcap^2), the Gram partial sums (GR_CTAS x 64 x 64) and the kept count on the device
+    double *gram = nullptr, *gpart = nullptr;
+    int32_t *gkout = nullptr;
+    int aorth_mode = 1;
 };
 
 namespace sg {
 
 static int ensure_kcap(sg_krylov *ws, int64_t k) {
     if (k <= ws->kcap) return SG_OK;
-    const int64_t cap = std::max<int64_t>(k, ws->kcap * 2 + 16);
+    const int64_t cap = std::max<int64_t>(k, std::max<int64_t>(64, ws->kcap * 2));
     double *part = nullptr, *hd = nullptr, *Wo = nullptr, *AWo = nullptr, *nt = nullptr, *sig = nullptr;
     const int64_t rows = std::max<int64_t>(cap, ws->maxit + 2);
     SG_CUDA(sg::device_alloc(&part, sizeof(double) * DOT_BLOCKS * rows));
@@ -74,6 +79,10 @@ static int ensure_kcap(sg_krylov *ws, int64_t k) {
     SG_CUDA(sg::device_alloc(&AWo, sizeof(double) * ws->n * cap));
     SG_CUDA(sg::device_alloc(&nt, sizeof(double) * (cap + 8)));
     SG_CUDA(sg::device_alloc(&sig, sizeof(double) * (cap + 8)));
+    double *gram = nullptr;
+    SG_CUDA(sg::device_alloc(&gram, sizeof(double) * 3 * cap * cap));
+    cudaFree(ws->gram);
+    ws->gram = gram;
     cudaFree(ws->part);
     cudaFree(ws->hd);
     cudaFree(ws->Worth);
@@ -425,6 +434,7 @@ extern "C" int sg_krylov_destroy(sg_krylov *ws) {
     cudaFree(ws->sig);
     graph_release(ws);
     cudaFree(ws->atb); cudaFree(ws->cblk); cudaFree(ws->tspart);
+    cudaFree(ws->gram); cudaFree(ws->gpart); cudaFree(ws->gkout);
     cudaFree(ws->u); cudaFree(ws->dstate); cudaFree(ws->dscal); cudaFree(ws->dH); cudaFree(ws->dcs);
     cudaFree(ws->dsn); cudaFree(ws->dg); cudaFree(ws->dy); cudaFree(ws->dhist); cudaFree(ws->dptr);
     if (ws->cap) cudaStreamDestroy(ws->cap);
@@ -440,6 +450,14 @@ extern "C" int sg_krylov_destroy(sg_krylov *ws) {
 extern "C" int sg_krylov_set_graph(sg_krylov *ws, int32_t on) {
     SG_CHECK_ARG(ws, "null workspace");
     ws->use_graph = on != 0;
+    return SG_OK;
+}
+
+// 1: the A-orthogonalisation through the Gram matrix (default); 0: the column-blocked
+// Gram-Schmidt (coefficients and norms from n-long vector passes per column)
+extern "C" int sg_krylov_set_aorth(sg_krylov *ws, int32_t mode) {
+    SG_CHECK_ARG(ws && (mode == 0 || mode == 1), "bad argument");
+    ws->aorth_mode = mode;
     return SG_OK;
 }
 
@@ -591,14 +609,43 @@ extern "C" int sg_a_orthogonalize(sg_krylov *ws, const sg_bsr *A, const double *
     // A times every input column up front (processing order i takes column k - 1 - i): the
     // products do not depend on the orthogonalisation, and one SpMM reads A once per eight
     // columns where a SpMV per column reads it k times
-    if (A->b == 3) {
+    if (A->b == 3 && k >= 4 && (double)n * 8 * 8 > 48e6) {
+        // long vectors: interleaved copies of 8 columns (scratch: the block buffer and Z)
+        if (!ws->atb) {
+            SG_CUDA(device_alloc(&ws->atb, sizeof(double) * n * 16));
+            SG_CUDA(device_alloc(&ws->cblk, sizeof(double) * 256 * 16));
+            SG_CUDA(device_alloc(&ws->tspart, sizeof(double) * TS_PART_CTAS * 256 * 16));
+        }
+        rc = bsr_spmm_interleaved(*A, Avals, W + (int64_t)(k - 1) * n, -n, AWo, n, k, ws->atb, ws->atb + n * 8, st);
+    } else if (A->b == 3) {
         rc = bsr_spmm(*A, Avals, W + (int64_t)(k - 1) * n, -n, AWo, n, k, st);
     } else {
         for (int i = 0; i < k && !rc; ++i)
             rc = bsr_spmv<double, double>(*A, Avals, W + (int64_t)(k - 1 - i) * n, AWo + (int64_t)i * n, 1.0, 0.0, st);
     }
     if (rc) return rc;
-    // Blocked one-pass Gram-Schmidt: columns are processed in blocks of AORTH_BLOCK; a block's
+    if (ws->aorth_mode == 1) {
+        // Gram matrix, recurrence on one CTA, then U = S T into Wo and A U = (A S) T into AW
+        if (!ws->gpart) {
+            SG_CUDA(device_alloc(&ws->gpart, sizeof(double) * GR_CTAS * 64 * 64));
+            SG_CUDA(device_alloc(&ws->gkout, sizeof(int32_t) * 4));
+        }
+        double *G = ws->gram, *Tp = G + (int64_t)k * k, *Ta = Tp + (int64_t)k * k;
+        const double *S = W + (int64_t)(k - 1) * n;   // processing order: column i is W's k - 1 - i
+        if ((rc = gram_upper(n, k, S, -n, AWo, n, G, ws->gpart, st))) return rc;
+        if ((rc = gram_recurrence(k, G, Tp, eps_add, Ta, nt, sig, ws->gkout, st))) return rc;
+        if ((rc = ts_apply(n, k, ws->gkout, S, -n, Ta, Wo, n, st))) return rc;
+        if (AW && (rc = ts_apply(n, k, ws->gkout, AWo, n, Ta, AW, n, st))) return rc;
+        int32_t ko = 0;
+        SG_CUDA(cudaMemcpyAsync(&ko, ws->gkout, sizeof(int32_t), cudaMemcpyDeviceToHost, st));
+        SG_CUDA(cudaStreamSynchronize(st));
+        if (ko > 0)
+            SG_CUDA(cudaMemcpyAsync(W, Wo, sizeof(double) * n * ko, cudaMemcpyDeviceToDevice, st));
+        *k_out = ko;
+        SG_CUDA(cudaStreamSynchronize(st));
+        return SG_OK;
+    }
+    // Blocked one-pass Gram-Schmidt (aorth_mode 0): columns are processed in blocks of AORTH_BLOCK; a block's
     // coefficients against all earlier (final) columns come from one tall-skinny product
     // c = diag(sig) U' (A S_blk), applied to the block's columns and their A-images by two more,
     // then the columns inside the block are treated one after another as before.  Every

@@ -327,6 +327,100 @@ static void spmm_pass(const sg_bsr &A, int G, const double *vals, const double *
     }
 }
 
+// Node-interleaved SpMM for many vectors: the 8 columns of a pass are packed so that node j's
+// three components of all 8 columns are one contiguous run of 24 doubles; a block's x gather is
+// then 192 contiguous bytes (12 16-byte loads) however far apart the original columns lie.  G
+// lanes per block row, lane l taking the row's blocks l, l + G, ...; the 24 partial sums of the
+// row are combined by a fixed shuffle tree (reproducible).
+constexpr int SPI_KC = 8;
+constexpr int SPI_G = 8;    // lanes per block row (8, 16, 32 measured: 8 fastest on the 3M-DOF slope)
+__global__ void k_pack_cols(int64_t n, int kc, const double *__restrict__ X, int64_t ldx,
+                            double *__restrict__ Xi) {
+    for (int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; r < n; r += (int64_t)gridDim.x * blockDim.x) {
+#pragma unroll
+        for (int c = 0; c < SPI_KC; ++c) Xi[r * SPI_KC + c] = c < kc ? X[c * ldx + r] : 0.0;
+    }
+}
+__global__ void k_unpack_cols(int64_t n, int kc, const double *__restrict__ Yi, double *__restrict__ Y,
+                              int64_t ldy) {
+    for (int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; r < n; r += (int64_t)gridDim.x * blockDim.x) {
+        for (int c = 0; c < kc; ++c) Y[c * ldy + r] = Yi[r * SPI_KC + c];
+    }
+}
+
+template <int G>
+__global__ void __launch_bounds__(256) k_spmm3i(int64_t nrows, const int32_t *__restrict__ rp,
+                                                const int32_t *__restrict__ col, const double *__restrict__ vals,
+                                                const double *__restrict__ Xi, double *__restrict__ Yi) {
+    constexpr int GPW = 32 / G;
+    const int lane = threadIdx.x & 31, g = lane / G, gl = lane - g * G;
+    const int64_t warp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+    const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    for (int64_t base = warp * GPW; base < nrows; base += nwarps * GPW) {
+        const int64_t row = base + g;
+        double acc[3][SPI_KC];
+#pragma unroll
+        for (int a = 0; a < 3; ++a)
+#pragma unroll
+            for (int c = 0; c < SPI_KC; ++c) acc[a][c] = 0.0;
+        if (row < nrows) {
+            const int32_t p1 = rp[row + 1];
+            for (int32_t p = rp[row] + gl; p < p1; p += G) {
+                const int64_t j = col[p];
+                double v[9];
+#pragma unroll
+                for (int t = 0; t < 9; ++t) v[t] = __ldg(vals + (int64_t)p * 9 + t);
+                const double2 *xj = reinterpret_cast<const double2 *>(Xi + j * 3 * SPI_KC);
+#pragma unroll
+                for (int b = 0; b < 3; ++b) {
+                    double x[SPI_KC];
+#pragma unroll
+                    for (int h = 0; h < SPI_KC / 2; ++h) {
+                        const double2 t = __ldg(xj + b * (SPI_KC / 2) + h);
+                        x[2 * h] = t.x;
+                        x[2 * h + 1] = t.y;
+                    }
+#pragma unroll
+                    for (int a = 0; a < 3; ++a)
+#pragma unroll
+                        for (int c = 0; c < SPI_KC; ++c) acc[a][c] += v[a * 3 + b] * x[c];
+                }
+            }
+        }
+#pragma unroll
+        for (int off = G / 2; off > 0; off >>= 1)
+#pragma unroll
+            for (int a = 0; a < 3; ++a)
+#pragma unroll
+                for (int c = 0; c < SPI_KC; ++c) acc[a][c] += __shfl_xor_sync(0xffffffffu, acc[a][c], off);
+        if (row < nrows && gl == 0) {
+            double2 *yr = reinterpret_cast<double2 *>(Yi + row * 3 * SPI_KC);
+#pragma unroll
+            for (int a = 0; a < 3; ++a)
+#pragma unroll
+                for (int h = 0; h < SPI_KC / 2; ++h) yr[a * (SPI_KC / 2) + h] = make_double2(acc[a][2 * h], acc[a][2 * h + 1]);
+        }
+    }
+}
+
+int bsr_spmm_interleaved(const sg_bsr &A, const double *vals, const double *X, int64_t ldx, double *Y, int64_t ldy,
+                         int k, double *Xi, double *Yi, cudaStream_t st) {
+    if (A.b != 3) return set_error(SG_ERR_ARG, "bsr_spmm: 3x3 blocks only");
+    const int64_t n = A.n_rows * 3;
+    for (int c0 = 0; c0 < k; c0 += SPI_KC) {
+        const int kc = std::min(SPI_KC, k - c0);
+        const InstrToken tk = instr_begin(IK_SPMM_AORTH, st);
+        instr_units(IK_SPMM_AORTH, kc);
+        const unsigned gp = grid_for(n, 256, 8);
+        k_pack_cols<<<gp, 256, 0, st>>>(n, kc, X + c0 * ldx, ldx, Xi);
+        k_spmm3i<SPI_G><<<grid_for(A.n_rows * SPI_G, 256, 16), 256, 0, st>>>(A.n_rows, A.d_row_ptr, A.d_col, vals, Xi, Yi);
+        k_unpack_cols<<<grid_for(n, 256, 8), 256, 0, st>>>(n, kc, Yi, Y + c0 * ldy, ldy);
+        instr_end(tk, st);
+        SG_CUDA(cudaGetLastError());
+    }
+    return SG_OK;
+}
+
 int bsr_spmm(const sg_bsr &A, const double *vals, const double *X, int64_t ldx, double *Y, int64_t ldy, int k,
              cudaStream_t st) {
     if (A.b != 3) return set_error(SG_ERR_ARG, "bsr_spmm: 3x3 blocks only");
@@ -645,6 +739,324 @@ int gemm_nn_sub(int64_t n, int m, int b, const double *U, int64_t ldu, const dou
     if (m <= 0 || b <= 0) return SG_OK;
     if (m > TS_MAXM || b > TS_B) return set_error(SG_ERR_ARG, "gemm_nn_sub: block too large");
     k_gemm_nn_sub<<<grid_for(n, 256, 8), 256, sizeof(double) * m * TS_B, st>>>(n, m, b, U, ldu, C, ldc, Y, ldy);
+    SG_CUDA(cudaGetLastError());
+    return SG_OK;
+}
+
+// ------------------------------------------------------------------ Gram-matrix A-orthogonalisation
+//
+// The one-pass recurrence of A_orthogonalize.m expressed in the coordinates of the input
+// columns S (processing order): with G = S' (A S), the kept columns are U = S T for an upper
+// triangular T, every coefficient (A s_i)' u_j = (T' G)(j, i) and every A-norm temp' (A s_i)
+// comes from G, so the n-long work is one Gram product and two tall-skinny products
+// (U = S T, A U = (A S) T) instead of a sequence of vector passes per column.
+
+__device__ __forceinline__ uint32_t sh_u32(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
+__device__ __forceinline__ void cp_async8(void *dst, const void *src) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(sh_u32(dst)), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait1() { asm volatile("cp.async.wait_group 1;" ::: "memory"); }
+
+// Partial sums of one 16 NA x 16 NA tile of G (rows m0 + [0, 16 NA), columns i0 + [0, 16 NA))
+// over this CTA's row range, in tiles of GR_R rows staged in shared memory ([column][row],
+// padded) by 8-byte cp.async, two stages; thread (mb, ib) owns the entries
+// (m0 + mb + 16 a, i0 + ib + 16 b).  part: gridDim.x x (16 NA)^2.
+constexpr int GR_R = 32, GR_LD = GR_R + 1;
+template <int NA>
+__global__ void __launch_bounds__(256) k_gram_partial(int64_t n, int k, const double *__restrict__ S, int64_t lds,
+                                                      const double *__restrict__ AS, int64_t ldas, int m0, int i0,
+                                                      double *__restrict__ part) {
+    constexpr int TW = 16 * NA;
+    extern __shared__ double gsm[];   // [2 stages][S tile, AS tile][TW][GR_LD]
+    const int t = threadIdx.x, ib = t & 15, mb = t >> 4;
+    const int64_t chunk = ((n + gridDim.x - 1) / gridDim.x + GR_R - 1) / GR_R * GR_R;
+    const int64_t r0 = blockIdx.x * chunk, r1 = min(n, r0 + chunk);
+    double acc[NA][NA];
+#pragma unroll
+    for (int a = 0; a < NA; ++a)
+#pragma unroll
+        for (int b = 0; b < NA; ++b) acc[a][b] = 0.0;
+    auto stage = [&](int st, int64_t rt) {
+        double *sS = gsm + st * 2 * TW * GR_LD, *sA = sS + TW * GR_LD;
+        for (int e = t; e < TW * GR_R; e += 256) {
+            const int c = e / GR_R, r = e - c * GR_R;
+            const int64_t row = rt + r;
+            const int cm = m0 + c, ci = i0 + c;
+            if (row < r1 && cm < k) cp_async8(sS + c * GR_LD + r, S + cm * lds + row);
+            else sS[c * GR_LD + r] = 0.0;
+            if (row < r1 && ci < k) cp_async8(sA + c * GR_LD + r, AS + ci * ldas + row);
+            else sA[c * GR_LD + r] = 0.0;
+        }
+    };
+    if (r0 < r1) stage(0, r0);
+    cp_async_commit();
+    int it = 0;
+    for (int64_t rt = r0; rt < r1; rt += GR_R, ++it) {
+        if (rt + GR_R < r1) stage((it + 1) & 1, rt + GR_R);
+        cp_async_commit();
+        cp_async_wait1();
+        __syncthreads();
+        const double *sS = gsm + (it & 1) * 2 * TW * GR_LD, *sA = sS + TW * GR_LD;
+#pragma unroll 4
+        for (int r = 0; r < GR_R; ++r) {
+            double sv[NA], xv[NA];
+#pragma unroll
+            for (int a = 0; a < NA; ++a) sv[a] = sS[(mb + 16 * a) * GR_LD + r];
+#pragma unroll
+            for (int b = 0; b < NA; ++b) xv[b] = sA[(ib + 16 * b) * GR_LD + r];
+#pragma unroll
+            for (int a = 0; a < NA; ++a)
+#pragma unroll
+                for (int b = 0; b < NA; ++b) acc[a][b] += sv[a] * xv[b];
+        }
+        __syncthreads();
+    }
+    double *out = part + (int64_t)blockIdx.x * TW * TW;
+#pragma unroll
+    for (int a = 0; a < NA; ++a)
+#pragma unroll
+        for (int b = 0; b < NA; ++b) out[(mb + 16 * a) * TW + ib + 16 * b] = acc[a][b];
+}
+
+// G(m0 + ml, i0 + il) = sum over the CTAs of the partials, in CTA order (ldg: G's leading dimension)
+__global__ void k_gram_reduce(int k, int TW, int nparts, const double *__restrict__ part, int m0, int i0,
+                              double *__restrict__ G, int ldg) {
+    for (int o = blockIdx.x * blockDim.x + threadIdx.x; o < TW * TW; o += gridDim.x * blockDim.x) {
+        const int ml = o / TW, il = o - ml * TW;
+        if (m0 + ml >= k || i0 + il >= k) continue;
+        double s = 0.0;
+        for (int p = 0; p < nparts; ++p) s += part[(int64_t)p * TW * TW + o];
+        G[(m0 + ml) + (int64_t)(i0 + il) * ldg] = s;
+    }
+}
+
+// The recurrence on one CTA.  G: k x k column-major (entries m <= i used); Tp: k x k scratch
+// (column p = the coefficients of kept column p in S, zero when dropped); out: Ta k x k,
+// row-major [m][o], the columns of T in output order (kept columns, last processed first);
+// nt[i] = the A-norm^2 of column i, sig[i] its sign; *kout = the number kept.  G and Tp are
+// staged in shared memory when 2 k^2 doubles fit (smem_k2 != 0).
+__global__ void __launch_bounds__(256) k_gram_recurrence(int k, const double *__restrict__ Gg, double *__restrict__ Tpg,
+                                                         double eps, double *__restrict__ Ta,
+                                                         double *__restrict__ nt, double *__restrict__ sig,
+                                                         int32_t *__restrict__ kout, int smem_k2) {
+    extern __shared__ double rsm[];   // [c: k][t: k][red: 256][map: k ints] (+ G, Tp when staged)
+    double *c = rsm, *tv = c + k, *red = tv + k;
+    int *map = reinterpret_cast<int *>(red + 256);
+    const double *G = Gg;
+    double *Tp = Tpg;
+    const int tid = threadIdx.x;
+    if (smem_k2) {
+        double *sG = red + 256 + (k + 1) / 2;
+        double *sT = sG + (int64_t)k * k;
+        for (int e = tid; e < k * k; e += 256) {
+            const int i = e / k, m = e - i * k;
+            sG[e] = m <= i ? Gg[e] : 0.0;
+        }
+        G = sG;
+        Tp = sT;
+    }
+    __syncthreads();
+    for (int i = 0; i < k; ++i) {
+        const double *Gi = G + (int64_t)i * k;
+        // c_j = sig_j (A s_i)' u_j for the columns processed before
+        for (int j = tid; j < i; j += 256) {
+            const double *Tj = Tp + (int64_t)j * k;
+            double s = 0.0;
+            for (int m = 0; m <= j; ++m) s += Tj[m] * Gi[m];
+            c[j] = sig[j] * s;
+        }
+        __syncthreads();
+        // temp = s_i - sum_j c_j u_j in S coordinates (entries m <= i)
+        for (int m = tid; m <= i; m += 256) {
+            double v = m == i ? 1.0 : 0.0;
+            for (int j = m; j < i; ++j) v -= c[j] * Tp[m + (int64_t)j * k];
+            tv[m] = v;
+        }
+        __syncthreads();
+        // temp' (A s_i), a fixed-order tree
+        double p = 0.0;
+        for (int m = tid; m <= i; m += 256) p += tv[m] * Gi[m];
+        red[tid] = p;
+        __syncthreads();
+        for (int h = 128; h > 0; h >>= 1) {
+            if (tid < h) red[tid] += red[tid + h];
+            __syncthreads();
+        }
+        const double nrm = red[0];
+        const bool keep = fabs(nrm) > eps;
+        const double sc = keep ? 1.0 / sqrt(fabs(nrm)) : 0.0;
+        double *Ti = Tp + (int64_t)i * k;
+        for (int m = tid; m < k; m += 256) Ti[m] = m <= i ? tv[m] * sc : 0.0;
+        if (tid == 0) {
+            nt[i] = nrm;
+            sig[i] = (keep && nrm < 0.0) ? -1.0 : 1.0;
+        }
+        __syncthreads();
+    }
+    if (tid == 0) {
+        int o = 0;
+        for (int i = k - 1; i >= 0; --i)
+            if (fabs(nt[i]) > eps) map[o++] = i;
+        *kout = o;
+        red[0] = (double)o;
+    }
+    __syncthreads();
+    const int ko = (int)red[0];
+    for (int e = tid; e < k * k; e += 256) {
+        const int m = e / k, o = e - m * k;
+        Ta[e] = o < ko ? Tp[m + (int64_t)map[o] * k] : 0.0;
+    }
+}
+
+// Y(:, o) = X(:, 0:k) Ta(:, o) for o < *kout, output columns in chunks of 8 NJ (blockIdx.y):
+// X rows in tiles of TA_R, columns of X (and rows of Ta) in stages of TA_MC through shared
+// memory (8-byte cp.async, two stages); thread (lane, warp) owns rows lane + 32 q and output
+// columns o0 + warp + 8 j.
+constexpr int TA_R = 128, TA_MC = 16;
+template <int NJ>
+__global__ void __launch_bounds__(256) k_ts_apply(int64_t n, int k, const int32_t *__restrict__ kout,
+                                                  const double *__restrict__ X, int64_t ldx,
+                                                  const double *__restrict__ Ta, double *__restrict__ Y,
+                                                  int64_t ldy) {
+    constexpr int OC = 8 * NJ;
+    __shared__ double sX[2][TA_MC][TA_R];
+    __shared__ double sT[2][TA_MC][OC];
+    const int ko = *kout;
+    const int o0 = blockIdx.y * OC;
+    if (o0 >= ko) return;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int nmc = (k + TA_MC - 1) / TA_MC;
+    const int64_t ntiles = (n + TA_R - 1) / TA_R;
+    const int64_t nsteps = ((ntiles - blockIdx.x + gridDim.x - 1) / gridDim.x) * nmc;   // (tile, chunk) pairs
+    if (blockIdx.x >= ntiles) return;
+    auto stage = [&](int st, int64_t s) {
+        const int64_t rt = (blockIdx.x + (s / nmc) * gridDim.x) * TA_R;
+        const int mc = (int)(s % nmc) * TA_MC;
+        for (int e = tid; e < TA_MC * TA_R; e += 256) {
+            const int cc = e / TA_R, r = e - cc * TA_R;
+            const int64_t row = rt + r;
+            const int col = mc + cc;
+            if (row < n && col < k) cp_async8(&sX[st][cc][r], X + col * ldx + row);
+            else sX[st][cc][r] = 0.0;
+        }
+        for (int e = tid; e < TA_MC * OC; e += 256) {
+            const int cc = e / OC, oo = e - cc * OC;
+            const int m = mc + cc, o = o0 + oo;
+            sT[st][cc][oo] = (m < k && o < ko) ? Ta[(int64_t)m * k + o] : 0.0;
+        }
+    };
+    double acc[4][NJ];
+    stage(0, 0);
+    cp_async_commit();
+    for (int64_t s = 0; s < nsteps; ++s) {
+        if (s % nmc == 0) {
+#pragma unroll
+            for (int q = 0; q < 4; ++q)
+#pragma unroll
+                for (int j = 0; j < NJ; ++j) acc[q][j] = 0.0;
+        }
+        if (s + 1 < nsteps) stage((int)((s + 1) & 1), s + 1);
+        cp_async_commit();
+        cp_async_wait1();
+        __syncthreads();
+        const int st = (int)(s & 1);
+#pragma unroll 4
+        for (int cc = 0; cc < TA_MC; ++cc) {
+            double xv[4], tw[NJ];
+#pragma unroll
+            for (int q = 0; q < 4; ++q) xv[q] = sX[st][cc][lane + 32 * q];
+#pragma unroll
+            for (int j = 0; j < NJ; ++j) tw[j] = sT[st][cc][warp + 8 * j];
+#pragma unroll
+            for (int q = 0; q < 4; ++q)
+#pragma unroll
+                for (int j = 0; j < NJ; ++j) acc[q][j] += xv[q] * tw[j];
+        }
+        __syncthreads();
+        if (s % nmc == nmc - 1) {
+            const int64_t rt = (blockIdx.x + (s / nmc) * gridDim.x) * TA_R;
+#pragma unroll
+            for (int j = 0; j < NJ; ++j) {
+                const int o = o0 + warp + 8 * j;
+                if (o >= ko) continue;
+#pragma unroll
+                for (int q = 0; q < 4; ++q) {
+                    const int64_t row = rt + lane + 32 * q;
+                    if (row < n) Y[o * ldy + row] = acc[q][j];
+                }
+            }
+        }
+    }
+}
+
+int gram_upper(int64_t n, int k, const double *S, int64_t lds, const double *AS, int64_t ldas, double *G,
+               double *part, cudaStream_t st) {
+    if (k <= 0) return SG_OK;
+    const int NA = k <= 16 ? 1 : (k <= 32 ? 2 : (k <= 48 ? 3 : 4));
+    const int TW = 16 * NA;
+    const size_t smem = sizeof(double) * 2 * 2 * TW * GR_LD;
+    static thread_local bool configured = false;
+    if (!configured) {   // stages of 48- and 64-wide tiles exceed the default 48 KB
+        SG_CUDA(cudaFuncSetAttribute(k_gram_partial<3>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)(sizeof(double) * 2 * 2 * 48 * GR_LD)));
+        SG_CUDA(cudaFuncSetAttribute(k_gram_partial<4>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)(sizeof(double) * 2 * 2 * 64 * GR_LD)));
+        configured = true;
+    }
+    const int nt = (k + TW - 1) / TW;
+    for (int p = 0; p < nt; ++p)
+        for (int q = 0; q <= p; ++q) {
+            count_launch(2);
+            const int m0 = q * TW, i0 = p * TW;
+            switch (NA) {
+                case 1: k_gram_partial<1><<<GR_CTAS, 256, smem, st>>>(n, k, S, lds, AS, ldas, m0, i0, part); break;
+                case 2: k_gram_partial<2><<<GR_CTAS, 256, smem, st>>>(n, k, S, lds, AS, ldas, m0, i0, part); break;
+                case 3: k_gram_partial<3><<<GR_CTAS, 256, smem, st>>>(n, k, S, lds, AS, ldas, m0, i0, part); break;
+                default: k_gram_partial<4><<<GR_CTAS, 256, smem, st>>>(n, k, S, lds, AS, ldas, m0, i0, part); break;
+            }
+            k_gram_reduce<<<(TW * TW + 255) / 256, 256, 0, st>>>(k, TW, GR_CTAS, part, m0, i0, G, k);
+            SG_CUDA(cudaGetLastError());
+        }
+    return SG_OK;
+}
+
+int gram_recurrence(int k, const double *G, double *Tp, double eps, double *Ta, double *nt, double *sig,
+                    int32_t *kout, cudaStream_t st) {
+    if (k <= 0) return SG_OK;
+    const size_t base = sizeof(double) * (2 * (size_t)k + 256 + (k + 1) / 2);
+    const size_t full = base + sizeof(double) * 2 * (size_t)k * k;
+    const bool staged = full <= 200 * 1024;
+    const size_t smem = staged ? full : base;
+    static thread_local size_t configured = 0;
+    if (smem > 48 * 1024 && smem > configured) {
+        SG_CUDA(cudaFuncSetAttribute(k_gram_recurrence, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        configured = smem;
+    }
+    count_launch();
+    k_gram_recurrence<<<1, 256, smem, st>>>(k, G, Tp, eps, Ta, nt, sig, kout, staged ? 1 : 0);
+    SG_CUDA(cudaGetLastError());
+    return SG_OK;
+}
+
+int ts_apply(int64_t n, int k, const int32_t *kout, const double *X, int64_t ldx, const double *Ta, double *Y,
+             int64_t ldy, cudaStream_t st) {
+    if (k <= 0 || n <= 0) return SG_OK;
+    const int nj = k >= 64 ? 8 : (k + 7) / 8;
+    const int oc = 8 * nj;
+    const int64_t ntiles = (n + TA_R - 1) / TA_R;
+    const dim3 grid((unsigned)std::min<int64_t>(ntiles, (int64_t)sm_count() * 2), (unsigned)((k + oc - 1) / oc));
+    count_launch();
+    switch (nj) {
+        case 1: k_ts_apply<1><<<grid, 256, 0, st>>>(n, k, kout, X, ldx, Ta, Y, ldy); break;
+        case 2: k_ts_apply<2><<<grid, 256, 0, st>>>(n, k, kout, X, ldx, Ta, Y, ldy); break;
+        case 3: k_ts_apply<3><<<grid, 256, 0, st>>>(n, k, kout, X, ldx, Ta, Y, ldy); break;
+        case 4: k_ts_apply<4><<<grid, 256, 0, st>>>(n, k, kout, X, ldx, Ta, Y, ldy); break;
+        case 5: k_ts_apply<5><<<grid, 256, 0, st>>>(n, k, kout, X, ldx, Ta, Y, ldy); break;
+        case 6: k_ts_apply<6><<<grid, 256, 0, st>>>(n, k, kout, X, ldx, Ta, Y, ldy); break;
+        case 7: k_ts_apply<7><<<grid, 256, 0, st>>>(n, k, kout, X, ldx, Ta, Y, ldy); break;
+        default: k_ts_apply<8><<<grid, 256, 0, st>>>(n, k, kout, X, ldx, Ta, Y, ldy); break;
+    }
     SG_CUDA(cudaGetLastError());
     return SG_OK;
 }

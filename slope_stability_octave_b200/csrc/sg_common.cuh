@@ -37,6 +37,10 @@ inline cudaError_t device_alloc(T **p, size_t bytes) {
     return device_alloc_raw(reinterpret_cast<void **>(p), bytes);
 }
 
+// The library's device status word on the current device (allocated and zeroed on first
+// use; null if that fails): kernels with bounded waits record there that a wait gave up.
+int32_t *device_status_word();
+
 // Launch shape: grid sized in multiples of the SM count (148 on B200) for
 // grid-stride kernels, capped by the work.
 int sm_count();

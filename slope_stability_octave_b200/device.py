@@ -170,6 +170,16 @@ class DeviceMesh:
         _lib.call("sg_bsr_spmv_dev", self.bsr, ptr(K), ptr(x), ptr(y), cur_stream())
 
 
+def check_device_status():
+    """Raises RuntimeError if a library kernel recorded in the device status word that a
+    bounded wait gave up (the matrices it assembled are then incomplete); clears the word."""
+    st = C.c_int32(0)
+    _lib.call("sg_device_status", 1, C.byref(st))
+    if st.value:
+        raise RuntimeError(f"slopegpu device status {st.value:#x}: a bulk-staged assembly kernel gave up "
+                           "waiting for its copies")
+
+
 def dot(x, y) -> float:
     out = C.c_double()
     _lib.call("sg_dot_dev", x.numel(), ptr(x), ptr(y), C.byref(out), cur_stream())

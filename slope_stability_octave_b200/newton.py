@@ -18,7 +18,7 @@ import time
 
 import torch
 
-from .device import dot, masked_diff_norm
+from .device import check_device_status, dot, masked_diff_norm
 
 
 def _norm_masked(x, Q):
@@ -134,6 +134,7 @@ def newton(U_ini, tol, it_newt_max, it_damp_max, r_min, K_elast, Q, f, cons, sol
     hist["status"] = status
     hist["wall_time"] = time.perf_counter() - t0
     hist["linear_iters_total"] = int(sum(hist["linear_iters"]))
+    check_device_status()
     return U_it, flag, it, hist
 
 
@@ -220,6 +221,7 @@ def newton_ind_SSR(U_ini, omega, lambda_ini, it_newt_max, it_damp_max, tol, r_mi
     hist["wall_time"] = time.perf_counter() - t0
     hist["linear_iters_W_total"] = int(sum(hist["linear_iters_W"]))
     hist["linear_iters_V_total"] = int(sum(hist["linear_iters_V"]))
+    check_device_status()
     return U_it, lambda_it, flag, it, hist
 
 
@@ -299,4 +301,5 @@ def newton_ind_LL(U_ini, t_ini, omega, it_newt_max, it_damp_max, tol, r_min, K_e
     hist["wall_time"] = time.perf_counter() - t0
     hist["linear_iters_W_total"] = int(sum(hist["linear_iters_W"]))
     hist["linear_iters_V_total"] = int(sum(hist["linear_iters_V"]))
+    check_device_status()
     return U_it, t_it, flag, it, hist

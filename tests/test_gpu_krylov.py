@@ -45,7 +45,11 @@ def basis(n_dof, q, k, seed):
     return W
 
 
-def test_a_orthogonalize_matches_reference(cuda_device):
+AORTH_MODES = pytest.mark.parametrize("mode", [1, 0], ids=["gram", "columns"])
+
+
+@AORTH_MODES
+def test_a_orthogonalize_matches_reference(cuda_device, mode):
     P, K, KQ, q = elastic_system()
     n = P.dmesh.n_dof
     k = 6
@@ -54,6 +58,7 @@ def test_a_orthogonalize_matches_reference(cuda_device):
     eps = 1e-3
     Wo_ref, norms = a_orthogonalize(W[:, q].T, KQ, eps)
     sol = DFGMRES(P.dmesh, 1e-8, 40, eps)
+    _lib.call("sg_krylov_set_aorth", sol._ws.handle, mode)
     sol.basis = torch.from_numpy(W).to(cuda_device)
     sol.A_orthogonalize(K)
     torch.cuda.synchronize()
@@ -193,10 +198,12 @@ def test_graph_replayed_solve_equals_host_loop(cuda_device, mixed):
         assert abs(rg - rh) <= 1e-12 + 1e-10 * rh
 
 
-def test_blocked_a_orthogonalize_matches_reference(cuda_device):
-    """A 40-column basis (three blocks of the blocked Gram-Schmidt) with a dependent column and
-    a column of zero A-norm: the same kept columns, the same A-orthonormal basis within 1e-10
-    and A W within 1e-10 as the column-by-column restatement of A_orthogonalize.m."""
+@AORTH_MODES
+def test_blocked_a_orthogonalize_matches_reference(cuda_device, mode):
+    """A 40-column basis (three blocks of the blocked Gram-Schmidt; a 48-wide tile of the Gram
+    matrix) with a dependent column and a column of zero A-norm: the same kept columns, the
+    same A-orthonormal basis within 1e-10 and A W within 1e-10 as the column-by-column
+    restatement of A_orthogonalize.m, in both modes."""
     P, K, KQ, q = elastic_system()
     n = P.dmesh.n_dof
     k = 40
@@ -205,6 +212,7 @@ def test_blocked_a_orthogonalize_matches_reference(cuda_device):
     eps = 1e-3
     Wo_ref, norms = a_orthogonalize(W[:, q].T, KQ, eps)
     sol = DFGMRES(P.dmesh, 1e-8, 40, eps)
+    _lib.call("sg_krylov_set_aorth", sol._ws.handle, mode)
     sol.basis = torch.from_numpy(W).to(cuda_device)
     sol.A_orthogonalize(K)
     torch.cuda.synchronize()
@@ -214,3 +222,58 @@ def test_blocked_a_orthogonalize_matches_reference(cuda_device):
     AW = sol.AW.cpu().numpy()
     KW = (KQ @ Wd[:, q].T).T
     assert np.abs(AW[:, q] - KW).max() <= 1e-10 * np.abs(KW).max()
+
+
+def test_a_orthogonalize_long_vectors_interleaved_products(cuda_device):
+    """On a mesh past 750k DOF the products A W are formed from node-interleaved copies of
+    eight columns at a time (two passes and a ragged third for 20 columns): the returned A W
+    equals the SpMV of every returned column within 1e-10 relative, and the returned basis is
+    A-orthonormal within 1e-10."""
+    P = problems.slope_3d(1, dims=(15, 10, 15, 10, 10, 50)).to_device()
+    assert P.dmesh.n_dof > 750_000
+    P.cons.init_K_r_pattern()
+    f = P.f_device()
+    P.cons.reduction(1.0)
+    P.cons.build_F_and_DS_reduced(torch.zeros_like(f))
+    K = P.cons.build_K_r_QQ_vals(1e-4)
+    n = P.dmesh.n_dof
+    mask = P.dmesh.mask
+    k = 20
+    g = torch.Generator(device=cuda_device).manual_seed(5)
+    W = torch.randn(k, n, dtype=torch.float64, device=cuda_device, generator=g) * mask
+    sol = DFGMRES(P.dmesh, 1e-8, 40, 1e-3)
+    sol.basis = W.clone()
+    sol.A_orthogonalize(K)
+    torch.cuda.synchronize()
+    Wd, AW = sol.basis, sol.AW
+    assert Wd.shape[0] == k
+    KW = torch.empty_like(AW)
+    for i in range(k):
+        P.dmesh.spmv(K, Wd[i].contiguous(), KW[i])
+    err = (AW - KW).abs().max() / KW.abs().max()
+    assert err.item() <= 1e-10, err.item()
+    G = Wd @ KW.T
+    assert (G - torch.eye(k, dtype=G.dtype, device=G.device)).abs().max().item() <= 1e-10
+
+
+@pytest.mark.parametrize("k", [1, 17, 33, 70, 140])
+def test_gram_a_orthogonalize_sizes(cuda_device, k):
+    """The Gram path across its tile shapes (16-, 48- and 64-wide tiles, several 64-wide tiles
+    with k > 64, and the recurrence with G in global memory for k = 140) against the
+    column-blocked path: the same kept count, bases within 1e-9 and A W within 1e-9."""
+    P, K, KQ, q = elastic_system()
+    n = P.dmesh.n_dof
+    W = torch.from_numpy(basis(n, q, k, 21 + k) if k > 2 else np.random.default_rng(2).normal(size=(k, n))
+                         * np.isin(np.arange(n), q)).to(cuda_device)
+    out = {}
+    for mode in (1, 0):
+        sol = DFGMRES(P.dmesh, 1e-8, 40, 1e-3)
+        _lib.call("sg_krylov_set_aorth", sol._ws.handle, mode)
+        sol.basis = W.clone()
+        sol.A_orthogonalize(K)
+        torch.cuda.synchronize()
+        out[mode] = (sol.basis.clone(), sol.AW.clone())
+    (B1, A1), (B0, A0) = out[1], out[0]
+    assert B1.shape == B0.shape
+    assert ((B1 - B0).abs().max() / B0.abs().max()).item() <= 1e-9
+    assert ((A1 - A0).abs().max() / A0.abs().max()).item() <= 1e-9

@@ -180,3 +180,37 @@ def transpose_blocks(mesh):
     tkey = col.astype(np.int64) * n + row
     order = np.argsort(key)
     return order[np.searchsorted(key[order], tkey)]
+
+
+def test_assembly_staging_paths_agree(cuda_device):
+    """The element blocks of P2 tetrahedra are staged by bulk copies when DS is 16-byte aligned
+    and by plain loads otherwise (DS 8 bytes off a 16-byte boundary here): both give bitwise
+    the same K_t, over a mesh whose last batch of eight elements is ragged, and the library's
+    device status word stays clear (no bounded wait gave up)."""
+    import ctypes as C
+
+    import torch
+    from slope_stability_octave_b200 import _lib
+    from slope_stability_octave_b200.device import ptr
+    mesh, dphi, w, nq, mat = build_case("slope3d")
+    dm = DeviceMesh(mesh, dphi, w, nq)
+    assert mesh.elem.shape[1] % 8 != 0
+    cons = CONSTITUTIVE(dm, mat["c0"], mat["phi"], mat["psi"], "B", mat["shear"], mat["bulk"], mat["lame"])
+    cons.init_K_r_pattern(mesh.Q)
+    rng = np.random.default_rng(12)
+    U = rng.normal(size=(mesh.dim, mesh.n_n)) * 3e-3 * mesh.Q
+    Ud = torch.from_numpy(np.ascontiguousarray(U.T).ravel()).to(cuda_device)
+    cons.build_F_and_DS_all(1.2, Ud)
+    DS = cons.DS.contiguous()
+    assert DS.data_ptr() % 16 == 0
+    off = torch.empty(DS.numel() + 1, dtype=torch.float64, device=cuda_device)[1:]
+    off.copy_(DS)
+    assert off.data_ptr() % 16 == 8
+    K1 = torch.zeros(dm.n_blocks * 9, dtype=torch.float64, device=cuda_device)
+    K2 = torch.full_like(K1, float("nan"))
+    dm.assemble(DS, K1)
+    dm.assemble(off, K2)
+    torch.cuda.synchronize()
+    assert torch.equal(K1, K2)
+    st = C.c_int32(-1)
+    assert _lib.lib().sg_device_status(1, C.byref(st)) == 0 and st.value == 0
