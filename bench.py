@@ -877,11 +877,22 @@ def main():
             forms_cfg[form]["network"] = r["learned"]
     for other in ("mixed", "learned"):
         if "plain" in timed and other in timed:
+            # the two forms take the same continuation steps until their trajectories part
+            # (near the limit load one form may need another Newton iteration and reach the
+            # stop a step earlier): λ and time are compared over the longest common run of
+            # identical step numbers, the whole-run ratio is kept beside it
+            sp = [s["step"] for s in timed["plain"]["steps"]]
+            so = [s["step"] for s in timed[other]["steps"]]
+            m = 0
+            while m < min(len(sp), len(so)) and sp[m] == so[m]:
+                m += 1
             lp, lm = timed["plain"]["lam"], timed[other]["lam"]
-            same = [s["step"] for s in timed["plain"]["steps"]] == [s["step"] for s in timed[other]["steps"]]
-            forms_cfg[f"lambda_rel_err_{other}_vs_plain"] = (max(abs(a - b) / abs(a) for a, b in zip(lp, lm))
-                                                            if same else None)
-            forms_cfg[f"speedup_{other}_vs_plain"] = timed["plain"]["t_dev"] / timed[other]["t_dev"]
+            tp, to = timed["plain"]["step_s"], timed[other]["step_s"]
+            forms_cfg[f"matched_steps_{other}_vs_plain"] = m
+            forms_cfg[f"lambda_rel_err_{other}_vs_plain"] = (max(abs(a - b) / abs(a) for a, b in zip(lp[:m], lm[:m]))
+                                                            if m else None)
+            forms_cfg[f"speedup_{other}_vs_plain"] = (sum(tp[:m]) / sum(to[:m])) if m else None
+            forms_cfg[f"speedup_{other}_vs_plain_whole_run"] = timed["plain"]["t_dev"] / timed[other]["t_dev"]
     line = dict(
         metric=METRIC, value=value_step, unit=UNIT, n_gpus=args.gpus, steps=K, warmup=args.warmup,
         ms_per_step=value_step * 1e3, higher_is_better=False, scaling="weak", vs_baseline=None,

@@ -494,16 +494,9 @@ __global__ void __launch_bounds__(KG_WARPS * 32) k_gather_blocks3(int64_t n_bloc
 #pragma unroll
         for (int k = 0; k < 9; ++k) acc[k] = 0.0;
         if (p < n_blocks) {
-            for (int32_t l = cptr[p]; l < cptr[p + 1]; ++l) {
-                const uint32_t src = contrib[l];
-                const double2 *v = reinterpret_cast<const double2 *>(Ke + (int64_t)(src & 0x7fffffffu) * KE_PITCH);
-                double x[10];
-#pragma unroll
-                for (int h = 0; h < 5; ++h) {
-                    const double2 t = __ldg(v + h);
-                    x[2 * h] = t.x;
-                    x[2 * h + 1] = t.y;
-                }
+            // contributions in list order, two in flight (both index and block loads issued
+            // before either is added)
+            auto add = [&](uint32_t src, const double *x) {
                 if (src >> 31) {
 #pragma unroll
                     for (int a = 0; a < 3; ++a)
@@ -513,6 +506,31 @@ __global__ void __launch_bounds__(KG_WARPS * 32) k_gather_blocks3(int64_t n_bloc
 #pragma unroll
                     for (int k = 0; k < 9; ++k) acc[k] += x[k];
                 }
+            };
+            auto fetch = [&](uint32_t src, double *x) {
+                const double2 *v = reinterpret_cast<const double2 *>(Ke + (int64_t)(src & 0x7fffffffu) * KE_PITCH);
+#pragma unroll
+                for (int h = 0; h < 5; ++h) {
+                    const double2 t = __ldg(v + h);
+                    x[2 * h] = t.x;
+                    x[2 * h + 1] = t.y;
+                }
+            };
+            const int32_t l1 = cptr[p + 1];
+            int32_t l = cptr[p];
+            for (; l + 1 < l1; l += 2) {
+                const uint32_t s0 = contrib[l], s1 = contrib[l + 1];
+                double x0[10], x1[10];
+                fetch(s0, x0);
+                fetch(s1, x1);
+                add(s0, x0);
+                add(s1, x1);
+            }
+            if (l < l1) {
+                const uint32_t s0 = contrib[l];
+                double x0[10];
+                fetch(s0, x0);
+                add(s0, x0);
             }
         }
 #pragma unroll

@@ -59,10 +59,12 @@ struct sg_krylov {
     // blocked A-orthogonalisation: A times the block's input columns (n x 16), the block's
     // coefficients against earlier columns (256 x 16) and the per-CTA partial sums
     double *atb = nullptr, *cblk = nullptr, *tspart = nullptr;
-    // Gram-matrix A-orthogonalisation (default, aorth_mode 1): G, T and the output-ordered T
-    // (3 kcap^2), the Gram partial sums (GR_CTAS x 64 x 64) and the kept count on the device
+    // Gram-matrix A-orthogonalisation (default, aorth_mode 1): G, T, the output-ordered T and
+    // the output columns' processing indices (3 kcap^2 + kcap), the Gram partial sums
+    // (GR_CTAS x 64 x 64) and the kept count on the device
     double *gram = nullptr, *gpart = nullptr;
     int32_t *gkout = nullptr;
+    double *spy = nullptr;      // n x 8: interleaved products of the long-vector SpMM
     int aorth_mode = 1;
 };
 
@@ -80,7 +82,7 @@ static int ensure_kcap(sg_krylov *ws, int64_t k) {
     SG_CUDA(sg::device_alloc(&nt, sizeof(double) * (cap + 8)));
     SG_CUDA(sg::device_alloc(&sig, sizeof(double) * (cap + 8)));
     double *gram = nullptr;
-    SG_CUDA(sg::device_alloc(&gram, sizeof(double) * 3 * cap * cap));
+    SG_CUDA(sg::device_alloc(&gram, sizeof(double) * (3 * cap * cap + cap)));
     cudaFree(ws->gram);
     ws->gram = gram;
     cudaFree(ws->part);
@@ -434,7 +436,7 @@ extern "C" int sg_krylov_destroy(sg_krylov *ws) {
     cudaFree(ws->sig);
     graph_release(ws);
     cudaFree(ws->atb); cudaFree(ws->cblk); cudaFree(ws->tspart);
-    cudaFree(ws->gram); cudaFree(ws->gpart); cudaFree(ws->gkout);
+    cudaFree(ws->gram); cudaFree(ws->gpart); cudaFree(ws->gkout); cudaFree(ws->spy);
     cudaFree(ws->u); cudaFree(ws->dstate); cudaFree(ws->dscal); cudaFree(ws->dH); cudaFree(ws->dcs);
     cudaFree(ws->dsn); cudaFree(ws->dg); cudaFree(ws->dy); cudaFree(ws->dhist); cudaFree(ws->dptr);
     if (ws->cap) cudaStreamDestroy(ws->cap);
@@ -610,13 +612,14 @@ extern "C" int sg_a_orthogonalize(sg_krylov *ws, const sg_bsr *A, const double *
     // products do not depend on the orthogonalisation, and one SpMM reads A once per eight
     // columns where a SpMV per column reads it k times
     if (A->b == 3 && k >= 4 && (double)n * 8 * 8 > 48e6) {
-        // long vectors: interleaved copies of 8 columns (scratch: the block buffer and Z)
+        // long vectors: interleaved copies of 8 columns (scratch: the block buffer and spy)
         if (!ws->atb) {
             SG_CUDA(device_alloc(&ws->atb, sizeof(double) * n * 16));
             SG_CUDA(device_alloc(&ws->cblk, sizeof(double) * 256 * 16));
             SG_CUDA(device_alloc(&ws->tspart, sizeof(double) * TS_PART_CTAS * 256 * 16));
         }
-        rc = bsr_spmm_interleaved(*A, Avals, W + (int64_t)(k - 1) * n, -n, AWo, n, k, ws->atb, ws->atb + n * 8, st);
+        if (!ws->spy) SG_CUDA(device_alloc(&ws->spy, sizeof(double) * n * 8));
+        rc = bsr_spmm_interleaved(*A, Avals, W + (int64_t)(k - 1) * n, -n, AWo, n, k, ws->atb, ws->spy, st);
     } else if (A->b == 3) {
         rc = bsr_spmm(*A, Avals, W + (int64_t)(k - 1) * n, -n, AWo, n, k, st);
     } else {
@@ -631,11 +634,12 @@ extern "C" int sg_a_orthogonalize(sg_krylov *ws, const sg_bsr *A, const double *
             SG_CUDA(device_alloc(&ws->gkout, sizeof(int32_t) * 4));
         }
         double *G = ws->gram, *Tp = G + (int64_t)k * k, *Ta = Tp + (int64_t)k * k;
+        int32_t *pmap = reinterpret_cast<int32_t *>(Ta + (int64_t)k * k);
         const double *S = W + (int64_t)(k - 1) * n;   // processing order: column i is W's k - 1 - i
         if ((rc = gram_upper(n, k, S, -n, AWo, n, G, ws->gpart, st))) return rc;
-        if ((rc = gram_recurrence(k, G, Tp, eps_add, Ta, nt, sig, ws->gkout, st))) return rc;
-        if ((rc = ts_apply(n, k, ws->gkout, S, -n, Ta, Wo, n, st))) return rc;
-        if (AW && (rc = ts_apply(n, k, ws->gkout, AWo, n, Ta, AW, n, st))) return rc;
+        if ((rc = gram_recurrence(k, G, Tp, eps_add, Ta, nt, sig, ws->gkout, pmap, st))) return rc;
+        if ((rc = ts_apply(n, k, ws->gkout, pmap, S, -n, Ta, Wo, n, st))) return rc;
+        if (AW && (rc = ts_apply(n, k, ws->gkout, pmap, AWo, n, Ta, AW, n, st))) return rc;
         int32_t ko = 0;
         SG_CUDA(cudaMemcpyAsync(&ko, ws->gkout, sizeof(int32_t), cudaMemcpyDeviceToHost, st));
         SG_CUDA(cudaStreamSynchronize(st));

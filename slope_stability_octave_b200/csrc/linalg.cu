@@ -327,78 +327,85 @@ static void spmm_pass(const sg_bsr &A, int G, const double *vals, const double *
     }
 }
 
-// Node-interleaved SpMM for many vectors: the 8 columns of a pass are packed so that node j's
-// three components of all 8 columns are one contiguous run of 24 doubles; a block's x gather is
-// then 192 contiguous bytes (12 16-byte loads) however far apart the original columns lie.  G
-// lanes per block row, lane l taking the row's blocks l, l + G, ...; the 24 partial sums of the
-// row are combined by a fixed shuffle tree (reproducible).
-constexpr int SPI_KC = 8;
-constexpr int SPI_G = 8;    // lanes per block row (8, 16, 32 measured: 8 fastest on the 3M-DOF slope)
+// Node-interleaved SpMM for many vectors: the KC (8 or 16) columns of a pass are packed so that
+// node j's three components of all KC columns are one contiguous run of 3 KC doubles
+// ([component][column]); a block's x gather is then 24 KC contiguous bytes however far apart
+// the original columns lie.  A warp computes one block row (the lane mapping is described at
+// the kernel); the sums are combined in a fixed order, so the result is reproducible.
+// pack: element (row r, column c) per thread, c fastest (whole 32-byte sectors of each column
+// read by neighbouring threads, consecutive doubles written)
+template <int KC>
 __global__ void k_pack_cols(int64_t n, int kc, const double *__restrict__ X, int64_t ldx,
                             double *__restrict__ Xi) {
-    for (int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; r < n; r += (int64_t)gridDim.x * blockDim.x) {
-#pragma unroll
-        for (int c = 0; c < SPI_KC; ++c) Xi[r * SPI_KC + c] = c < kc ? X[c * ldx + r] : 0.0;
+    const int64_t total = n * KC;
+    for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < total; e += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t r = e / KC;
+        const int c = (int)(e - r * KC);
+        Xi[e] = c < kc ? X[c * ldx + r] : 0.0;
     }
 }
+template <int KC>
 __global__ void k_unpack_cols(int64_t n, int kc, const double *__restrict__ Yi, double *__restrict__ Y,
                               int64_t ldy) {
-    for (int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; r < n; r += (int64_t)gridDim.x * blockDim.x) {
-        for (int c = 0; c < kc; ++c) Y[c * ldy + r] = Yi[r * SPI_KC + c];
+    const int64_t total = n * KC;
+    for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < total; e += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t r = e / KC;
+        const int c = (int)(e - r * KC);
+        if (c < kc) Y[c * ldy + r] = Yi[e];
     }
 }
 
-template <int G>
+template <int KC>
 __global__ void __launch_bounds__(256) k_spmm3i(int64_t nrows, const int32_t *__restrict__ rp,
                                                 const int32_t *__restrict__ col, const double *__restrict__ vals,
                                                 const double *__restrict__ Xi, double *__restrict__ Yi) {
-    constexpr int GPW = 32 / G;
-    const int lane = threadIdx.x & 31, g = lane / G, gl = lane - g * G;
-    const int64_t warp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
-    const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
-    for (int64_t base = warp * GPW; base < nrows; base += nwarps * GPW) {
-        const int64_t row = base + g;
-        double acc[3][SPI_KC];
-#pragma unroll
-        for (int a = 0; a < 3; ++a)
-#pragma unroll
-            for (int c = 0; c < SPI_KC; ++c) acc[a][c] = 0.0;
-        if (row < nrows) {
-            const int32_t p1 = rp[row + 1];
-            for (int32_t p = rp[row] + gl; p < p1; p += G) {
-                const int64_t j = col[p];
-                double v[9];
-#pragma unroll
-                for (int t = 0; t < 9; ++t) v[t] = __ldg(vals + (int64_t)p * 9 + t);
-                const double2 *xj = reinterpret_cast<const double2 *>(Xi + j * 3 * SPI_KC);
-#pragma unroll
-                for (int b = 0; b < 3; ++b) {
-                    double x[SPI_KC];
-#pragma unroll
-                    for (int h = 0; h < SPI_KC / 2; ++h) {
-                        const double2 t = __ldg(xj + b * (SPI_KC / 2) + h);
-                        x[2 * h] = t.x;
-                        x[2 * h + 1] = t.y;
-                    }
-#pragma unroll
-                    for (int a = 0; a < 3; ++a)
-#pragma unroll
-                        for (int c = 0; c < SPI_KC; ++c) acc[a][c] += v[a * 3 + b] * x[c];
-                }
+    // a warp per block row; lane = (block slot bs in 0 .. 32/KC - 1, column c in 0 .. KC - 1):
+    // the warp takes the row's blocks 32/KC at a time, the lanes of a slot load their block's
+    // nine values together (coalesced requests) and hand them round by shuffles, each lane
+    // reads column c of x_j; the slots' sums are combined by a fixed tree at the end
+    constexpr int NS = 32 / KC;
+    const int lane = threadIdx.x & 31, c = lane & (KC - 1), bs = lane / KC, base = lane & ~(KC - 1);
+    const int64_t w0 = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+    const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    for (int64_t row = w0; row < nrows; row += nw) {
+        double y0 = 0.0, y1 = 0.0, y2 = 0.0;
+        const int32_t p1 = rp[row + 1];
+        for (int32_t p0 = rp[row]; p0 < p1; p0 += NS) {
+            const int32_t p = p0 + bs;
+            const bool live = p < p1;
+            int64_t j = 0;
+            double av = 0.0, a8 = 0.0;
+            if (live) {
+                j = col[p];
+                if (c < 9) av = __ldg(vals + (int64_t)p * 9 + c);
+                if (KC == 8 && c == 0) a8 = __ldg(vals + (int64_t)p * 9 + 8);
             }
+            double u0 = 0.0, u1 = 0.0, u2 = 0.0;
+            if (live) {
+                const double *x = Xi + j * 3 * KC + c;
+                u0 = __ldg(x);
+                u1 = __ldg(x + KC);
+                u2 = __ldg(x + 2 * KC);
+            }
+            double a[9];
+#pragma unroll
+            for (int t = 0; t < 8; ++t) a[t] = __shfl_sync(0xffffffffu, av, base + t);
+            a[8] = KC == 8 ? __shfl_sync(0xffffffffu, a8, base) : __shfl_sync(0xffffffffu, av, base + 8);
+            y0 += a[0] * u0 + a[1] * u1 + a[2] * u2;
+            y1 += a[3] * u0 + a[4] * u1 + a[5] * u2;
+            y2 += a[6] * u0 + a[7] * u1 + a[8] * u2;
         }
 #pragma unroll
-        for (int off = G / 2; off > 0; off >>= 1)
-#pragma unroll
-            for (int a = 0; a < 3; ++a)
-#pragma unroll
-                for (int c = 0; c < SPI_KC; ++c) acc[a][c] += __shfl_xor_sync(0xffffffffu, acc[a][c], off);
-        if (row < nrows && gl == 0) {
-            double2 *yr = reinterpret_cast<double2 *>(Yi + row * 3 * SPI_KC);
-#pragma unroll
-            for (int a = 0; a < 3; ++a)
-#pragma unroll
-                for (int h = 0; h < SPI_KC / 2; ++h) yr[a * (SPI_KC / 2) + h] = make_double2(acc[a][2 * h], acc[a][2 * h + 1]);
+        for (int off = KC; off < 32; off <<= 1) {
+            y0 += __shfl_xor_sync(0xffffffffu, y0, off);
+            y1 += __shfl_xor_sync(0xffffffffu, y1, off);
+            y2 += __shfl_xor_sync(0xffffffffu, y2, off);
+        }
+        if (bs == 0) {
+            double *yr = Yi + row * 3 * KC + c;
+            yr[0] = y0;
+            yr[KC] = y1;
+            yr[2 * KC] = y2;
         }
     }
 }
@@ -407,14 +414,24 @@ int bsr_spmm_interleaved(const sg_bsr &A, const double *vals, const double *X, i
                          int k, double *Xi, double *Yi, cudaStream_t st) {
     if (A.b != 3) return set_error(SG_ERR_ARG, "bsr_spmm: 3x3 blocks only");
     const int64_t n = A.n_rows * 3;
-    for (int c0 = 0; c0 < k; c0 += SPI_KC) {
-        const int kc = std::min(SPI_KC, k - c0);
+    // columns per pass: 16-column passes measured no faster per column than 8-column ones
+    // (the cost per block column is the L2 traffic of the x gathers), so 8, with less scratch
+    const int KC = 8;
+    for (int c0 = 0; c0 < k; c0 += KC) {
+        const int kc = std::min(KC, k - c0);
         const InstrToken tk = instr_begin(IK_SPMM_AORTH, st);
         instr_units(IK_SPMM_AORTH, kc);
-        const unsigned gp = grid_for(n, 256, 8);
-        k_pack_cols<<<gp, 256, 0, st>>>(n, kc, X + c0 * ldx, ldx, Xi);
-        k_spmm3i<SPI_G><<<grid_for(A.n_rows * SPI_G, 256, 16), 256, 0, st>>>(A.n_rows, A.d_row_ptr, A.d_col, vals, Xi, Yi);
-        k_unpack_cols<<<grid_for(n, 256, 8), 256, 0, st>>>(n, kc, Yi, Y + c0 * ldy, ldy);
+        const unsigned gp = grid_for(n * KC, 256, 16), gm = grid_for(A.n_rows * 32, 256, 8),
+                       gu = grid_for(n * KC, 256, 16);
+        if (KC == 16) {
+            k_pack_cols<16><<<gp, 256, 0, st>>>(n, kc, X + c0 * ldx, ldx, Xi);
+            k_spmm3i<16><<<gm, 256, 0, st>>>(A.n_rows, A.d_row_ptr, A.d_col, vals, Xi, Yi);
+            k_unpack_cols<16><<<gu, 256, 0, st>>>(n, kc, Yi, Y + c0 * ldy, ldy);
+        } else {
+            k_pack_cols<8><<<gp, 256, 0, st>>>(n, kc, X + c0 * ldx, ldx, Xi);
+            k_spmm3i<8><<<gm, 256, 0, st>>>(A.n_rows, A.d_row_ptr, A.d_col, vals, Xi, Yi);
+            k_unpack_cols<8><<<gu, 256, 0, st>>>(n, kc, Yi, Y + c0 * ldy, ldy);
+        }
         instr_end(tk, st);
         SG_CUDA(cudaGetLastError());
     }
@@ -761,9 +778,10 @@ __device__ __forceinline__ void cp_async_wait1() { asm volatile("cp.async.wait_g
 // Partial sums of one 16 NA x 16 NA tile of G (rows m0 + [0, 16 NA), columns i0 + [0, 16 NA))
 // over this CTA's row range, in tiles of GR_R rows staged in shared memory ([column][row],
 // padded) by 8-byte cp.async, two stages; thread (mb, ib) owns the entries
-// (m0 + mb + 16 a, i0 + ib + 16 b).  part: gridDim.x x (16 NA)^2.
+// (m0 + mb + 16 a, i0 + ib + 16 b).  part: gridDim.x x (16 NA)^2.  On a diagonal tile
+// (DIAG, m0 == i0) the products with a > b, all below the diagonal, are not formed.
 constexpr int GR_R = 32, GR_LD = GR_R + 1;
-template <int NA>
+template <int NA, bool DIAG>
 __global__ void __launch_bounds__(256) k_gram_partial(int64_t n, int k, const double *__restrict__ S, int64_t lds,
                                                       const double *__restrict__ AS, int64_t ldas, int m0, int i0,
                                                       double *__restrict__ part) {
@@ -808,7 +826,8 @@ __global__ void __launch_bounds__(256) k_gram_partial(int64_t n, int k, const do
 #pragma unroll
             for (int a = 0; a < NA; ++a)
 #pragma unroll
-                for (int b = 0; b < NA; ++b) acc[a][b] += sv[a] * xv[b];
+                for (int b = 0; b < NA; ++b)
+                    if (!DIAG || a <= b) acc[a][b] += sv[a] * xv[b];   // (a > b): m > i, unused
         }
         __syncthreads();
     }
@@ -819,27 +838,35 @@ __global__ void __launch_bounds__(256) k_gram_partial(int64_t n, int k, const do
         for (int b = 0; b < NA; ++b) out[(mb + 16 * a) * TW + ib + 16 * b] = acc[a][b];
 }
 
-// G(m0 + ml, i0 + il) = sum over the CTAs of the partials, in CTA order (ldg: G's leading dimension)
+// G(m0 + ml, i0 + il) = the sum of the CTAs' partials: a warp per entry, lane l adding the
+// partials l, l + 32, ... and a fixed shuffle tree combining the lanes (ldg: G's leading
+// dimension)
 __global__ void k_gram_reduce(int k, int TW, int nparts, const double *__restrict__ part, int m0, int i0,
                               double *__restrict__ G, int ldg) {
-    for (int o = blockIdx.x * blockDim.x + threadIdx.x; o < TW * TW; o += gridDim.x * blockDim.x) {
+    const int lane = threadIdx.x & 31;
+    const int nw = (gridDim.x * blockDim.x) >> 5;
+    for (int o = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; o < TW * TW; o += nw) {
         const int ml = o / TW, il = o - ml * TW;
-        if (m0 + ml >= k || i0 + il >= k) continue;
+        if (m0 + ml >= k || i0 + il >= k) continue;   // uniform over the warp
         double s = 0.0;
-        for (int p = 0; p < nparts; ++p) s += part[(int64_t)p * TW * TW + o];
-        G[(m0 + ml) + (int64_t)(i0 + il) * ldg] = s;
+        for (int p = lane; p < nparts; p += 32) s += part[(int64_t)p * TW * TW + o];
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1) s += __shfl_xor_sync(0xffffffffu, s, off);
+        if (lane == 0) G[(m0 + ml) + (int64_t)(i0 + il) * ldg] = s;
     }
 }
 
 // The recurrence on one CTA.  G: k x k column-major (entries m <= i used); Tp: k x k scratch
 // (column p = the coefficients of kept column p in S, zero when dropped); out: Ta k x k,
 // row-major [m][o], the columns of T in output order (kept columns, last processed first);
-// nt[i] = the A-norm^2 of column i, sig[i] its sign; *kout = the number kept.  G and Tp are
-// staged in shared memory when 2 k^2 doubles fit (smem_k2 != 0).
+// nt[i] = the A-norm^2 of column i, sig[i] its sign; *kout = the number kept and pmap[o] the
+// processing index of output column o (decreasing in o).  G and Tp are staged in shared
+// memory when 2 k^2 doubles fit (smem_k2 != 0).
 __global__ void __launch_bounds__(256) k_gram_recurrence(int k, const double *__restrict__ Gg, double *__restrict__ Tpg,
                                                          double eps, double *__restrict__ Ta,
                                                          double *__restrict__ nt, double *__restrict__ sig,
-                                                         int32_t *__restrict__ kout, int smem_k2) {
+                                                         int32_t *__restrict__ kout, int32_t *__restrict__ pmap,
+                                                         int smem_k2) {
     extern __shared__ double rsm[];   // [c: k][t: k][red: 256][map: k ints] (+ G, Tp when staged)
     double *c = rsm, *tv = c + k, *red = tv + k;
     int *map = reinterpret_cast<int *>(red + 256);
@@ -903,6 +930,7 @@ __global__ void __launch_bounds__(256) k_gram_recurrence(int k, const double *__
     }
     __syncthreads();
     const int ko = (int)red[0];
+    for (int o = tid; o < ko; o += 256) pmap[o] = map[o];
     for (int e = tid; e < k * k; e += 256) {
         const int m = e / k, o = e - m * k;
         Ta[e] = o < ko ? Tp[m + (int64_t)map[o] * k] : 0.0;
@@ -912,21 +940,23 @@ __global__ void __launch_bounds__(256) k_gram_recurrence(int k, const double *__
 // Y(:, o) = X(:, 0:k) Ta(:, o) for o < *kout, output columns in chunks of 8 NJ (blockIdx.y):
 // X rows in tiles of TA_R, columns of X (and rows of Ta) in stages of TA_MC through shared
 // memory (8-byte cp.async, two stages); thread (lane, warp) owns rows lane + 32 q and output
-// columns o0 + warp + 8 j.
+// columns o0 + warp NJ + j.
 constexpr int TA_R = 128, TA_MC = 16;
 template <int NJ>
-__global__ void __launch_bounds__(256) k_ts_apply(int64_t n, int k, const int32_t *__restrict__ kout,
-                                                  const double *__restrict__ X, int64_t ldx,
-                                                  const double *__restrict__ Ta, double *__restrict__ Y,
+__global__ void __launch_bounds__(256, (NJ > 4 ? 2 : 3)) k_ts_apply(int64_t n, int k, const int32_t *__restrict__ kout,
+                                                  const int32_t *__restrict__ pmap, const double *__restrict__ X,
+                                                  int64_t ldx, const double *__restrict__ Ta, double *__restrict__ Y,
                                                   int64_t ldy) {
     constexpr int OC = 8 * NJ;
     __shared__ double sX[2][TA_MC][TA_R];
-    __shared__ double sT[2][TA_MC][OC];
+    __shared__ __align__(16) double sT[2][TA_MC][OC];
     const int ko = *kout;
     const int o0 = blockIdx.y * OC;
     if (o0 >= ko) return;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    const int nmc = (k + TA_MC - 1) / TA_MC;
+    // the chunk's columns depend on inputs 0 .. pmap[o0] only (Ta is zero below)
+    const int kk = min(k, pmap[o0] + 1);
+    const int nmc = (kk + TA_MC - 1) / TA_MC;
     const int64_t ntiles = (n + TA_R - 1) / TA_R;
     const int64_t nsteps = ((ntiles - blockIdx.x + gridDim.x - 1) / gridDim.x) * nmc;   // (tile, chunk) pairs
     if (blockIdx.x >= ntiles) return;
@@ -937,13 +967,13 @@ __global__ void __launch_bounds__(256) k_ts_apply(int64_t n, int k, const int32_
             const int cc = e / TA_R, r = e - cc * TA_R;
             const int64_t row = rt + r;
             const int col = mc + cc;
-            if (row < n && col < k) cp_async8(&sX[st][cc][r], X + col * ldx + row);
+            if (row < n && col < kk) cp_async8(&sX[st][cc][r], X + col * ldx + row);
             else sX[st][cc][r] = 0.0;
         }
         for (int e = tid; e < TA_MC * OC; e += 256) {
             const int cc = e / OC, oo = e - cc * OC;
             const int m = mc + cc, o = o0 + oo;
-            sT[st][cc][oo] = (m < k && o < ko) ? Ta[(int64_t)m * k + o] : 0.0;
+            sT[st][cc][oo] = (m < kk && o < ko) ? Ta[(int64_t)m * k + o] : 0.0;
         }
     };
     double acc[4][NJ];
@@ -966,8 +996,18 @@ __global__ void __launch_bounds__(256) k_ts_apply(int64_t n, int k, const int32_
             double xv[4], tw[NJ];
 #pragma unroll
             for (int q = 0; q < 4; ++q) xv[q] = sX[st][cc][lane + 32 * q];
+            if constexpr (NJ % 2 == 0) {   // the warp's NJ coefficients as NJ/2 16-byte broadcasts
+                const double2 *t2 = reinterpret_cast<const double2 *>(&sT[st][cc][warp * NJ]);
 #pragma unroll
-            for (int j = 0; j < NJ; ++j) tw[j] = sT[st][cc][warp + 8 * j];
+                for (int j = 0; j < NJ / 2; ++j) {
+                    const double2 v = t2[j];
+                    tw[2 * j] = v.x;
+                    tw[2 * j + 1] = v.y;
+                }
+            } else {
+#pragma unroll
+                for (int j = 0; j < NJ; ++j) tw[j] = sT[st][cc][warp * NJ + j];
+            }
 #pragma unroll
             for (int q = 0; q < 4; ++q)
 #pragma unroll
@@ -978,7 +1018,7 @@ __global__ void __launch_bounds__(256) k_ts_apply(int64_t n, int k, const int32_
             const int64_t rt = (blockIdx.x + (s / nmc) * gridDim.x) * TA_R;
 #pragma unroll
             for (int j = 0; j < NJ; ++j) {
-                const int o = o0 + warp + 8 * j;
+                const int o = o0 + warp * NJ + j;
                 if (o >= ko) continue;
 #pragma unroll
                 for (int q = 0; q < 4; ++q) {
@@ -998,9 +1038,11 @@ int gram_upper(int64_t n, int k, const double *S, int64_t lds, const double *AS,
     const size_t smem = sizeof(double) * 2 * 2 * TW * GR_LD;
     static thread_local bool configured = false;
     if (!configured) {   // stages of 48- and 64-wide tiles exceed the default 48 KB
-        SG_CUDA(cudaFuncSetAttribute(k_gram_partial<3>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        SG_CUDA(cudaFuncSetAttribute(k_gram_partial<3, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                      (int)(sizeof(double) * 2 * 2 * 48 * GR_LD)));
-        SG_CUDA(cudaFuncSetAttribute(k_gram_partial<4>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        SG_CUDA(cudaFuncSetAttribute(k_gram_partial<4, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)(sizeof(double) * 2 * 2 * 64 * GR_LD)));
+        SG_CUDA(cudaFuncSetAttribute(k_gram_partial<4, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                      (int)(sizeof(double) * 2 * 2 * 64 * GR_LD)));
         configured = true;
     }
@@ -1010,19 +1052,22 @@ int gram_upper(int64_t n, int k, const double *S, int64_t lds, const double *AS,
             count_launch(2);
             const int m0 = q * TW, i0 = p * TW;
             switch (NA) {
-                case 1: k_gram_partial<1><<<GR_CTAS, 256, smem, st>>>(n, k, S, lds, AS, ldas, m0, i0, part); break;
-                case 2: k_gram_partial<2><<<GR_CTAS, 256, smem, st>>>(n, k, S, lds, AS, ldas, m0, i0, part); break;
-                case 3: k_gram_partial<3><<<GR_CTAS, 256, smem, st>>>(n, k, S, lds, AS, ldas, m0, i0, part); break;
-                default: k_gram_partial<4><<<GR_CTAS, 256, smem, st>>>(n, k, S, lds, AS, ldas, m0, i0, part); break;
+                case 1: k_gram_partial<1, true><<<GR_CTAS, 256, smem, st>>>(n, k, S, lds, AS, ldas, m0, i0, part); break;
+                case 2: k_gram_partial<2, true><<<GR_CTAS, 256, smem, st>>>(n, k, S, lds, AS, ldas, m0, i0, part); break;
+                case 3: k_gram_partial<3, true><<<GR_CTAS, 256, smem, st>>>(n, k, S, lds, AS, ldas, m0, i0, part); break;
+                default:
+                    if (q == p) k_gram_partial<4, true><<<GR_CTAS, 256, smem, st>>>(n, k, S, lds, AS, ldas, m0, i0, part);
+                    else k_gram_partial<4, false><<<GR_CTAS, 256, smem, st>>>(n, k, S, lds, AS, ldas, m0, i0, part);
+                    break;
             }
-            k_gram_reduce<<<(TW * TW + 255) / 256, 256, 0, st>>>(k, TW, GR_CTAS, part, m0, i0, G, k);
+            k_gram_reduce<<<(TW * TW * 32 + 255) / 256, 256, 0, st>>>(k, TW, GR_CTAS, part, m0, i0, G, k);
             SG_CUDA(cudaGetLastError());
         }
     return SG_OK;
 }
 
 int gram_recurrence(int k, const double *G, double *Tp, double eps, double *Ta, double *nt, double *sig,
-                    int32_t *kout, cudaStream_t st) {
+                    int32_t *kout, int32_t *pmap, cudaStream_t st) {
     if (k <= 0) return SG_OK;
     const size_t base = sizeof(double) * (2 * (size_t)k + 256 + (k + 1) / 2);
     const size_t full = base + sizeof(double) * 2 * (size_t)k * k;
@@ -1034,28 +1079,40 @@ int gram_recurrence(int k, const double *G, double *Tp, double eps, double *Ta, 
         configured = smem;
     }
     count_launch();
-    k_gram_recurrence<<<1, 256, smem, st>>>(k, G, Tp, eps, Ta, nt, sig, kout, staged ? 1 : 0);
+    k_gram_recurrence<<<1, 256, smem, st>>>(k, G, Tp, eps, Ta, nt, sig, kout, pmap, staged ? 1 : 0);
     SG_CUDA(cudaGetLastError());
     return SG_OK;
 }
 
-int ts_apply(int64_t n, int k, const int32_t *kout, const double *X, int64_t ldx, const double *Ta, double *Y,
-             int64_t ldy, cudaStream_t st) {
+int ts_apply(int64_t n, int k, const int32_t *kout, const int32_t *pmap, const double *X, int64_t ldx,
+             const double *Ta, double *Y, int64_t ldy, cudaStream_t st) {
     if (k <= 0 || n <= 0) return SG_OK;
     const int nj = k >= 64 ? 8 : (k + 7) / 8;
     const int oc = 8 * nj;
     const int64_t ntiles = (n + TA_R - 1) / TA_R;
-    const dim3 grid((unsigned)std::min<int64_t>(ntiles, (int64_t)sm_count() * 2), (unsigned)((k + oc - 1) / oc));
+    // CTAs resident per SM for this variant (registers and shared memory), once per variant
+    static thread_local int resident[9] = {};
+    if (!resident[nj]) {
+        const void *fn = nj == 1 ? (const void *)k_ts_apply<1> : nj == 2 ? (const void *)k_ts_apply<2>
+                       : nj == 3 ? (const void *)k_ts_apply<3> : nj == 4 ? (const void *)k_ts_apply<4>
+                       : nj == 5 ? (const void *)k_ts_apply<5> : nj == 6 ? (const void *)k_ts_apply<6>
+                       : nj == 7 ? (const void *)k_ts_apply<7> : (const void *)k_ts_apply<8>;
+        int r = 0;
+        SG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&r, fn, 256, 0));
+        resident[nj] = std::max(1, r);
+    }
+    const dim3 grid((unsigned)std::min<int64_t>(ntiles, (int64_t)sm_count() * resident[nj]),
+                    (unsigned)((k + oc - 1) / oc));
     count_launch();
     switch (nj) {
-        case 1: k_ts_apply<1><<<grid, 256, 0, st>>>(n, k, kout, X, ldx, Ta, Y, ldy); break;
-        case 2: k_ts_apply<2><<<grid, 256, 0, st>>>(n, k, kout, X, ldx, Ta, Y, ldy); break;
-        case 3: k_ts_apply<3><<<grid, 256, 0, st>>>(n, k, kout, X, ldx, Ta, Y, ldy); break;
-        case 4: k_ts_apply<4><<<grid, 256, 0, st>>>(n, k, kout, X, ldx, Ta, Y, ldy); break;
-        case 5: k_ts_apply<5><<<grid, 256, 0, st>>>(n, k, kout, X, ldx, Ta, Y, ldy); break;
-        case 6: k_ts_apply<6><<<grid, 256, 0, st>>>(n, k, kout, X, ldx, Ta, Y, ldy); break;
-        case 7: k_ts_apply<7><<<grid, 256, 0, st>>>(n, k, kout, X, ldx, Ta, Y, ldy); break;
-        default: k_ts_apply<8><<<grid, 256, 0, st>>>(n, k, kout, X, ldx, Ta, Y, ldy); break;
+        case 1: k_ts_apply<1><<<grid, 256, 0, st>>>(n, k, kout, pmap, X, ldx, Ta, Y, ldy); break;
+        case 2: k_ts_apply<2><<<grid, 256, 0, st>>>(n, k, kout, pmap, X, ldx, Ta, Y, ldy); break;
+        case 3: k_ts_apply<3><<<grid, 256, 0, st>>>(n, k, kout, pmap, X, ldx, Ta, Y, ldy); break;
+        case 4: k_ts_apply<4><<<grid, 256, 0, st>>>(n, k, kout, pmap, X, ldx, Ta, Y, ldy); break;
+        case 5: k_ts_apply<5><<<grid, 256, 0, st>>>(n, k, kout, pmap, X, ldx, Ta, Y, ldy); break;
+        case 6: k_ts_apply<6><<<grid, 256, 0, st>>>(n, k, kout, pmap, X, ldx, Ta, Y, ldy); break;
+        case 7: k_ts_apply<7><<<grid, 256, 0, st>>>(n, k, kout, pmap, X, ldx, Ta, Y, ldy); break;
+        default: k_ts_apply<8><<<grid, 256, 0, st>>>(n, k, kout, pmap, X, ldx, Ta, Y, ldy); break;
     }
     SG_CUDA(cudaGetLastError());
     return SG_OK;

@@ -28,8 +28,8 @@ int bsr_spmm(const sg_bsr &A, const double *vals, const double *X, int64_t ldx, 
              cudaStream_t st);
 
 // The same product through node-interleaved copies of 8 columns at a time (Xi, Yi: 8 n
-// doubles each, 16-byte aligned scratch): for many columns of long vectors, whose column-wise
-// gathers would not stay in L2.
+// doubles each of scratch): for many columns of long vectors, whose column-wise gathers would
+// not stay in L2.
 int bsr_spmm_interleaved(const sg_bsr &A, const double *vals, const double *X, int64_t ldx, double *Y, int64_t ldy,
                          int k, double *Xi, double *Yi, cudaStream_t st);
 
@@ -69,15 +69,17 @@ int gemm_nn_sub(int64_t n, int m, int b, const double *U, int64_t ldu, const dou
 //                    part: GR_CTAS * 64 * 64 doubles of scratch), deterministic;
 //   gram_recurrence  T, the A-norms^2 nt, the signs sig and *kout (device) from G on one CTA;
 //                    Ta (k x k, row-major [m][o]) holds the kept columns' coefficients in
-//                    output order (last processed first); Tp: k x k scratch;
-//   ts_apply         Y(:, o) = X(:, 0:k) Ta(:, o) for o < *kout.
-constexpr int GR_CTAS = 296;
+//                    output order (last processed first), pmap (k ints) their processing
+//                    indices; Tp: k x k scratch;
+//   ts_apply         Y(:, o) = X(:, 0:k) Ta(:, o) for o < *kout (inputs past pmap[o] skipped:
+//                    their coefficients are zero).
+constexpr int GR_CTAS = 444;   // 3 per SM
 int gram_upper(int64_t n, int k, const double *S, int64_t lds, const double *AS, int64_t ldas, double *G,
                double *part, cudaStream_t st);
 int gram_recurrence(int k, const double *G, double *Tp, double eps, double *Ta, double *nt, double *sig,
-                    int32_t *kout, cudaStream_t st);
-int ts_apply(int64_t n, int k, const int32_t *kout, const double *X, int64_t ldx, const double *Ta, double *Y,
-             int64_t ldy, cudaStream_t st);
+                    int32_t *kout, int32_t *pmap, cudaStream_t st);
+int ts_apply(int64_t n, int k, const int32_t *kout, const int32_t *pmap, const double *X, int64_t ldx,
+             const double *Ta, double *Y, int64_t ldy, cudaStream_t st);
 
 // Device-count variants for graph-replayed loops// Device-count variants for graph-replayed loops: m = min(cnt[0] + add, mmax) columns, basis
 // V, or *Vp when V is null (both on the device)
