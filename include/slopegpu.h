@@ -174,6 +174,38 @@ int sg_assemble_kr_dev(sg_mesh *mesh, const double *DS, double r, const double *
 int sg_bsr_to_ref_dev(sg_mesh *mesh, const double *K, double *V_ref, void *stream);
 
 /* ------------------------------------------------------------------------------
+ * Unconfined seepage (+SEEPAGE: seepage_problem_3D.m / seepage_problem_2D.m, newton_flow.m)
+ * on the mechanical mesh.  The pore pressure is one value per node; its systems live in the
+ * mesh's node adjacency with 1 x 1 blocks (sg_mesh_bsr_scalar), usable with sg_amg_create
+ * (near-null space: the constant, nns = 1), sg_dfgmres_solve and sg_a_orthogonalize.
+ *   hat      n_q x n_p basis values at the quadrature points (HatP transposed: point-major)
+ *   conduct  n_int conductivity per point (heter_conduct.m); eps n_e penalty per element
+ *            (penalty_parameters_3D.m / _2D.m); gy dim x n_int = Bw * y (the gradient of the
+ *            vertical coordinate, q2 of seepage_problem_3D.m:43)
+ *   mask     n_n, 1 free / 0 Dirichlet node (Q_w); NULL leaves K and F unmasked
+ * ---------------------------------------------------------------------------- */
+/* borrowed pointer to the node adjacency with 1 x 1 blocks (device arrays shared with
+ * sg_mesh_bsr's pattern; valid until sg_mesh_destroy) */
+int sg_mesh_bsr_scalar(sg_mesh *mesh, const sg_bsr **bsr);
+/* K (n_blocks of the pattern, zeroed first, may be NULL) and F (n_n, zeroed first, may be
+ * NULL) at the pressure pw:
+ *   F = -Bw'(wc .* (Bw pw + grho kappa .* gy))      (newton_flow.m:120-123)
+ *   K = K_D + Bw' E C, E = conduct .* perm_r' .* weight .* (grho gy)   (newton_flow.m:104-118)
+ * kappa_mode 0: kappa = 0 and K = K_D (seepage_problem_2D.m initial right-hand side);
+ * 1: kappa = 1, K = K_D (seepage_problem_3D.m:42-46); 2: kappa = perm_r(pw_int), Newton
+ * tangent.  With mask, Dirichlet rows/columns of K become identity and F is zero there. */
+int sg_seepage_system_dev(const sg_mesh *mesh, const double *hat, const double *pw, const double *conduct,
+                          const double *eps, const double *gy, double grho, int32_t kappa_mode,
+                          const double *mask, double *K, double *F, void *stream);
+/* grad = Bw * field per integration point: field n_n, grad dim x n_int (point-major):
+ * q2 = Bw y (seepage_problem_3D.m:43) and grad_p = Bw pw (:62) */
+int sg_point_gradient_dev(const sg_mesh *mesh, const double *field, double *grad, void *stream);
+/* per element: mean (n_e, may be NULL) = weighted mean of pw over its integration points,
+ * sat (n_e, may be NULL) = mean >= 0.1 eps (seepage_problem_3D.m:63-74) */
+int sg_seepage_saturation_dev(const sg_mesh *mesh, const double *hat, const double *pw, const double *eps,
+                              double *mean, uint8_t *sat, void *stream);
+
+/* ------------------------------------------------------------------------------
  * (c2) Block sparse matrix-vector product and reductions (device pointers).
  * ---------------------------------------------------------------------------- */
 /* info[0..2] = block size, block rows, blocks */
@@ -198,11 +230,16 @@ int sg_axpby_dev(int64_t n, double a, const double *x, double b, double *y, void
  *              block graph); the numeric set-up runs during creation when given
  *   nullspace  (n_rows*b) x nns column-major host array; fixed: per-DOF 1 = Dirichlet (host)
  *   opts       [max_levels, coarse_size, cheb_degree, cheb_ratio, power_its, mixed(0/1),
- *               omega_scale, theta, fine_half(0/1)]; entries <= 0 keep the defaults (10, 1200,
- *               3, 10, 10, 0, 4/3, 0.02, 0) except theta, where 0 selects the whole block graph.
+ *               omega_scale, theta, fine_half(0/1), symmetric(0/1)]; entries <= 0 keep the
+ *               defaults (10, 1200, 3, 10, 10, 0, 4/3, 0.02, 0, 0) except theta, where 0 selects
+ *               the whole block graph.
  *               fine_half (mixed cycle, 3x3 blocks, theta > 0): the cycle's level-0 SpMVs read
  *               an FP16 copy of A scaled by a power of two (FP32 accumulation); the numeric
- *               set-up stays FP32
+ *               set-up stays FP32.
+ *               symmetric: the caller's A is symmetric (as K_r is), so each Galerkin matrix
+ *               P'AP is formed on and above its diagonal only and mirrored below it (half the
+ *               P'(AP) work, and A P only where those blocks read it); leave 0 for a
+ *               non-symmetric A (the seepage tangent)
  * ---------------------------------------------------------------------------- */
 typedef struct sg_amg sg_amg;
 int sg_amg_create(const sg_bsr *A, const double *A_vals, const double *nullspace, int32_t nns,

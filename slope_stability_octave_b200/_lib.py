@@ -48,6 +48,11 @@ SIGNATURES = {
     "sg_kr_blend_dev": [vp, f64, vp, vp, vp, vp],
     "sg_assemble_kr_dev": [vp, vp, f64, vp, vp, vp, vp],
     "sg_bsr_to_ref_dev": [vp, vp, vp, vp],
+    # seepage (pore pressure) systems on the mesh
+    "sg_mesh_bsr_scalar": [vp, vp],
+    "sg_seepage_system_dev": [vp, vp, vp, vp, vp, vp, f64, i32, vp, vp, vp, vp],
+    "sg_point_gradient_dev": [vp, vp, vp, vp],
+    "sg_seepage_saturation_dev": [vp, vp, vp, vp, vp, vp, vp],
     # sparse and vector operations
     "sg_bsr_info": [vp, vp],
     "sg_bsr_spmv_dev": [vp, vp, vp, vp, vp],
@@ -118,7 +123,10 @@ def lib() -> C.CDLL:
                 f"{LIB_PATH} not found: build it with `python -m slope_stability_octave_b200.build`")
         L = C.CDLL(LIB_PATH)
         for name, args in SIGNATURES.items():
-            fn = getattr(L, name)
+            # a symbol missing from an out-of-date build fails when it is called (AttributeError)
+            fn = getattr(L, name, None)
+            if fn is None:
+                continue
             fn.argtypes = args
             fn.restype = _RESTYPES.get(name, cint)
         _lib = L

@@ -80,6 +80,11 @@ struct Level {
     int32_t *d_R_from_P = nullptr;
     Plan at_plan, ap_plan, ac_plan;  // at: (A block) per P block; ap: (A, P); ac: (P, AP)
     int64_t ap_pairs = 0, ac_pairs = 0;  // plan lengths (pairs of input blocks)
+    // symmetric Galerkin product (option symmetric): ac_plan covers the coarse blocks (I, J)
+    // with I <= J only, d_ac_out[t] being their indices in the coarse pattern; the blocks
+    // below the diagonal are copied transposed from d_ac_lower_src into d_ac_lower
+    int64_t n_ac_items = 0, n_ac_lower = 0;
+    int32_t *d_ac_out = nullptr, *d_ac_lower = nullptr, *d_ac_lower_src = nullptr;
     double *Pv = nullptr, *Rv = nullptr, *APv = nullptr;
     float *P32 = nullptr, *R32 = nullptr;
     float *T32 = nullptr, *APv32 = nullptr;   // mixed form: FP32 numeric updates
@@ -101,6 +106,8 @@ struct AmgOptions {
     double omega_scale = 4.0 / 3.0;
     double theta = 0.02;      // strength threshold (0: whole block graph)
     int fine_half = 0;        // mixed form, 3x3 level 0: the cycle's level-0 SpMVs read an FP16 copy
+    int symmetric = 0;        // 1: A is symmetric, so every Galerkin matrix P'AP is: only its blocks
+                              // on and above the diagonal are formed, the others mirrored
 };
 
 }  // namespace sg
@@ -573,20 +580,23 @@ __global__ void k_gather_AP(int64_t nblk, const int64_t *__restrict__ lptr, cons
 
 // Ac block (I,J) = sum over plan pairs P_a' (BC x B) * AP_b (B x BC); dead DOFs get identity.
 // One thread per coarse block.
+// With qmap (symmetric Galerkin product) item t of the plan is coarse block qmap[t].
 template <int B, int BC, typename V = double>
-__global__ void k_gather_Ac(int64_t nblk, const int32_t *__restrict__ row, const int32_t *__restrict__ col,
-                            const int64_t *__restrict__ lptr, const int32_t *__restrict__ la,
-                            const int32_t *__restrict__ lb, const V *__restrict__ P,
-                            const V *__restrict__ AP, const uint8_t *__restrict__ dead,
+__global__ void k_gather_Ac(int64_t nitems, const int32_t *__restrict__ qmap, const int32_t *__restrict__ row,
+                            const int32_t *__restrict__ col, const int64_t *__restrict__ lptr,
+                            const int32_t *__restrict__ la, const int32_t *__restrict__ lb,
+                            const V *__restrict__ P, const V *__restrict__ AP, const uint8_t *__restrict__ dead,
                             V *__restrict__ Ac) {
-    for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q < nblk; q += (int64_t)gridDim.x * blockDim.x) {
+    for (int64_t it = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; it < nitems;
+         it += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t q = qmap ? (int64_t)qmap[it] : it;
         const int64_t I = row[q];
         {
             const int64_t J = col[q];
             double acc[BC * BC];
 #pragma unroll
             for (int t = 0; t < BC * BC; ++t) acc[t] = 0.0;
-            for (int64_t l = lptr[q]; l < lptr[q + 1]; ++l) {
+            for (int64_t l = lptr[it]; l < lptr[it + 1]; ++l) {
                 double p[B * BC], ap[B * BC];
                 load_block<B * BC>(P + (int64_t)la[l] * B * BC, p);
                 load_block<B * BC>(AP + (int64_t)lb[l] * B * BC, ap);
@@ -654,22 +664,22 @@ __global__ void k_gather_AP_warp(int64_t nblk, const int64_t *__restrict__ lptr,
 }
 
 template <int B, int BC, typename V = double, int G = 32>
-__global__ void k_gather_Ac_warp(int64_t nblk, const int32_t *__restrict__ row, const int32_t *__restrict__ col,
-                                 const int64_t *__restrict__ lptr, const int32_t *__restrict__ la,
-                                 const int32_t *__restrict__ lb, const V *__restrict__ P,
-                                 const V *__restrict__ AP, const uint8_t *__restrict__ dead,
-                                 V *__restrict__ Ac) {
+__global__ void k_gather_Ac_warp(int64_t nitems, const int32_t *__restrict__ qmap, const int32_t *__restrict__ row,
+                                 const int32_t *__restrict__ col, const int64_t *__restrict__ lptr,
+                                 const int32_t *__restrict__ la, const int32_t *__restrict__ lb,
+                                 const V *__restrict__ P, const V *__restrict__ AP,
+                                 const uint8_t *__restrict__ dead, V *__restrict__ Ac) {
     const int lane = threadIdx.x & 31, gl = lane % G;
     const int64_t ng = ((int64_t)gridDim.x * blockDim.x) / G;
     const int64_t q0 = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) / G;
-    const int64_t span = ((nblk + ng - 1) / ng) * ng;
-    for (int64_t q = q0; q < span; q += ng) {
-        const bool live = q < nblk;
+    const int64_t span = ((nitems + ng - 1) / ng) * ng;
+    for (int64_t it = q0; it < span; it += ng) {
+        const bool live = it < nitems;
         typename GAcc<V>::type acc[BC * BC];
 #pragma unroll
         for (int t = 0; t < BC * BC; ++t) acc[t] = 0;
         if (live) {
-            for (int64_t l = lptr[q] + gl; l < lptr[q + 1]; l += G) {
+            for (int64_t l = lptr[it] + gl; l < lptr[it + 1]; l += G) {
                 V p[B * BC], ap[B * BC];
                 load_raw<B * BC>(P + (int64_t)la[l] * B * BC, p);
                 load_raw<B * BC>(AP + (int64_t)lb[l] * B * BC, ap);
@@ -686,6 +696,7 @@ __global__ void k_gather_Ac_warp(int64_t nblk, const int32_t *__restrict__ row, 
 #pragma unroll
             for (int off = G / 2; off > 0; off >>= 1) acc[t] += __shfl_xor_sync(0xffffffffu, acc[t], off);
         if (live && gl == 0) {
+            const int64_t q = qmap ? (int64_t)qmap[it] : it;
             const int64_t I = row[q], J = col[q];
 #pragma unroll
             for (int r = 0; r < BC; ++r)
@@ -716,14 +727,50 @@ static void gather_AP_groups(int64_t nblk, int64_t pairs, const int64_t *ptr, co
 }
 
 template <int B, int BC, typename V>
-static void gather_Ac_groups(int64_t nblk, int64_t pairs, const int32_t *row, const int32_t *col, const int64_t *ptr,
-                             const int32_t *la, const int32_t *lb, const V *P, const V *AP, const uint8_t *dead,
-                             V *Ac, cudaStream_t st) {
-    switch (gather_lanes(nblk, pairs)) {
-        case 32: k_gather_Ac_warp<B, BC, V, 32><<<grid_for(nblk * 32, 128), 128, 0, st>>>(nblk, row, col, ptr, la, lb, P, AP, dead, Ac); break;
-        case 16: k_gather_Ac_warp<B, BC, V, 16><<<grid_for(nblk * 16, 128), 128, 0, st>>>(nblk, row, col, ptr, la, lb, P, AP, dead, Ac); break;
-        default: k_gather_Ac_warp<B, BC, V, 8><<<grid_for(nblk * 8, 128), 128, 0, st>>>(nblk, row, col, ptr, la, lb, P, AP, dead, Ac); break;
+static void gather_Ac_groups(int64_t nitems, int64_t pairs, const int32_t *qmap, const int32_t *row,
+                             const int32_t *col, const int64_t *ptr, const int32_t *la, const int32_t *lb, const V *P,
+                             const V *AP, const uint8_t *dead, V *Ac, cudaStream_t st) {
+    switch (gather_lanes(nitems, pairs)) {
+        case 32: k_gather_Ac_warp<B, BC, V, 32><<<grid_for(nitems * 32, 128), 128, 0, st>>>(nitems, qmap, row, col, ptr, la, lb, P, AP, dead, Ac); break;
+        case 16: k_gather_Ac_warp<B, BC, V, 16><<<grid_for(nitems * 16, 128), 128, 0, st>>>(nitems, qmap, row, col, ptr, la, lb, P, AP, dead, Ac); break;
+        default: k_gather_Ac_warp<B, BC, V, 8><<<grid_for(nitems * 8, 128), 128, 0, st>>>(nitems, qmap, row, col, ptr, la, lb, P, AP, dead, Ac); break;
     }
+}
+
+// Blocks below the diagonal of a symmetric Galerkin matrix: A(dst) = A(src)'.
+template <int BC, typename V>
+__global__ void k_mirror_blocks(int64_t n, const int32_t *__restrict__ dst, const int32_t *__restrict__ src,
+                                V *__restrict__ A) {
+    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < n; t += (int64_t)gridDim.x * blockDim.x) {
+        const V *a = A + (int64_t)src[t] * BC * BC;
+        V *o = A + (int64_t)dst[t] * BC * BC;
+#pragma unroll
+        for (int r = 0; r < BC; ++r)
+#pragma unroll
+            for (int c = 0; c < BC; ++c) o[r * BC + c] = a[c * BC + r];
+    }
+}
+
+// P'(A P) into the next level's values: every block, or (symmetric) the blocks on and
+// above the diagonal followed by the mirrored ones
+template <int B, int BC, typename V>
+static void galerkin_Ac(const Level &L, const Level &C, const V *P, const V *AP, V *Ac, cudaStream_t st) {
+    const bool sym = L.d_ac_out != nullptr;
+    const int64_t items = sym ? L.n_ac_items : C.Anblk;
+    const int32_t *qmap = sym ? L.d_ac_out : nullptr;
+    // one thread per output block, or a group of lanes per block where blocks are few or
+    // each sums many pairs (on the SSR hierarchy: fine-level P'(A P), ~63 pairs per block,
+    // 1.3x faster per lane group; the small coarse levels 10-20x faster)
+    if (!(items < 32768 || L.ac_pairs >= 24 * items))
+        k_gather_Ac<B, BC, V><<<grid_for(items, 128), 128, 0, st>>>(items, qmap, C.Aown.d_row, C.d_Acol,
+                                                                    L.ac_plan.d_ptr, L.ac_plan.d_a, L.ac_plan.d_b, P,
+                                                                    AP, C.d_dead, Ac);
+    else
+        gather_Ac_groups<B, BC, V>(items, L.ac_pairs, qmap, C.Aown.d_row, C.d_Acol, L.ac_plan.d_ptr, L.ac_plan.d_a,
+                                   L.ac_plan.d_b, P, AP, C.d_dead, Ac, st);
+    if (sym && L.n_ac_lower > 0)
+        k_mirror_blocks<BC, V><<<grid_for(L.n_ac_lower, 256), 256, 0, st>>>(L.n_ac_lower, L.d_ac_lower,
+                                                                           L.d_ac_lower_src, Ac);
 }
 
 __global__ void k_to_float(int64_t n, const double *__restrict__ a, float *__restrict__ b) {
@@ -891,10 +938,11 @@ __global__ void k_dense_gemv(int64_t N, const T *__restrict__ M, const T *__rest
 
 #define SG_B_DISPATCH(bval, BODY)                                 \
     switch (bval) {                                               \
+        case 1: { constexpr int BB = 1; BODY; } break;            \
         case 2: { constexpr int BB = 2; BODY; } break;            \
         case 3: { constexpr int BB = 3; BODY; } break;            \
         case 6: { constexpr int BB = 6; BODY; } break;            \
-        default: return set_error(SG_ERR_ARG, "AMG block size must be 2, 3 or 6"); \
+        default: return set_error(SG_ERR_ARG, "AMG block size must be 1, 2, 3 or 6"); \
     }
 
 #define SG_BBC_DISPATCH(bv, bcv, BODY)                                            \
@@ -902,13 +950,14 @@ __global__ void k_dense_gemv(int64_t N, const T *__restrict__ M, const T *__rest
     else if (bv == 6 && bcv == 6) { constexpr int BB = 6, BC = 6; BODY; }         \
     else if (bv == 2 && bcv == 3) { constexpr int BB = 2, BC = 3; BODY; }         \
     else if (bv == 3 && bcv == 3) { constexpr int BB = 3, BC = 3; BODY; }         \
+    else if (bv == 1 && bcv == 1) { constexpr int BB = 1, BC = 1; BODY; }         \
     else return set_error(SG_ERR_ARG, "unsupported AMG block shape");
 
 static int free_level(Level &l) {
     auto F = [](void *p) { if (p) cudaFree(p); };
     F(l.Aown.d_rp); F(l.Aown.d_col); F(l.d_diag_own); F(l.Aown_vals); F(l.A32); F(l.A16); F(l.Dinv); F(l.Dinv32);
     F(l.lmax); F(l.d_dead); F(l.d_agg); F(l.T); F(l.P.d_rp); F(l.P.d_col); F(l.R.d_rp); F(l.R.d_col);
-    F(l.AP.d_rp); F(l.AP.d_col); F(l.d_R_from_P);
+    F(l.AP.d_rp); F(l.AP.d_col); F(l.d_R_from_P); F(l.d_ac_out); F(l.d_ac_lower); F(l.d_ac_lower_src);
     F(l.Aown.d_row); F(l.P.d_row); F(l.R.d_row); F(l.AP.d_row);
     for (Plan *p : {&l.at_plan, &l.ap_plan, &l.ac_plan}) { F(p->d_ptr); F(p->d_a); F(p->d_b); }
     F(l.Pv); F(l.Rv); F(l.APv); F(l.P32); F(l.R32); F(l.T32); F(l.APv32);
@@ -941,7 +990,7 @@ static int alloc_level_buffers(Level &L, int mixed) {
 // level.  Returns the coarse pattern, coarse near-null space and dead-DOF flags.
 static int setup_transfer(Level &L, const std::vector<int32_t> &rp, const std::vector<int32_t> &col,
                           const std::vector<double> &B, int nns, int64_t na, Pattern &Ac, std::vector<double> &Bc,
-                          std::vector<uint8_t> &dead, int mixed) {
+                          std::vector<uint8_t> &dead, int mixed, int symmetric) {
     const int64_t n = L.n;
     const int b = L.b, bc = nns;
     L.bc = bc;
@@ -971,24 +1020,76 @@ static int setup_transfer(Level &L, const std::vector<int32_t> &rp, const std::v
             R.col[fill[I]] = (int32_t)i;
             from[fill[I]++] = q;
         }
-    // AP pattern + plan: (i, J) <- pairs (A block (i, k), P block (k, J))
+    // AP pattern + plan: (i, J) <- pairs (A block (i, k), P block (k, J)).  With a symmetric A
+    // only the coarse blocks (I, J), I <= J, are formed, and AP(i, J) enters them only through
+    // P(i, I)' AP(i, J) with I <= J: blocks with J below the smallest coarse column of P's row
+    // i are never read and are left out.
+    std::vector<int32_t> lo_col(n, 0);
+    if (symmetric)
+        for (int64_t i = 0; i < n; ++i)
+            lo_col[i] = L.P.rp[i] < L.P.rp[i + 1] ? L.P.col[L.P.rp[i]] : INT32_MAX;
     build_product(n, L.AP, L.ap_plan, [&](int64_t i, std::vector<std::array<int32_t, 3>> &tr) {
         for (int32_t p = rp[i]; p < rp[i + 1]; ++p) {
             const int32_t k = col[p];
-            for (int32_t q = L.P.rp[k]; q < L.P.rp[k + 1]; ++q) tr.push_back({L.P.col[q], p, q});
+            for (int32_t q = L.P.rp[k]; q < L.P.rp[k + 1]; ++q)
+                if (L.P.col[q] >= lo_col[i]) tr.push_back({L.P.col[q], p, q});
         }
     });
     L.AP.ncols = na;
     // Ac pattern + plan: (I, J) <- pairs (P block (i, I), AP block (i, J))
-    build_product(na, Ac, L.ac_plan, [&](int64_t I, std::vector<std::array<int32_t, 3>> &tr) {
-        for (int32_t k = R.rp[I]; k < R.rp[I + 1]; ++k) {
-            const int32_t i = R.col[k];
-            const int32_t pblk = from[k];
-            for (int32_t q = L.AP.rp[i]; q < L.AP.rp[i + 1]; ++q) tr.push_back({L.AP.col[q], pblk, q});
+    auto ac_pairs_of = [&](bool upper) {
+        return [&, upper](int64_t I, std::vector<std::array<int32_t, 3>> &tr) {
+            for (int32_t k = R.rp[I]; k < R.rp[I + 1]; ++k) {
+                const int32_t i = R.col[k];
+                const int32_t pblk = from[k];
+                for (int32_t q = L.AP.rp[i]; q < L.AP.rp[i + 1]; ++q)
+                    if (!upper || L.AP.col[q] >= I) tr.push_back({L.AP.col[q], pblk, q});
+            }
+        };
+    };
+    std::vector<int32_t> ac_out, ac_lower, ac_lower_src;
+    if (!symmetric) {
+        build_product(na, Ac, L.ac_plan, ac_pairs_of(false));
+    } else {
+        // plan over the upper blocks U (I <= J); the coarse pattern is U and its transpose:
+        // row I holds the columns J < I of the mirrored blocks, then U's row I
+        Pattern U;
+        build_product(na, U, L.ac_plan, ac_pairs_of(true));
+        std::vector<std::vector<int32_t>> low(na);
+        for (int64_t J = 0; J < na; ++J)
+            for (int32_t u = U.rp[J]; u < U.rp[J + 1]; ++u)
+                if (U.col[u] > J) low[U.col[u]].push_back((int32_t)J);
+        Ac.nrows = na;
+        Ac.rp.assign(na + 1, 0);
+        for (int64_t I = 0; I < na; ++I)
+            Ac.rp[I + 1] = Ac.rp[I] + (int32_t)low[I].size() + (U.rp[I + 1] - U.rp[I]);
+        Ac.nblk = Ac.rp[na];
+        Ac.col.resize(Ac.nblk);
+        ac_out.resize(U.nblk);
+        for (int64_t I = 0; I < na; ++I) {
+            int32_t o = Ac.rp[I];
+            for (int32_t J : low[I]) Ac.col[o++] = J;
+            for (int32_t u = U.rp[I]; u < U.rp[I + 1]; ++u) {
+                ac_out[u] = o;
+                Ac.col[o++] = U.col[u];
+            }
         }
-    });
+        for (int64_t I = 0; I < na; ++I)
+            for (size_t m = 0; m < low[I].size(); ++m) {
+                const int32_t J = low[I][m];
+                const int32_t *b0 = U.col.data() + U.rp[J], *b1 = U.col.data() + U.rp[J + 1];
+                const int32_t u = (int32_t)(std::lower_bound(b0, b1, (int32_t)I) - U.col.data());
+                ac_lower.push_back(Ac.rp[I] + (int32_t)m);
+                ac_lower_src.push_back(ac_out[u]);
+            }
+        L.n_ac_items = U.nblk;
+        L.n_ac_lower = (int64_t)ac_lower.size();
+    }
     Ac.ncols = na;
     int rc = dup(&L.d_R_from_P, from);
+    if (!rc && symmetric) rc = dup(&L.d_ac_out, ac_out);
+    if (!rc && symmetric) rc = dup(&L.d_ac_lower, ac_lower);
+    if (!rc && symmetric) rc = dup(&L.d_ac_lower_src, ac_lower_src);
     if (!rc) rc = dup(&L.d_agg, L.agg);
     if (!rc) rc = dup(&L.T, T);
     if (!rc) rc = upload_pattern(L.P);
@@ -1100,14 +1201,7 @@ static int numeric_transfer(sg_amg *h, int l, cudaStream_t st) {
         else
             gather_AP_groups<BB, BC, double>(L.AP.nblk, L.ap_pairs, L.ap_plan.d_ptr, L.ap_plan.d_a, L.ap_plan.d_b, A,
                                              L.Pv, L.APv, st);
-        if (!per_warp(C.Anblk, L.ac_pairs))
-            k_gather_Ac<BB, BC><<<grid_for(C.Anblk, 128), 128, 0, st>>>(C.Anblk, C.Aown.d_row, C.d_Acol,
-                                                                        L.ac_plan.d_ptr, L.ac_plan.d_a,
-                                                                        L.ac_plan.d_b, L.Pv, L.APv, C.d_dead,
-                                                                        C.Aown_vals);
-        else
-            gather_Ac_groups<BB, BC, double>(C.Anblk, L.ac_pairs, C.Aown.d_row, C.d_Acol, L.ac_plan.d_ptr,
-                                             L.ac_plan.d_a, L.ac_plan.d_b, L.Pv, L.APv, C.d_dead, C.Aown_vals, st);
+        galerkin_Ac<BB, BC, double>(L, C, L.Pv, L.APv, C.Aown_vals, st);
     }));
     SG_CUDA(cudaGetLastError());
     if (h->opt.mixed) {
@@ -1202,13 +1296,7 @@ static int numeric_update32(sg_amg *h, cudaStream_t st) {
             else
                 gather_AP_groups<BB, BC, float>(L.AP.nblk, L.ap_pairs, L.ap_plan.d_ptr, L.ap_plan.d_a, L.ap_plan.d_b,
                                                 L.A32, L.P32, L.APv32, st);
-            if (!per_warp(C.Anblk, L.ac_pairs))
-                k_gather_Ac<BB, BC, float><<<grid_for(C.Anblk, 128), 128, 0, st>>>(
-                    C.Anblk, C.Aown.d_row, C.d_Acol, L.ac_plan.d_ptr, L.ac_plan.d_a, L.ac_plan.d_b, L.P32, L.APv32,
-                    C.d_dead, C.A32);
-            else
-                gather_Ac_groups<BB, BC, float>(C.Anblk, L.ac_pairs, C.Aown.d_row, C.d_Acol, L.ac_plan.d_ptr,
-                                                L.ac_plan.d_a, L.ac_plan.d_b, L.P32, L.APv32, C.d_dead, C.A32, st);
+            galerkin_Ac<BB, BC, float>(L, C, L.P32, L.APv32, C.A32, st);
         }));
         SG_CUDA(cudaGetLastError());
     }
@@ -1348,7 +1436,7 @@ static int build_hierarchy(sg_amg *h, const sg_bsr *A0, const double *A0vals, co
         Pattern Ac;
         std::vector<double> Bc;
         std::vector<uint8_t> dead_c;
-        rc = setup_transfer(L, rp, col, B, nns, na, Ac, Bc, dead_c, o.mixed);
+        rc = setup_transfer(L, rp, col, B, nns, na, Ac, Bc, dead_c, o.mixed, o.symmetric);
         if (rc) return rc;
         rc = make_level(h, nullptr, Ac.rp, Ac.col, nns, na, dead_c);
         if (rc) return rc;
@@ -1459,8 +1547,9 @@ extern "C" int sg_amg_create(const sg_bsr *A, const double *A_vals, const double
     *out = nullptr;
     SG_CHECK_ARG(A && nullspace, "null pattern or near-null space");
     SG_CHECK_ARG(nns > 0 && nns <= 6, "near-null space dimension must be 1..6");
-    SG_CHECK_ARG((A->b == 3 && nns == 6) || (A->b == 2 && nns == 3) || (A->b == 3 && nns == 3),
-                 "supported (block, near-null) sizes: (3,6), (3,3), (2,3)");
+    SG_CHECK_ARG((A->b == 3 && nns == 6) || (A->b == 2 && nns == 3) || (A->b == 3 && nns == 3) ||
+                     (A->b == 1 && nns == 1),
+                 "supported (block, near-null) sizes: (3,6), (3,3), (2,3), (1,1)");
     sg_amg *h = new (std::nothrow) sg_amg();
     if (!h) return set_error(SG_ERR_NOMEM, "host allocation");
     cudaGetDevice(&h->device);
@@ -1476,6 +1565,7 @@ extern "C" int sg_amg_create(const sg_bsr *A, const double *A_vals, const double
         if (n_opts > 6 && opts[6] > 0) h->opt.omega_scale = opts[6];
         if (n_opts > 7 && opts[7] >= 0) h->opt.theta = opts[7];
         if (n_opts > 8) h->opt.fine_half = opts[8] != 0.0;
+        if (n_opts > 9) h->opt.symmetric = opts[9] != 0.0;
     }
     int rc = dalloc(&h->dots, DOT_BLOCKS + 64);
     if (!rc) rc = build_hierarchy(h, A, A_vals, nullspace, nns, fixed, as_stream(stream));

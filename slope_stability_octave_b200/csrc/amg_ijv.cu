@@ -296,11 +296,12 @@ extern "C" int sg_amg_setup_ijv(const char *id, const double *I, const double *J
     SG_CHECK_ARG(id && id[0], "empty instance id");
     SG_CHECK_ARG(nnz >= 0 && n > 0, "n must be positive and nnz non-negative");
     SG_CHECK_ARG(nnz == 0 || (I && J && V), "null I, J or V");
-    SG_CHECK_ARG(num_functions == 2 || num_functions == 3,
-                 "num_functions must be 2 or 3 (the AMG works on 2 x 2 or 3 x 3 node blocks)");
+    SG_CHECK_ARG(num_functions >= 1 && num_functions <= 3,
+                 "num_functions must be 1, 2 or 3 (the AMG works on 1 x 1, 2 x 2 or 3 x 3 node blocks)");
     SG_CHECK_ARG(nns >= 0 && nns <= 6 && (nns == 0 || Z), "near-null space: 0..6 columns, non-null when given");
-    SG_CHECK_ARG(nns == 0 || (num_functions == 3 && (nns == 6 || nns == 3)) || (num_functions == 2 && nns == 3),
-                 "near-null space dimension: 6 or 3 for 3 functions, 3 for 2 functions");
+    SG_CHECK_ARG(nns == 0 || (num_functions == 3 && (nns == 6 || nns == 3)) || (num_functions == 2 && nns == 3) ||
+                     (num_functions == 1 && nns == 1),
+                 "near-null space dimension: 6 or 3 for 3 functions, 3 for 2 functions, 1 for 1 function");
     SG_CHECK_ARG(!(num_functions == 2 && nns == 0), "2 functions need the 3 rigid-body modes (Z)");
     std::lock_guard<std::mutex> lock(g_mu);
     const auto t0 = std::chrono::steady_clock::now();

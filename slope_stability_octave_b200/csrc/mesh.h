@@ -28,6 +28,10 @@ struct sg_mesh {
     std::vector<int64_t> dof2q;       // dof -> free index, -1 if Dirichlet
     int64_t n_Q = 0, nnz_ref = 0;
     sg_bsr bsr;                       // node adjacency, b = dim
+    // the same node adjacency with 1 x 1 blocks for scalar (pore-pressure) systems: device
+    // arrays shared with bsr (not freed through bsr1), host copies made on first request
+    sg_bsr bsr1;
+    bool bsr1_ready = false;
     // device
     int32_t *d_elem = nullptr;        // n_e * np
     double *d_dphi = nullptr;         // n_int * dim * np, per point [d][i]

@@ -454,3 +454,54 @@ def integration_points(mesh: Mesh, hat):
     (the point order of the per-point fields)."""
     X = mesh.coord[:, mesh.elem]                      # (dim, n_p, n_e)
     return np.einsum("dpe,pq->deq", X, hat).reshape(mesh.dim, -1)
+
+
+def vector_volume(mesh: Mesh, hat, weight, f_int):
+    """Load vector (dim, n_n) of a body force given per integration point, f_int (dim, n_int):
+    f_V(d, node) = sum over the node's elements and their points of w * HatP * f_int(d)
+    (vector_volume_3D.m / vector_volume_2D.m)."""
+    n_q = hat.shape[1]
+    n_e = mesh.n_e
+    f_int = np.asarray(f_int, np.float64).reshape(mesh.dim, n_e, n_q)
+    out = np.zeros((mesh.dim, mesh.n_n))
+    w = np.asarray(weight, np.float64).reshape(n_e, n_q)
+    for d in range(mesh.dim):
+        contrib = np.einsum("iq,eq->ie", hat, w * f_int[d])          # (n_p, n_e)
+        np.add.at(out[d], mesh.elem.ravel(), contrib.ravel())
+    return out
+
+
+def midpoints_p2_2d(coord, elem):
+    """P1 -> P2 for triangles in the numbering of +MESH/midpoints_P2.m: the midpoint of every
+    edge is numbered at its first occurrence when the elements are visited in order and, in
+    each, the edges V2-V3, V3-V1, V1-V2; elem_mid rows are those three edges.  ``surf`` lists
+    the boundary edges in the same order as columns [V3; V2; mid] -- V3 and V2 of the element
+    the edge belongs to, for every one of its three edges (the reference's list keeps these
+    two vertices whichever edge it is).  coord (2, n_n), elem (3, n_e) 0-based.  Returns
+    coord_mid (2, n_mid), elem_mid (3, n_e), surf (3, n_s), all ids 0-based."""
+    coord = np.asarray(coord, np.float64)
+    elem = np.asarray(elem, np.int64)
+    n_n, n_e = coord.shape[1], elem.shape[1]
+    a = np.stack([elem[1], elem[2], elem[0]], 1)          # first vertex of edges 1, 2, 3
+    b = np.stack([elem[2], elem[0], elem[1]], 1)          # second vertex
+    lo, hi = np.minimum(a, b).ravel(), np.maximum(a, b).ravel()   # occurrence order: element, edge
+    key = lo * n_n + hi
+    uniq, first, inv, cnt = np.unique(key, return_index=True, return_inverse=True, return_counts=True)
+    order = np.argsort(first, kind="stable")               # edges by first occurrence
+    rank = np.empty_like(order)
+    rank[order] = np.arange(order.size)
+    mid_of_occ = rank[inv]                                 # midpoint number of every occurrence
+    elem_mid = (n_n + mid_of_occ).reshape(n_e, 3).T.copy()
+    fo = first[order]                                      # first occurrence of midpoint m
+    coord_mid = (coord[:, lo[fo]] + coord[:, hi[fo]]) / 2
+    bnd = order[cnt[order] == 1]                           # boundary edges in midpoint order
+    occ = first[bnd]
+    e_of = occ // 3
+    surf = np.vstack([elem[2, e_of], elem[1, e_of], n_n + rank[bnd]])
+    return coord_mid, elem_mid, surf
+
+
+def mesh_p2_from_p1_2d(coord_p1, elem_p1):
+    """(coord, elem, surf) of the P2 mesh built from a P1 triangulation by midpoints_p2_2d."""
+    cm, em, surf = midpoints_p2_2d(coord_p1, elem_p1)
+    return np.hstack([np.asarray(coord_p1, np.float64), cm]), np.vstack([np.asarray(elem_p1, np.int64), em]), surf

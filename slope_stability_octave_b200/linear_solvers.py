@@ -59,15 +59,26 @@ class AMG:
     numeric set-up on the device (the pattern is fixed per mesh)."""
 
     def __init__(self, dmesh: DeviceMesh, coord=None, mixed=False, max_levels=10, coarse_size=1200,
-                 cheb_degree=3, cheb_ratio=10.0, power_its=10, theta=0.02, fine_half=False):
+                 cheb_degree=3, cheb_ratio=10.0, power_its=10, theta=0.02, fine_half=False, symmetric=None):
         self.dmesh = dmesh
         coord = dmesh.mesh.coord if coord is None else coord
-        Z = near_null_space_elasticity(coord, dmesh.mesh.Q)
+        if getattr(dmesh, "scalar", False):
+            # scalar (pore-pressure) systems: the constant vector, zero on Dirichlet nodes
+            Z = np.asarray(dmesh.mesh.Q, np.float64).reshape(-1, 1).copy()
+        else:
+            Z = near_null_space_elasticity(coord, dmesh.mesh.Q)
         self._nns = Z.shape[1]
         self._Z = np.ascontiguousarray(Z.T)                  # column-major n_dof x nns
         self._fixed = np.ascontiguousarray((~dmesh.mesh.Q.T.ravel()).astype(np.uint8))
+        # the elasticity matrices K_r are symmetric (symmetrised in their assembly), so every
+        # Galerkin matrix is formed on and above its diagonal and mirrored; the seepage
+        # tangent is not symmetric (its E term) and takes the full product
+        if symmetric is None:
+            symmetric = not getattr(dmesh, "scalar", False)
+        self.symmetric = bool(symmetric)
         self._opts = np.array([max_levels, coarse_size, cheb_degree, cheb_ratio, power_its, 1.0 if mixed else 0.0,
-                               0.0, theta, 1.0 if (mixed and fine_half) else 0.0], dtype=np.float64)
+                               0.0, theta, 1.0 if (mixed and fine_half) else 0.0, 1.0 if symmetric else 0.0],
+                              dtype=np.float64)
         self.handle = None
         self.setup_time = 0.0
         self.mixed = mixed
@@ -196,6 +207,9 @@ class DFGMRES:
         # kernels then share the GPU, so per-kernel timings of a step are no longer those of a
         # kernel running alone; off unless asked for
         self.concurrent_pair = False
+        # the projection of the deflated solve forms W'(A z) as (A W)' z, which needs a
+        # symmetric A; False (the seepage tangent) makes the solve form A z instead
+        self.symmetric_operator = True
 
     @property
     def k(self):
@@ -357,7 +371,8 @@ class DFGMRES:
             self.preconditioner.wait()
         if M is None:
             M = self.preconditioner.handle if self.preconditioner is not None else None
-        aw_ok = self.k > 0 and self.AW is not None and self._aw_key == (K.data_ptr(), matrix_generation())
+        aw_ok = (self.symmetric_operator and self.k > 0 and self.AW is not None
+                 and self._aw_key == (K.data_ptr(), matrix_generation()))
         _lib.call("sg_dfgmres_solve", ws.handle, self.dmesh.bsr, ptr(K), M, ptr(B) if self.k else None,
                   ptr(self.AW) if aw_ok else None, self.k, ptr(b), ptr(x), tol, self.max_iterations,
                   C.byref(it), C.byref(rr), None, cur_stream())
@@ -391,6 +406,7 @@ class DFGMRES:
         new.profiler = self.profiler
         new.learned = self.learned
         new.overlap_update = self.overlap_update
+        new.symmetric_operator = self.symmetric_operator
         return new
 
 

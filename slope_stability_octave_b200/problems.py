@@ -9,6 +9,11 @@ slope_3d_random_field   3D slope with lognormal random-field strength (limit-loa
 slope_3d_from_mesh      a P2 tetrahedral mesh given as arrays (e.g. one of the reference's HDF5
                         meshes read by h5mesh.load_mesh_P2), homogeneous or with per-element
                         material ids (slope_stability_3D_{homo,hetero}_SSR.m)
+slope_3d_seepage        the 3D homogeneous slope with a phreatic surface: seepage on the GPU,
+                        then saturated unit weights and pore-pressure forces in the load
+                        (slope_stability_3D_homo_seepage_SSR.m)
+franz_dam               the 2D Franz dam of slope_stability_2D_Franz_dam_SSR.m (P1 mesh arrays of
+                        meshes/Franz_dam, ten material zones, seepage on the GPU)
 
 Material rows are (c0 [kPa], phi [deg], psi [deg], E [kPa], nu, gamma_sat, gamma_unsat).
 """
@@ -71,7 +76,8 @@ class Problem:
         return self.mesh.dim
 
     def to_device(self):
-        self.dmesh = DeviceMesh(self.mesh, self.dphi, self.weight, self.n_q)
+        if self.dmesh is None:
+            self.dmesh = DeviceMesh(self.mesh, self.dphi, self.weight, self.n_q)
         m = self.mat
         self.cons = CONSTITUTIVE(self.dmesh, m["c0"], m["phi"], m["psi"], self.Davis_type, m["shear"], m["bulk"],
                                  m["lame"])
@@ -183,3 +189,123 @@ def slope_3d_random_field(N_h=1, dims=(15, 10, 15, 10, 10, 40), seed=20261203, r
     P = Problem(mesh, (D1, D2, D3), W, hat, wf.size, mat, f, "B")
     mesh.info["random_field"] = info
     return P
+
+
+# ----------------------------------------------------------------- seepage-coupled problems
+
+
+def seepage_coupled(mesh, mat_ids, table, hat, dphi, W, n_q, Q_w, pw_D, conduct0, solver_opts=None, davis="B",
+                    log=None):
+    """Problem whose load carries the pore pressure of an unconfined seepage solution:
+    the seepage problem runs on the device (seepage.seepage_problem), its element saturation
+    selects gamma_sat / gamma_unsat per point (heterogenous_materials.m:84-86) and the body
+    force is f_V_int = [-grad_p(1); -grad_p(2) - gamma; -grad_p(3)] (the seepage scripts'
+    f_V_int, integrated by vector_volume).  The device mesh is kept for the mechanics."""
+    from . import seepage
+    dmesh = DeviceMesh(mesh, dphi, W, n_q)
+    o = dict(tolerance=1e-6, max_iterations=200, deflation_tolerance=1e-3)
+    o.update(solver_opts or {})
+    solver = seepage.seepage_solver(dmesh, Q_w, **o)
+    pw, grad_p, sat, stats = seepage.seepage_problem(dmesh, hat, Q_w, pw_D, conduct0, solver=solver, log=log)
+    sat_e = sat.cpu().numpy()
+    saturation = np.repeat(sat_e, n_q)
+    mat = fem.materials(mat_ids, n_q, table, saturation=saturation)
+    gp = grad_p.cpu().numpy().T                                    # (dim, n_int)
+    f_int = -gp
+    f_int[1] -= mat["gamma"]
+    f = fem.vector_volume(mesh, hat, W, f_int)
+    P = Problem(mesh, dphi, W, hat, n_q, mat, f, davis, dmesh=dmesh)
+    P.seepage = dict(pw=pw, grad_p=grad_p, mater_sat=sat, stats=stats, Q_w=Q_w, pw_D=pw_D)
+    return P
+
+
+SEEPAGE_HOMO = dict(k=1.0, y21=2.0, y22=6.0)
+
+
+def homo_slope_seepage_bc(coord, x1=15.0, x2=10.0, x3=15.0, y1=10.0, y2=10.0, y21=2.0, y22=6.0, grho=9.81):
+    """Q_w and pw_D of slope_stability_3D_homo_seepage_SSR.m:108-133: the pressure head of a
+    phreatic line y21 above the toe level at the slope face and y22 higher at x = 0."""
+    x, y = coord[0], coord[1]
+    Q_w = np.ones(coord.shape[1], bool)
+    Q_w[x <= 0.001] = False
+    Q_w[x >= x1 + x2 + x3 - 0.001] = False
+    Q_w[y >= y1 + y2 - 0.001] = False
+    Q_w[(y >= y1 - 0.001) & (x >= x1 + x2 - 0.001)] = False
+    Q_w[(y >= y1 - 0.001) & (y >= -(y2 / x2) * x + y1 + y2 * (1 + x1 / x2) - 0.001)] = False
+    pw_D = np.zeros(coord.shape[1])
+    x_bar = x1 + (1 - y21 / y2) * x2
+    left = (x < x_bar) & (y <= -(y22 / x_bar) * x + y1 + y21 + y22)
+    right = x >= x_bar
+    pw_D[left] = grho * ((y22 / x_bar) * (x_bar - x[left]) + y1 + y21 - y[left])
+    pw_D[right] = grho * (y1 + y21 - y[right])
+    return Q_w, pw_D
+
+
+def slope_3d_seepage(N_h=1, dims=(15, 10, 15, 10, 10, 5), mat=HOMO, solver_opts=None, log=None):
+    """The 3D homogeneous slope of slope_stability_3D_homo_seepage_SSR.m (z = 5 m, k = 1)."""
+    mesh = fem.mesh_p2_3d(N_h, *dims)
+    xi, wf = fem.quadrature_p2_tet()
+    hat, d1, d2, d3 = fem.local_basis_p2_tet(xi)
+    D1, D2, D3, W = fem.geometry_3d(mesh, d1, d2, d3, wf)
+    x1, x2, x3, y1, y2, _ = dims
+    Q_w, pw_D = homo_slope_seepage_bc(mesh.coord, x1, x2, x3, y1, y2, SEEPAGE_HOMO["y21"], SEEPAGE_HOMO["y22"])
+    conduct0 = np.full(mesh.n_e * wf.size, SEEPAGE_HOMO["k"])
+    return seepage_coupled(mesh, np.zeros(mesh.n_e, int), mat, hat, (D1, D2, D3), W, wf.size, Q_w, pw_D, conduct0,
+                           solver_opts, log=log)
+
+
+# slope_stability_2D_Franz_dam_SSR.m:30-64: ten zones (c0, phi, psi, E, nu, gamma_sat,
+# gamma_unsat) and their conductivities
+FRANZ_DAM_MATERIALS = [[50.0, 42.0, 42.0, 16000.0, 0.4, 27.0, 27.0],
+                       [0.5, 41.0, 0.0, 16000.0, 0.4, 22.0, 22.0],
+                       [0.5, 40.0, 0.0, 16000.0, 0.4, 23.0, 23.0],
+                       [0.0, 38.0, 0.0, 16000.0, 0.4, 23.0, 23.0],
+                       [10.0, 25.0, 0.0, 16000.0, 0.4, 22.0, 22.0],
+                       [0.5, 41.0, 0.0, 16000.0, 0.4, 22.0, 22.0],
+                       [75.0, 42.0, 42.0, 16000.0, 0.4, 27.0, 27.0],
+                       [0.0, 38.0, 0.0, 16000.0, 0.4, 23.0, 23.0],
+                       [0.5, 41.0, 0.0, 16000.0, 0.4, 23.0, 23.0],
+                       [0.5, 41.0, 0.0, 16000.0, 0.4, 21.0, 21.0]]
+FRANZ_DAM_K = [1.0e-5, 1.0e-4, 5.0e-5, 5.0e-6, 1.0e-9, 1.0e-4, 2.0e-9, 5.0e-6, 5.0e-5, 5.0e-4]
+# continuation parameters of the same script (:151-162)
+SSR_FRANZ_DAM = dict(lambda_init=0.7, d_lambda_init=0.05, d_lambda_min=1e-5, d_lambda_diff_scaled_min=0.01,
+                     step_max=100, omega_max_stop=1e10, it_newt_max=30, it_damp_max=10, tol=1e-5, r_min=1e-4)
+
+
+def franz_dam_seepage_bc(coord, surf, grho=9.81):
+    """Q_w and pw_D of slope_stability_2D_Franz_dam_SSR.m:100-128: the boundary edges whose
+    (first two listed) vertices lie above y = -399.9 are Dirichlet for the pressure, which
+    follows the upstream and downstream water levels (piecewise linear between x1 and x2)."""
+    Q_D = (coord[1, surf[0]] + coord[1, surf[1]]) / 2 >= -400 + 1e-1
+    Q_w = np.ones(coord.shape[1], bool)
+    Q_w[np.unique(surf[:, Q_D])] = False
+    x1, y1, x2, y2 = -82.5, -50.0, 172.5, -112.0
+    x, y = coord
+    pw_D = np.zeros(coord.shape[1])
+    up = (x < x1 + 1e-9) & (y < y1)
+    mid = (x >= x1 + 1e-9) & (x < x2 + 1e-9) & (y < ((y2 - y1) / (x2 - x1)) * (x - x1) + y1)
+    down = (x >= x2 + 1e-9) & (y < y2)
+    pw_D[up] = grho * (y1 - y[up])
+    pw_D[mid] = grho * (((y2 - y1) / (x2 - x1)) * (x[mid] - x1) + y1 - y[mid])
+    pw_D[down] = grho * (y2 - y[down])
+    return Q_w, pw_D
+
+
+def franz_dam(coords_p1, elems_p1, materials_1based, solver_opts=None, log=None):
+    """The 2D Franz dam (load_mesh_Franz_dam.m with 'P2', the script's seepage and
+    materials).  coords_p1 (n, 2), elems_p1 (n_e, 3) 0-based, materials_1based (n_e,): the
+    arrays of meshes/Franz_dam/{coordinates,elements,materials}.txt."""
+    coord, elem, surf = fem.mesh_p2_from_p1_2d(np.asarray(coords_p1, np.float64).T, np.asarray(elems_p1).T)
+    mater = np.asarray(materials_1based, np.int64).reshape(-1) - 1
+    x_max, x_min, y_min = coord[0].max(), coord[0].min(), coord[1].min()
+    Q = np.zeros((2, coord.shape[1]), bool)
+    Q[0] = (coord[0] > x_min + 0.2) & (coord[1] > y_min + 0.2) & (coord[0] < x_max - 0.2)
+    Q[1] = coord[1] > y_min + 0.2
+    mesh = fem.Mesh(coord, elem, Q, dict(kind="franz_dam"))
+    xi, wf = fem.quadrature_p2_tri()
+    hat, d1, d2 = fem.local_basis_p2_tri(xi)
+    D1, D2, W = fem.geometry_2d(mesh, d1, d2, wf)
+    Q_w, pw_D = franz_dam_seepage_bc(coord, surf)
+    conduct0 = np.repeat(np.asarray(FRANZ_DAM_K)[mater], wf.size)
+    return seepage_coupled(mesh, mater, FRANZ_DAM_MATERIALS, hat, (D1, D2), W, wf.size, Q_w, pw_D, conduct0,
+                           solver_opts, log=log)

@@ -82,9 +82,23 @@ def test_ijv_instances_reject_bad_arguments_without_device():
     assert L.sg_amg_apply_host(b"no_such_id", buf, buf, 1) == -4
     rc = L.sg_amg_setup_ijv(b"x", None, None, None, 0, 0, None, 0, None, 3, None, 0, 0, None)
     assert rc == -1 and b"n must be positive" in L.sg_last_error()
-    rc = L.sg_amg_setup_ijv(b"x", buf, buf, buf, 1, 4, None, 0, None, 1, None, 0, 0, None)
+    rc = L.sg_amg_setup_ijv(b"x", buf, buf, buf, 1, 4, None, 0, None, 4, None, 0, 0, None)
     assert rc == -1 and b"num_functions" in L.sg_last_error()
     rc = L.sg_amg_setup_ijv(b"", buf, buf, buf, 1, 4, None, 0, None, 3, None, 0, 0, None)
     assert rc == -1
     assert L.sg_amg_clear(b"no_such_id") == 0
     assert L.sg_amg_ijv_info(None, buf, 8) == 0 and buf[0] == 0
+
+
+def test_seepage_entry_points_reject_bad_arguments_without_device():
+    """The seepage entry points check their arguments before any device work."""
+    L = _lib.lib()
+    rc = L.sg_seepage_system_dev(None, None, None, None, None, None, 9.81, 2, None, None, None, None)
+    assert rc == -1 and b"null" in L.sg_last_error()
+    rc = L.sg_point_gradient_dev(None, None, None, None)
+    assert rc == -1
+    rc = L.sg_seepage_saturation_dev(None, None, None, None, None, None, None)
+    assert rc == -1
+    out = ctypes.c_void_p()
+    rc = L.sg_mesh_bsr_scalar(None, ctypes.byref(out))
+    assert rc == -1 and out.value is None

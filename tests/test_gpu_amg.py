@@ -159,3 +159,28 @@ def test_amg_apply_before_update_is_an_error(cuda_device):
     rc = _lib.lib().sg_amg_apply(h, ptr(r), ptr(r), None)
     assert rc == -4
     _lib.lib().sg_amg_destroy(h)
+
+
+def test_symmetric_galerkin_mirror(cuda_device):
+    """K_r is symmetric, so the AMG forms each coarse matrix on and above its block diagonal
+    and mirrors it (option symmetric): the blocks off the diagonal of every coarse level are
+    exact transposes of each other, and the matrices agree with the full product (option off)
+    to rounding."""
+    P, K = elastic_problem()
+    a_sym = AMG(P.dmesh)
+    a_full = AMG(P.dmesh, symmetric=False)
+    assert a_sym.symmetric and not a_full.symmetric
+    a_sym.update(K)
+    a_full.update(K)
+    nlev = len(a_sym.info()["levels"])
+    ls, lf = export(a_sym, nlev), export(a_full, nlev)
+    for l in range(1, nlev):
+        As, Af = ls[l][0], lf[l][0]
+        b = ls[l][2]
+        D = (As - As.T).tocoo()
+        off = (D.row // b) != (D.col // b)
+        # blocks off the diagonal are mirrored copies; inside a diagonal block the two
+        # triangles are separate sums and agree to rounding
+        assert np.all(D.data[off] == 0.0)
+        assert abs(D.data).max(initial=0.0) <= 1e-14 * abs(As).max()
+        assert abs(As - Af).max() <= 1e-12 * abs(Af).max()
