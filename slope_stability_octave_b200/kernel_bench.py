@@ -1,6 +1,8 @@
 """Kernel timings of the Newton-step hot path on one GPU (CUDA events, inputs resident).
 
-    python -m slope_stability_octave_b200.kernel_bench [--workload box|slope] [--kernels sds,s,assembly,spmv]
+    python -m slope_stability_octave_b200.kernel_bench [--workload box|slope]
+                                                       [--kernels sds,s,assembly,spmv,aorth8,aorth32,aorth64,
+                                                                  vcycle64,vcycle32]
                                                        [--reps 20] [--order shuffled|sorted]
 
 Workloads:
@@ -20,6 +22,7 @@ the 126 MB L2, so launches need no flush in between.
 from __future__ import annotations
 
 import argparse
+import ctypes as C
 import json
 import os
 import time
@@ -124,11 +127,64 @@ def main(argv=None):
                  "k_spmv_blk 3x3"),
     }
     dm.assemble(DS, K)
+
+    # A-orthogonalisation of k seeded random columns against K (sg_a_orthogonalize: the
+    # multi-vector SpMM A S, the Gram matrix, the recurrence, U = S T and A U = (A S) T)
+    ws = {}
+
+    def aorth(k):
+        if "h" not in ws:
+            h = C.c_void_p()
+            _lib.call("sg_krylov_create", dm.n_dof, 100, C.byref(h))
+            ws["h"] = h
+            g = torch.Generator(device=dev).manual_seed(5)
+            kmax = max(int(x[5:]) for x in kernels if x.startswith("aorth"))
+            ws["S0"] = torch.randn((kmax, dm.n_dof), dtype=F64, device=dev, generator=g) * dm.mask
+            ws["W"] = torch.empty_like(ws["S0"])
+            ws["AW"] = torch.empty_like(ws["S0"])
+        W = ws["W"][:k]
+        W.copy_(ws["S0"][:k])
+        kout = C.c_int32()
+        _lib.call("sg_a_orthogonalize", ws["h"], dm.bsr, ptr(K), ptr(W), ptr(ws["AW"]), k, 1e-300, C.byref(kout),
+                  st)
+
+    # one V-cycle of the AMG preconditioner (FP64, and the mixed form's FP32 cycle) on the
+    # elastic stiffness of the mesh (SPD), hierarchy and values set up once
+    amgs = {}
+
+    def vcycle(mixed):
+        if mixed not in amgs:
+            from .linear_solvers import AMG
+            if "Kel" not in amgs:
+                DSel = torch.empty_like(DS)
+                dm.elastic_ds(pts["shear"], pts["bulk"], DSel)
+                Kel = dm.new_block_values()
+                dm.assemble(DSel, Kel)
+                amgs["Kel"] = Kel
+                amgs["r"] = torch.randn(dm.n_dof, dtype=F64, device=dev) * dm.mask
+                amgs["z"] = torch.empty_like(amgs["r"])
+            a = AMG(dm, mixed=mixed)
+            a.update(amgs["Kel"])
+            amgs[mixed] = a
+        amgs[mixed].apply(amgs["r"], amgs["z"])
+
+    specs["vcycle64"] = (lambda: vcycle(False), 0, "AMG V-cycle, FP64")
+    specs["vcycle32"] = (lambda: vcycle(True), 0, "AMG V-cycle, FP32 (mixed form)")
+    for kk in (8, 32, 64):
+        # per pass of 8 columns: K once (76 B per block) + 8 columns in and out; Gram and
+        # products: S, A S read, U, A U written (k columns each, 8 B per entry)
+        specs[f"aorth{kk}"] = (lambda kk=kk: aorth(kk),
+                               -(-kk // 8) * dm.n_blocks * 76 + 6 * kk * 8 * dm.n_dof,
+                               f"sg_a_orthogonalize, k = {kk}")
     for k in kernels:
         fn, nbytes, name = specs[k]
+        torch.cuda.nvtx.range_push(f"kb_{k}")      # for NVTX-filtered profiler captures
         ms = timed(fn, args.reps)
+        torch.cuda.nvtx.range_pop()
         gbs = nbytes / (ms * 1e-3) / 1e9
         line = dict(base, kernel=name, ms=ms, algorithmic_bytes=nbytes, achieved_gbs=gbs, frac=gbs / peak)
+        if k.startswith("vcycle"):
+            line["levels"] = amgs[k == "vcycle32"].info()["levels"]
         if k == "assembly":
             line["fp64_tflops"] = dm.n_e * 71280 / (ms * 1e-3) / 1e12
         print(json.dumps(line), flush=True)
