@@ -106,7 +106,7 @@ def parse():
     ap.add_argument("--concurrent-solves", action="store_true",
                     help="run the two Krylov solves of each Newton step side by side (DFGMRES.solve_pair); "
                          "per-kernel timings then include the sharing of the GPU")
-    ap.add_argument("--workload", default="hetero", choices=["hetero", "ssr", "ll", "box"],
+    ap.add_argument("--workload", default="hetero", choices=["hetero", "ssr", "ll", "box", "seepage"],
                     help="hetero: the SSR continuation step on the layered slope at h = 0.6 m (headline); ssr: the "
                          "same on the homogeneous 40 m slope at h = 1 m; ll: limit-load continuation on the "
                          "random-field slope at h = 0.45 m; box: the return-map microbenchmark")
@@ -798,6 +798,108 @@ def roofline_report(head, kbytes, K, peak, peak_kind, n_blocks):
 
 
 
+SEEPAGE_METRIC = "s per seepage solve (initial linear solve + damped Newton to 1e-10), 3D P2 slope with phreatic line"
+SEEPAGE_WORKLOAD = ("unconfined seepage of slope_stability_3D_homo_seepage_SSR.m (k = 1, phreatic line y21 = 2 m at the "
+                    "face, y22 = 6 m higher at x = 0, penalty eps = grho h_min / 2) on mesh_P2_3D(N_h=1, 15,10,15,10,10, "
+                    "z=40): 156,000 P2 tets, 220,401 pressure nodes; DFGMRES tol 1e-6 (200 iterations) with the scalar "
+                    "AMG V-cycle, as the script's seepage solver")
+SEEPAGE_SAMPLE_DIMS = (15, 10, 15, 10, 10, 1)
+
+
+def seepage_problem_inputs(dims):
+    import numpy as np
+
+    from slope_stability_octave_b200 import fem, problems
+    mesh = fem.mesh_p2_3d(1, *dims)
+    xi, wf = fem.quadrature_p2_tet()
+    hat, d1, d2, d3 = fem.local_basis_p2_tet(xi)
+    D1, D2, D3, W = fem.geometry_3d(mesh, d1, d2, d3, wf)
+    Q_w, pw_D = problems.homo_slope_seepage_bc(mesh.coord, *dims[:5])
+    return mesh, hat, (D1, D2, D3), W, wf.size, Q_w, pw_D, np.ones(mesh.n_e * wf.size)
+
+
+def seepage_cpu_seconds(reps=1):
+    """The oracle's seepage solve (sparse direct solves) on a z = 1 m slice of the workload,
+    scaled by the node count to the full mesh; one host thread for the sparse LU."""
+    from oracle import seepage_ref as sr
+    mesh, hat, dphi, W, n_q, Q_w, pw_D, conduct = seepage_problem_inputs(SEEPAGE_SAMPLE_DIMS)
+    best = float("inf")
+    for _ in range(reps):
+        t0 = time.perf_counter()
+        sr.seepage_problem(mesh.coord, mesh.elem, Q_w, pw_D, sr.GRHO, conduct, hat, dphi, W)
+        best = min(best, time.perf_counter() - t0)
+    return best, mesh.n_n
+
+
+def run_seepage(args, rank):
+    """K timed seepage solves from scratch (W warm-up solves before): each solve uploads its
+    inputs (Dirichlet pressure, conductivity per point, penalty per element), runs the initial
+    linear solve and the damped Newton on the device and, for e2e, copies the pressure back.
+    value: CUDA-event time of the solves; e2e: host wall time with the copies."""
+    import numpy as np
+    import torch
+
+    from slope_stability_octave_b200 import _lib, seepage
+    from slope_stability_octave_b200.device import DeviceMesh
+    mesh, hat, dphi, W, n_q, Q_w, pw_D, conduct = seepage_problem_inputs((15, 10, 15, 10, 10, 40))
+    dm = DeviceMesh(mesh, dphi, W, n_q)
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    out_h = torch.empty(mesh.n_n, dtype=torch.float64).pin_memory()
+    stats = []
+
+    def solve(e2e):
+        solver = seepage.seepage_solver(dm, Q_w)
+        pw, grad_p, sat, st = seepage.seepage_problem(dm, hat, Q_w, pw_D, conduct, solver=solver)
+        if e2e:
+            out_h.copy_(pw)
+        stats.append(st)
+        return pw
+
+    for _ in range(args.warmup):
+        solve(False)
+    torch.cuda.synchronize()
+    barrier(world)
+    clocks = ClockSampler(torch.cuda.current_device()).start()
+    L = _lib.lib()
+    L.sg_launch_count(1)
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record()
+    for _ in range(args.steps):
+        solve(False)
+    b.record()
+    torch.cuda.synchronize()
+    launches = int(L.sg_launch_count(1))
+    t_dev = a.elapsed_time(b) / 1e3 / args.steps
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        solve(True)
+    torch.cuda.synchronize()
+    t_e2e = (time.perf_counter() - t0) / args.steps
+    clk = clocks.stop()
+    t_dev = max_over_ranks([t_dev], world, device="cuda")[0]
+    if rank != 0:
+        return
+    st = stats[-1]
+    cpu = None
+    if not args.no_cpu_baseline:
+        c_s, n_sample = seepage_cpu_seconds()
+        cpu = dict(value=c_s * mesh.n_n / n_sample, unit="s/solve", cores=1, kind="port",
+                   sample=f"the oracle's seepage solve (SciPy sparse LU) on the z = 1 m slice ({n_sample} nodes, "
+                          f"{c_s:.2f} s), scaled by the node count to {mesh.n_n} nodes")
+    line = dict(metric=SEEPAGE_METRIC, value=t_dev, unit="s/solve", n_gpus=args.gpus, steps=args.steps,
+                warmup=args.warmup, ms_per_step=t_dev * 1e3, higher_is_better=False, scaling="weak",
+                vs_baseline=None, dtype="f64", data="synthetic (generated mesh)",
+                config=dict(workload=SEEPAGE_WORKLOAD, nodes=mesh.n_n, tets=mesh.n_e, free_nodes=int(Q_w.sum()),
+                            newton_iterations=st["iterations"], linear_iterations=st["linear_iterations"],
+                            initial_linear_iterations=st["initial_linear_iterations"], status=st["status"],
+                            l2="working set > L2 on the Krylov bases; no flush"),
+                e2e=dict(value=t_e2e, unit="s/solve",
+                         h2d_bytes_per_step=2 * 8 * mesh.n_n + 8 * conduct.size + 8 * mesh.n_e,
+                         d2h_bytes_per_step=8 * mesh.n_n),
+                gpu_launches=launches, clocks=clk, cpu_baseline=cpu)
+    print(json.dumps(line))
+
+
 def main():
     args = parse()
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -805,6 +907,21 @@ def main():
     if args.impl == "reference":
         if args.workload == "box":
             box_reference_arm(args, rank)
+        elif args.workload == "seepage":
+            if rank == 0:
+                res = [seepage_cpu_seconds() for _ in range(max(1, min(args.steps, 3)))]
+                n_full, n_sample = 220401, res[0][1]
+                vals = [r[0] for r in res]
+                v = sum(vals) / len(vals) * n_full / n_sample
+                print(json.dumps(dict(metric=SEEPAGE_METRIC, value=v, unit="s/solve", n_gpus=args.gpus,
+                                      steps=len(vals), warmup=0, ms_per_step=v * 1e3, higher_is_better=False,
+                                      scaling="weak", vs_baseline=None, dtype="f64", data="synthetic",
+                                      impl="reference", config=dict(workload=SEEPAGE_WORKLOAD),
+                                      cpu_baseline=dict(value=v, unit="s/solve", cores=1, kind="port",
+                                                        sample=f"oracle seepage on the z = 1 m slice ({n_sample} "
+                                                               "nodes) scaled by the node count"),
+                                      e2e=dict(value=v, unit="s/solve", h2d_bytes_per_step=0,
+                                               d2h_bytes_per_step=0))))
         elif args.workload == "ll":
             if rank == 0:
                 print(json.dumps(dict(impl="reference", metric=LL_METRIC,
@@ -821,9 +938,11 @@ def main():
     if world > 1:
         torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
                                              device_id=torch.device("cuda", torch.cuda.current_device()))
-    if args.workload in ("box", "ll"):
+    if args.workload in ("box", "ll", "seepage"):
         if args.workload == "box":
             run_box(args, rank)
+        elif args.workload == "seepage":
+            run_seepage(args, rank)
         else:
             run_ll(args, rank, world)
         if world > 1:
