@@ -64,7 +64,7 @@ struct sg_krylov {
     // (GR_CTAS x 64 x 64) and the kept count on the device
     double *gram = nullptr, *gpart = nullptr;
     int32_t *gkout = nullptr;
-    double *spy = nullptr;      // n x 8: interleaved products of the long-vector SpMM
+    double *spy = nullptr;      // n x 16: interleaved products of the long-vector SpMM
     int aorth_mode = 1;
 };
 
@@ -612,13 +612,13 @@ extern "C" int sg_a_orthogonalize(sg_krylov *ws, const sg_bsr *A, const double *
     // products do not depend on the orthogonalisation, and one SpMM reads A once per eight
     // columns where a SpMV per column reads it k times
     if (A->b == 3 && k >= 4 && (double)n * 8 * 8 > 48e6) {
-        // long vectors: interleaved copies of 8 columns (scratch: the block buffer and spy)
+        // long vectors: interleaved copies of 16 columns (scratch: the block buffer and spy)
         if (!ws->atb) {
             SG_CUDA(device_alloc(&ws->atb, sizeof(double) * n * 16));
             SG_CUDA(device_alloc(&ws->cblk, sizeof(double) * 256 * 16));
             SG_CUDA(device_alloc(&ws->tspart, sizeof(double) * TS_PART_CTAS * 256 * 16));
         }
-        if (!ws->spy) SG_CUDA(device_alloc(&ws->spy, sizeof(double) * n * 8));
+        if (!ws->spy) SG_CUDA(device_alloc(&ws->spy, sizeof(double) * n * 16));
         rc = bsr_spmm_interleaved(*A, Avals, W + (int64_t)(k - 1) * n, -n, AWo, n, k, ws->atb, ws->spy, st);
     } else if (A->b == 3) {
         rc = bsr_spmm(*A, Avals, W + (int64_t)(k - 1) * n, -n, AWo, n, k, st);

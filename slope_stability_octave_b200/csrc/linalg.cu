@@ -332,29 +332,6 @@ static void spmm_pass(const sg_bsr &A, int G, const double *vals, const double *
 // ([component][column]); a block's x gather is then 24 KC contiguous bytes however far apart
 // the original columns lie.  A warp computes one block row (the lane mapping is described at
 // the kernel); the sums are combined in a fixed order, so the result is reproducible.
-// pack: element (row r, column c) per thread, c fastest (whole 32-byte sectors of each column
-// read by neighbouring threads, consecutive doubles written)
-template <int KC>
-__global__ void k_pack_cols(int64_t n, int kc, const double *__restrict__ X, int64_t ldx,
-                            double *__restrict__ Xi) {
-    const int64_t total = n * KC;
-    for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < total; e += (int64_t)gridDim.x * blockDim.x) {
-        const int64_t r = e / KC;
-        const int c = (int)(e - r * KC);
-        Xi[e] = c < kc ? X[c * ldx + r] : 0.0;
-    }
-}
-template <int KC>
-__global__ void k_unpack_cols(int64_t n, int kc, const double *__restrict__ Yi, double *__restrict__ Y,
-                              int64_t ldy) {
-    const int64_t total = n * KC;
-    for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < total; e += (int64_t)gridDim.x * blockDim.x) {
-        const int64_t r = e / KC;
-        const int c = (int)(e - r * KC);
-        if (c < kc) Y[c * ldy + r] = Yi[e];
-    }
-}
-
 template <int KC>
 __global__ void __launch_bounds__(256) k_spmm3i(int64_t nrows, const int32_t *__restrict__ rp,
                                                 const int32_t *__restrict__ col, const double *__restrict__ vals,
@@ -410,30 +387,137 @@ __global__ void __launch_bounds__(256) k_spmm3i(int64_t nrows, const int32_t *__
     }
 }
 
+// Column-major <-> node-interleaved copies through shared-memory tiles of 64 rows x KC
+// columns: every global access runs along a column (read) or along the interleaved rows
+// (write) of the tile, so both sides are coalesced.
+constexpr int PK_ROWS = 64;
+template <int KC>
+__global__ void __launch_bounds__(256) k_pack_tiles(int64_t n, int kc, const double *__restrict__ X, int64_t ldx,
+                                                    double *__restrict__ Xi) {
+    __shared__ double t[PK_ROWS][KC + 1];
+    const int64_t ntiles = (n + PK_ROWS - 1) / PK_ROWS;
+    for (int64_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+        const int64_t r0 = tile * PK_ROWS;
+        __syncthreads();
+        for (int e = threadIdx.x; e < PK_ROWS * KC; e += blockDim.x) {
+            const int c = e / PK_ROWS, r = e - c * PK_ROWS;
+            const int64_t rr = r0 + r;
+            t[r][c] = (c < kc && rr < n) ? X[(int64_t)c * ldx + rr] : 0.0;
+        }
+        __syncthreads();
+        for (int e = threadIdx.x; e < PK_ROWS * KC; e += blockDim.x) {
+            const int r = e / KC, c = e - r * KC;
+            const int64_t rr = r0 + r;
+            if (rr < n) Xi[rr * KC + c] = t[r][c];
+        }
+    }
+}
+template <int KC>
+__global__ void __launch_bounds__(256) k_unpack_tiles(int64_t n, int kc, const double *__restrict__ Yi,
+                                                      double *__restrict__ Y, int64_t ldy) {
+    __shared__ double t[PK_ROWS][KC + 1];
+    const int64_t ntiles = (n + PK_ROWS - 1) / PK_ROWS;
+    for (int64_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+        const int64_t r0 = tile * PK_ROWS;
+        __syncthreads();
+        for (int e = threadIdx.x; e < PK_ROWS * KC; e += blockDim.x) {
+            const int r = e / KC, c = e - r * KC;
+            const int64_t rr = r0 + r;
+            t[r][c] = rr < n ? Yi[rr * KC + c] : 0.0;
+        }
+        __syncthreads();
+        for (int e = threadIdx.x; e < PK_ROWS * KC; e += blockDim.x) {
+            const int c = e / PK_ROWS, r = e - c * PK_ROWS;
+            const int64_t rr = r0 + r;
+            if (c < kc && rr < n) Y[(int64_t)c * ldy + rr] = t[r][c];
+        }
+    }
+}
+
+// k_spmm3i for 16 columns with a column pair per lane: lane = (block slot bs in 0..3,
+// pair s in 0..7) takes columns 2s and 2s + 1, loading them as one 16-byte word per component
+// from the node-interleaved copy.  The nine values of a slot's block are loaded by its eight
+// lanes together and handed round by shuffles (the ninth by lane 0), as in k_spmm3i, but one
+// set of shuffles now serves 16 columns instead of 8, as does each warp-wide gather of x.
+__global__ void __launch_bounds__(256, 4) k_spmm3p(int64_t nrows, const int32_t *__restrict__ rp,
+                                                const int32_t *__restrict__ col, const double *__restrict__ vals,
+                                                const double *__restrict__ Xi, double *__restrict__ Yi) {
+    constexpr int KC = 16, NS = 4;
+    const int lane = threadIdx.x & 31, s = lane & 7, bs = lane >> 3, base = lane & ~7;
+    const int64_t w0 = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+    const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    for (int64_t row = w0; row < nrows; row += nw) {
+        double y[3][2] = {{0.0, 0.0}, {0.0, 0.0}, {0.0, 0.0}};
+        const int32_t p1 = rp[row + 1];
+        for (int32_t p0 = rp[row]; p0 < p1; p0 += NS) {
+            const int32_t p = p0 + bs;
+            const bool live = p < p1;
+            int64_t j = 0;
+            double av = 0.0, a8 = 0.0;
+            if (live) {
+                j = col[p];
+                av = __ldg(vals + (int64_t)p * 9 + s);
+                if (s == 0) a8 = __ldg(vals + (int64_t)p * 9 + 8);
+            }
+            double2 u[3] = {make_double2(0.0, 0.0), make_double2(0.0, 0.0), make_double2(0.0, 0.0)};
+            if (live) {
+                const double2 *x = reinterpret_cast<const double2 *>(Xi + j * 3 * KC) + s;
+                u[0] = __ldg(x);
+                u[1] = __ldg(x + KC / 2);
+                u[2] = __ldg(x + KC);
+            }
+            double a[9];
+#pragma unroll
+            for (int t = 0; t < 8; ++t) a[t] = __shfl_sync(0xffffffffu, av, base + t);
+            a[8] = __shfl_sync(0xffffffffu, a8, base);
+#pragma unroll
+            for (int r = 0; r < 3; ++r) {
+                y[r][0] += a[3 * r] * u[0].x + a[3 * r + 1] * u[1].x + a[3 * r + 2] * u[2].x;
+                y[r][1] += a[3 * r] * u[0].y + a[3 * r + 1] * u[1].y + a[3 * r + 2] * u[2].y;
+            }
+        }
+#pragma unroll
+        for (int off = 8; off < 32; off <<= 1)
+#pragma unroll
+            for (int r = 0; r < 3; ++r) {
+                y[r][0] += __shfl_xor_sync(0xffffffffu, y[r][0], off);
+                y[r][1] += __shfl_xor_sync(0xffffffffu, y[r][1], off);
+            }
+        if (bs == 0) {
+            double2 *yr = reinterpret_cast<double2 *>(Yi + row * 3 * KC) + s;
+#pragma unroll
+            for (int r = 0; r < 3; ++r) yr[r * KC / 2] = make_double2(y[r][0], y[r][1]);
+        }
+    }
+}
+
 int bsr_spmm_interleaved(const sg_bsr &A, const double *vals, const double *X, int64_t ldx, double *Y, int64_t ldy,
                          int k, double *Xi, double *Yi, cudaStream_t st) {
     if (A.b != 3) return set_error(SG_ERR_ARG, "bsr_spmm: 3x3 blocks only");
     const int64_t n = A.n_rows * 3;
-    // columns per pass: 16-column passes measured no faster per column than 8-column ones
-    // (the cost per block column is the L2 traffic of the x gathers), so 8, with less scratch
-    const int KC = 8;
-    for (int c0 = 0; c0 < k; c0 += KC) {
-        const int kc = std::min(KC, k - c0);
+    // 16 columns per pass with a column pair per lane (k_spmm3p, about 10 % less per column
+    // than the 8-column k_spmm3i at 32-64 columns); a last pass of at most 8 columns takes
+    // k_spmm3i, which reads half the gathered bytes of a half-empty 16-column pass
+    for (int c0 = 0; c0 < k;) {
+        const int rest = k - c0;
+        const int KC = rest > 8 ? 16 : 8;
+        const int kc = std::min(KC, rest);
         const InstrToken tk = instr_begin(IK_SPMM_AORTH, st);
         instr_units(IK_SPMM_AORTH, kc);
-        const unsigned gp = grid_for(n * KC, 256, 16), gm = grid_for(A.n_rows * 32, 256, 8),
-                       gu = grid_for(n * KC, 256, 16);
+        const int64_t tiles = (n + PK_ROWS - 1) / PK_ROWS;
+        const unsigned gt = grid_for(tiles * 256, 256, 8), gm = grid_for(A.n_rows * 32, 256, 8);
         if (KC == 16) {
-            k_pack_cols<16><<<gp, 256, 0, st>>>(n, kc, X + c0 * ldx, ldx, Xi);
-            k_spmm3i<16><<<gm, 256, 0, st>>>(A.n_rows, A.d_row_ptr, A.d_col, vals, Xi, Yi);
-            k_unpack_cols<16><<<gu, 256, 0, st>>>(n, kc, Yi, Y + c0 * ldy, ldy);
+            k_pack_tiles<16><<<gt, 256, 0, st>>>(n, kc, X + c0 * ldx, ldx, Xi);
+            k_spmm3p<<<gm, 256, 0, st>>>(A.n_rows, A.d_row_ptr, A.d_col, vals, Xi, Yi);
+            k_unpack_tiles<16><<<gt, 256, 0, st>>>(n, kc, Yi, Y + c0 * ldy, ldy);
         } else {
-            k_pack_cols<8><<<gp, 256, 0, st>>>(n, kc, X + c0 * ldx, ldx, Xi);
+            k_pack_tiles<8><<<gt, 256, 0, st>>>(n, kc, X + c0 * ldx, ldx, Xi);
             k_spmm3i<8><<<gm, 256, 0, st>>>(A.n_rows, A.d_row_ptr, A.d_col, vals, Xi, Yi);
-            k_unpack_cols<8><<<gu, 256, 0, st>>>(n, kc, Yi, Y + c0 * ldy, ldy);
+            k_unpack_tiles<8><<<gt, 256, 0, st>>>(n, kc, Yi, Y + c0 * ldy, ldy);
         }
         instr_end(tk, st);
         SG_CUDA(cudaGetLastError());
+        c0 += kc;
     }
     return SG_OK;
 }

@@ -27,7 +27,7 @@ int rect_spmv(int br, int bc, int64_t nrows, const int32_t *rp, const int32_t *c
 int bsr_spmm(const sg_bsr &A, const double *vals, const double *X, int64_t ldx, double *Y, int64_t ldy, int k,
              cudaStream_t st);
 
-// The same product through node-interleaved copies of 8 columns at a time (Xi, Yi: 8 n
+// The same product through node-interleaved copies of 16 columns at a time (Xi, Yi: 16 n
 // doubles each of scratch): for many columns of long vectors, whose column-wise gathers would
 // not stay in L2.
 int bsr_spmm_interleaved(const sg_bsr &A, const double *vals, const double *X, int64_t ldx, double *Y, int64_t ldy,
