@@ -2,7 +2,7 @@
 
     python -m slope_stability_octave_b200.kernel_bench [--workload box|slope]
                                                        [--kernels sds,s,assembly,spmv,aorth8,aorth32,aorth64,
-                                                                  vcycle64,vcycle32]
+                                                                  vcycle64,vcycle32,amgupdate64,amgupdate32]
                                                        [--reps 20] [--order shuffled|sorted]
 
 Workloads:
@@ -168,6 +168,13 @@ def main(argv=None):
             amgs[mixed] = a
         amgs[mixed].apply(amgs["r"], amgs["z"])
 
+    def amg_update(mixed):
+        if mixed not in amgs:
+            vcycle(mixed)
+        amgs[mixed].update(amgs["Kel"])
+
+    specs["amgupdate64"] = (lambda: amg_update(False), 0, "AMG numeric value update, FP64")
+    specs["amgupdate32"] = (lambda: amg_update(True), 0, "AMG numeric value update, FP32 (mixed form)")
     specs["vcycle64"] = (lambda: vcycle(False), 0, "AMG V-cycle, FP64")
     specs["vcycle32"] = (lambda: vcycle(True), 0, "AMG V-cycle, FP32 (mixed form)")
     for kk in (8, 32, 64):
@@ -183,8 +190,8 @@ def main(argv=None):
         torch.cuda.nvtx.range_pop()
         gbs = nbytes / (ms * 1e-3) / 1e9
         line = dict(base, kernel=name, ms=ms, algorithmic_bytes=nbytes, achieved_gbs=gbs, frac=gbs / peak)
-        if k.startswith("vcycle"):
-            line["levels"] = amgs[k == "vcycle32"].info()["levels"]
+        if k.startswith("vcycle") or k.startswith("amgupdate"):
+            line["levels"] = amgs[k.endswith("32")].info()["levels"]
         if k == "assembly":
             line["fp64_tflops"] = dm.n_e * 71280 / (ms * 1e-3) / 1e12
         print(json.dumps(line), flush=True)
