@@ -859,6 +859,14 @@ __device__ __forceinline__ void cp_async8(void *dst, const void *src) {
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
 __device__ __forceinline__ void cp_async_wait1() { asm volatile("cp.async.wait_group 1;" ::: "memory"); }
 
+// One FP64 MMA of the tensor cores: the 8 x 8 tile (c0, c1) += A (8 x 4, a) B (4 x 8, b),
+// fragments as in the PTX m8n8k4 .f64 layout.
+__device__ __forceinline__ void dmma(double &c0, double &c1, double a, double b) {
+    asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};"
+                 : "+d"(c0), "+d"(c1)
+                 : "d"(a), "d"(b));
+}
+
 // Partial sums of one 16 NA x 16 NA tile of G (rows m0 + [0, 16 NA), columns i0 + [0, 16 NA))
 // over this CTA's row range, in tiles of GR_R rows staged in shared memory ([column][row],
 // padded) by 8-byte cp.async, two stages; thread (mb, ib) owns the entries
@@ -920,6 +928,70 @@ __global__ void __launch_bounds__(256) k_gram_partial(int64_t n, int k, const do
     for (int a = 0; a < NA; ++a)
 #pragma unroll
         for (int b = 0; b < NA; ++b) out[(mb + 16 * a) * TW + ib + 16 * b] = acc[a][b];
+}
+
+// k_gram_partial for 64 x 64 tiles on the FP64 tensor cores (mma.sync m8n8k4 .f64): the
+// same row tiles and stages (pitch padded to GR_R + 4 for conflict-free fragment reads);
+// warp w owns G rows m0 + 32 (w & 1) .. + 32 and columns i0 + 16 (w >> 1) .. + 16 as 4 x 2
+// tiles of 8 x 8; A = S' (a = S[row t][column m0 + g]), B = AS (b = AS[row t][column g]).
+constexpr int GM_TW = 64, GM_LD = GR_R + 4;
+constexpr size_t GM_SMEM = sizeof(double) * 2 * 2 * GM_TW * GM_LD;
+__global__ void __launch_bounds__(256) k_gram_partial_mma(int64_t n, int k, const double *__restrict__ S,
+                                                          int64_t lds, const double *__restrict__ AS, int64_t ldas,
+                                                          int m0, int i0, double *__restrict__ part) {
+    extern __shared__ double gmsm[];   // [2 stages][S tile, AS tile][GM_TW][GM_LD]
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int g = lane >> 2, t = lane & 3;
+    const int wm = (warp & 1) * 32, wi = (warp >> 1) * 16;
+    const int64_t chunk = ((n + gridDim.x - 1) / gridDim.x + GR_R - 1) / GR_R * GR_R;
+    const int64_t r0 = blockIdx.x * chunk, r1 = min(n, r0 + chunk);
+    double acc[4][2][2];
+#pragma unroll
+    for (int a = 0; a < 4; ++a)
+#pragma unroll
+        for (int b = 0; b < 2; ++b) acc[a][b][0] = acc[a][b][1] = 0.0;
+    auto stage = [&](int st, int64_t rt) {
+        double *sS = gmsm + st * 2 * GM_TW * GM_LD, *sA = sS + GM_TW * GM_LD;
+        for (int e = tid; e < GM_TW * GR_R; e += 256) {
+            const int c = e / GR_R, r = e - c * GR_R;
+            const int64_t row = rt + r;
+            const int cm = m0 + c, ci = i0 + c;
+            if (row < r1 && cm < k) cp_async8(sS + c * GM_LD + r, S + cm * lds + row);
+            else sS[c * GM_LD + r] = 0.0;
+            if (row < r1 && ci < k) cp_async8(sA + c * GM_LD + r, AS + ci * ldas + row);
+            else sA[c * GM_LD + r] = 0.0;
+        }
+    };
+    if (r0 < r1) stage(0, r0);
+    cp_async_commit();
+    int it = 0;
+    for (int64_t rt = r0; rt < r1; rt += GR_R, ++it) {
+        if (rt + GR_R < r1) stage((it + 1) & 1, rt + GR_R);
+        cp_async_commit();
+        cp_async_wait1();
+        __syncthreads();
+        const double *sS = gmsm + (it & 1) * 2 * GM_TW * GM_LD, *sA = sS + GM_TW * GM_LD;
+#pragma unroll
+        for (int k4 = 0; k4 < GR_R; k4 += 4) {
+            double a[4], b[2];
+#pragma unroll
+            for (int i = 0; i < 4; ++i) a[i] = sS[(wm + 8 * i + g) * GM_LD + k4 + t];
+#pragma unroll
+            for (int j = 0; j < 2; ++j) b[j] = sA[(wi + 8 * j + g) * GM_LD + k4 + t];
+#pragma unroll
+            for (int i = 0; i < 4; ++i)
+#pragma unroll
+                for (int j = 0; j < 2; ++j) dmma(acc[i][j][0], acc[i][j][1], a[i], b[j]);
+        }
+        __syncthreads();
+    }
+    double *out = part + (int64_t)blockIdx.x * GM_TW * GM_TW;
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < 2; ++j)
+#pragma unroll
+            for (int h = 0; h < 2; ++h) out[(wm + 8 * i + g) * GM_TW + wi + 8 * j + 2 * t + h] = acc[i][j][h];
 }
 
 // G(m0 + ml, i0 + il) = the sum of the CTAs' partials: a warp per entry, lane l adding the
@@ -1124,10 +1196,8 @@ int gram_upper(int64_t n, int k, const double *S, int64_t lds, const double *AS,
     if (!configured) {   // stages of 48- and 64-wide tiles exceed the default 48 KB
         SG_CUDA(cudaFuncSetAttribute(k_gram_partial<3, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                      (int)(sizeof(double) * 2 * 2 * 48 * GR_LD)));
-        SG_CUDA(cudaFuncSetAttribute(k_gram_partial<4, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     (int)(sizeof(double) * 2 * 2 * 64 * GR_LD)));
-        SG_CUDA(cudaFuncSetAttribute(k_gram_partial<4, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     (int)(sizeof(double) * 2 * 2 * 64 * GR_LD)));
+        SG_CUDA(cudaFuncSetAttribute(k_gram_partial_mma, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)GM_SMEM));
         configured = true;
     }
     const int nt = (k + TW - 1) / TW;
@@ -1139,9 +1209,8 @@ int gram_upper(int64_t n, int k, const double *S, int64_t lds, const double *AS,
                 case 1: k_gram_partial<1, true><<<GR_CTAS, 256, smem, st>>>(n, k, S, lds, AS, ldas, m0, i0, part); break;
                 case 2: k_gram_partial<2, true><<<GR_CTAS, 256, smem, st>>>(n, k, S, lds, AS, ldas, m0, i0, part); break;
                 case 3: k_gram_partial<3, true><<<GR_CTAS, 256, smem, st>>>(n, k, S, lds, AS, ldas, m0, i0, part); break;
-                default:
-                    if (q == p) k_gram_partial<4, true><<<GR_CTAS, 256, smem, st>>>(n, k, S, lds, AS, ldas, m0, i0, part);
-                    else k_gram_partial<4, false><<<GR_CTAS, 256, smem, st>>>(n, k, S, lds, AS, ldas, m0, i0, part);
+                default:   // 64-wide tiles on the FP64 tensor cores
+                    k_gram_partial_mma<<<GR_CTAS, 256, GM_SMEM, st>>>(n, k, S, lds, AS, ldas, m0, i0, part);
                     break;
             }
             k_gram_reduce<<<(TW * TW * 32 + 255) / 256, 256, 0, st>>>(k, TW, GR_CTAS, part, m0, i0, G, k);
@@ -1168,12 +1237,118 @@ int gram_recurrence(int k, const double *G, double *Tp, double eps, double *Ta, 
     return SG_OK;
 }
 
+// The 64-column variant of k_ts_apply on the FP64 tensor cores (mma.sync m8n8k4 .f64, the
+// FP64 MMA of sm_100a): CTA tile 128 rows x 64 output columns, inputs in stages of TM_MC
+// columns of X / rows of Ta staged by 8-byte cp.async (two stages, pitches padded by 4
+// doubles so the fragment reads are free of bank conflicts); warp w owns rows 32 (w & 3) ..
+// + 32 and columns 32 (w >> 2) .. + 32 as 4 x 4 tiles of 8 x 8, an MMA per tile and step of 4
+// inputs.  Fragments (PTX m8n8k4 f64): A (8 x 4) a = X[row g][input t], B (4 x 8)
+// b = Ta[input t][column g], C (8 x 8) c0, c1 = [row g][columns 2 t, 2 t + 1], with
+// g = lane / 4, t = lane % 4.
+constexpr int TM_MC = 16, TM_OC = 64, TM_XP = TA_R + 4, TM_TP = TM_OC + 4;
+constexpr size_t TM_SMEM = sizeof(double) * 2 * TM_MC * (TM_XP + TM_TP);
+
+__global__ void __launch_bounds__(256) k_ts_apply_mma(int64_t n, int k, const int32_t *__restrict__ kout,
+                                                      const int32_t *__restrict__ pmap, const double *__restrict__ X,
+                                                      int64_t ldx, const double *__restrict__ Ta, double *__restrict__ Y,
+                                                      int64_t ldy) {
+    extern __shared__ double tmsm[];
+    double *sXb = tmsm, *sTb = tmsm + 2 * TM_MC * TM_XP;   // [stage][input][row] / [stage][input][column]
+    const int ko = *kout;
+    const int o0 = blockIdx.y * TM_OC;
+    if (o0 >= ko) return;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int g = lane >> 2, t = lane & 3;
+    const int wr = (warp & 3) * 32, wc = (warp >> 2) * 32;
+    const int kk = min(k, pmap[o0] + 1);
+    const int nmc = (kk + TM_MC - 1) / TM_MC;
+    const int64_t ntiles = (n + TA_R - 1) / TA_R;
+    if (blockIdx.x >= ntiles) return;
+    const int64_t nsteps = ((ntiles - blockIdx.x + gridDim.x - 1) / gridDim.x) * nmc;
+    auto stage = [&](int stg, int64_t s) {
+        const int64_t rt = (blockIdx.x + (s / nmc) * gridDim.x) * TA_R;
+        const int mc = (int)(s % nmc) * TM_MC;
+        double *sX = sXb + stg * TM_MC * TM_XP, *sT = sTb + stg * TM_MC * TM_TP;
+        for (int e = tid; e < TM_MC * TA_R; e += 256) {
+            const int cc = e / TA_R, r = e - cc * TA_R;
+            const int64_t row = rt + r;
+            const int col = mc + cc;
+            if (row < n && col < kk) cp_async8(sX + cc * TM_XP + r, X + col * ldx + row);
+            else sX[cc * TM_XP + r] = 0.0;
+        }
+        for (int e = tid; e < TM_MC * TM_OC; e += 256) {
+            const int cc = e / TM_OC, oo = e - cc * TM_OC;
+            const int m = mc + cc, o = o0 + oo;
+            sT[cc * TM_TP + oo] = (m < kk && o < ko) ? Ta[(int64_t)m * k + o] : 0.0;
+        }
+    };
+    double acc[4][4][2];
+    stage(0, 0);
+    cp_async_commit();
+    for (int64_t s = 0; s < nsteps; ++s) {
+        if (s % nmc == 0) {
+#pragma unroll
+            for (int i = 0; i < 4; ++i)
+#pragma unroll
+                for (int j = 0; j < 4; ++j) acc[i][j][0] = acc[i][j][1] = 0.0;
+        }
+        if (s + 1 < nsteps) stage((int)((s + 1) & 1), s + 1);
+        cp_async_commit();
+        cp_async_wait1();
+        __syncthreads();
+        const double *sX = sXb + (int)(s & 1) * TM_MC * TM_XP, *sT = sTb + (int)(s & 1) * TM_MC * TM_TP;
+#pragma unroll
+        for (int k4 = 0; k4 < TM_MC; k4 += 4) {
+            double a[4], b[4];
+#pragma unroll
+            for (int i = 0; i < 4; ++i) a[i] = sX[(k4 + t) * TM_XP + wr + 8 * i + g];
+#pragma unroll
+            for (int j = 0; j < 4; ++j) b[j] = sT[(k4 + t) * TM_TP + wc + 8 * j + g];
+#pragma unroll
+            for (int i = 0; i < 4; ++i)
+#pragma unroll
+                for (int j = 0; j < 4; ++j) dmma(acc[i][j][0], acc[i][j][1], a[i], b[j]);
+        }
+        __syncthreads();
+        if (s % nmc == nmc - 1) {
+            const int64_t rt = (blockIdx.x + (s / nmc) * gridDim.x) * TA_R;
+#pragma unroll
+            for (int i = 0; i < 4; ++i) {
+                const int64_t row = rt + wr + 8 * i + g;
+                if (row >= n) continue;
+#pragma unroll
+                for (int j = 0; j < 4; ++j)
+#pragma unroll
+                    for (int h = 0; h < 2; ++h) {
+                        const int o = o0 + wc + 8 * j + 2 * t + h;
+                        if (o < ko) Y[o * ldy + row] = acc[i][j][h];
+                    }
+            }
+        }
+    }
+}
+
 int ts_apply(int64_t n, int k, const int32_t *kout, const int32_t *pmap, const double *X, int64_t ldx,
              const double *Ta, double *Y, int64_t ldy, cudaStream_t st) {
     if (k <= 0 || n <= 0) return SG_OK;
-    const int nj = k >= 64 ? 8 : (k + 7) / 8;
-    const int oc = 8 * nj;
     const int64_t ntiles = (n + TA_R - 1) / TA_R;
+    if (k >= 64) {   // 64-column chunks on the FP64 tensor cores
+        static thread_local int resident_mma = 0;
+        if (!resident_mma) {
+            SG_CUDA(cudaFuncSetAttribute(k_ts_apply_mma, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TM_SMEM));
+            int r = 0;
+            SG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&r, k_ts_apply_mma, 256, TM_SMEM));
+            resident_mma = std::max(1, r);
+        }
+        const dim3 grid((unsigned)std::min<int64_t>(ntiles, (int64_t)sm_count() * resident_mma),
+                        (unsigned)((k + TM_OC - 1) / TM_OC));
+        count_launch();
+        k_ts_apply_mma<<<grid, 256, TM_SMEM, st>>>(n, k, kout, pmap, X, ldx, Ta, Y, ldy);
+        SG_CUDA(cudaGetLastError());
+        return SG_OK;
+    }
+    const int nj = (k + 7) / 8;
+    const int oc = 8 * nj;
     // CTAs resident per SM for this variant (registers and shared memory), once per variant
     static thread_local int resident[9] = {};
     if (!resident[nj]) {

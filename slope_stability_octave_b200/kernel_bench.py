@@ -177,7 +177,7 @@ def main(argv=None):
     specs["amgupdate32"] = (lambda: amg_update(True), 0, "AMG numeric value update, FP32 (mixed form)")
     specs["vcycle64"] = (lambda: vcycle(False), 0, "AMG V-cycle, FP64")
     specs["vcycle32"] = (lambda: vcycle(True), 0, "AMG V-cycle, FP32 (mixed form)")
-    for kk in (8, 32, 64):
+    for kk in (8, 32, 64, 128):
         # per pass of 8 columns: K once (76 B per block) + 8 columns in and out; Gram and
         # products: S, A S read, U, A U written (k columns each, 8 B per entry)
         specs[f"aorth{kk}"] = (lambda kk=kk: aorth(kk),
