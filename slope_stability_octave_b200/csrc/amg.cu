@@ -422,9 +422,10 @@ __global__ void k_smooth_prolongator(int64_t nblk, const int32_t *__restrict__ P
                                      const int32_t *__restrict__ Acol, const V *__restrict__ A,
                                      const V *__restrict__ T, const int32_t *__restrict__ agg,
                                      const double *__restrict__ Dinv, const double *__restrict__ lmax, double oscale,
-                                     V *__restrict__ P) {
+                                     V *__restrict__ P, int64_t chunk) {
     const double omega = oscale / lmax[0];
-    for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q < nblk; q += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t q0 = (int64_t)blockIdx.x * chunk, q1 = q0 + chunk < nblk ? q0 + chunk : nblk;
+    for (int64_t q = q0 + threadIdx.x; q < q1; q += blockDim.x) {
         const int64_t i = Prow[q];
         {
             double acc[B * BC];
@@ -537,9 +538,10 @@ template <> struct GAcc<float> { using type = float; };
 template <int B, int BC, typename V = double>
 __global__ void k_gather_AP(int64_t nblk, const int64_t *__restrict__ lptr, const int32_t *__restrict__ la,
                             const int32_t *__restrict__ lb, const V *__restrict__ A, const V *__restrict__ P,
-                            V *__restrict__ AP) {
+                            V *__restrict__ AP, int64_t chunk) {
     using T = typename GAcc<V>::type;
-    for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q < nblk; q += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t q0 = (int64_t)blockIdx.x * chunk, q1 = q0 + chunk < nblk ? q0 + chunk : nblk;
+    for (int64_t q = q0 + threadIdx.x; q < q1; q += blockDim.x) {
         T acc[B * BC];
 #pragma unroll
         for (int t = 0; t < B * BC; ++t) acc[t] = 0;
@@ -586,9 +588,9 @@ __global__ void k_gather_Ac(int64_t nitems, const int32_t *__restrict__ qmap, co
                             const int32_t *__restrict__ col, const int64_t *__restrict__ lptr,
                             const int32_t *__restrict__ la, const int32_t *__restrict__ lb,
                             const V *__restrict__ P, const V *__restrict__ AP, const uint8_t *__restrict__ dead,
-                            V *__restrict__ Ac) {
-    for (int64_t it = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; it < nitems;
-         it += (int64_t)gridDim.x * blockDim.x) {
+                            V *__restrict__ Ac, int64_t chunk) {
+    const int64_t i0 = (int64_t)blockIdx.x * chunk, i1 = i0 + chunk < nitems ? i0 + chunk : nitems;
+    for (int64_t it = i0 + threadIdx.x; it < i1; it += blockDim.x) {
         const int64_t q = qmap ? (int64_t)qmap[it] : it;
         const int64_t I = row[q];
         {
@@ -629,14 +631,13 @@ __global__ void k_gather_Ac(int64_t nitems, const int32_t *__restrict__ qmap, co
 template <int B, int BC, typename V = double, int G = 32>
 __global__ void k_gather_AP_warp(int64_t nblk, const int64_t *__restrict__ lptr, const int32_t *__restrict__ la,
                                  const int32_t *__restrict__ lb, const V *__restrict__ A,
-                                 const V *__restrict__ P, V *__restrict__ AP) {
+                                 const V *__restrict__ P, V *__restrict__ AP, int64_t chunk) {
     const int lane = threadIdx.x & 31, gl = lane % G;
-    const int64_t ng = ((int64_t)gridDim.x * blockDim.x) / G;
-    const int64_t q0 = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) / G;
+    // a CTA owns `chunk` consecutive output blocks (a multiple of its blockDim / G groups), so
     // every lane of a warp runs the same number of outer iterations (the shuffles need them)
-    const int64_t span = ((nblk + ng - 1) / ng) * ng;
-    for (int64_t q = q0; q < span; q += ng) {
-        const bool live = q < nblk;
+    const int64_t c0 = (int64_t)blockIdx.x * chunk, c1 = c0 + chunk < nblk ? c0 + chunk : nblk;
+    for (int64_t q = c0 + threadIdx.x / G; q < c0 + chunk; q += blockDim.x / G) {
+        const bool live = q < c1;
         typename GAcc<V>::type acc[B * BC];
 #pragma unroll
         for (int t = 0; t < B * BC; ++t) acc[t] = 0;
@@ -668,13 +669,11 @@ __global__ void k_gather_Ac_warp(int64_t nitems, const int32_t *__restrict__ qma
                                  const int32_t *__restrict__ col, const int64_t *__restrict__ lptr,
                                  const int32_t *__restrict__ la, const int32_t *__restrict__ lb,
                                  const V *__restrict__ P, const V *__restrict__ AP,
-                                 const uint8_t *__restrict__ dead, V *__restrict__ Ac) {
+                                 const uint8_t *__restrict__ dead, V *__restrict__ Ac, int64_t chunk) {
     const int lane = threadIdx.x & 31, gl = lane % G;
-    const int64_t ng = ((int64_t)gridDim.x * blockDim.x) / G;
-    const int64_t q0 = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) / G;
-    const int64_t span = ((nitems + ng - 1) / ng) * ng;
-    for (int64_t it = q0; it < span; it += ng) {
-        const bool live = it < nitems;
+    const int64_t c0 = (int64_t)blockIdx.x * chunk, c1 = c0 + chunk < nitems ? c0 + chunk : nitems;
+    for (int64_t it = c0 + threadIdx.x / G; it < c0 + chunk; it += blockDim.x / G) {
+        const bool live = it < c1;
         typename GAcc<V>::type acc[BC * BC];
 #pragma unroll
         for (int t = 0; t < BC * BC; ++t) acc[t] = 0;
@@ -719,10 +718,13 @@ inline int gather_lanes(int64_t nblk, int64_t pairs) {
 template <int B, int BC, typename V>
 static void gather_AP_groups(int64_t nblk, int64_t pairs, const int64_t *ptr, const int32_t *la, const int32_t *lb,
                              const V *A, const V *P, V *AP, cudaStream_t st) {
-    switch (gather_lanes(nblk, pairs)) {
-        case 32: k_gather_AP_warp<B, BC, V, 32><<<grid_for(nblk * 32, 128), 128, 0, st>>>(nblk, ptr, la, lb, A, P, AP); break;
-        case 16: k_gather_AP_warp<B, BC, V, 16><<<grid_for(nblk * 16, 128), 128, 0, st>>>(nblk, ptr, la, lb, A, P, AP); break;
-        default: k_gather_AP_warp<B, BC, V, 8><<<grid_for(nblk * 8, 128), 128, 0, st>>>(nblk, ptr, la, lb, A, P, AP); break;
+    const int G = gather_lanes(nblk, pairs);
+    const int64_t ch = chunk_len(nblk, 128 / G, 8 * 128 / G);
+    const unsigned grid = grid_chunks(nblk, ch);
+    switch (G) {
+        case 32: k_gather_AP_warp<B, BC, V, 32><<<grid, 128, 0, st>>>(nblk, ptr, la, lb, A, P, AP, ch); break;
+        case 16: k_gather_AP_warp<B, BC, V, 16><<<grid, 128, 0, st>>>(nblk, ptr, la, lb, A, P, AP, ch); break;
+        default: k_gather_AP_warp<B, BC, V, 8><<<grid, 128, 0, st>>>(nblk, ptr, la, lb, A, P, AP, ch); break;
     }
 }
 
@@ -730,10 +732,13 @@ template <int B, int BC, typename V>
 static void gather_Ac_groups(int64_t nitems, int64_t pairs, const int32_t *qmap, const int32_t *row,
                              const int32_t *col, const int64_t *ptr, const int32_t *la, const int32_t *lb, const V *P,
                              const V *AP, const uint8_t *dead, V *Ac, cudaStream_t st) {
-    switch (gather_lanes(nitems, pairs)) {
-        case 32: k_gather_Ac_warp<B, BC, V, 32><<<grid_for(nitems * 32, 128), 128, 0, st>>>(nitems, qmap, row, col, ptr, la, lb, P, AP, dead, Ac); break;
-        case 16: k_gather_Ac_warp<B, BC, V, 16><<<grid_for(nitems * 16, 128), 128, 0, st>>>(nitems, qmap, row, col, ptr, la, lb, P, AP, dead, Ac); break;
-        default: k_gather_Ac_warp<B, BC, V, 8><<<grid_for(nitems * 8, 128), 128, 0, st>>>(nitems, qmap, row, col, ptr, la, lb, P, AP, dead, Ac); break;
+    const int G = gather_lanes(nitems, pairs);
+    const int64_t ch = chunk_len(nitems, 128 / G, 8 * 128 / G);
+    const unsigned grid = grid_chunks(nitems, ch);
+    switch (G) {
+        case 32: k_gather_Ac_warp<B, BC, V, 32><<<grid, 128, 0, st>>>(nitems, qmap, row, col, ptr, la, lb, P, AP, dead, Ac, ch); break;
+        case 16: k_gather_Ac_warp<B, BC, V, 16><<<grid, 128, 0, st>>>(nitems, qmap, row, col, ptr, la, lb, P, AP, dead, Ac, ch); break;
+        default: k_gather_Ac_warp<B, BC, V, 8><<<grid, 128, 0, st>>>(nitems, qmap, row, col, ptr, la, lb, P, AP, dead, Ac, ch); break;
     }
 }
 
@@ -761,11 +766,12 @@ static void galerkin_Ac(const Level &L, const Level &C, const V *P, const V *AP,
     // one thread per output block, or a group of lanes per block where blocks are few or
     // each sums many pairs (on the SSR hierarchy: fine-level P'(A P), ~63 pairs per block,
     // 1.3x faster per lane group; the small coarse levels 10-20x faster)
-    if (!(items < 32768 || L.ac_pairs >= 24 * items))
-        k_gather_Ac<B, BC, V><<<grid_for(items, 128), 128, 0, st>>>(items, qmap, C.Aown.d_row, C.d_Acol,
-                                                                    L.ac_plan.d_ptr, L.ac_plan.d_a, L.ac_plan.d_b, P,
-                                                                    AP, C.d_dead, Ac);
-    else
+    if (!(items < 32768 || L.ac_pairs >= 24 * items)) {
+        const int64_t ch = chunk_len(items, 128, 8 * 128);
+        k_gather_Ac<B, BC, V><<<grid_chunks(items, ch), 128, 0, st>>>(items, qmap, C.Aown.d_row, C.d_Acol,
+                                                                      L.ac_plan.d_ptr, L.ac_plan.d_a, L.ac_plan.d_b,
+                                                                      P, AP, C.d_dead, Ac, ch);
+    } else
         gather_Ac_groups<B, BC, V>(items, L.ac_pairs, qmap, C.Aown.d_row, C.d_Acol, L.ac_plan.d_ptr, L.ac_plan.d_a,
                                    L.ac_plan.d_b, P, AP, C.d_dead, Ac, st);
     if (sym && L.n_ac_lower > 0)
@@ -1185,20 +1191,22 @@ static int numeric_transfer(sg_amg *h, int l, cudaStream_t st) {
     int rc = power_lmax(h, L, A, st);
     if (rc) return rc;
     SG_BBC_DISPATCH(L.b, L.bc, ({
-        k_smooth_prolongator<BB, BC><<<grid_for(L.P.nblk, 128), 128, 0, st>>>(
+        const int64_t pch = chunk_len(L.P.nblk, 128, 8 * 128);
+        k_smooth_prolongator<BB, BC><<<grid_chunks(L.P.nblk, pch), 128, 0, st>>>(
             L.P.nblk, L.P.d_row, L.P.d_col, L.at_plan.d_ptr, L.at_plan.d_a, L.d_Acol, A, L.T, L.d_agg, L.Dinv, L.lmax,
-            h->opt.omega_scale, L.Pv);
+            h->opt.omega_scale, L.Pv, pch);
         k_transpose_blocks<BB, BC><<<grid_for(L.P.nblk * BB * BC, 256), 256, 0, st>>>(L.P.nblk, L.d_R_from_P, L.Pv, L.Rv);
         // one thread per output block, or a warp per block where blocks are few or each sums
         // many pairs (measured on the SSR hierarchy: fine-level A P, ~15 pairs per block, is
         // faster per thread; P'(A P), ~63 pairs per block, 1.3x faster per warp; the small
         // coarse levels 10-20x faster per warp)
         auto per_warp = [](int64_t nblk, int64_t pairs) { return nblk < 32768 || pairs >= 24 * nblk; };
-        if (!per_warp(L.AP.nblk, L.ap_pairs))
-            k_gather_AP<BB, BC><<<grid_for(L.AP.nblk, 128), 128, 0, st>>>(L.AP.nblk, L.ap_plan.d_ptr,
-                                                                          L.ap_plan.d_a, L.ap_plan.d_b, A, L.Pv,
-                                                                          L.APv);
-        else
+        if (!per_warp(L.AP.nblk, L.ap_pairs)) {
+            const int64_t ach = chunk_len(L.AP.nblk, 128, 8 * 128);
+            k_gather_AP<BB, BC><<<grid_chunks(L.AP.nblk, ach), 128, 0, st>>>(L.AP.nblk, L.ap_plan.d_ptr,
+                                                                             L.ap_plan.d_a, L.ap_plan.d_b, A, L.Pv,
+                                                                             L.APv, ach);
+        } else
             gather_AP_groups<BB, BC, double>(L.AP.nblk, L.ap_pairs, L.ap_plan.d_ptr, L.ap_plan.d_a, L.ap_plan.d_b, A,
                                              L.Pv, L.APv, st);
         galerkin_Ac<BB, BC, double>(L, C, L.Pv, L.APv, C.Aown_vals, st);
@@ -1284,16 +1292,18 @@ static int numeric_update32(sg_amg *h, cudaStream_t st) {
         int rc = power_lmax32(h, L, st);
         if (rc) return rc;
         SG_BBC_DISPATCH(L.b, L.bc, ({
-            k_smooth_prolongator<BB, BC, float><<<grid_for(L.P.nblk, 128), 128, 0, st>>>(
+            const int64_t pch = chunk_len(L.P.nblk, 128, 8 * 128);
+            k_smooth_prolongator<BB, BC, float><<<grid_chunks(L.P.nblk, pch), 128, 0, st>>>(
                 L.P.nblk, L.P.d_row, L.P.d_col, L.at_plan.d_ptr, L.at_plan.d_a, L.d_Acol, L.A32, L.T32, L.d_agg,
-                L.Dinv, L.lmax, h->opt.omega_scale, L.P32);
+                L.Dinv, L.lmax, h->opt.omega_scale, L.P32, pch);
             k_transpose_blocks<BB, BC, float><<<grid_for(L.P.nblk * BB * BC, 256), 256, 0, st>>>(
                 L.P.nblk, L.d_R_from_P, L.P32, L.R32);
             auto per_warp = [](int64_t nblk, int64_t pairs) { return nblk < 32768 || pairs >= 24 * nblk; };
-            if (!per_warp(L.AP.nblk, L.ap_pairs))
-                k_gather_AP<BB, BC, float><<<grid_for(L.AP.nblk, 128), 128, 0, st>>>(
-                    L.AP.nblk, L.ap_plan.d_ptr, L.ap_plan.d_a, L.ap_plan.d_b, L.A32, L.P32, L.APv32);
-            else
+            if (!per_warp(L.AP.nblk, L.ap_pairs)) {
+                const int64_t ach = chunk_len(L.AP.nblk, 128, 8 * 128);
+                k_gather_AP<BB, BC, float><<<grid_chunks(L.AP.nblk, ach), 128, 0, st>>>(
+                    L.AP.nblk, L.ap_plan.d_ptr, L.ap_plan.d_a, L.ap_plan.d_b, L.A32, L.P32, L.APv32, ach);
+            } else
                 gather_AP_groups<BB, BC, float>(L.AP.nblk, L.ap_pairs, L.ap_plan.d_ptr, L.ap_plan.d_a, L.ap_plan.d_b,
                                                 L.A32, L.P32, L.APv32, st);
             galerkin_Ac<BB, BC, float>(L, C, L.P32, L.APv32, C.A32, st);

@@ -34,18 +34,22 @@ template <int BR, int BC, int G, typename VT, typename XT>
 __global__ void __launch_bounds__(256) k_spmv_blk(int64_t nrows, const int32_t *__restrict__ rp,
                                                   const int32_t *__restrict__ col, const VT *__restrict__ vals,
                                                   const XT *__restrict__ x, XT *__restrict__ y, double alpha,
-                                                  double beta, const XT *__restrict__ bvec, int mode) {
+                                                  double beta, const XT *__restrict__ bvec, int mode,
+                                                  int64_t rows_per_cta) {
     using A = typename Acc<XT>::type;
     constexpr int GPW = 32 / G;  // rows per warp
     const int lane = threadIdx.x & 31, g = lane / G, gl = lane - g * G;
-    const int64_t warp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
-    const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
-    for (int64_t base = warp * GPW; base < nrows; base += nwarps * GPW) {
+    // a CTA owns rows_per_cta consecutive rows and its warps walk them in order, so the x
+    // entries of neighbouring rows are still in L1 when the next rows gather them
+    const int64_t r0 = (int64_t)blockIdx.x * rows_per_cta;
+    const int64_t rend = r0 + rows_per_cta < nrows ? r0 + rows_per_cta : nrows;
+    const int64_t wstep = (int64_t)(blockDim.x >> 5) * GPW;
+    for (int64_t base = r0 + (int64_t)(threadIdx.x >> 5) * GPW; base < rend; base += wstep) {
         const int64_t row = base + g;
         A acc[BR];
 #pragma unroll
         for (int a = 0; a < BR; ++a) acc[a] = 0;
-        if (row < nrows) {
+        if (row < rend) {
             const int32_t p1 = rp[row + 1];
             for (int32_t p = rp[row] + gl; p < p1; p += G) {
                 const int64_t j = col[p];
@@ -63,7 +67,7 @@ __global__ void __launch_bounds__(256) k_spmv_blk(int64_t nrows, const int32_t *
         for (int off = G / 2; off > 0; off >>= 1)
 #pragma unroll
             for (int a = 0; a < BR; ++a) acc[a] += __shfl_xor_sync(0xffffffffu, acc[a], off);
-        if (row < nrows && gl == 0) {
+        if (row < rend && gl == 0) {
 #pragma unroll
             for (int a = 0; a < BR; ++a) {
                 const int64_t k = row * BR + a;
@@ -213,11 +217,13 @@ static void spmv_launch(int64_t nrows, int64_t nblk, const int32_t *rp, const in
         }
     } else {
         const int G = avg >= 16.0 ? 32 : (avg >= 8.0 ? 16 : 8);
-        const unsigned grid = grid_for(nrows * G, 256, 16);
+        // up to eight rows (G = 32) or 32 rows (G = 8) per warp
+        const int64_t rpc = chunk_len(nrows, 8 * (32 / G), 64 * (32 / G));
+        const unsigned grid = grid_chunks(nrows, rpc);
         switch (G) {
-            case 32: k_spmv_blk<BR, BC, 32, VT, XT><<<grid, 256, 0, st>>>(nrows, rp, col, vals, x, y, alpha, beta, bvec, mode); break;
-            case 16: k_spmv_blk<BR, BC, 16, VT, XT><<<grid, 256, 0, st>>>(nrows, rp, col, vals, x, y, alpha, beta, bvec, mode); break;
-            default: k_spmv_blk<BR, BC, 8, VT, XT><<<grid, 256, 0, st>>>(nrows, rp, col, vals, x, y, alpha, beta, bvec, mode); break;
+            case 32: k_spmv_blk<BR, BC, 32, VT, XT><<<grid, 256, 0, st>>>(nrows, rp, col, vals, x, y, alpha, beta, bvec, mode, rpc); break;
+            case 16: k_spmv_blk<BR, BC, 16, VT, XT><<<grid, 256, 0, st>>>(nrows, rp, col, vals, x, y, alpha, beta, bvec, mode, rpc); break;
+            default: k_spmv_blk<BR, BC, 8, VT, XT><<<grid, 256, 0, st>>>(nrows, rp, col, vals, x, y, alpha, beta, bvec, mode, rpc); break;
         }
     }
     if (fine) instr_end(tk, st);
@@ -333,7 +339,7 @@ static void spmm_pass(const sg_bsr &A, int G, const double *vals, const double *
 // the original columns lie.  A warp computes one block row (the lane mapping is described at
 // the kernel); the sums are combined in a fixed order, so the result is reproducible.
 template <int KC>
-__global__ void __launch_bounds__(256) k_spmm3i(int64_t nrows, const int32_t *__restrict__ rp,
+__global__ void __launch_bounds__(256) k_spmm3i(int64_t nrows, int64_t rows_per_cta, const int32_t *__restrict__ rp,
                                                 const int32_t *__restrict__ col, const double *__restrict__ vals,
                                                 const double *__restrict__ Xi, double *__restrict__ Yi) {
     // a warp per block row; lane = (block slot bs in 0 .. 32/KC - 1, column c in 0 .. KC - 1):
@@ -342,9 +348,10 @@ __global__ void __launch_bounds__(256) k_spmm3i(int64_t nrows, const int32_t *__
     // reads column c of x_j; the slots' sums are combined by a fixed tree at the end
     constexpr int NS = 32 / KC;
     const int lane = threadIdx.x & 31, c = lane & (KC - 1), bs = lane / KC, base = lane & ~(KC - 1);
-    const int64_t w0 = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
-    const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
-    for (int64_t row = w0; row < nrows; row += nw) {
+    // a CTA owns rows_per_cta consecutive rows, walked in order by its warps
+    const int64_t r0 = (int64_t)blockIdx.x * rows_per_cta;
+    const int64_t rend = r0 + rows_per_cta < nrows ? r0 + rows_per_cta : nrows;
+    for (int64_t row = r0 + (threadIdx.x >> 5); row < rend; row += blockDim.x >> 5) {
         double y0 = 0.0, y1 = 0.0, y2 = 0.0;
         const int32_t p1 = rp[row + 1];
         for (int32_t p0 = rp[row]; p0 < p1; p0 += NS) {
@@ -439,41 +446,59 @@ __global__ void __launch_bounds__(256) k_unpack_tiles(int64_t n, int kc, const d
 // from the node-interleaved copy.  The nine values of a slot's block are loaded by its eight
 // lanes together and handed round by shuffles (the ninth by lane 0), as in k_spmm3i, but one
 // set of shuffles now serves 16 columns instead of 8, as does each warp-wide gather of x.
-__global__ void __launch_bounds__(256, 4) k_spmm3p(int64_t nrows, const int32_t *__restrict__ rp,
-                                                const int32_t *__restrict__ col, const double *__restrict__ vals,
-                                                const double *__restrict__ Xi, double *__restrict__ Yi) {
-    constexpr int KC = 16, NS = 4;
+// Each step issues the loads of two groups of four blocks before either group's products
+// (eight x gathers in flight per warp), and a CTA owns rows_per_cta consecutive rows that its
+// warps walk in order, so the x runs of neighbouring rows are reused from L1.
+__global__ void __launch_bounds__(256, 4) k_spmm3p(int64_t nrows, int64_t rows_per_cta,
+                                                const int32_t *__restrict__ rp, const int32_t *__restrict__ col,
+                                                const double *__restrict__ vals, const double *__restrict__ Xi,
+                                                double *__restrict__ Yi) {
+    constexpr int KC = 16, NS = 4, UNR = 2;
     const int lane = threadIdx.x & 31, s = lane & 7, bs = lane >> 3, base = lane & ~7;
-    const int64_t w0 = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
-    const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
-    for (int64_t row = w0; row < nrows; row += nw) {
+    const int64_t r0 = (int64_t)blockIdx.x * rows_per_cta;
+    const int64_t rend = r0 + rows_per_cta < nrows ? r0 + rows_per_cta : nrows;
+    for (int64_t row = r0 + (threadIdx.x >> 5); row < rend; row += blockDim.x >> 5) {
         double y[3][2] = {{0.0, 0.0}, {0.0, 0.0}, {0.0, 0.0}};
         const int32_t p1 = rp[row + 1];
-        for (int32_t p0 = rp[row]; p0 < p1; p0 += NS) {
-            const int32_t p = p0 + bs;
-            const bool live = p < p1;
-            int64_t j = 0;
-            double av = 0.0, a8 = 0.0;
-            if (live) {
-                j = col[p];
-                av = __ldg(vals + (int64_t)p * 9 + s);
-                if (s == 0) a8 = __ldg(vals + (int64_t)p * 9 + 8);
-            }
-            double2 u[3] = {make_double2(0.0, 0.0), make_double2(0.0, 0.0), make_double2(0.0, 0.0)};
-            if (live) {
-                const double2 *x = reinterpret_cast<const double2 *>(Xi + j * 3 * KC) + s;
-                u[0] = __ldg(x);
-                u[1] = __ldg(x + KC / 2);
-                u[2] = __ldg(x + KC);
-            }
-            double a[9];
+        for (int32_t p0 = rp[row]; p0 < p1; p0 += NS * UNR) {
+            int64_t j[UNR];
+            double av[UNR], a8[UNR];
+            bool live[UNR];
 #pragma unroll
-            for (int t = 0; t < 8; ++t) a[t] = __shfl_sync(0xffffffffu, av, base + t);
-            a[8] = __shfl_sync(0xffffffffu, a8, base);
+            for (int q = 0; q < UNR; ++q) {
+                const int32_t p = p0 + q * NS + bs;
+                live[q] = p < p1;
+                j[q] = 0;
+                av[q] = 0.0;
+                a8[q] = 0.0;
+                if (live[q]) {
+                    j[q] = col[p];
+                    av[q] = __ldg(vals + (int64_t)p * 9 + s);
+                    if (s == 0) a8[q] = __ldg(vals + (int64_t)p * 9 + 8);
+                }
+            }
+            double2 u[UNR][3];
 #pragma unroll
-            for (int r = 0; r < 3; ++r) {
-                y[r][0] += a[3 * r] * u[0].x + a[3 * r + 1] * u[1].x + a[3 * r + 2] * u[2].x;
-                y[r][1] += a[3 * r] * u[0].y + a[3 * r + 1] * u[1].y + a[3 * r + 2] * u[2].y;
+            for (int q = 0; q < UNR; ++q) {
+                u[q][0] = u[q][1] = u[q][2] = make_double2(0.0, 0.0);
+                if (live[q]) {
+                    const double2 *x = reinterpret_cast<const double2 *>(Xi + j[q] * 3 * KC) + s;
+                    u[q][0] = __ldg(x);
+                    u[q][1] = __ldg(x + KC / 2);
+                    u[q][2] = __ldg(x + KC);
+                }
+            }
+#pragma unroll
+            for (int q = 0; q < UNR; ++q) {
+                double a[9];
+#pragma unroll
+                for (int t = 0; t < 8; ++t) a[t] = __shfl_sync(0xffffffffu, av[q], base + t);
+                a[8] = __shfl_sync(0xffffffffu, a8[q], base);
+#pragma unroll
+                for (int r = 0; r < 3; ++r) {
+                    y[r][0] += a[3 * r] * u[q][0].x + a[3 * r + 1] * u[q][1].x + a[3 * r + 2] * u[q][2].x;
+                    y[r][1] += a[3 * r] * u[q][0].y + a[3 * r + 1] * u[q][1].y + a[3 * r + 2] * u[q][2].y;
+                }
             }
         }
 #pragma unroll
@@ -505,14 +530,15 @@ int bsr_spmm_interleaved(const sg_bsr &A, const double *vals, const double *X, i
         const InstrToken tk = instr_begin(IK_SPMM_AORTH, st);
         instr_units(IK_SPMM_AORTH, kc);
         const int64_t tiles = (n + PK_ROWS - 1) / PK_ROWS;
-        const unsigned gt = grid_for(tiles * 256, 256, 8), gm = grid_for(A.n_rows * 32, 256, 8);
+        const unsigned gt = grid_for(tiles * 256, 256, 8);
+        const int64_t rpc = chunk_len(A.n_rows, 8, 64);
         if (KC == 16) {
             k_pack_tiles<16><<<gt, 256, 0, st>>>(n, kc, X + c0 * ldx, ldx, Xi);
-            k_spmm3p<<<gm, 256, 0, st>>>(A.n_rows, A.d_row_ptr, A.d_col, vals, Xi, Yi);
+            k_spmm3p<<<grid_chunks(A.n_rows, rpc), 256, 0, st>>>(A.n_rows, rpc, A.d_row_ptr, A.d_col, vals, Xi, Yi);
             k_unpack_tiles<16><<<gt, 256, 0, st>>>(n, kc, Yi, Y + c0 * ldy, ldy);
         } else {
             k_pack_tiles<8><<<gt, 256, 0, st>>>(n, kc, X + c0 * ldx, ldx, Xi);
-            k_spmm3i<8><<<gm, 256, 0, st>>>(A.n_rows, A.d_row_ptr, A.d_col, vals, Xi, Yi);
+            k_spmm3i<8><<<grid_chunks(A.n_rows, rpc), 256, 0, st>>>(A.n_rows, rpc, A.d_row_ptr, A.d_col, vals, Xi, Yi);
             k_unpack_tiles<8><<<gt, 256, 0, st>>>(n, kc, Yi, Y + c0 * ldy, ldy);
         }
         instr_end(tk, st);

@@ -52,6 +52,22 @@ inline unsigned grid_for(int64_t work, int block, int per_sm = 8) {
     return (unsigned)(need < cap ? need : cap);
 }
 
+// Launch shape for kernels that give each CTA a run of `chunk` consecutive items (rows or
+// output blocks) and walk it in order: ceil(n / chunk) CTAs.
+inline unsigned grid_chunks(int64_t n, int64_t chunk) {
+    count_launch();
+    const int64_t g = (n + chunk - 1) / chunk;
+    return (unsigned)(g < 1 ? 1 : g);
+}
+// Chunk length for that mapping: a multiple of `unit`, at most `most`, and short enough to
+// give every SM eight CTAs when n is small.
+inline int64_t chunk_len(int64_t n, int64_t unit, int64_t most) {
+    const int64_t slots = (int64_t)sm_count() * 8;
+    const int64_t want = (n + slots - 1) / slots;
+    const int64_t c = ((want + unit - 1) / unit) * unit;
+    return c < unit ? unit : (c > most ? most : c);
+}
+
 // Growable device scratch owned by the library (host-buffer entry points only).
 struct Scratch {
     void *ptr = nullptr;
