@@ -217,8 +217,8 @@ static void spmv_launch(int64_t nrows, int64_t nblk, const int32_t *rp, const in
         }
     } else {
         const int G = avg >= 16.0 ? 32 : (avg >= 8.0 ? 16 : 8);
-        // up to eight rows (G = 32) or 32 rows (G = 8) per warp
-        const int64_t rpc = chunk_len(nrows, 8 * (32 / G), 64 * (32 / G));
+        // up to four rows (G = 32) or 16 rows (G = 8) per warp
+        const int64_t rpc = chunk_len(nrows, 8 * (32 / G), 32 * (32 / G));
         const unsigned grid = grid_chunks(nrows, rpc);
         switch (G) {
             case 32: k_spmv_blk<BR, BC, 32, VT, XT><<<grid, 256, 0, st>>>(nrows, rp, col, vals, x, y, alpha, beta, bvec, mode, rpc); break;

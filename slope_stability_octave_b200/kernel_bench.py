@@ -1,6 +1,6 @@
 """Kernel timings of the Newton-step hot path on one GPU (CUDA events, inputs resident).
 
-    python -m slope_stability_octave_b200.kernel_bench [--workload box|slope]
+    python -m slope_stability_octave_b200.kernel_bench [--workload box|slope|layered]
                                                        [--kernels sds,s,assembly,spmv,aorth8,aorth32,aorth64,
                                                                   vcycle64,vcycle32,amgupdate64,amgupdate32]
                                                        [--reps 20] [--order shuffled|sorted]
@@ -11,7 +11,11 @@ Workloads:
          (8,448,000 points); per-point strains seeded so that the five return-map branches
          each take 20 % (2^20 distinct seeded points repeated over the mesh), c ~ U[5,15] kPa,
          phi ~ U[25,45] deg, psi = 0, E = 40 MPa, nu = 0.3;
-  slope  the 3D slope of the SSR benchmark (mesh_P2_3D(1, 15,10,15,10,10, z=40)), same draws.
+  slope  the 3D slope of the SSR benchmark (mesh_P2_3D(1, 15,10,15,10,10, z=40)), same draws;
+  layered  the four-layer slope of the headline SSR step (mesh_P2_3D(5/3, 15,10,15,10,10,
+         z=40): 1,005,075 nodes, 2,932,430 free DOFs), same draws.
+The A-orthogonalisation runs against the assembled tangent of the seeded points, the AMG
+kernels on the elastic stiffness of the draws' moduli.
 
 Per kernel it prints one JSON line: mean time per launch and the algorithmic bytes per
 launch (return mapping: 416 B per point with the tangent, 128 B without; assembly: 5,896 B
@@ -65,7 +69,7 @@ def build(workload):
         _, d1, d2, d3 = fem.local_basis_p2_tet(xi)
         D1, D2, D3, W = fem.geometry_3d(mesh, d1, d2, d3, wf)
         return mesh, (D1, D2, D3), W, wf.size
-    P = problems.slope_3d(1)
+    P = problems.slope_3d_layered(5 / 3) if workload == "layered" else problems.slope_3d(1)
     return P.mesh, P.dphi, P.weight, P.n_q
 
 
@@ -85,7 +89,7 @@ def points_on_device(n, order, dev):
 
 def main(argv=None):
     ap = argparse.ArgumentParser()
-    ap.add_argument("--workload", default="box", choices=["box", "slope"])
+    ap.add_argument("--workload", default="box", choices=["box", "slope", "layered"])
     ap.add_argument("--kernels", default="sds,s,assembly,spmv")
     ap.add_argument("--reps", type=int, default=20)
     ap.add_argument("--order", default="shuffled", choices=["shuffled", "sorted"])
